@@ -1,0 +1,238 @@
+/*
+ * tortoise_b200.h -- C ABI of the B200 (sm_100a) collision operator and
+ * Dormand-Prince 5(4) time stepper for TORTOISE-style Boltzmann transport on
+ * P1 discontinuous-Galerkin simplex meshes in 2D k-space.
+ *
+ * Plain C types only: pointers, sizes, doubles.  No exceptions cross this
+ * boundary; every entry point returns a tb_status code and tb_last_error()
+ * gives a one-line message for the calling thread.
+ *
+ * State layout (the "status" vector).  All bands are concatenated in band
+ * order.  Band b occupies Ne_b * 3 doubles starting at tb_band_offset(b);
+ * inside a band the layout is element-major, basis-minor:
+ *     f[off_b + 3*e + 0] = f(v0)            (value at the element's first vertex)
+ *     f[off_b + 3*e + 1] = f(v1) - f(v0)
+ *     f[off_b + 3*e + 2] = f(v2) - f(v0)
+ * which is the linear-form layout of the reference's Function<2>::vec
+ * (src/Geometry/Structured/FunctionSpace/Function.cpp:60-68,
+ *  include/Geometry/Structured/FunctionSpace/Function.hpp:352-369).
+ *
+ * Element numbering follows Mesh<2>::elemID (src/Geometry/Structured/
+ * DirectSpace/Mesh.cpp:407-411): e = 2*(sx + sy*nx) + elemInSection, with
+ * element 0 of a section spanning section-relative vertices (0,0),(1,0),(1,1)
+ * and element 1 spanning (0,0),(0,1),(1,1).
+ */
+#ifndef TORTOISE_B200_H
+#define TORTOISE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+typedef enum tb_status {
+    TB_OK              = 0,
+    TB_ERR_BAD_DESC    = 1,  /* malformed problem description               */
+    TB_ERR_OOM         = 2,  /* device or host allocation failed            */
+    TB_ERR_CUDA        = 3,  /* a CUDA runtime call failed                  */
+    TB_ERR_DT_UNDERFLOW= 4,  /* DP45 step below denseStep/1e4 (reference's
+                                "step size has become too small")           */
+    TB_ERR_NONFINITE   = 5,  /* NaN/Inf met in the state or error norm      */
+    TB_ERR_TIMEOUT     = 6,  /* bounded device wait ran out                 */
+    TB_ERR_NO_DEVICE   = 7,  /* no CUDA device / library built without it   */
+    TB_ERR_ARG         = 8,  /* bad argument (index out of range, NULL ...)  */
+    TB_ERR_CAPACITY    = 9   /* an output buffer was too small              */
+} tb_status;
+
+/* scattLegDirection of the reference (include/Geometry/GeometryCore/Geometry.hpp:119) */
+#define TB_IN   1
+#define TB_OUT (-1)
+/* statisticType of the reference (include/Physics/Material/Material.hpp:51) */
+#define TB_FERMION (-1)
+#define TB_BOSON     1
+
+#define TB_MAX_LEGS 4
+
+/* ------------------------------------------------------ problem description */
+/* Region<2> (include/Geometry/Structured/DirectSpace/Region.hpp): origin and
+ * the two side vectors, stored column-major: gvec[0..1] = side 0, gvec[2..3] = side 1. */
+typedef struct tb_region {
+    double origin[2];
+    double gvec[4];
+} tb_region;
+
+/* Mesh<2>(region, relativeOrigin, relativeSize, nSecSplits)
+ * (src/Geometry/Structured/DirectSpace/Mesh.cpp:319-347). */
+typedef struct tb_mesh_desc {
+    double  rel_origin[2];
+    double  rel_size[2];
+    int32_t nsplit[2];
+} tb_mesh_desc;
+
+/* Band<2> (include/Physics/Material/Band.hpp:49-113).  The dispersion is
+ * given as linear-form coefficients (Ne*3 doubles, layout above); the crystal
+ * momentum functions kx, ky are rebuilt from the mesh exactly as
+ * costructCrystalMomentum<2> does (src/Physics/Material/Band.cpp:45-56). */
+typedef struct tb_band_desc {
+    int32_t       mesh;            /* index into tb_problem_desc.meshes        */
+    double        charge;
+    double        statistics;      /* TB_FERMION or TB_BOSON                   */
+    const double* dispersion;      /* [Ne*3] linear-form coefficients          */
+    double        abs_tol;         /* absoluteErrorTolerance  (Band.hpp:77)    */
+    double        rel_tol;         /* relativeErrorTolerance  (Band.hpp:78)    */
+    double        penalisation;    /* penalisationUnphysicalPopulation (:82)   */
+    int32_t       constrained;     /* Band::constrained (Band.hpp:66)          */
+    const double* constrained_population; /* [Ne*3] time-independent
+                                     constrainedPopulation, or NULL            */
+    double        drift_velocity[2]; /* dk/dt of the Vlasov drift term for this
+                                     band (Vlasov<2>::vlasovFlux velocity,
+                                     include/Physics/Transport/Vlasov.hpp:69);
+                                     (0,0) disables drift for the band         */
+} tb_band_desc;
+
+/* ScatteringChannel<2,L> (include/Physics/Scattering/ScatteringChannel.hpp:54-192). */
+typedef struct tb_channel_desc {
+    int32_t        nlegs;              /* 2, 3 or 4                               */
+    int32_t        band[TB_MAX_LEGS];  /* legBandNumber                           */
+    int32_t        dir[TB_MAX_LEGS];   /* legDirection: TB_IN / TB_OUT            */
+    double         amplitude;          /* amplitude (functAmplitude == 1)         */
+    int32_t        n_mc;               /* numMCPoints                             */
+    double         min_det;            /* minimumDeterminant                      */
+    double         threshold;          /* scattElemeThreshold                     */
+    int32_t        n_umklapp;          /* columns of umklappUnitVectors           */
+    const double*  umklapp;            /* [n_umklapp*2], in units of region gvec  */
+    /* Monte-Carlo table (ScatteringChannel::mCPoints, ScatteringChannel.cpp:677-688)
+     * as an explicit seeded input, point-major: n_mc rows of R = 2*(L-2)+1
+     * doubles: (L-2) points of the reference triangle followed by one
+     * coordinate in [0,1] for the partially constrained leg.               */
+    const double*  mc_points;
+    /* Points for the tuple-survival test of precalculateIndices
+     * (ScatteringChannel.cpp:476-504 via IntegratorCore.hpp:382-388); same
+     * shape.  NULL: reuse mc_points.                                        */
+    const double*  mc_points_precalc;
+    /* Optional caller-supplied tuple list (the content of a .scattIndices
+     * cache, ScatteringChannel.cpp:421-458).  n_tuples == 0: enumerate.     */
+    int64_t        n_tuples;
+    const int32_t* tuples;             /* [n_tuples*L] element ids              */
+    const int32_t* tuple_umklapp;      /* [n_tuples] umklapp column index       */
+} tb_channel_desc;
+
+typedef struct tb_problem_desc {
+    tb_region              region;
+    int32_t                n_meshes;
+    const tb_mesh_desc*    meshes;
+    int32_t                n_bands;
+    const tb_band_desc*    bands;
+    int32_t                n_channels;
+    const tb_channel_desc* channels;
+} tb_problem_desc;
+
+
+/* ------------------------------------------------------------ entry points */
+typedef struct tb_handle tb_handle;
+
+/* Collision-kernel layouts (tb_options.layout / tb_channel_info) */
+#define TB_LAYOUT_AUTO   0  /* per channel: fastest layout that fits the budget  */
+#define TB_LAYOUT_MC64   1  /* Monte-Carlo quadrature per tuple, FP64 (TypeB)    */
+#define TB_LAYOUT_T64    2  /* precomputed moment tensor, FP64 storage            */
+#define TB_LAYOUT_T32    3  /* precomputed moment tensor, FP32 storage, FP64 accumulate */
+
+typedef struct tb_options {
+    int32_t device;               /* CUDA device ordinal                            */
+    int32_t layout;               /* TB_LAYOUT_*                                    */
+    int32_t allow_fp32;           /* AUTO may pick TB_LAYOUT_T32                    */
+    int64_t tensor_budget_bytes;  /* cap on precomputed-tensor memory (0: 60% free) */
+    int32_t verbose;
+} tb_options;
+
+/* Pointer flags */
+#define TB_PTR_HOST       1   /* f / out / dense buffers are host memory (copies inside) */
+#define TB_NO_DRIFT       2   /* skip the Vlasov drift term                            */
+#define TB_NO_COLLISIONS  4   /* skip all scattering channels                          */
+
+typedef struct tb_dp45_stats {
+    double  t;            /* time reached                                   */
+    double  dt;           /* next step size                                 */
+    double  last_err;     /* last normalised error                          */
+    int64_t attempts, accepted, rejected, rhs_evals;
+    int64_t n_dense;      /* dense outputs produced                         */
+    int32_t status;       /* tb_status of the integration                   */
+    int32_t done;         /* 1 once t >= t_final or the integration failed  */
+} tb_dp45_stats;
+
+const char* tb_last_error(void);
+
+/* Builds device tables, enumerates (or uploads) the tuple lists and, for the
+ * tensor layouts, precomputes the moment tensors.  Replaces the setup half of
+ * Material::addScatteringChannelsWildcards (src/Physics/Material/Material.cpp:
+ * 209-364: findUmklappVectors -> constructMCPoints -> precalculateIndices). */
+int tb_create(tb_handle** h, const tb_problem_desc* desc, const tb_options* opts);
+int tb_destroy(tb_handle* h);
+
+int64_t tb_num_dofs(const tb_handle* h);
+int64_t tb_band_offset(const tb_handle* h, int band);
+int     tb_num_channels(const tb_handle* h);
+/* tuples kept, tuples passing the element energy window, tuples passing the
+ * determinant filter, and the collision layout chosen for the channel. */
+int tb_channel_info(const tb_handle* h, int ch, int64_t* n_tuples, int64_t* n_prefilter, int64_t* n_det,
+                    int32_t* layout);
+/* Copies a channel's tuple list to host memory: ids[n*L] (tuple-major), umk[n]. */
+int tb_get_tuples(const tb_handle* h, int ch, int32_t* ids, int32_t* umk);
+/* ScatteringChannel::amplitude (coupling constant); 0 disables the channel
+ * like MaterialStatus::propagate does (MaterialStatus.cpp:149). */
+int tb_set_amplitude(tb_handle* h, int ch, double amplitude);
+
+/* dfdt = sum over channels of ScatteringChannel::propagate(f) (each including
+ * M^-1) plus the Vlasov drift of bands with nonzero drift velocity.
+ * Replaces MaterialStatus<2>::propagate() (src/Physics/Status/MaterialStatus.cpp:146-161). */
+int tb_rhs(tb_handle* h, const double* f, double* dfdt, int flags);
+
+/* One channel: ScatteringChannel<2,L>::propagate (src/Physics/Scattering/
+ * ScatteringChannel.cpp:651-670), M^-1 included. */
+int tb_channel_propagate(tb_handle* h, int ch, const double* f, double* out, int flags);
+
+/* MaterialStatus::relativeError(err, pop) (MaterialStatus.cpp:189-196). */
+int tb_relative_error(tb_handle* h, const double* err, const double* pop, double* result, int flags);
+
+/* MaterialStatus::applyConstraints for time-independent constraints. */
+int tb_apply_constraints(tb_handle* h, double* f, int flags);
+
+/* Dormand-Prince 5(4) from t0 to t_final with dense output every dense_step,
+ * entirely on the device: Algorithms::dormandPrince54 (include/Generics/
+ * Algorithms/DormandPrince54.hpp:479-665) as called by MaterialTimeStatus::
+ * propagate (src/Physics/Status/MaterialTimeStatus.cpp:102-137).
+ * f_inout: state at t0 on entry, state at the last accepted step on exit.
+ * dense_out[max_dense*ndofs], dense_times[max_dense] receive the dense outputs. */
+int tb_dp45_integrate(tb_handle* h, double* f_inout, double t0, double t_final, double dense_step,
+                      double* dense_out, double* dense_times, int64_t max_dense, tb_dp45_stats* stats,
+                      int flags);
+
+/* The same integration in pieces: begin, advance by whole attempts (one CUDA
+ * graph launch each, asynchronous; attempts after the end are no-ops), poll,
+ * end.  max_dense == 0 keeps no dense output. */
+int tb_dp45_begin(tb_handle* h, const double* f0, double t0, double t_final, double dense_step, int64_t max_dense,
+                  int flags);
+int tb_dp45_advance(tb_handle* h, int64_t n_attempts);
+int tb_dp45_poll(tb_handle* h, tb_dp45_stats* stats);
+int tb_dp45_end(tb_handle* h, double* f_out, double* dense_out, double* dense_times, int64_t max_dense,
+                tb_dp45_stats* stats, int flags);
+
+/* Synchronises the handle's stream. */
+int tb_synchronize(tb_handle* h);
+
+/* The cudaStream_t every launch of this handle goes to (for event timing). */
+void* tb_get_stream(tb_handle* h);
+
+/* acc += collision terms before M^-1 (device pointers): the scatter-adds of
+ * singleScatteringPropagator (ScatteringChannel.cpp:649) for one channel, or
+ * all channels with ch = -1.  The bare collision kernels, for timing and for
+ * callers that compose their own right-hand side. */
+int tb_collision_accumulate(tb_handle* h, int ch, const double* f, double* acc);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TORTOISE_B200_H */

@@ -1,0 +1,145 @@
+"""GPU parity: the CUDA library against the oracle and the golden fixtures.
+
+Tolerances: tuple lists bit-exact (integer work); FP64 collision / drift /
+RHS within 1e-12 relative L2 (only the summation order differs: FP64 atomics
+and fused multiply-adds on the device); error norm within 1e-13 relative;
+DP45 trajectories within 1e-11 relative L2 with identical accept/reject
+sequences.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden, rel_l2
+from tortoise_b200 import engine as E
+from tortoise_b200 import workloads as W
+from tests.golden.make_golden import cases, tuple_hash
+
+pytestmark = pytest.mark.gpu
+
+CASES = list(cases().keys())
+
+
+def _setup(name):
+    build, seed, kT = cases()[name]
+    mat = build()
+    f0 = W.initial_status(mat, kT=kT, seed=seed).vec
+    return mat, f0
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_enumeration_bit_exact(gpu_lib, name):
+    g = golden(name)
+    mat, f0 = _setup(name)
+    eng = E.Engine(mat, layout=E.LAYOUT_MC64)
+    for ch in range(len(mat.channels)):
+        ids, umk = eng.tuples(ch)
+        info = eng.channel_info(ch)
+        assert [info["n_tuples"], info["n_prefilter"], info["n_det"]] == list(g["ch%d_counts" % ch])
+        assert tuple_hash(ids, umk) == str(g["ch%d_hash" % ch])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_channel_and_rhs_parity_fp64(gpu_lib, name):
+    g = golden(name)
+    mat, f0 = _setup(name)
+    eng = E.Engine(mat, layout=E.LAYOUT_MC64)
+    for ch in range(len(mat.channels)):
+        assert rel_l2(eng.channel_propagate(ch, f0), g["ch%d_prop" % ch]) < 1e-12
+    assert rel_l2(eng.rhs(f0, drift=True), g["rhs"]) < 1e-12
+    assert rel_l2(eng.rhs(f0, drift=False), g["rhs_nodrift"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_relative_error_parity(gpu_lib, name):
+    g = golden(name)
+    mat, f0 = _setup(name)
+    eng = E.Engine(mat, layout=E.LAYOUT_MC64)
+    r = eng.relative_error(g["err"], f0)
+    assert abs(r - float(g["relerr"])) <= 1e-13 * float(g["relerr"])
+
+
+@pytest.mark.parametrize("name", ["eph_n4", "eph_bath_n4", "ee_n3"])
+def test_dp45_trajectory_parity(gpu_lib, name):
+    g = golden(name)
+    mat, f0 = _setup(name)
+    eng = E.Engine(mat, layout=E.LAYOUT_MC64)
+    r = eng.dp45(f0, 0.0, 0.4, 0.1)
+    assert r["status"] == 0 and r["done"] == 1
+    assert [r["attempts"], r["accepted"], r["rejected"], r["rhs_evals"]] == list(g["dp_stats"])
+    assert np.allclose(r["dense_t"], g["dp_dense_t"], rtol=0, atol=1e-14)
+    assert rel_l2(r["dense"], g["dp_dense"]) < 1e-11
+    assert rel_l2(r["y"], g["dp_y"]) < 1e-11
+    assert abs(r["t"] - float(g["dp_t"][0])) < 1e-13
+
+
+def test_caller_supplied_tuples_match(gpu_lib):
+    """A tuple list handed in (the .scattIndices path) gives the same operator."""
+    name = "eph_n4"
+    g = golden(name)
+    mat, f0 = _setup(name)
+    o = oracle.Oracle(mat)
+    for ch, c in enumerate(mat.channels):
+        c.tuples, c.tuple_umklapp = o.tuples(ch)
+    eng = E.Engine(mat, layout=E.LAYOUT_MC64)
+    assert rel_l2(eng.rhs(f0), g["rhs"]) < 1e-12
+    assert eng.channel_info(0)["n_prefilter"] == -1
+
+
+def test_larger_ee_against_live_oracle(gpu_lib):
+    """1.7 M four-leg tuples at N=8."""
+    mat = W.config0(8)
+    f0 = W.initial_status(mat, kT=0.1, seed=11).vec
+    o = oracle.Oracle(mat)
+    eng = E.Engine(mat, layout=E.LAYOUT_MC64)
+    ids_o, umk_o = o.tuples(0)
+    ids_g, umk_g = eng.tuples(0)
+    assert np.array_equal(ids_o, ids_g) and np.array_equal(umk_o, umk_g)
+    assert rel_l2(eng.rhs(f0), o.rhs(f0)) < 1e-12
+
+
+@pytest.mark.parametrize("variant", ["umklapp", "nonsquare", "partial_mesh", "empty_channel", "zero_amplitude"])
+def test_edge_cases(gpu_lib, variant):
+    from tortoise_b200.model import Material, Mesh, Region, IN, OUT, FERMION, BOSON
+    region = Region((-1.0, -1.0), ((2.0, 0.0), (0.0, 2.0)))
+    if variant == "umklapp":
+        mat = W.build_material(3, ("P",), (0.2,), ee=False, eph=False)
+        for c in mat.addScatteringChannelsWildcards(["el:*", "pn:*", "el:*"], [IN, IN, OUT], 1):
+            pass
+        assert mat.channels[0].umklappUnitVectors.shape == (9, 2)
+    elif variant == "nonsquare":
+        mat = W.build_material(4, ("P", "D"), (0.2,), ee=False, eph=True, field=(0.05, -0.02), mesh_nsplit=(5, 3))
+    elif variant == "partial_mesh":
+        mat = Material("partial", region)
+        full = Mesh(region, (0.0, 0.0), (1.0, 1.0), (6, 6))
+        part = Mesh(region, (0.2, 0.25), (0.5, 0.4), (4, 3))
+        mat.addBand("pn:ac", 0, BOSON, full, lambda x, y: 0.05 + 0.1 * np.sqrt(x * x + y * y))
+        mat.addBand("el:C", -1, FERMION, part, lambda x, y: 0.5 * (x * x + y * y))
+        mat.addScatteringChannelsWildcards(["el:*", "pn:*", "el:*"], [IN, IN, OUT], 0)
+    elif variant == "empty_channel":
+        mat = W.build_material(3, ("P",), (50.0,), ee=False, eph=True)
+    else:
+        mat = W.build_material(3, ("P", "D"), (0.2,), ee=False, eph=True)
+        mat.channels[1].amplitude = 0.0
+    f0 = W.initial_status(mat, seed=7).vec
+    o = oracle.Oracle(mat)
+    eng = E.Engine(mat, layout=E.LAYOUT_MC64)
+    for ch in range(len(mat.channels)):
+        a, ua = o.tuples(ch)
+        b, ub = eng.tuples(ch)
+        assert np.array_equal(a, b) and np.array_equal(ua, ub)
+    ref = o.rhs(f0)
+    got = eng.rhs(f0)
+    if np.linalg.norm(ref) == 0.0:
+        assert np.linalg.norm(got) == 0.0
+    else:
+        assert rel_l2(got, ref) < 1e-12
+
+
+def test_bad_descriptions_are_rejected(gpu_lib):
+    mat = W.config0(3)
+    mat.channels[0].tuples = np.array([[0, 1, 2, 99999]], dtype=np.int32)
+    mat.channels[0].tuple_umklapp = np.array([0], dtype=np.int32)
+    with pytest.raises(E.TortoiseError) as ei:
+        E.Engine(mat)
+    assert ei.value.rc == 1

@@ -1,0 +1,129 @@
+"""CPU tests of the oracle: identities the reference algorithm obeys, the
+DP54 documentation example, and regression against the golden fixtures."""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden, rel_l2
+from tortoise_b200 import workloads as W
+from tortoise_b200.model import linform_to_nodal
+from tests.golden.make_golden import cases, tuple_hash
+
+
+def test_mass_matrix_identities():
+    mat = W.config0(4)
+    o = oracle.Oracle(mat)
+    M, Mi = o.mass_matrix(0)
+    vol = mat.bands[0].mesh.elemVolume
+    # exact P1 mass matrix on the reference triangle scaled by |T|/|T_ref|
+    exact = vol * np.array([[1, 1 / 3, 1 / 3], [1 / 3, 1 / 6, 1 / 12], [1 / 3, 1 / 12, 1 / 6]])
+    assert np.allclose(M, exact, rtol=1e-12)
+    assert np.allclose(M @ Mi, np.eye(3), atol=1e-12)
+
+
+def _integral(o, band, coeffs, weight=None):
+    mat = o.material
+    ne = mat.bands[band].mesh.ne
+    w = np.tile([1.0, 0.0, 0.0], ne) if weight is None else weight
+    return o.integrate(band, coeffs, w)
+
+
+@pytest.mark.parametrize("name", ["ee_n4", "eph_n4"])
+def test_conservation_laws(name):
+    """Particle number (e-e), energy and crystal momentum are conserved by
+    every tuple: the delta constraint makes sum_l dir_l E_l(p_l) = 0 exactly
+    for the P1 energy (IntegratorCore.hpp:298-320)."""
+    build, seed, kT = cases()[name]
+    mat = build()
+    o = oracle.Oracle(mat)
+    f0 = W.initial_status(mat, kT=kT, seed=seed).vec
+    d = o.rhs(f0, drift=False)
+    offs, _ = mat.band_offsets()
+    tot_e = 0.0
+    scale_e = 0.0
+    tot_n = 0.0
+    scale_n = 0.0
+    for b, band in enumerate(mat.bands):
+        sl = slice(offs[b], offs[b] + band.mesh.ne * 3)
+        tot_e += o.integrate(b, d[sl], band.dispersion_coeffs)
+        scale_e += abs(o.integrate(b, np.abs(d[sl]), np.abs(band.dispersion_coeffs)))
+        if band.statistics == -1:
+            one = np.tile([1.0, 0.0, 0.0], band.mesh.ne)
+            tot_n += o.integrate(b, d[sl], one)
+            scale_n += o.integrate(b, np.abs(d[sl]), one)
+    assert abs(tot_e) <= 1e-12 * scale_e
+    if name.startswith("ee"):
+        assert abs(tot_n) <= 1e-12 * scale_n
+
+
+def test_equilibrium_is_nearly_stationary():
+    """Fermi-Dirac at common T and mu: gain and loss balance up to the P1
+    interpolation of f along the energy shell, so the residual is small when
+    the mesh resolves kT and shrinks under refinement."""
+    ratios = []
+    for N in (4, 6):
+        mat = W.config0(N)
+        o = oracle.Oracle(mat)
+        eq = W.initial_status(mat, kT=3.0, seed=0, bump_amplitude=0.0).vec
+        neq = W.initial_status(mat, kT=3.0, seed=0, bump_amplitude=0.3).vec
+        ratios.append(np.linalg.norm(o.rhs(eq, drift=False)) / np.linalg.norm(o.rhs(neq, drift=False)))
+    assert ratios[0] < 1e-2 and ratios[1] < ratios[0]
+
+
+def test_dp54_documentation_example():
+    """DormandPrince54.hpp:80-106: y' = cos t from 0 to 10, dense step 1."""
+    d, t, st = oracle.scalar_example()
+    assert len(t) == 10
+    assert np.allclose(t, np.arange(1, 11))
+    assert np.max(np.abs(d - np.sin(t))) < 5e-6
+    g = golden("dp54_scalar")
+    assert np.array_equal(d, g["dense"]) and np.array_equal(st, g["stats"])
+
+
+@pytest.mark.parametrize("name", list(cases().keys()))
+def test_oracle_matches_golden(name):
+    g = golden(name)
+    build, seed, kT = cases()[name]
+    mat = build()
+    o = oracle.Oracle(mat)
+    f0 = W.initial_status(mat, kT=kT, seed=seed).vec
+    assert np.array_equal(f0, g["f0"])
+    for ch in range(len(mat.channels)):
+        ids, umk = o.tuples(ch)
+        pre, det = o.enum_counts(ch)
+        assert [len(umk), pre, det] == list(g["ch%d_counts" % ch])
+        assert tuple_hash(ids, umk) == str(g["ch%d_hash" % ch])
+        assert rel_l2(o.channel_propagate(ch, f0), g["ch%d_prop" % ch]) < 1e-14
+    assert rel_l2(o.rhs(f0, drift=True), g["rhs"]) < 1e-14
+    assert abs(o.relative_error(g["err"], f0) - float(g["relerr"])) <= 1e-14 * float(g["relerr"])
+    if "dp_y" in g:
+        r = o.dp45(f0, 0.0, 0.4, 0.1)
+        assert [r["attempts"], r["accepted"], r["rejected"], r["rhs_evals"]] == list(g["dp_stats"])
+        assert rel_l2(r["y"], g["dp_y"]) < 1e-13
+
+
+def test_tuples_are_valid_and_ordered():
+    mat = W.build_material(4, ("P", "D"), (0.2,), ee=False, eph=True)
+    o = oracle.Oracle(mat)
+    for ch, c in enumerate(mat.channels):
+        ids, umk = o.tuples(ch)
+        ne = [mat.bands[b].mesh.ne for b in c.legBandNumber]
+        for l in range(c.nlegs):
+            assert ids[:, l].min() >= 0 and ids[:, l].max() < ne[l]
+        # reference loop order: sections of legs 0..L-2, then elements
+        sec = ids[:, :-1] // 2
+        key = np.lexsort(tuple([ids[:, -1]] + [ids[:, l] % 2 for l in reversed(range(c.nlegs - 1))]
+                               + [sec[:, l] for l in reversed(range(c.nlegs - 1))]))
+        assert np.array_equal(key, np.arange(len(key)))
+
+
+def test_single_tuple_partition_additivity():
+    """propagate over a tuple range is additive (the TBB reduction split)."""
+    mat = W.config0(4)
+    o = oracle.Oracle(mat)
+    f0 = W.initial_status(mat, seed=2).vec
+    n = o.num_tuples(0)
+    full = o.channel_propagate(0, f0)
+    a = o.channel_propagate(0, f0, 0, n // 3)
+    b = o.channel_propagate(0, f0, n // 3, n)
+    assert rel_l2(a + b, full) < 1e-13

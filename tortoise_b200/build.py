@@ -1,0 +1,53 @@
+"""Builds libtortoise_b200.so in-tree with nvcc for sm_100a.
+
+Usage: python -m tortoise_b200.build   (or tortoise_b200.build.build()).
+The enumeration kernel is compiled with --fmad=false so that its
+floating-point filters round like the reference's unfused C++.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "libtortoise_b200.so")
+BUILD = os.path.join(HERE, "_build")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+          "-I" + os.path.join(HERE, "..", "include"), "--expt-relaxed-constexpr"]
+SOURCES = {
+    "tb_api.cu": [],
+    "tb_enumerate.cu": ["--fmad=false"],
+    "tb_collision.cu": [],
+    "tb_drift.cu": [],
+    "tb_dp45.cu": [],
+    "tb_tensor.cu": [],
+}
+
+
+def nvcc():
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if c and (os.path.sep not in c or os.path.exists(c)):
+            return c
+    return "nvcc"
+
+
+def build(verbose=False, extra=()):
+    os.makedirs(BUILD, exist_ok=True)
+    objs = []
+    for src, flags in SOURCES.items():
+        obj = os.path.join(BUILD, src.replace(".cu", ".o"))
+        cmd = [nvcc(), *ARCH, *COMMON, *flags, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.check_call(cmd)
+        objs.append(obj)
+    cmd = [nvcc(), *ARCH, "-shared", "-o", OUT, *objs, "-lcudart"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.check_call(cmd)
+    return OUT
+
+
+if __name__ == "__main__":
+    build(verbose="-v" in sys.argv, extra=[a for a in sys.argv[1:] if a != "-v"])

@@ -1,0 +1,110 @@
+// tb_common.cuh -- shared device/host definitions of the tortoise_b200 library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/tortoise_b200.h"
+
+namespace tb {
+
+// ----------------------------------------------------------------- errors
+void set_error(const std::string& msg);
+const char* get_error();
+
+#define TB_CUDA(call)                                                                  \
+    do {                                                                               \
+        cudaError_t _e = (call);                                                       \
+        if (_e != cudaSuccess) {                                                       \
+            ::tb::set_error(std::string(#call) + ": " + cudaGetErrorString(_e));      \
+            return TB_ERR_CUDA;                                                        \
+        }                                                                              \
+    } while (0)
+
+#define TB_TRY(call)                      \
+    do {                                  \
+        int _rc = (call);                 \
+        if (_rc != TB_OK) return _rc;     \
+    } while (0)
+
+// --------------------------------------------------------------- constants
+// Order-2 Gauss rule on the reference triangle with the reference's 14-digit
+// constants (GaussQuadratureConst.hpp:84-90) and on [0,1] (:60-61).
+#define TB_GP2_A 0.16666666666667
+#define TB_GP2_B 0.66666666666667
+#define TB_GW2 0.33333333333333
+#define TB_GP1_0 0.2113248654051871
+#define TB_GP1_1 0.7886751345948129
+
+// ------------------------------------------------------------ host mirrors
+struct HostMesh {
+    int nx, ny, ne;
+    double origin[2];
+    double dG[2][2];
+    double invdG[2][2];
+    double vol;
+    double rel_origin[2];
+    double M[3][3], Minv[3][3];
+};
+
+struct HostBand {
+    int mesh, ne;
+    int64_t off;
+    double charge, stat, abs_tol, rel_tol, penal;
+    int constrained;
+    double vel[2];
+    std::vector<double> disp, kx, ky, minE, maxE, cpop;
+};
+
+// ---------------------------------------------------- device-side records
+// Everything a kernel needs about one leg of a channel.
+struct LegDev {
+    const double* disp;   // [ne*3]
+    const double* kx;     // [ne*3]
+    const double* ky;     // [ne*3]
+    int64_t foff;         // band offset in the status vector
+    double dir;           // +1 in, -1 out
+    double stat;          // -1 fermion, +1 boson
+    int ne;
+};
+
+struct ChanDev {
+    int L;
+    int nmc;
+    int R;                // MC table row length 2*(L-2)+1
+    int n_umk;
+    LegDev leg[TB_MAX_LEGS];
+    double amp_vol;       // prod_l (elemVolume_l * 2) (constructAmplitude without amplitude)
+    double fact;          // (NDim!)^(L-2) * (NDim-1)!
+    double min_det;
+    double threshold;
+    double gvec[4];       // region gVec, column-major
+    const double* umk;    // [n_umk*2] device
+    const double* mc;     // [nmc*R] device
+};
+
+// Mesh data needed by the element-wise kernels.
+struct MeshDev {
+    int nx, ny, ne;
+    double dG[2][2];
+    double vol;
+    double rel_origin[2];
+    double Minv[3][3];
+    double M[3][3];
+};
+
+// Element-wise per-band record (drift, inverse mass, error norm, constraints).
+struct BandDev {
+    MeshDev mesh;
+    int64_t off;
+    int ne;
+    double stat, abs_tol, rel_tol, penal;
+    int constrained;
+    const double* cpop;   // device, [ne*3] or null
+    double vel[2];
+};
+
+}  // namespace tb

@@ -1,0 +1,443 @@
+// tb_dp45.cu -- fused Dormand-Prince 5(4) stage kernels, on-device error norm
+// and step-size controller.
+//
+// Reference: Algorithms::dormandPrince54, third overload
+// (include/Generics/Algorithms/DormandPrince54.hpp:479-665) as driven by
+// MaterialTimeStatus::propagate (src/Physics/Status/MaterialTimeStatus.cpp:
+// 102-137); error norm MaterialStatus::relativeError / Band::relativeError
+// (src/Physics/Status/MaterialStatus.cpp:189-196, src/Physics/Material/
+// Band.cpp:87-101); constraints MaterialStatus::applyConstraints
+// (MaterialStatus.cpp:198-206).
+//
+// Each stage kernel fuses, per element: M^-1 of the freshly accumulated RHS,
+// the reset of the accumulator, the Butcher combination of the next stage
+// input and the constraint enforcement -- one pass over the state per RHS
+// evaluation instead of the reference's chain of vector temporaries.  The
+// last stage kernel also forms y4, err = y5 - y4 and per-block partial sums of
+// the Gauss-2 error integrals; the single-thread controller kernel reduces
+// them in a fixed order (deterministic), applies the PI controller and
+// schedules dense output.  dt never leaves the device.
+#include <math.h>
+
+#include "tb_dp45.cuh"
+
+namespace tb {
+
+// Butcher tableau, DormandPrince54.hpp:502-511
+__constant__ double c_A[7][6] = {
+    {0, 0, 0, 0, 0, 0},
+    {1. / 5., 0, 0, 0, 0, 0},
+    {3. / 40., 9. / 40., 0, 0, 0, 0},
+    {44. / 45., -56. / 15., 32. / 9., 0, 0, 0},
+    {19372. / 6561., -25360. / 2187., 64448. / 6561., -212. / 729., 0, 0},
+    {9017. / 3168., -355. / 33., 46732. / 5247., 49. / 176., -5103. / 18656., 0},
+    {0, 0, 0, 0, 0, 0}};
+__constant__ double c_b[6] = {35. / 384., 0., 500. / 1113., 125. / 192., -2187. / 6784., 11. / 84.};
+__constant__ double c_bh[7] = {5179. / 57600., 0., 7571. / 16695., 393. / 640., -92097. / 339200., 187. / 2100.,
+                               1. / 40.};
+
+__device__ __forceinline__ void to_nodal(const double c[3], double n[3]) { n[0] = c[0]; n[1] = c[1] + c[0]; n[2] = c[2] + c[0]; }
+__device__ __forceinline__ void to_lin(const double n[3], double c[3]) { c[0] = n[0]; c[1] = n[1] - n[0]; c[2] = n[2] - n[0]; }
+
+__device__ __forceinline__ double gauss2_sq(const double c[3]) {
+    const double a = TB_GP2_A, b = TB_GP2_B, w = TB_GW2;
+    const double v0 = (c[1] * a + c[2] * a) + c[0];
+    const double v1 = (c[1] * b + c[2] * a) + c[0];
+    const double v2 = (c[1] * a + c[2] * b) + c[0];
+    return ((v0 * v0) * w + (v1 * v1) * w) + (v2 * v2) * w;
+}
+
+// Per-element integrands of Band::relativeError with the reference's exact
+// sequence of nodal <-> linear-form conversions (Function.cpp:75-109, 152-159).
+__device__ __forceinline__ void elem_rel_err(const BandDev& b, const double* err, const double* p, double& rel,
+                                             double& pen) {
+    double np[3];
+    to_nodal(p, np);
+    double sc[3];
+    double pe[3];
+    if (b.stat == -1.0) {
+        const double om[3] = {-(p[0] - 1.0), -p[1], -p[2]};
+        double nom[3], fa[3], fb[3], la[3], lb[3], na[3], nb[3], mn[3], lm[3];
+        to_nodal(om, nom);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { fa[k] = fabs(np[k]); fb[k] = fabs(nom[k]); }
+        to_lin(fa, la); to_lin(fb, lb);
+        to_nodal(la, na); to_nodal(lb, nb);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) mn[k] = fmin(na[k], nb[k]);
+        to_lin(mn, lm);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) sc[k] = b.rel_tol * lm[k];
+        sc[0] += b.abs_tol;
+        if (b.penal != 0.0) {
+            double m0[3], lm0[3], pm1[3] = {p[0] - 1.0, p[1], p[2]}, npm1[3], x1[3], lx1[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) m0[k] = fmin(np[k], 0.);
+            to_lin(m0, lm0);
+            to_nodal(pm1, npm1);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) x1[k] = fmax(npm1[k], 0.);
+            to_lin(x1, lx1);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) pe[k] = -lm0[k] + lx1[k];
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) sc[k] = b.rel_tol * p[k];
+        sc[0] += b.abs_tol;
+        if (b.penal != 0.0) {
+            double m0[3], lm0[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) m0[k] = fmin(np[k], 0.);
+            to_lin(m0, lm0);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) pe[k] = -lm0[k];
+        }
+    }
+    double nsc[3], ner[3], r[3];
+    to_nodal(sc, nsc);
+    to_nodal(err, ner);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) ner[k] /= nsc[k];
+    to_lin(ner, r);
+    rel = gauss2_sq(r);
+    pen = 0.0;
+    if (b.penal != 0.0) {
+        double npe[3], q[3];
+        to_nodal(pe, npe);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) npe[k] /= nsc[k];
+        to_lin(npe, q);
+        pen = gauss2_sq(q);
+    }
+}
+
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int i = 0; i < NT / 32; ++i) s += sh[i];
+    return s;
+}
+
+__device__ __forceinline__ void enforce3(const BandDev& bd, int e, double v[3]) {
+    if (bd.constrained) {
+        const double* cp = bd.cpop + 3 * (int64_t)e;
+        v[0] = cp[0]; v[1] = cp[1]; v[2] = cp[2];
+    }
+}
+
+// Element-wise stage kernel (see tb_dp45.cuh for the meaning of s).
+template <int S>
+__global__ void __launch_bounds__(256) k_stage(BandsDev bands, DPBufs B) {
+    __shared__ double sh[8];
+    const DPCtl* ctl = B.ctl;
+    if (ctl->done) return;
+    const double dt = ctl->dt;
+    for (int bi = 0; bi < bands.nb; ++bi) {
+        const BandDev& bd = bands.b[bi];
+        double srel = 0.0, spen = 0.0;
+        const int e = blockIdx.x * blockDim.x + threadIdx.x;
+        if (e < bd.ne) {
+            const int64_t o = bd.off + 3 * (int64_t)e;
+            if (S >= 1) {
+                // k_{S+1} = acc * M^-1, acc = 0
+                const double x = B.acc[o], y = B.acc[o + 1], z = B.acc[o + 2];
+                double* kk = B.k[S];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) kk[o + j] = x * bd.mesh.Minv[0][j] + y * bd.mesh.Minv[1][j] + z * bd.mesh.Minv[2][j];
+                B.acc[o] = 0.0; B.acc[o + 1] = 0.0; B.acc[o + 2] = 0.0;
+            }
+            double v[3];
+            if (S <= 4) {
+                // input of k_{S+2}: y + sum_{j<=S} (a_{S+1,j} dt) k_{j+1}
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    double t = B.y[o + c];
+#pragma unroll
+                    for (int j = 0; j <= S; ++j) t = t + (c_A[S + 1][j] * dt) * B.k[j][o + c];
+                    v[c] = t;
+                }
+                enforce3(bd, e, v);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) B.tmp[o + c] = v[c];
+            } else if (S == 5) {
+                // y5 = y + (dt b1) k1 + (dt b3) k3 + (dt b4) k4 + (dt b5) k5 + (dt b6) k6
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    double t = B.y[o + c];
+                    t = t + (dt * c_b[0]) * B.k[0][o + c];
+                    t = t + (dt * c_b[2]) * B.k[2][o + c];
+                    t = t + (dt * c_b[3]) * B.k[3][o + c];
+                    t = t + (dt * c_b[4]) * B.k[4][o + c];
+                    t = t + (dt * c_b[5]) * B.k[5][o + c];
+                    v[c] = t;
+                }
+                enforce3(bd, e, v);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) B.y5[o + c] = v[c];
+            } else {
+                // y4 and the error
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    double t = B.y[o + c];
+                    t = t + (dt * c_bh[0]) * B.k[0][o + c];
+                    t = t + (dt * c_bh[2]) * B.k[2][o + c];
+                    t = t + (dt * c_bh[3]) * B.k[3][o + c];
+                    t = t + (dt * c_bh[4]) * B.k[4][o + c];
+                    t = t + (dt * c_bh[5]) * B.k[5][o + c];
+                    t = t + (dt * c_bh[6]) * B.k[6][o + c];
+                    v[c] = t;
+                }
+                enforce3(bd, e, v);
+                double err[3], p5[3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) { p5[c] = B.y5[o + c]; err[c] = p5[c] - v[c]; }
+                elem_rel_err(bd, err, p5, srel, spen);
+            }
+        }
+        if (S == 6) {
+            const double r = block_sum<256>(srel, sh);
+            const double p = block_sum<256>(spen, sh);
+            if (threadIdx.x == 0) {
+                B.part[(2 * bi) * B.nblk + blockIdx.x] = r;
+                B.part[(2 * bi + 1) * B.nblk + blockIdx.x] = p;
+            }
+        }
+    }
+}
+
+int launch_stage(const BandsDev& bands, const DPBufs& B, int s, cudaStream_t st) {
+    switch (s) {
+        case 0: k_stage<0><<<B.nblk, 256, 0, st>>>(bands, B); break;
+        case 1: k_stage<1><<<B.nblk, 256, 0, st>>>(bands, B); break;
+        case 2: k_stage<2><<<B.nblk, 256, 0, st>>>(bands, B); break;
+        case 3: k_stage<3><<<B.nblk, 256, 0, st>>>(bands, B); break;
+        case 4: k_stage<4><<<B.nblk, 256, 0, st>>>(bands, B); break;
+        case 5: k_stage<5><<<B.nblk, 256, 0, st>>>(bands, B); break;
+        default: k_stage<6><<<B.nblk, 256, 0, st>>>(bands, B); break;
+    }
+    TB_CUDA(cudaGetLastError());
+    return TB_OK;
+}
+
+// Single-thread controller: DormandPrince54.hpp:580-661.
+__global__ void k_controller(BandsDev bands, DPBufs B) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    DPCtl* c = B.ctl;
+    if (c->done) { c->skip = 1; return; }
+    c->skip = 0;
+    c->attempts += 1;
+    c->rhs_evals += 6;
+    double errNorm = 0.0;
+    bool nonfinite = false;
+    for (int bi = 0; bi < bands.nb; ++bi) {
+        const BandDev& bd = bands.b[bi];
+        double sr = 0.0, sp = 0.0;
+        for (int k = 0; k < B.nblk; ++k) { sr += B.part[(2 * bi) * B.nblk + k]; sp += B.part[(2 * bi + 1) * B.nblk + k]; }
+        const double ir = bd.mesh.vol * sr, ip = bd.mesh.vol * sp;
+        const double be = sqrt((ir + bd.penal * ip) / (double(bd.ne) * bd.mesh.vol));
+        if (!isfinite(be)) nonfinite = true;
+        if (be >= errNorm) errNorm = be;   // a NaN never replaces the running max
+    }
+    c->last_err = errNorm;
+    const double minscale = 0.333333, maxscale = 3.0, safety = 0.98, alpha = 0.7 / 5., beta = 0.4 / 5.;
+    c->n_now = 0;
+    c->acc_now = 0;
+    if (nonfinite) {
+        c->status = TB_ERR_NONFINITE;
+        c->done = 1;
+        return;
+    }
+    double dt = c->dt, t = c->t;
+    c->step_t = t;
+    c->step_dt = dt;
+    if (errNorm <= 1.) {
+        c->acc_now = 1;
+        int k = 0;
+        double dtime = c->dense_time;
+        while (dtime <= t + (1.0001) * dt && dtime <= c->tf + .0001 * dt) {
+            if (k < TB_MAX_DENSE_PER_STEP) {
+                c->dense_s[k] = (dtime - t) / dt;
+                c->dense_t[k] = dtime;
+            }
+            ++k;
+            dtime += c->dense_step;
+        }
+        if (k > TB_MAX_DENSE_PER_STEP) { c->status = TB_ERR_CAPACITY; k = TB_MAX_DENSE_PER_STEP; }
+        c->n_now = k;
+        c->dense_time = dtime;
+        t += dt;
+        double scale;
+        if (errNorm == 0.) scale = maxscale;
+        else {
+            scale = safety * pow(1. / errNorm, alpha) * pow(c->olderror, beta);
+            scale = fmin(fmax(scale, minscale), maxscale);
+        }
+        if (c->rejected) dt *= fmin(1.0, scale);
+        else dt *= scale;
+        dt = fmin(dt, (t + dt) - t);
+        c->rejected = 0;
+        c->olderror = errNorm;
+        c->accepted += 1;
+    } else {
+        double scale = safety * pow(1. / errNorm, 1 / 5.);
+        scale = fmin(fmax(scale, minscale), maxscale);
+        dt *= scale;
+        c->rejected = 1;
+        c->rejected_n += 1;
+        if (dt < c->min_step) { c->status = TB_ERR_DT_UNDERFLOW; c->done = 1; }
+    }
+    c->t = t;
+    c->dt = dt;
+    if (!(t < c->tf)) c->done = 1;
+    if (c->status == TB_ERR_CAPACITY) c->done = 1;
+    if (c->max_attempts > 0 && c->attempts >= c->max_attempts) c->done = 1;
+}
+
+int launch_controller(const BandsDev& bands, const DPBufs& B, cudaStream_t st) {
+    k_controller<<<1, 32, 0, st>>>(bands, B);
+    TB_CUDA(cudaGetLastError());
+    return TB_OK;
+}
+
+// Dense output (DormandPrince54.hpp:598-611) followed by the FSAL commit
+// y <- y5, k1 <- k7 of an accepted attempt.  The dense outputs use the
+// pre-commit y and the time-base of the step: s = (denseTime - t_old)/dt_old,
+// which the controller stored.
+__global__ void __launch_bounds__(256) k_dense_commit(BandsDev bands, DPBufs B) {
+    const DPCtl* c = B.ctl;
+    if (c->skip || !c->acc_now) return;
+    for (int bi = 0; bi < bands.nb; ++bi) {
+        const BandDev& bd = bands.b[bi];
+        const int e = blockIdx.x * blockDim.x + threadIdx.x;
+        if (e >= bd.ne) continue;
+        const int64_t o = bd.off + 3 * (int64_t)e;
+        const long long base = c->n_dense;
+        for (int k = 0; k < c->n_now; ++k) {
+            const long long slot = base + k;
+            if (slot >= c->dense_cap) break;
+            const double s = c->dense_s[k];
+            const double dt = c->step_dt;
+            const double bt1 = -(435. * s * s * s - 1184. * s * s + 1098. * s - 384.) / (384.);
+            const double bt3 = 500. * s * (6. * s * s - 14. * s + 9.) / (1113.);
+            const double bt4 = -125. * s * (9. * s * s - 16. * s + 6.) / (192.);
+            const double bt5 = 729. * s * (35. * s * s - 64. * s + 26.) / (6784.);
+            const double bt6 = -11. * s * (3. * s - 2.) * (5. * s - 6.) / (84.);
+            const double bt7 = s * (s - 1.) * (5. * s - 3.) / (2.);
+            double v[3];
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) {
+                double t = B.y[o + cc];
+                t = t + (s * dt * bt1) * B.k[0][o + cc];
+                t = t + (s * dt * bt3) * B.k[2][o + cc];
+                t = t + (s * dt * bt4) * B.k[3][o + cc];
+                t = t + (s * dt * bt5) * B.k[4][o + cc];
+                t = t + (s * dt * bt6) * B.k[5][o + cc];
+                t = t + (s * dt * bt7) * B.k[6][o + cc];
+                v[cc] = t;
+            }
+            enforce3(bd, e, v);
+            double* out = B.dense + slot * bands.ndofs + o;
+            out[0] = v[0]; out[1] = v[1]; out[2] = v[2];
+        }
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+            B.y[o + cc] = B.y5[o + cc];
+            B.k[0][o + cc] = B.k[6][o + cc];
+        }
+    }
+}
+
+__global__ void k_dense_count(DPBufs B) {
+    DPCtl* c = B.ctl;
+    if (c->skip || !c->acc_now) return;
+    for (int k = 0; k < c->n_now; ++k) {
+        const long long slot = c->n_dense + k;
+        if (slot < c->dense_cap) B.dense_t[slot] = c->dense_t[k];
+    }
+    c->n_dense += c->n_now;
+    if (c->n_dense > c->dense_cap) { c->status = TB_ERR_CAPACITY; c->done = 1; }
+}
+
+int launch_dense_commit(const BandsDev& bands, const DPBufs& B, cudaStream_t st) {
+    k_dense_commit<<<B.nblk, 256, 0, st>>>(bands, B);
+    TB_CUDA(cudaGetLastError());
+    k_dense_count<<<1, 1, 0, st>>>(B);
+    TB_CUDA(cudaGetLastError());
+    return TB_OK;
+}
+
+__global__ void k_first(BandsDev bands, DPBufs B) {
+    for (int bi = 0; bi < bands.nb; ++bi) {
+        const BandDev& bd = bands.b[bi];
+        const int e = blockIdx.x * blockDim.x + threadIdx.x;
+        if (e >= bd.ne) continue;
+        const int64_t o = bd.off + 3 * (int64_t)e;
+        const double x = B.acc[o], y = B.acc[o + 1], z = B.acc[o + 2];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) B.k[0][o + j] = x * bd.mesh.Minv[0][j] + y * bd.mesh.Minv[1][j] + z * bd.mesh.Minv[2][j];
+        B.acc[o] = 0.0; B.acc[o + 1] = 0.0; B.acc[o + 2] = 0.0;
+    }
+}
+
+int launch_k1(const BandsDev& bands, const DPBufs& B, cudaStream_t st) {
+    k_first<<<B.nblk, 256, 0, st>>>(bands, B);
+    TB_CUDA(cudaGetLastError());
+    return TB_OK;
+}
+
+__global__ void k_enforce(BandsDev bands, const double* src, double* dst) {
+    for (int bi = 0; bi < bands.nb; ++bi) {
+        const BandDev& bd = bands.b[bi];
+        for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < bd.ne; e += gridDim.x * blockDim.x) {
+            const int64_t o = bd.off + 3 * (int64_t)e;
+            double v[3] = {src[o], src[o + 1], src[o + 2]};
+            enforce3(bd, e, v);
+            dst[o] = v[0]; dst[o + 1] = v[1]; dst[o + 2] = v[2];
+        }
+    }
+}
+
+int launch_enforce(const BandsDev& bands, const double* src, double* dst, cudaStream_t st) {
+    int maxne = 1;
+    for (int b = 0; b < bands.nb; ++b) maxne = bands.b[b].ne > maxne ? bands.b[b].ne : maxne;
+    k_enforce<<<(maxne + 255) / 256, 256, 0, st>>>(bands, src, dst);
+    TB_CUDA(cudaGetLastError());
+    return TB_OK;
+}
+
+__global__ void __launch_bounds__(256) k_error_norm(BandsDev bands, const double* err, const double* pop, double* part,
+                                                    int nblk) {
+    __shared__ double sh[8];
+    for (int bi = 0; bi < bands.nb; ++bi) {
+        const BandDev& bd = bands.b[bi];
+        double r = 0.0, p = 0.0;
+        const int e = blockIdx.x * blockDim.x + threadIdx.x;
+        if (e < bd.ne) {
+            const int64_t o = bd.off + 3 * (int64_t)e;
+            elem_rel_err(bd, err + o, pop + o, r, p);
+        }
+        const double rs = block_sum<256>(r, sh);
+        const double ps = block_sum<256>(p, sh);
+        if (threadIdx.x == 0) {
+            part[(2 * bi) * nblk + blockIdx.x] = rs;
+            part[(2 * bi + 1) * nblk + blockIdx.x] = ps;
+        }
+    }
+}
+
+int launch_error_norm(const BandsDev& bands, const double* err, const double* pop, double* part, int nblk,
+                      cudaStream_t st) {
+    k_error_norm<<<nblk, 256, 0, st>>>(bands, err, pop, part, nblk);
+    TB_CUDA(cudaGetLastError());
+    return TB_OK;
+}
+
+}  // namespace tb

@@ -1,0 +1,23 @@
+// tb_tensor.cuh -- precomputed moment tensors of the collision operator.
+#pragma once
+
+#include "tb_common.cuh"
+
+namespace tb {
+
+struct MomentTensor {
+    void* d = nullptr;        // moments, tile-major (see tb_tensor.cu)
+    int64_t n = 0;            // tuples
+    int64_t ntiles = 0;
+    int nmom = 0;             // moments per tuple
+    bool fp32 = false;
+    void release();
+};
+
+int64_t tensor_bytes(int L, bool fp32, int64_t n_tuples);
+int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, bool fp32, MomentTensor& T,
+                 cudaStream_t s);
+int launch_collision_tensor(const ChanDev& c, double amplitude, const MomentTensor& T, const int32_t* tup,
+                            int64_t stride, int64_t n, const double* f, double* acc, const int* done, cudaStream_t s);
+
+}  // namespace tb

@@ -1,0 +1,198 @@
+"""ctypes binding of libtortoise_b200.so (include/tortoise_b200.h).
+
+There is no CPU fallback: if the CUDA library is missing or no device is
+present every call raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from .abi import STATUS_NAMES
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtortoise_b200.so")
+
+LAYOUT_AUTO, LAYOUT_MC64, LAYOUT_T64, LAYOUT_T32 = 0, 1, 2, 3
+LAYOUT_NAMES = {1: "mc64", 2: "t64", 3: "t32"}
+PTR_HOST, NO_DRIFT, NO_COLLISIONS = 1, 2, 4
+
+_lib = None
+
+
+class TortoiseError(RuntimeError):
+    def __init__(self, rc, where):
+        self.rc = rc
+        msg = lib().tb_last_error().decode(errors="replace")
+        super().__init__("%s failed: %s (%s)" % (where, STATUS_NAMES.get(rc, rc), msg))
+
+
+class Options(C.Structure):
+    _fields_ = [("device", C.c_int32), ("layout", C.c_int32), ("allow_fp32", C.c_int32),
+                ("tensor_budget_bytes", C.c_int64), ("verbose", C.c_int32)]
+
+
+class DP45Stats(C.Structure):
+    _fields_ = [("t", C.c_double), ("dt", C.c_double), ("last_err", C.c_double),
+                ("attempts", C.c_int64), ("accepted", C.c_int64), ("rejected", C.c_int64),
+                ("rhs_evals", C.c_int64), ("n_dense", C.c_int64), ("status", C.c_int32),
+                ("done", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def lib():
+    """Loads the in-tree CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libtortoise_b200.so is not built: run `python -m tortoise_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        vp, dp, ip, i64 = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32), C.c_int64
+        L.tb_last_error.restype = C.c_char_p
+        L.tb_create.argtypes = [C.POINTER(vp), vp, C.POINTER(Options)]
+        L.tb_destroy.argtypes = [vp]
+        L.tb_num_dofs.restype = i64
+        L.tb_num_dofs.argtypes = [vp]
+        L.tb_band_offset.restype = i64
+        L.tb_band_offset.argtypes = [vp, C.c_int]
+        L.tb_num_channels.argtypes = [vp]
+        L.tb_channel_info.argtypes = [vp, C.c_int, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64), C.POINTER(C.c_int32)]
+        L.tb_get_tuples.argtypes = [vp, C.c_int, ip, ip]
+        L.tb_set_amplitude.argtypes = [vp, C.c_int, C.c_double]
+        L.tb_rhs.argtypes = [vp, vp, vp, C.c_int]
+        L.tb_channel_propagate.argtypes = [vp, C.c_int, vp, vp, C.c_int]
+        L.tb_relative_error.argtypes = [vp, vp, vp, dp, C.c_int]
+        L.tb_apply_constraints.argtypes = [vp, vp, C.c_int]
+        L.tb_dp45_integrate.argtypes = [vp, vp, C.c_double, C.c_double, C.c_double, vp, vp, i64,
+                                        C.POINTER(DP45Stats), C.c_int]
+        L.tb_dp45_begin.argtypes = [vp, vp, C.c_double, C.c_double, C.c_double, i64, C.c_int]
+        L.tb_dp45_advance.argtypes = [vp, i64]
+        L.tb_dp45_poll.argtypes = [vp, C.POINTER(DP45Stats)]
+        L.tb_dp45_end.argtypes = [vp, vp, vp, vp, i64, C.POINTER(DP45Stats), C.c_int]
+        L.tb_synchronize.argtypes = [vp]
+        L.tb_get_stream.restype = vp
+        L.tb_get_stream.argtypes = [vp]
+        L.tb_collision_accumulate.argtypes = [vp, C.c_int, vp, vp]
+        _lib = L
+    return _lib
+
+
+def _check(rc, where):
+    if rc != 0:
+        raise TortoiseError(rc, where)
+
+
+def _hp(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+class Engine:
+    """One device handle for a Material (tb_create ... tb_destroy)."""
+
+    def __init__(self, material, layout=LAYOUT_AUTO, allow_fp32=False, device=0, tensor_budget_bytes=0):
+        self.material = material
+        self.packed = material.pack()
+        opts = Options(device, layout, 1 if allow_fp32 else 0, tensor_budget_bytes, 0)
+        h = C.c_void_p()
+        _check(lib().tb_create(C.byref(h), C.addressof(self.packed.desc), C.byref(opts)), "tb_create")
+        self.h = h
+        self.ndofs = lib().tb_num_dofs(h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().tb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- introspection --------------------------------------------------
+    def channel_info(self, ch):
+        n, p, d = C.c_int64(), C.c_int64(), C.c_int64()
+        lay = C.c_int32()
+        _check(lib().tb_channel_info(self.h, ch, C.byref(n), C.byref(p), C.byref(d), C.byref(lay)), "tb_channel_info")
+        return {"n_tuples": n.value, "n_prefilter": p.value, "n_det": d.value, "layout": LAYOUT_NAMES.get(lay.value)}
+
+    def tuples(self, ch):
+        info = self.channel_info(ch)
+        L = self.material.channels[ch].nlegs
+        ids = np.zeros((info["n_tuples"], L), dtype=np.int32)
+        umk = np.zeros(info["n_tuples"], dtype=np.int32)
+        _check(lib().tb_get_tuples(self.h, ch, ids.ctypes.data_as(C.POINTER(C.c_int32)),
+                                   umk.ctypes.data_as(C.POINTER(C.c_int32))), "tb_get_tuples")
+        return ids, umk
+
+    def set_amplitude(self, ch, a):
+        _check(lib().tb_set_amplitude(self.h, ch, float(a)), "tb_set_amplitude")
+
+    # -- host-pointer calls ----------------------------------------------
+    def rhs(self, f, drift=True, collisions=True):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        out = np.empty(self.ndofs)
+        flags = PTR_HOST | (0 if drift else NO_DRIFT) | (0 if collisions else NO_COLLISIONS)
+        _check(lib().tb_rhs(self.h, _hp(f), _hp(out), flags), "tb_rhs")
+        return out
+
+    def channel_propagate(self, ch, f):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        out = np.empty(self.ndofs)
+        _check(lib().tb_channel_propagate(self.h, ch, _hp(f), _hp(out), PTR_HOST), "tb_channel_propagate")
+        return out
+
+    def relative_error(self, err, pop):
+        err = np.ascontiguousarray(err, dtype=np.float64)
+        pop = np.ascontiguousarray(pop, dtype=np.float64)
+        r = C.c_double()
+        _check(lib().tb_relative_error(self.h, _hp(err), _hp(pop), C.byref(r), PTR_HOST), "tb_relative_error")
+        return r.value
+
+    def apply_constraints(self, f):
+        f = np.ascontiguousarray(f, dtype=np.float64).copy()
+        _check(lib().tb_apply_constraints(self.h, _hp(f), PTR_HOST), "tb_apply_constraints")
+        return f
+
+    def dp45(self, y0, t0, tf, dense, max_dense=None, drift=True):
+        y = np.ascontiguousarray(y0, dtype=np.float64).copy()
+        if max_dense is None:
+            max_dense = int(np.ceil((tf - t0) / dense)) + 2
+        dout = np.zeros((max(max_dense, 1), self.ndofs))
+        dt_ = np.zeros(max(max_dense, 1))
+        st = DP45Stats()
+        flags = PTR_HOST | (0 if drift else NO_DRIFT)
+        rc = lib().tb_dp45_integrate(self.h, _hp(y), t0, tf, dense, _hp(dout), _hp(dt_), max_dense, C.byref(st), flags)
+        n = min(st.n_dense, max_dense)
+        res = st.as_dict()
+        res.update({"rc": rc, "y": y, "dense": dout[:n], "dense_t": dt_[:n]})
+        return res
+
+    # -- device-pointer calls (torch tensors or raw addresses) --------------
+    def rhs_device(self, f_ptr, out_ptr, flags=0):
+        _check(lib().tb_rhs(self.h, C.c_void_p(f_ptr), C.c_void_p(out_ptr), flags), "tb_rhs")
+
+    def dp45_begin(self, y0, t0, tf, dense, max_dense=0, drift=True):
+        y0 = np.ascontiguousarray(y0, dtype=np.float64)
+        flags = PTR_HOST | (0 if drift else NO_DRIFT)
+        _check(lib().tb_dp45_begin(self.h, _hp(y0), t0, tf, dense, max_dense, flags), "tb_dp45_begin")
+
+    def dp45_advance(self, n):
+        _check(lib().tb_dp45_advance(self.h, int(n)), "tb_dp45_advance")
+
+    def dp45_poll(self):
+        st = DP45Stats()
+        _check(lib().tb_dp45_poll(self.h, C.byref(st)), "tb_dp45_poll")
+        return st.as_dict()
+
+    def stream_ptr(self):
+        return lib().tb_get_stream(self.h)
+
+    def collision_accumulate(self, f_ptr, acc_ptr, ch=-1):
+        _check(lib().tb_collision_accumulate(self.h, ch, C.c_void_p(f_ptr), C.c_void_p(acc_ptr)),
+               "tb_collision_accumulate")
+
+    def synchronize(self):
+        _check(lib().tb_synchronize(self.h), "tb_synchronize")

@@ -1,0 +1,367 @@
+"""Host-side model objects shaped like the reference's public API.
+
+Region, Mesh, Band, ScatteringChannel, Material, MaterialStatus and
+MaterialTimeStatus keep the reference's names and argument meaning
+(include/Geometry/Structured/DirectSpace/Region.hpp, Mesh.hpp,
+include/Physics/Material/Band.hpp, Material.hpp,
+include/Physics/Scattering/ScatteringChannel.hpp,
+include/Physics/Status/MaterialStatus.hpp, MaterialTimeStatus.hpp).  They
+hold geometry and parameters only; every propagation goes through the CUDA
+library bound in ``tortoise_b200.engine``.
+"""
+import numpy as np
+
+from .abi import BOSON, FERMION, IN, OUT, PackedProblem
+
+__all__ = ["Region", "Mesh", "Band", "ScatteringChannel", "Material", "MaterialStatus",
+           "MaterialTimeStatus", "IN", "OUT", "FERMION", "BOSON", "match_string",
+           "random_points_reference"]
+
+# Section-relative vertices of the two elements of a section
+# (src/Geometry/Structured/DirectSpace/Mesh.cpp:48-84).
+_VERT = np.array([[[0, 0], [1, 0], [1, 1]], [[0, 0], [0, 1], [1, 1]]], dtype=np.float64)
+
+
+def match_string(pattern, candidate):
+    """'*' / '?' wildcard match of src/Generics/Utilities/StringUtilities.cpp:44-61."""
+    def rec(p, c):
+        if p == len(pattern):
+            return c == len(candidate)
+        if pattern[p] == "*":
+            for cc in range(c, len(candidate) + 1):
+                if rec(p + 1, cc):
+                    return True
+            return False
+        if c == len(candidate) or (pattern[p] != "?" and pattern[p] != candidate[c]):
+            return False
+        return rec(p + 1, c + 1)
+    return rec(0, 0)
+
+
+def random_points_reference(rng, ndim, n):
+    """Uniform points in the reference simplex by the cut-and-fold of
+    include/Geometry/GeometryCore/Point.hpp:44-68, drawn from a seeded numpy
+    generator instead of the reference's unseeded Eigen::Random."""
+    pts = rng.random((n, ndim))
+    if ndim == 2:
+        fold = pts[:, 0] + pts[:, 1] > 1.0
+        pts[fold] = 1.0 - pts[fold]
+    return pts
+
+
+class Region:
+    """Region<2>: origin plus two side vectors (the columns of gvec)."""
+
+    def __init__(self, origin, sides):
+        self.origin = np.asarray(origin, dtype=np.float64).reshape(2)
+        s = np.asarray(sides, dtype=np.float64).reshape(2, 2)
+        self.gvec = s.T.copy()  # columns are the sides
+
+
+class Mesh:
+    """Mesh<2>(region, relativeOrigin, relativeSize, nSecSplits)
+    (src/Geometry/Structured/DirectSpace/Mesh.cpp:319-347)."""
+
+    def __init__(self, region, rel_origin, rel_size, nsplit):
+        self.region = region
+        self.rel_origin = np.asarray(rel_origin, dtype=np.float64).reshape(2)
+        self.rel_size = np.asarray(rel_size, dtype=np.float64).reshape(2)
+        self.nsplit = (int(nsplit[0]), int(nsplit[1]))
+        G = region.gvec
+        self.origin = region.origin + (G[:, 0] * self.rel_origin[0] + G[:, 1] * self.rel_origin[1])
+        gv = G * self.rel_size[None, :]
+        self.dG = gv * (1.0 / np.array(self.nsplit, dtype=np.float64))[None, :]
+        self.numberElements = 2 * self.nsplit[0] * self.nsplit[1]
+        self.elemVolume = abs((self.dG[0, 0] * self.dG[1, 1] - self.dG[0, 1] * self.dG[1, 0]) / 2.0)
+
+    @property
+    def ne(self):
+        return self.numberElements
+
+    def vertices(self):
+        """(Ne, 3, 2) absolute vertex coordinates (Mesh.cpp:488-494)."""
+        e = np.arange(self.ne)
+        s, par = e // 2, e % 2
+        sx = (s % self.nsplit[0]).astype(np.float64)
+        sy = (s // self.nsplit[0]).astype(np.float64)
+        px = sx[:, None] + _VERT[par][:, :, 0]
+        py = sy[:, None] + _VERT[par][:, :, 1]
+        x = self.origin[0] + (self.dG[0, 0] * px + self.dG[0, 1] * py)
+        y = self.origin[1] + (self.dG[1, 0] * px + self.dG[1, 1] * py)
+        return np.stack([x, y], axis=-1)
+
+    def function(self, fn):
+        """Function<2>(mesh, lambda): nodal samples -> linear-form coefficients
+        (src/Geometry/Structured/FunctionSpace/Function.cpp:60-68).
+        ``fn(kx, ky)`` is evaluated on arrays; scalars give constant functions."""
+        v = self.vertices()
+        if callable(fn):
+            nodal = np.asarray(fn(v[..., 0], v[..., 1]), dtype=np.float64)
+            nodal = np.broadcast_to(nodal, (self.ne, 3)).copy()
+        else:
+            nodal = np.full((self.ne, 3), float(fn))
+        return nodal_to_linform(nodal)
+
+
+def nodal_to_linform(nodal):
+    nodal = np.asarray(nodal, dtype=np.float64).reshape(-1, 3)
+    out = nodal.copy()
+    out[:, 1] = nodal[:, 1] - nodal[:, 0]
+    out[:, 2] = nodal[:, 2] - nodal[:, 0]
+    return out.reshape(-1)
+
+
+def linform_to_nodal(lin):
+    lin = np.asarray(lin, dtype=np.float64).reshape(-1, 3)
+    out = lin.copy()
+    out[:, 1] = lin[:, 1] + lin[:, 0]
+    out[:, 2] = lin[:, 2] + lin[:, 0]
+    return out
+
+
+class Band:
+    """Band<2> (include/Physics/Material/Band.hpp:49-113)."""
+
+    def __init__(self, name, charge, statistics, mesh, dispersion):
+        self.name = name
+        self.charge = float(charge)
+        self.statistics = float(statistics)
+        self.mesh = mesh
+        self.dispersion_coeffs = mesh.function(dispersion)
+        self.absoluteErrorTolerance = 1.0e-3
+        self.relativeErrorTolerance = 1.0e-3
+        self.penalisationUnphysicalPopulation = 0.0
+        self.constrained = False
+        self.constrainedPopulation = None
+        self.drift_velocity = (0.0, 0.0)
+
+    def constrain(self, population_coeffs):
+        """Band::constrained with a time-independent constrainedPopulation."""
+        self.constrained = True
+        self.constrainedPopulation = np.ascontiguousarray(population_coeffs, dtype=np.float64)
+
+
+class ScatteringChannel:
+    """ScatteringChannel<2,L> parameters (ScatteringChannel.hpp:54-102).  The
+    Monte-Carlo table is an explicit seeded input (the reference redraws it
+    from std::rand at every propagation, MaterialTimeStatus.cpp:104)."""
+
+    def __init__(self, material, band_numbers, directions, mc_seed):
+        self.material = material
+        self.nlegs = len(band_numbers)
+        self.legBandNumber = [int(b) for b in band_numbers]
+        self.legDirection = [int(d) for d in directions]
+        self.amplitude = 1.0
+        self.numMCPoints = material.defaultNMCPointsScatterings
+        self.minimumDeterminant = material.defaultMinimumDeterminantScatterings
+        self.scattElemeThreshold = material.defaultScattElemeThresholdScatterings
+        self.umklappUnitVectors = np.zeros((1, 2))
+        self.mc_seed = int(mc_seed)
+        self.tuples = None
+        self.tuple_umklapp = None
+        self.constructMCPoints()
+
+    def scatteringName(self):
+        m = self.material
+        ins = "".join("(" + m.band_names[b] + ")" for b, d in zip(self.legBandNumber, self.legDirection) if d > 0)
+        outs = "".join("(" + m.band_names[b] + ")" for b, d in zip(self.legBandNumber, self.legDirection) if d < 0)
+        return "[" + ins + "]-[" + outs + "]"
+
+    def findUmklappVectors(self, n):
+        """All (2n+1)^2 test vectors are kept (ScatteringChannel.cpp:194-215)."""
+        r = range(-n, n + 1)
+        self.umklappUnitVectors = np.array([[i, j] for i in r for j in r], dtype=np.float64)
+        return len(self.umklappUnitVectors) != 0
+
+    def constructMCPoints(self, seed=None):
+        """Rows: (L-2) reference-triangle points then one [0,1] coordinate
+        (ScatteringChannel.cpp:677-688); a second independent table stands in
+        for the per-tuple draws of the survival test (IntegratorCore.hpp:382-388)."""
+        if seed is not None:
+            self.mc_seed = int(seed)
+        L, n = self.nlegs, self.numMCPoints
+        for which, off in (("mc_points", 0), ("mc_points_precalc", 1)):
+            rng = np.random.default_rng([self.mc_seed, off])
+            cols = [random_points_reference(rng, 2, n) for _ in range(L - 2)]
+            cols.append(random_points_reference(rng, 1, n))
+            setattr(self, which, np.ascontiguousarray(np.concatenate(cols, axis=1)))
+
+
+class Material:
+    """Material<2> (include/Physics/Material/Material.hpp:58-188)."""
+
+    def __init__(self, matID, region):
+        self.matID = matID
+        self.region = region
+        self.bands = []
+        self.band_names = []
+        self.channels = []
+        self.defaultNMCPointsScatterings = 50
+        self.defaultMinimumDeterminantScatterings = 1.0e-9
+        self.defaultScattElemeThresholdScatterings = 1.0e-9
+        self._mc_seed_base = 0x5EED
+        self._engine = None
+
+    # -- bands -----------------------------------------------------------
+    def addBand(self, t_id, t_charge, t_statistics, t_mesh, t_dispersion):
+        assert t_mesh.region is self.region
+        b = Band(t_id, t_charge, t_statistics, t_mesh, t_dispersion)
+        self.bands.append(b)
+        self.band_names.append(t_id)
+        self._engine = None
+        return b
+
+    def __getitem__(self, name):
+        return self.bands[self.id(name)]
+
+    def id(self, name):
+        return self.band_names.index(name)
+
+    def matchListId(self, wildcard):
+        return [n for n in self.band_names if match_string(wildcard, n)]
+
+    @property
+    def meshes(self):
+        out = []
+        for b in self.bands:
+            if all(m is not b.mesh for m in out):
+                out.append(b.mesh)
+        return out
+
+    # -- channels --------------------------------------------------------
+    def addScatteringChannel(self, band_names, directions):
+        c = ScatteringChannel(self, [self.id(n) for n in band_names], directions,
+                              self._mc_seed_base + len(self.channels))
+        self.channels.append(c)
+        self._engine = None
+        return c
+
+    def addScatteringChannelsWildcards(self, band_names, directions, numUmklappSteps):
+        """Band combinations with exchange / time-reversal deduplication
+        (src/Physics/Material/Material.cpp:209-364).  Channels whose tuple list
+        turns out empty contribute nothing (the reference pops them)."""
+        L = len(band_names)
+        lists = [self.matchListId(w) for w in band_names]
+        added = []
+
+        def groups(names, dirs):
+            gi = sorted(n for n, d in zip(names, dirs) if d == IN)
+            go = sorted(n for n, d in zip(names, dirs) if d != IN)
+            return gi, go
+
+        import itertools
+        for combo in itertools.product(*lists):
+            if L == 2:
+                found = False
+                for c in self.channels:
+                    if c.nlegs != 2:
+                        continue
+                    have = sorted(self.band_names[b] for b in c.legBandNumber)
+                    if have == sorted(combo) and directions[0] * directions[1] == c.legDirection[0] * c.legDirection[1]:
+                        found = True
+                        break
+            else:
+                gi, go = groups(combo, directions)
+                found = False
+                for c in self.channels:
+                    if c.nlegs != L:
+                        continue
+                    ci, co = groups([self.band_names[b] for b in c.legBandNumber], c.legDirection)
+                    if (len(gi) == len(ci) and gi == ci and go == co) or (len(gi) == len(co) and gi == co and go == ci):
+                        found = True
+                        break
+            if found:
+                continue
+            c = self.addScatteringChannel(list(combo), directions)
+            c.findUmklappVectors(numUmklappSteps)
+            added.append(c)
+        return added
+
+    # -- packing ---------------------------------------------------------
+    def pack(self):
+        return PackedProblem(self.region, self.meshes, self.bands, self.channels)
+
+    def band_offsets(self):
+        off, out = 0, []
+        for b in self.bands:
+            out.append(off)
+            off += b.mesh.ne * 3
+        return out, off
+
+    def engine(self, **opts):
+        """The CUDA handle for this material (built on first use)."""
+        from .engine import Engine
+        if self._engine is None or opts:
+            self._engine = Engine(self, **opts)
+        return self._engine
+
+
+class MaterialStatus:
+    """MaterialStatus<2>: the concatenated band populations
+    (include/Physics/Status/MaterialStatus.hpp:46-140)."""
+
+    def __init__(self, material, vec=None):
+        self.material = material
+        self.offsets, self.ndofs = material.band_offsets()
+        self.vec = np.zeros(self.ndofs) if vec is None else np.ascontiguousarray(vec, dtype=np.float64).copy()
+
+    def __getitem__(self, name):
+        b = self.material.id(name)
+        o = self.offsets[b]
+        return self.vec[o:o + self.material.bands[b].mesh.ne * 3]
+
+    def __setitem__(self, name, coeffs):
+        self[name][:] = coeffs
+
+    def copy(self):
+        return MaterialStatus(self.material, self.vec)
+
+    def setToEquilibrium(self, temperature, chemicalPotentialFermions, chemicalPotentialBosons):
+        """MaterialStatus.cpp:212-220: Fermi-Dirac / Bose-Einstein of the
+        dispersion, evaluated nodally (Function.cpp:75-89)."""
+        for b in self.material.bands:
+            e = linform_to_nodal(b.dispersion_coeffs)
+            if b.statistics == FERMION:
+                nod = 1.0 / (np.exp((e - chemicalPotentialFermions) / temperature) + 1.0)
+            else:
+                nod = 1.0 / (np.exp((e - chemicalPotentialBosons) / temperature) - 1.0)
+            self[b.name] = nodal_to_linform(nod)
+
+    def propagate(self):
+        """MaterialStatus::propagate (MaterialStatus.cpp:146-161) on the GPU,
+        plus the drift term of bands with a nonzero drift velocity."""
+        return MaterialStatus(self.material, self.material.engine().rhs(self.vec))
+
+    def relativeError(self, population):
+        return self.material.engine().relative_error(self.vec, population.vec)
+
+
+class MaterialTimeStatus:
+    """MaterialTimeStatus<2>: dense-output trajectory
+    (include/Physics/Status/MaterialTimeStatus.hpp)."""
+
+    def __init__(self, status, time0=0.0):
+        self.material = status.material
+        self.times = [float(time0)]
+        self.statuses = [status.copy()]
+        self.stats = None
+
+    def __len__(self):
+        return len(self.times)
+
+    def __getitem__(self, i):
+        return self.statuses[i]
+
+    def back(self):
+        return self.statuses[-1]
+
+    def propagate(self, finalTime, denseStep, max_dense=None):
+        """DP5(4) from the last stored time to finalTime
+        (MaterialTimeStatus.cpp:102-137), integrated entirely on the GPU."""
+        eng = self.material.engine()
+        res = eng.dp45(self.statuses[-1].vec, self.times[-1], finalTime, denseStep, max_dense=max_dense)
+        for t, v in zip(res["dense_t"], res["dense"]):
+            self.times.append(float(t))
+            self.statuses.append(MaterialStatus(self.material, v))
+        self.stats = res
+        return res
