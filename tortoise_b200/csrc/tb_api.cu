@@ -710,6 +710,9 @@ int tb_dp45_poll(tb_handle* h, tb_dp45_stats* st) {
     TB_CUDA(cudaMemcpyAsync(h->h_ctl, h->dp.ctl, sizeof(DPCtl), cudaMemcpyDeviceToHost, h->stream));
     TB_CUDA(cudaStreamSynchronize(h->stream));
     fill_stats(*h->h_ctl, st);
+    int tflag = 0;
+    TB_TRY(tensor_error_flag(&tflag));
+    if (tflag && st) { st->status = TB_ERR_TIMEOUT; st->done = 1; }
     return TB_OK;
 }
 

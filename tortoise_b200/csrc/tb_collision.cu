@@ -38,13 +38,32 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, double amp_full
         if (fabs(g.det) < c.min_det) continue;
         double Ci[3][3];
         dc_inverse<L>(g, Ci);
-        // alpha = -Ci (DF q - N) = G q + alpha0
-        double G[3][R], a0[3];
+        // alpha = -Ci (DF q - N) = G q + alpha0 (fast path, FMA).  The
+        // simplex tests must agree with the unfused reference evaluation,
+        // so every point whose fast alpha lies within a rigorous rounding
+        // bound of a test boundary is re-evaluated in the exact order.
+        double G[3][R], a0[3], mg[3];
+        {
+            double rho[3];
 #pragma unroll
-        for (int r = 0; r < 3; ++r) {
-            a0[r] = Ci[r][0] * g.N[0] + Ci[r][1] * g.N[1] + Ci[r][2] * g.N[2];
+            for (int k = 0; k < 3; ++k) {
+                double t = fabs(g.N[k]);
 #pragma unroll
-            for (int j = 0; j < R; ++j) G[r][j] = -(Ci[r][0] * g.D[0][j] + Ci[r][1] * g.D[1][j] + Ci[r][2] * g.D[2][j]);
+                for (int j = 0; j < R; ++j) t += fabs(g.D[k][j]);
+                rho[k] = t;
+            }
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                a0[r] = Ci[r][0] * g.N[0] + Ci[r][1] * g.N[1] + Ci[r][2] * g.N[2];
+                double sg = 0.0;
+#pragma unroll
+                for (int j = 0; j < R; ++j) {
+                    G[r][j] = -(Ci[r][0] * g.D[0][j] + Ci[r][1] * g.D[1][j] + Ci[r][2] * g.D[2][j]);
+                    sg += fabs(G[r][j]);
+                }
+                const double sc = fabs(Ci[r][0]) * rho[0] + fabs(Ci[r][1]) * rho[1] + fabs(Ci[r][2]) * rho[2];
+                mg[r] = 32.0 * 1.1102230246251565e-16 * (sc + fabs(a0[r]) + sg);
+            }
         }
         // commonLinForm0 (A, direct) and commonLinForm1 (B, time reversed),
         // ScatteringChannel.cpp:633-641
@@ -81,8 +100,12 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, double amp_full
                 al[r] = t;
             }
             const double kp0 = qv[R - 1];
-            const bool thp = (kp0 > 0.0) && (al[0] > 0.0) && (kp0 + al[0] < 1.0);
-            const bool thc = (al[1] > 0.0) && (al[2] > 0.0) && (al[1] + al[2] < 1.0);
+            const double tiny = 8.0 * 1.1102230246251565e-16;
+            const bool near = (fabs(al[0]) <= mg[0]) || (fabs(al[1]) <= mg[1]) || (fabs(al[2]) <= mg[2]) ||
+                              (fabs(kp0 + al[0] - 1.0) <= mg[0] + tiny * (2.0 + fabs(al[0]))) ||
+                              (fabs(al[1] + al[2] - 1.0) <= mg[1] + mg[2] + tiny * (1.0 + fabs(al[1]) + fabs(al[2])));
+            if (near) exact_alpha<L>(g, Ci, qv, al);
+            const bool th = theta_of(kp0, al);
             double px[L], py[L];
 #pragma unroll
             for (int l = 0; l < L - 2; ++l) { px[l] = qv[2 * l]; py[l] = qv[2 * l + 1]; }
@@ -94,7 +117,7 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, double amp_full
                 pa *= (A[l][1] * px[l] + A[l][2] * py[l]) + A[l][0];
                 pb *= (B[l][1] * px[l] + B[l][2] * py[l]) + B[l][0];
             }
-            const double common = (thp && thc) ? (pa + pb) : 0.0 * (pa + pb);
+            const double common = (pa + pb) * (th ? 1.0 : 0.0);
             s0 += common;
 #pragma unroll
             for (int l = 0; l < L; ++l) {

@@ -13,6 +13,14 @@
 
 namespace tb {
 
+// Explicitly rounded FP64 operations: never contracted into FMAs, so these
+// expressions round exactly like the unfused C++ of the reference (and the
+// oracle) whatever --fmad says.  Every quantity that feeds a discrete
+// decision (determinant filter, simplex tests Theta) is computed with them.
+__device__ __forceinline__ double xm(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xa(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xs(double a, double b) { return __dsub_rn(a, b); }
+
 template <int L>
 struct TupleGeom {
     double D[3][2 * L];
@@ -39,21 +47,22 @@ __device__ __forceinline__ void tuple_geometry(const ChanDev& c, const int (&e)[
 #pragma unroll
     for (int l = 0; l < L; ++l) {
         const double d = c.leg[l].dir;
-        g.N[0] -= d * __ldg(c.leg[l].kx + 3 * (int64_t)e[l]);
-        g.N[1] -= d * __ldg(c.leg[l].ky + 3 * (int64_t)e[l]);
-        g.N[2] -= d * __ldg(c.leg[l].disp + 3 * (int64_t)e[l]);
+        g.N[0] = xs(g.N[0], xm(d, __ldg(c.leg[l].kx + 3 * (int64_t)e[l])));
+        g.N[1] = xs(g.N[1], xm(d, __ldg(c.leg[l].ky + 3 * (int64_t)e[l])));
+        g.N[2] = xs(g.N[2], xm(d, __ldg(c.leg[l].disp + 3 * (int64_t)e[l])));
     }
     const double u0 = c.umk[2 * umk], u1 = c.umk[2 * umk + 1];
 #pragma unroll
     for (int dim = 0; dim < 2; ++dim) {
-        g.N[dim] -= u0 * c.gvec[dim];
-        g.N[dim] -= u1 * c.gvec[2 + dim];
+        g.N[dim] = xs(g.N[dim], xm(u0, c.gvec[dim]));
+        g.N[dim] = xs(g.N[dim], xm(u1, c.gvec[2 + dim]));
     }
     const int c0 = 2 * L - 3;
     const double a00 = g.D[0][c0], a01 = g.D[0][c0 + 1], a02 = g.D[0][c0 + 2];
     const double a10 = g.D[1][c0], a11 = g.D[1][c0 + 1], a12 = g.D[1][c0 + 2];
     const double a20 = g.D[2][c0], a21 = g.D[2][c0 + 1], a22 = g.D[2][c0 + 2];
-    g.det = a00 * (a11 * a22 - a12 * a21) - a01 * (a10 * a22 - a12 * a20) + a02 * (a10 * a21 - a11 * a20);
+    g.det = xa(xs(xm(a00, xs(xm(a11, a22), xm(a12, a21))), xm(a01, xs(xm(a10, a22), xm(a12, a20)))),
+               xm(a02, xs(xm(a10, a21), xm(a11, a20))));
 }
 
 // Inverse of DC by cofactors scaled with the reciprocal of the column-0
@@ -72,14 +81,41 @@ __device__ __forceinline__ void dc_inverse(const TupleGeom<L>& g, double Ci[3][3
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             const int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
-            cof[i][j] = a[i1][j1] * a[i2][j2] - a[i1][j2] * a[i2][j1];
+            cof[i][j] = xs(xm(a[i1][j1], a[i2][j2]), xm(a[i1][j2], a[i2][j1]));
         }
-    const double det = (cof[0][0] * a[0][0] + cof[1][0] * a[1][0]) + cof[2][0] * a[2][0];
-    const double invdet = 1.0 / det;
+    const double det = xa(xa(xm(cof[0][0], a[0][0]), xm(cof[1][0], a[1][0])), xm(cof[2][0], a[2][0]));
+    const double invdet = __ddiv_rn(1.0, det);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) Ci[j][i] = cof[i][j] * invdet;
+        for (int j = 0; j < 3; ++j) Ci[j][i] = xm(cof[i][j], invdet);
+}
+
+// alpha = -DC^-1 (DF q - N) in the reference's evaluation order, unfused.
+template <int L>
+__device__ __forceinline__ void exact_alpha(const TupleGeom<L>& g, const double (&Ci)[3][3], const double* q,
+                                            double (&alpha)[3]) {
+    constexpr int R = 2 * (L - 2) + 1;
+    const double kp0 = q[R - 1];
+    double r[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        double s = 0.0;
+        if (L >= 3) s = xa(s, xa(xm(g.D[i][0], q[0]), xm(g.D[i][1], q[1])));
+        if (L >= 4) s = xa(s, xa(xm(g.D[i][2], q[2]), xm(g.D[i][3], q[3])));
+        s = xa(s, xm(g.D[i][2 * (L - 2)], kp0));
+        r[i] = xs(s, g.N[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) alpha[i] = -xa(xa(xm(Ci[i][0], r[0]), xm(Ci[i][1], r[1])), xm(Ci[i][2], r[2]));
+}
+
+// ThetapC * ThetaFC (IntegratorCore.hpp:318-320): both partially and fully
+// constrained legs strictly inside the reference triangle.
+__device__ __forceinline__ bool theta_of(double kp0, const double (&al)[3]) {
+    const bool thp = (kp0 > 0.0) && (al[0] > 0.0) && (xa(kp0, al[0]) < 1.0);
+    const bool thc = (al[1] > 0.0) && (al[2] > 0.0) && (xa(al[1], al[2]) < 1.0);
+    return thp && thc;
 }
 
 // Constrained coordinates of one MC point q (row of the MC table),
@@ -91,27 +127,15 @@ __device__ __forceinline__ bool mc_point_exact(const TupleGeom<L>& g, const doub
                                                double (&p)[L][2]) {
     constexpr int R = 2 * (L - 2) + 1;
     const double kp0 = q[R - 1];
-    double r[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        double s = 0.0;
-        if (L >= 3) s += g.D[i][0] * q[0] + g.D[i][1] * q[1];
-        if (L >= 4) s += g.D[i][2] * q[2] + g.D[i][3] * q[3];
-        s += g.D[i][2 * (L - 2)] * kp0;
-        r[i] = s - g.N[i];
-    }
     double alpha[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) alpha[i] = -(Ci[i][0] * r[0] + Ci[i][1] * r[1] + Ci[i][2] * r[2]);
+    exact_alpha<L>(g, Ci, q, alpha);
 #pragma unroll
     for (int l = 0; l < L - 2; ++l) { p[l][0] = q[2 * l]; p[l][1] = q[2 * l + 1]; }
     p[L - 2][0] = kp0;
     p[L - 2][1] = alpha[0];
     p[L - 1][0] = alpha[1];
     p[L - 1][1] = alpha[2];
-    const bool thp = (kp0 > 0.0) && (alpha[0] > 0.0) && (kp0 + alpha[0] < 1.0);
-    const bool thc = (alpha[1] > 0.0) && (alpha[2] > 0.0) && (alpha[1] + alpha[2] < 1.0);
-    return thp && thc;
+    return theta_of(kp0, alpha);
 }
 
 }  // namespace tb

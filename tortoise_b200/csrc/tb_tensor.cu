@@ -1,19 +1,412 @@
-// tb_tensor.cu -- placeholder until the moment-tensor layout lands.
+// tb_tensor.cu -- the collision operator as a precomputed sparse tensor.
+//
+// The reference declares a precomputed scattering matrix (scatteringMatrix,
+// precalculate(), propagatePrecalculatedSingle in include/Physics/Scattering/
+// ScatteringChannel.hpp:90,129,176) but never implements it; every RHS
+// evaluation re-runs the Monte-Carlo quadrature of scatteringIntegrationTypeB
+// (IntegratorCore.hpp:260-357).  Because each leg's gain/loss factor is an
+// affine function of its element's 3 P1 coefficients, the quadrature factors
+// exactly into f-independent moments of the delta-constrained MC points:
+//
+//   result[lam][beta] = amp * sum_J W[lam,beta][J] * (prod_l a_{l,J_l} + prod_l b_{l,J_l})
+//   W[lam,beta][J]    = norm * sum_m Theta_m phi_beta(p_lam,m) prod_l phi_{J_l}(p_l,m)
+//
+// with phi = (1, x, y) on the reference triangle.  Only 3^L (1+L) of the
+// 3L*3^L entries of W are distinct:
+//   S0[J]            (beta = 0, identical for every lam)           3^L
+//   Q_lam[t][J_-lam] (t = xx, xy, yy: the degree-2 monomial of leg lam)   3L * 3^(L-1)
+// which is 108 numbers per 3-leg tuple and 405 per 4-leg tuple.
+//
+// Storage is tile-major: a tile of TT tuples is one contiguous block
+// [nmom][TT], so the contraction kernel streams whole tiles into shared memory
+// with one 1-D bulk TMA copy (cp.async.bulk + mbarrier, double buffered) and
+// each thread reads its tuple's moments bank-conflict free.  FP32 storage
+// halves the bytes; products and accumulation stay FP64, and the
+// gain-minus-loss vector v = ka + kb is formed in FP64 from f.
+#include "tb_geom.cuh"
 #include "tb_tensor.cuh"
 
 namespace tb {
+
+template <int L> struct TDim {
+    static constexpr int K = (L == 2) ? 9 : (L == 3) ? 27 : 81;     // 3^L
+    static constexpr int KM = K / 3;                                // 3^(L-1)
+    static constexpr int NMOM = K * (1 + L);
+};
+
+template <int L, bool F32> struct TTile {
+    // tuples per tile: keeps one stage at <= ~56 KB of shared memory
+    static constexpr int TT = (L == 4) ? 32 : (F32 ? 128 : 64);
+};
+
+static int tile_tuples(int L, bool fp32) {
+    if (L == 4) return 32;
+    return fp32 ? 128 : 64;
+}
+
+static int nmom_of(int L) { return (L == 2 ? 9 : L == 3 ? 27 : 81) * (1 + L); }
+
+int64_t tensor_bytes(int L, bool fp32, int64_t n) {
+    const int64_t TT = tile_tuples(L, fp32);
+    const int64_t ntiles = (n + TT - 1) / TT;
+    return ntiles * TT * nmom_of(L) * (fp32 ? 4 : 8);
+}
+
 void MomentTensor::release() {
     if (d) cudaFree(d);
     d = nullptr;
+    n = ntiles = 0;
 }
-int64_t tensor_bytes(int L, bool fp32, int64_t n) { return INT64_MAX; }
-int build_tensor(const ChanDev&, const int32_t*, int64_t, int64_t, bool, MomentTensor&, cudaStream_t) {
-    set_error("moment tensor layout not available");
+
+// ------------------------------------------------------------ precompute
+// One warp per tuple; every lane recomputes the MC point (cheap) and owns a
+// strided subset of the moments.
+template <int L, typename T>
+__global__ void __launch_bounds__(256) k_build_moments(ChanDev c, const int32_t* __restrict__ tup, int64_t stride,
+                                                       int64_t n, T* __restrict__ out, int TT) {
+    extern __shared__ double s_mc[];
+    constexpr int R = 2 * (L - 2) + 1;
+    constexpr int K = TDim<L>::K, KM = TDim<L>::KM, NMOM = TDim<L>::NMOM;
+    constexpr int PER = (NMOM + 31) / 32;
+    for (int i = threadIdx.x; i < c.nmc * R; i += blockDim.x) s_mc[i] = c.mc[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    // decode the owned moments: factor selector per leg (0:1, 1:x, 2:y, 3:xx, 4:xy, 5:yy)
+    int sel[PER][L];
+    bool own[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int k = lane + 32 * q;
+        own[q] = k < NMOM;
+        int J[L];
+        if (k < K) {
+            int r = k;
+#pragma unroll
+            for (int l = L - 1; l >= 0; --l) { J[l] = r % 3; r /= 3; }
+#pragma unroll
+            for (int l = 0; l < L; ++l) sel[q][l] = J[l];
+        } else {
+            const int kk = own[q] ? k - K : 0;
+            const int lam = kk / (3 * KM);
+            const int rr = kk % (3 * KM);
+            const int t = rr / KM;
+            int jm = rr % KM;
+#pragma unroll
+            for (int l = L - 1; l >= 0; --l) {
+                if (l == lam) continue;
+                sel[q][l] = jm % 3;
+                jm /= 3;
+            }
+#pragma unroll
+            for (int l = 0; l < L; ++l)
+                if (l == lam) sel[q][l] = 3 + t;
+        }
+    }
+    for (int64_t i = warp; i < n; i += nwarps) {
+        int e[L];
+#pragma unroll
+        for (int l = 0; l < L; ++l) e[l] = __ldg(tup + l * stride + i);
+        const int u = __ldg(tup + L * stride + i);
+        TupleGeom<L> g;
+        tuple_geometry<L>(c, e, u, g);
+        double acc[PER];
+#pragma unroll
+        for (int q = 0; q < PER; ++q) acc[q] = 0.0;
+        double norm = 0.0;
+        if (fabs(g.det) >= c.min_det) {
+            double Ci[3][3];
+            dc_inverse<L>(g, Ci);
+            for (int m = 0; m < c.nmc; ++m) {
+                double qv[R];
+#pragma unroll
+                for (int j = 0; j < R; ++j) qv[j] = s_mc[m * R + j];
+                // exact (unfused) evaluation: Theta decisions identical to the reference order
+                double al[3];
+                exact_alpha<L>(g, Ci, qv, al);
+                const double kp0 = qv[R - 1];
+                if (!theta_of(kp0, al)) continue;   // warp-uniform: every lane evaluates the same point
+                double px[L], py[L];
+#pragma unroll
+                for (int l = 0; l < L - 2; ++l) { px[l] = qv[2 * l]; py[l] = qv[2 * l + 1]; }
+                px[L - 2] = kp0; py[L - 2] = al[0];
+                px[L - 1] = al[1]; py[L - 1] = al[2];
+#pragma unroll
+                for (int q = 0; q < PER; ++q) {
+                    double v = 1.0;
+#pragma unroll
+                    for (int l = 0; l < L; ++l) {
+                        const int s = sel[q][l];
+                        const double f = (s == 0) ? 1.0 : (s == 1) ? px[l] : (s == 2) ? py[l]
+                                       : (s == 3) ? px[l] * px[l] : (s == 4) ? px[l] * py[l] : py[l] * py[l];
+                        v *= f;
+                    }
+                    acc[q] += v;
+                }
+            }
+            norm = c.amp_vol / (c.fact * double(c.nmc) * fabs(g.det));
+        }
+        const int64_t tile = i / TT, pos = i % TT;
+        T* base = out + tile * (int64_t)NMOM * TT + pos;
+#pragma unroll
+        for (int q = 0; q < PER; ++q)
+            if (own[q]) base[(int64_t)(lane + 32 * q) * TT] = T(acc[q] * norm);
+    }
+}
+
+// ------------------------------------------------------------ contraction
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx_arrive(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Bounded wait on an mbarrier phase; returns false when the spin limit is
+// reached (the caller records an error and abandons the tile).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int limit = (1 << 22)) {
+    for (int it = 0; it < limit; ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+template <int L, typename T, int TT, int STAGES>
+__global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, double amplitude, const T* __restrict__ mom,
+                                                         int64_t ntiles, const int32_t* __restrict__ tup,
+                                                         int64_t stride, int64_t n, const double* __restrict__ f,
+                                                         double* __restrict__ acc, const int* __restrict__ done,
+                                                         int* __restrict__ err_flag) {
+    constexpr int K = TDim<L>::K, KM = TDim<L>::KM, NMOM = TDim<L>::NMOM;
+    constexpr uint32_t TILE_BYTES = uint32_t(NMOM) * TT * sizeof(T);
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    T* stage_buf = reinterpret_cast<T*>(smem_raw);
+    __shared__ __align__(8) uint64_t bars[STAGES];
+    if (done && *done) return;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            const int64_t tile = blockIdx.x + (int64_t)s * gridDim.x;
+            if (tile < ntiles) {
+                mbar_expect_tx_arrive(&bars[s], TILE_BYTES);
+                bulk_g2s(stage_buf + (size_t)s * NMOM * TT, mom + tile * (int64_t)NMOM * TT, TILE_BYTES, &bars[s]);
+            }
+        }
+    }
+    for (int64_t it = 0;; ++it) {
+        const int64_t tile = blockIdx.x + it * gridDim.x;
+        if (tile >= ntiles) break;
+        const int s = int(it % STAGES);
+        const uint32_t parity = uint32_t((it / STAGES) & 1);
+        if (!mbar_wait(&bars[s], parity)) {
+            // record the failure, then give every copy still in flight a
+            // bounded chance to land before the CTA releases its shared memory
+            if (tid == 0) atomicExch(err_flag, 1);
+            for (int k = 0; k < STAGES; ++k) {
+                const int64_t itk = it + ((k - s + STAGES) % STAGES);
+                if (blockIdx.x + itk * gridDim.x < ntiles) mbar_wait(&bars[k], uint32_t((itk / STAGES) & 1), 1 << 16);
+            }
+            return;
+        }
+        const T* sm = stage_buf + (size_t)s * NMOM * TT;
+        const int64_t i = tile * TT + tid;
+        if (i < n) {
+            int e[L];
+#pragma unroll
+            for (int l = 0; l < L; ++l) e[l] = __ldg(tup + l * stride + i);
+            // gain (B) / loss (A) forms, ScatteringChannel.cpp:633-641
+            double A[L][3], B[L][3];
+#pragma unroll
+            for (int l = 0; l < L; ++l) {
+                const double d = c.leg[l].dir, st = c.leg[l].stat;
+                const double* fe = f + c.leg[l].foff + 3 * (int64_t)e[l];
+                const double ka = (l == 0 ? -1.0 : 1.0) * 0.5;
+                const double ca = (1. - d) * st + (1. + d);
+                const double cb = (1. + d) * st + (1. - d);
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const double unit = (j == 0) ? 1.0 : 0.0;
+                    const double fj = __ldg(fe + j);
+                    A[l][j] = ka * ((1. - d) * unit + ca * fj);
+                    B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
+                }
+            }
+            // v = kron(A) + kron(B), leg 0 most significant
+            double v[K];
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                int r = j;
+                double pa = 1.0, pb = 1.0;
+#pragma unroll
+                for (int l = L - 1; l >= 0; --l) {
+                    const int Jl = r % 3;
+                    r /= 3;
+                    pa *= A[l][Jl];
+                    pb *= B[l][Jl];
+                }
+                v[j] = pa + pb;
+            }
+            double r0 = 0.0;
+#pragma unroll
+            for (int j = 0; j < K; ++j) r0 = fma(double(sm[j * TT + tid]), v[j], r0);
+#pragma unroll
+            for (int lam = 0; lam < L; ++lam) {
+                int sstep = 1;
+#pragma unroll
+                for (int l = L - 1; l > lam; --l) sstep *= 3;
+                double r1 = 0.0, r2 = 0.0;
+#pragma unroll
+                for (int km = 0; km < KM; ++km) {
+                    // J with J_lam = 0 whose other legs enumerate km in leg order
+                    int hi = km / sstep, lo = km % sstep;
+                    const int j0 = hi * 3 * sstep + lo;
+                    const int j1 = j0 + sstep, j2 = j0 + 2 * sstep;
+                    const double qxx = double(sm[(K + (lam * 3 + 0) * KM + km) * TT + tid]);
+                    const double qxy = double(sm[(K + (lam * 3 + 1) * KM + km) * TT + tid]);
+                    const double qyy = double(sm[(K + (lam * 3 + 2) * KM + km) * TT + tid]);
+                    const double s1 = double(sm[j1 * TT + tid]);
+                    const double s2 = double(sm[j2 * TT + tid]);
+                    r1 = fma(s1, v[j0], r1);
+                    r1 = fma(qxx, v[j1], r1);
+                    r1 = fma(qxy, v[j2], r1);
+                    r2 = fma(s2, v[j0], r2);
+                    r2 = fma(qxy, v[j1], r2);
+                    r2 = fma(qyy, v[j2], r2);
+                }
+                const double d = c.leg[lam].dir;
+                double* o = acc + c.leg[lam].foff + 3 * (int64_t)e[lam];
+                atomicAdd(o + 0, d * (r0 * amplitude));
+                atomicAdd(o + 1, d * (r1 * amplitude));
+                atomicAdd(o + 2, d * (r2 * amplitude));
+            }
+        }
+        __syncthreads();   // every thread is done with stage s
+        if (tid == 0) {
+            const int64_t next = tile + (int64_t)STAGES * gridDim.x;
+            if (next < ntiles) {
+                mbar_expect_tx_arrive(&bars[s], TILE_BYTES);
+                bulk_g2s(stage_buf + (size_t)s * NMOM * TT, mom + next * (int64_t)NMOM * TT, TILE_BYTES, &bars[s]);
+            }
+        }
+    }
+}
+
+template <int L, bool F32>
+static int build_t(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, MomentTensor& T, cudaStream_t s) {
+    using E = typename std::conditional<F32, float, double>::type;
+    constexpr int TT = TTile<L, F32>::TT;
+    const int64_t ntiles = (n + TT - 1) / TT;
+    const size_t bytes = size_t(ntiles) * TT * TDim<L>::NMOM * sizeof(E);
+    T.release();
+    if (cudaMalloc(&T.d, bytes) != cudaSuccess) {
+        T.d = nullptr;
+        set_error("moment tensor allocation failed");
+        return TB_ERR_OOM;
+    }
+    TB_CUDA(cudaMemsetAsync(T.d, 0, bytes, s));
+    const size_t smem = sizeof(double) * size_t(c.nmc) * c.R;
+    int64_t blocks = (n * 32 + 255) / 256;
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    k_build_moments<L, E><<<unsigned(blocks), 256, smem, s>>>(c, tup, stride, n, reinterpret_cast<E*>(T.d), TT);
+    TB_CUDA(cudaGetLastError());
+    T.n = n;
+    T.ntiles = ntiles;
+    T.nmom = TDim<L>::NMOM;
+    T.fp32 = F32;
+    return TB_OK;
+}
+
+int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, bool fp32, MomentTensor& T,
+                 cudaStream_t s) {
+    switch (c.L * 2 + (fp32 ? 1 : 0)) {
+        case 4: return build_t<2, false>(c, tup, stride, n, T, s);
+        case 5: return build_t<2, true>(c, tup, stride, n, T, s);
+        case 6: return build_t<3, false>(c, tup, stride, n, T, s);
+        case 7: return build_t<3, true>(c, tup, stride, n, T, s);
+        case 8: return build_t<4, false>(c, tup, stride, n, T, s);
+        case 9: return build_t<4, true>(c, tup, stride, n, T, s);
+    }
+    set_error("nlegs must be 2..4");
     return TB_ERR_ARG;
 }
-int launch_collision_tensor(const ChanDev&, double, const MomentTensor&, const int32_t*, int64_t, int64_t,
-                            const double*, double*, const int*, cudaStream_t) {
-    set_error("moment tensor layout not available");
+
+static int* g_err_flag = nullptr;
+
+template <int L, bool F32>
+static int launch_t(const ChanDev& c, double amplitude, const MomentTensor& T, const int32_t* tup, int64_t stride,
+                    int64_t n, const double* f, double* acc, const int* done, cudaStream_t s) {
+    using E = typename std::conditional<F32, float, double>::type;
+    constexpr int TT = TTile<L, F32>::TT;
+    constexpr int STAGES = 2;
+    const size_t smem = size_t(STAGES) * TDim<L>::NMOM * TT * sizeof(E);
+    static bool attr = false;
+    if (!attr) {
+        TB_CUDA(cudaFuncSetAttribute(k_collision_tensor<L, E, TT, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(smem)));
+        attr = true;
+    }
+    if (!g_err_flag) {
+        TB_CUDA(cudaMalloc(&g_err_flag, sizeof(int)));
+        TB_CUDA(cudaMemset(g_err_flag, 0, sizeof(int)));
+    }
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_collision_tensor<L, E, TT, STAGES>, TT, smem);
+    if (per_sm < 1) per_sm = 1;
+    int64_t grid = int64_t(nsm) * per_sm;
+    if (grid > T.ntiles) grid = T.ntiles;
+    if (grid < 1) return TB_OK;
+    k_collision_tensor<L, E, TT, STAGES><<<unsigned(grid), TT, smem, s>>>(
+        c, amplitude, reinterpret_cast<const E*>(T.d), T.ntiles, tup, stride, n, f, acc, done, g_err_flag);
+    TB_CUDA(cudaGetLastError());
+    return TB_OK;
+}
+
+int launch_collision_tensor(const ChanDev& c, double amplitude, const MomentTensor& T, const int32_t* tup,
+                            int64_t stride, int64_t n, const double* f, double* acc, const int* done,
+                            cudaStream_t s) {
+    if (n <= 0) return TB_OK;
+    switch (c.L * 2 + (T.fp32 ? 1 : 0)) {
+        case 4: return launch_t<2, false>(c, amplitude, T, tup, stride, n, f, acc, done, s);
+        case 5: return launch_t<2, true>(c, amplitude, T, tup, stride, n, f, acc, done, s);
+        case 6: return launch_t<3, false>(c, amplitude, T, tup, stride, n, f, acc, done, s);
+        case 7: return launch_t<3, true>(c, amplitude, T, tup, stride, n, f, acc, done, s);
+        case 8: return launch_t<4, false>(c, amplitude, T, tup, stride, n, f, acc, done, s);
+        case 9: return launch_t<4, true>(c, amplitude, T, tup, stride, n, f, acc, done, s);
+    }
+    set_error("nlegs must be 2..4");
     return TB_ERR_ARG;
 }
+
+int tensor_error_flag(int* value) {
+    if (!g_err_flag) { *value = 0; return TB_OK; }
+    TB_CUDA(cudaMemcpy(value, g_err_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    return TB_OK;
+}
+
 }  // namespace tb

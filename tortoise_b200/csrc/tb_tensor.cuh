@@ -20,4 +20,7 @@ int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n
 int launch_collision_tensor(const ChanDev& c, double amplitude, const MomentTensor& T, const int32_t* tup,
                             int64_t stride, int64_t n, const double* f, double* acc, const int* done, cudaStream_t s);
 
+// 1 once a bulk-copy wait of the contraction kernel ran out (then TB_ERR_TIMEOUT)
+int tensor_error_flag(int* value);
+
 }  // namespace tb
