@@ -1,0 +1,334 @@
+"""Benchmark: Dormand-Prince 5(4) attempts per second on the 64x64 two-band
+electron-phonon workload, with the collision operator's HBM roofline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--layout auto|mc64|t64|t32] [--mixed]
+
+A "step" is one DP45 attempt: six right-hand-side evaluations (collision
+operator over all scattering channels + Vlasov drift + M^-1), the fused stage
+combinations, the embedded error norm and the step-size controller, all on the
+device (one CUDA graph launch).  Workload (synthetic, seeded): k-space
+[-1,1]^2, 64x64 sections (8192 P1 triangles per band), bands parabola
+E=|k|^2/2 and Dirac cone E=|k|+0.5 plus a dispersionless optical phonon
+(hw = 0.2, Bose occupation at kT = 0.05), e-ph channels {el,pn,el} {in,in,out}
+with unit coupling, drift field (0.1, 0), rtol 1e-8 / atol 1e-9, NMC = 50.
+The four-leg e-e channel of that configuration is left out: at 64x64 it has
+~9e10 surviving tuples per channel per RHS evaluation (measured scaling
+~N^5.2), beyond any single GPU for a time integration.
+
+Multi-GPU: runs are independent replicas (the path has no exchange step);
+`value` is the aggregate over ranks, timed as the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DP45 steps/s & collision-op HBM GB/s, batched mixed vs plain FP64 GPU at ≤1e-8 rel err"
+N_MESH = 64
+T_END = 20.0
+DENSE = T_END / 10.0
+
+
+def workload():
+    from tortoise_b200 import workloads as W
+    mat = W.config1(N_MESH)
+    f0 = W.initial_status(mat, kT=0.1, seed=1).vec
+    return mat, f0
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "bench_clocks_%d.csv" % os.getpid())
+
+    def __enter__(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if not self.proc or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        loaded = [x for x in sm if x > 0.5 * (mx or max(sm))] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def reduce_max(pg, x, device):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_rhs_sample(o, mat, f, frac):
+    """One RHS evaluation of the oracle on the first `frac` of every channel's
+    tuples plus the full drift term; returns seconds scaled to the full list."""
+    t0 = time.perf_counter()
+    acc = np.zeros(o.ndofs)
+    t_coll = 0.0
+    for ch in range(len(mat.channels)):
+        n = o.num_tuples(ch)
+        m = max(1, int(n * frac))
+        a = time.perf_counter()
+        o.channel_propagate(ch, f, 0, m, out=acc)
+        t_coll += (time.perf_counter() - a) * (n / m)
+    a = time.perf_counter()
+    for b, band in enumerate(mat.bands):
+        if band.drift_velocity != (0.0, 0.0):
+            off = o.band_offset(b)
+            o.vlasov(b, f[off:off + band.mesh.ne * 3])
+    t_drift = time.perf_counter() - a
+    return t_coll + t_drift, time.perf_counter() - t0
+
+
+def reference_arm(args, world, rank):
+    """The reference's CPU path (restated: the reference itself needs Eigen
+    and oneTBB, which are absent), timed on all host cores."""
+    if rank != 0:
+        return
+    import oracle
+    mat, f0 = workload()
+    o = oracle.Oracle(mat, nthreads=os.cpu_count())
+    ntup = sum(o.num_tuples(c) for c in range(len(mat.channels)))
+    frac = min(1.0, 2.0e5 / max(1, ntup))
+    times = []
+    for i in range(args.warmup + args.steps):
+        # one attempt = six RHS evaluations (k2..k7) on a bounded tuple sample
+        t_att = 0.0
+        for _ in range(6):
+            t_att += cpu_rhs_sample(o, mat, f0, frac)[0]
+        if i >= args.warmup:
+            times.append(t_att)
+    v = len(times) / sum(times)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "DP45 steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded PCG64)",
+            "config": {"workload": "2-band e-ph + drift, 64x64 mesh (8192 triangles/band), NMC=50",
+                       "tuples": ntup, "parallelism": "host threads"},
+            "cpu_baseline": {"value": v, "unit": "DP45 steps/s", "cores": os.cpu_count(), "kind": "port",
+                             "sample": "each step: 6 RHS evaluations on the first %.2f%% of every channel's "
+                                       "tuples (time scaled to the full list) + full drift" % (100 * frac)},
+            "e2e": {"value": v, "unit": "DP45 steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def ours(args, world, rank, local, pg):
+    import torch
+    from tortoise_b200 import engine as E
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    mat, f0 = workload()
+    layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32}[args.layout]
+    eng = E.Engine(mat, layout=layout, allow_fp32=args.mixed, device=local)
+    nch = len(mat.channels)
+    infos = [eng.channel_info(c) for c in range(nch)]
+    ntup = sum(i["n_tuples"] for i in infos)
+    stream = torch.cuda.ExternalStream(eng.stream_ptr(), device=dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    # ---- collision kernels alone (roofline) -----------------------------
+    f = torch.tensor(f0, device=dev)
+    acc = torch.zeros_like(f)
+    torch.cuda.synchronize()
+    for _ in range(3):
+        eng.collision_accumulate(f.data_ptr(), acc.data_ptr())
+    eng.synchronize()
+    reps = 20
+    ev0.record(stream)
+    for _ in range(reps):
+        eng.collision_accumulate(f.data_ptr(), acc.data_ptr())
+    ev1.record(stream)
+    ev1.synchronize()
+    t_coll = ev0.elapsed_time(ev1) * 1e-3 / reps
+    nmom = {2: 27, 3: 108, 4: 405}
+    bytes_coll = 0
+    for c, inf in zip(mat.channels, infos):
+        L, n = c.nlegs, inf["n_tuples"]
+        if inf["layout"] in ("t64", "t32"):
+            bytes_coll += n * nmom[L] * (4 if inf["layout"] == "t32" else 8)
+        bytes_coll += n * 4 * (L + 1)
+    bytes_coll += eng.ndofs * 8 * 3   # f read once, accumulator read + written once
+    hbm, peak_kind = peaks()
+    achieved = bytes_coll / t_coll / 1e9
+
+    # ---- DP45 attempts on the device ------------------------------------
+    eng.dp45_begin(f0, 0.0, 1.0e9, DENSE, 0)
+    eng.dp45_advance(args.warmup)
+    eng.synchronize()
+    with ClockSampler(local) as clk:
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        eng.dp45_advance(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+        torch.cuda.synchronize()
+        if pg is not None:
+            pg.barrier()
+    t_dev = ev0.elapsed_time(ev1) * 1e-3
+    st = eng.dp45_poll()
+    t_max = reduce_max(pg, t_dev, dev)
+    value = world * args.steps / t_max
+    drift_launch = 1 if any(b.drift_velocity != (0.0, 0.0) for b in mat.bands) else 0
+    active = sum(1 for c, i in zip(mat.channels, infos) if c.amplitude != 0 and i["n_tuples"] > 0)
+    launches = args.steps * (7 + 6 * (active + drift_launch) + 3)
+
+    # ---- end to end through the C ABI with host buffers ------------------
+    # tb_dp45_integrate from host memory to host memory (k1 evaluation, graph
+    # launches, polling and the copies of the state and dense output inside).
+    t_e2e_final = max(st["t"], 1e-3)
+    y = np.ascontiguousarray(f0).copy()
+    if pg is not None:
+        pg.barrier()
+    w0 = time.perf_counter()
+    r = eng.dp45(y, 0.0, t_e2e_final, DENSE)
+    w1 = time.perf_counter()
+    e2e_t = reduce_max(pg, w1 - w0, dev)
+    e2e_val = world * r["attempts"] / e2e_t
+    h2d = eng.ndofs * 8 / max(1, r["attempts"])
+    d2h = eng.ndofs * 8 * (1 + r["n_dense"]) / max(1, r["attempts"])
+
+    # ---- CPU baseline (oracle on the host cores, bounded sample) ----------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        import oracle
+        o = oracle.Oracle(mat, nthreads=os.cpu_count())
+        ntup_o = sum(o.num_tuples(c) for c in range(nch))
+        frac = min(1.0, 2.0e5 / max(1, ntup_o))
+        samples = [cpu_rhs_sample(o, mat, f0, frac)[0] for _ in range(3)]
+        t_att = 6 * statistics.median(samples)
+        cpu = {"value": 1.0 / t_att, "unit": "DP45 steps/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": "6 x one RHS evaluation on the first %.2f%% of every channel's tuples, time scaled to "
+                         "the full list (+ full drift), median of 3" % (100 * frac)}
+
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "collision_traffic.json")
+    if os.path.exists(tp):
+        d = json.load(open(tp))
+        key = "t32" if args.mixed else "t64"
+        if key in d and d[key].get("bytes_per_tuple"):
+            traffic = d[key]["bytes_per_tuple"] * ntup
+    line = {"metric": METRIC, "value": value, "unit": "DP45 steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if not args.mixed else "f32-storage/f64-accumulate",
+            "data": "synthetic (seeded PCG64 bump on Fermi-Dirac, Bose phonons)",
+            "config": {"workload": "2-band e-ph + drift, 64x64 mesh (8192 triangles/band), NMC=50, rtol 1e-8",
+                       "tuples": ntup, "channels": nch, "layouts": [i["layout"] for i in infos],
+                       "dofs": eng.ndofs, "parallelism": "replicas x%d" % world,
+                       "l2": "moment tensors (%.1f GB) exceed L2; no flush" % (bytes_coll / 1e9)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic,
+                         "kernel": "collision contraction, all channels, per RHS evaluation",
+                         "algorithmic_bytes": bytes_coll, "seconds_per_launch": t_coll,
+                         "peak_source": peak_kind},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_val, "unit": "DP45 steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "attempts": r["attempts"], "seconds": e2e_t},
+            "gpu_launches": launches,
+            "dp45": {"t": st["t"], "dt": st["dt"], "attempts": st["attempts"], "rejected": st["rejected"],
+                     "status": st["status"]}}
+    clk_s = clk.summary()
+    if clk_s:
+        line["clocks"] = clk_s
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--layout", default="auto", choices=["auto", "mc64", "t64", "t32"])
+    ap.add_argument("--mixed", action="store_true", help="allow FP32 moment storage (FP64 accumulate)")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world, rank, local, pg = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            reference_arm(args, world, rank)
+        else:
+            ours(args, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -26,7 +26,7 @@ def lib():
         L = C.CDLL(_LIB_PATH)
         vp, dp, ip, i64 = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32), C.c_int64
         L.or_create.restype = vp
-        L.or_create.argtypes = [vp, C.c_int]
+        L.or_create.argtypes = [vp, C.c_int, C.c_int]
         L.or_destroy.argtypes = [vp]
         L.or_last_error.restype = C.c_char_p
         L.or_num_dofs.restype = i64
@@ -72,16 +72,19 @@ class Oracle:
     def __init__(self, material, enumerate_tuples=True, nthreads=None):
         self.material = material
         self.packed = material.pack()
-        self.h = lib().or_create(C.addressof(self.packed.desc), 1 if enumerate_tuples else 0)
+        self.nthreads = nthreads or os.cpu_count() or 1
+        self.h = lib().or_create(C.addressof(self.packed.desc), 1 if enumerate_tuples else 0, self.nthreads)
         if not self.h:
             raise RuntimeError("oracle: " + lib().or_last_error().decode())
         self.ndofs = lib().or_num_dofs(self.h)
-        self.nthreads = nthreads or os.cpu_count() or 1
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().or_destroy(self.h)
-            self.h = None
+        try:
+            if getattr(self, "h", None):
+                lib().or_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
 
     def band_offset(self, b):
         return lib().or_band_offset(self.h, b)

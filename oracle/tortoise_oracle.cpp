@@ -356,17 +356,13 @@ static int tuple_survives(const Problem& P, const Channel& c, const int32_t* e, 
     return std::fabs(res) > c.threshold ? 1 : 0;
 }
 
-// deterministicIteration / nestedForSections / nestedForElements,
-// ScatteringChannel.hpp:205-255, driven by precalculateIndices
-// (ScatteringChannel.cpp:461-507).  Tuples are produced in the reference's
-// loop order: umklapp, sections of legs 0..L-2, elements of legs 0..L-1.
-static void enumerate(const Problem& P, Channel& c) {
+struct EnumPart {
+    std::vector<int32_t> tuples, tumk;
+    int64_t n_pre = 0, n_det = 0;
+};
+
+static void enumerate_range(const Problem& P, const Channel& c, int u, int s0_begin, int s0_end, EnumPart& out) {
     const int L = c.L;
-    const int nU = int(c.umk.size() / 2);
-    c.tuples.clear();
-    c.tumk.clear();
-    c.n_prefilter = 0;
-    c.n_det = 0;
     const Mesh* ms[4];
     const Band* bs[4];
     for (int l = 0; l < L; ++l) { bs[l] = &P.bands[c.band[l]]; ms[l] = &P.meshes[bs[l]->mesh]; }
@@ -375,55 +371,86 @@ static void enumerate(const Problem& P, Channel& c) {
     int nsec[3] = {1, 1, 1};
     for (int l = 0; l < L - 1; ++l) nsec[l] = ms[l]->nx * ms[l]->ny;
     int32_t e[4];
-    for (int u = 0; u < nU; ++u) {
-        const double ux = c.umk[2 * u], uy = c.umk[2 * u + 1];
-        const double gu[2] = {G[0] * ux + G[2] * uy, G[1] * ux + G[3] * uy};
-        for (sec[0] = 0; sec[0] < nsec[0]; ++sec[0])
-        for (sec[1] = 0; sec[1] < nsec[1]; ++sec[1])
-        for (sec[2] = 0; sec[2] < nsec[2]; ++sec[2]) {
-            // box of the last leg: -dir[L-1] * (sum_l dir[l]*box_l + gVec*umklapp)
-            Box acc{};
+    const double ux = c.umk[2 * u], uy = c.umk[2 * u + 1];
+    const double gu[2] = {G[0] * ux + G[2] * uy, G[1] * ux + G[3] * uy};
+    for (sec[0] = s0_begin; sec[0] < s0_end; ++sec[0])
+    for (sec[1] = 0; sec[1] < nsec[1]; ++sec[1])
+    for (sec[2] = 0; sec[2] < nsec[2]; ++sec[2]) {
+        // box of the last leg: -dir[L-1] * (sum_l dir[l]*box_l + gVec*umklapp)
+        Box acc{};
+        for (int l = 0; l < L - 1; ++l) {
+            Box b = box_scale(section_box(*ms[l], sec[l] % ms[l]->nx, sec[l] / ms[l]->nx), double(c.dir[l]));
+            if (l == 0) acc = b;
+            else for (int i = 0; i < 2; ++i) { acc.l[i] += b.l[i]; acc.h[i] += b.h[i]; }
+        }
+        for (int i = 0; i < 2; ++i) { acc.l[i] += gu[i]; acc.h[i] += gu[i]; }
+        acc = box_scale(acc, -double(c.dir[L - 1]));
+        int lo[2], hi[2];
+        box_to_sections(*ms[L - 1], acc, lo, hi);
+        if (!(lo[0] != hi[0] && lo[1] != hi[1])) continue;
+        const int ncomb = 1 << (L - 1);
+        for (int comb = 0; comb < ncomb; ++comb) {
+            // element of leg l within its section: bit (L-2-l) of comb
+            double minE = 0.0, maxE = 0.0;
+            double mn[4], mx[4];
             for (int l = 0; l < L - 1; ++l) {
-                Box b = box_scale(section_box(*ms[l], sec[l] % ms[l]->nx, sec[l] / ms[l]->nx), double(c.dir[l]));
-                if (l == 0) acc = b;
-                else for (int i = 0; i < 2; ++i) { acc.l[i] += b.l[i]; acc.h[i] += b.h[i]; }
+                int i = (comb >> (L - 2 - l)) & 1;
+                e[l] = 2 * sec[l] + i;
+                mn[l] = (c.dir[l] > 0) ? bs[l]->minE[e[l]] : -bs[l]->maxE[e[l]];
+                mx[l] = (c.dir[l] > 0) ? bs[l]->maxE[e[l]] : -bs[l]->minE[e[l]];
             }
-            for (int i = 0; i < 2; ++i) { acc.l[i] += gu[i]; acc.h[i] += gu[i]; }
-            acc = box_scale(acc, -double(c.dir[L - 1]));
-            int lo[2], hi[2];
-            box_to_sections(*ms[L - 1], acc, lo, hi);
-            if (!(lo[0] != hi[0] && lo[1] != hi[1])) continue;
-            const int ncomb = 1 << (L - 1);
-            for (int comb = 0; comb < ncomb; ++comb) {
-                // element of leg l within its section: bit (L-2-l) of comb
-                double minE = 0.0, maxE = 0.0;
-                double mn[4], mx[4];
-                for (int l = 0; l < L - 1; ++l) {
-                    int i = (comb >> (L - 2 - l)) & 1;
-                    e[l] = 2 * sec[l] + i;
-                    mn[l] = (c.dir[l] > 0) ? bs[l]->minE[e[l]] : -bs[l]->maxE[e[l]];
-                    mx[l] = (c.dir[l] > 0) ? bs[l]->maxE[e[l]] : -bs[l]->minE[e[l]];
-                }
-                const Mesh& ml = *ms[L - 1];
-                for (int sy = lo[1]; sy < hi[1]; ++sy)
-                    for (int sx = lo[0]; sx < hi[0]; ++sx)
-                        for (int i = 0; i < 2; ++i) {
-                            e[L - 1] = 2 * (sx + sy * ml.nx) + i;
-                            const int l = L - 1;
-                            mn[l] = (c.dir[l] > 0) ? bs[l]->minE[e[l]] : -bs[l]->maxE[e[l]];
-                            mx[l] = (c.dir[l] > 0) ? bs[l]->maxE[e[l]] : -bs[l]->minE[e[l]];
-                            minE = 0.0; maxE = 0.0;
-                            for (int k = 0; k < L; ++k) { minE += mn[k]; maxE += mx[k]; }
-                            if (!((minE <= 0.0) && (maxE >= 0.0))) continue;
-                            ++c.n_prefilter;
-                            bool det_ok;
-                            if (tuple_survives(P, c, e, u, det_ok)) {
-                                for (int k = 0; k < L; ++k) c.tuples.push_back(e[k]);
-                                c.tumk.push_back(u);
-                            }
-                            if (det_ok) ++c.n_det;
+            const Mesh& ml = *ms[L - 1];
+            for (int sy = lo[1]; sy < hi[1]; ++sy)
+                for (int sx = lo[0]; sx < hi[0]; ++sx)
+                    for (int i = 0; i < 2; ++i) {
+                        e[L - 1] = 2 * (sx + sy * ml.nx) + i;
+                        const int l = L - 1;
+                        mn[l] = (c.dir[l] > 0) ? bs[l]->minE[e[l]] : -bs[l]->maxE[e[l]];
+                        mx[l] = (c.dir[l] > 0) ? bs[l]->maxE[e[l]] : -bs[l]->minE[e[l]];
+                        minE = 0.0; maxE = 0.0;
+                        for (int k = 0; k < L; ++k) { minE += mn[k]; maxE += mx[k]; }
+                        if (!((minE <= 0.0) && (maxE >= 0.0))) continue;
+                        ++out.n_pre;
+                        bool det_ok;
+                        if (tuple_survives(P, c, e, u, det_ok)) {
+                            for (int k = 0; k < L; ++k) out.tuples.push_back(e[k]);
+                            out.tumk.push_back(u);
                         }
-            }
+                        if (det_ok) ++out.n_det;
+                    }
+        }
+    }
+}
+
+// deterministicIteration / nestedForSections / nestedForElements,
+// ScatteringChannel.hpp:205-255, driven by precalculateIndices
+// (ScatteringChannel.cpp:461-507).  Tuples are produced in the reference's
+// loop order: umklapp, sections of legs 0..L-2, elements of legs 0..L-1.
+// The outermost section loop is split into contiguous ranges over threads and
+// the per-range lists are concatenated in order.
+static void enumerate(const Problem& P, Channel& c, int nthreads) {
+    const int nU = int(c.umk.size() / 2);
+    c.tuples.clear();
+    c.tumk.clear();
+    c.n_prefilter = 0;
+    c.n_det = 0;
+    const Mesh& m0 = P.meshes[P.bands[c.band[0]].mesh];
+    const int ns0 = m0.nx * m0.ny;
+    nthreads = std::max(1, std::min(nthreads, ns0));
+    for (int u = 0; u < nU; ++u) {
+        std::vector<EnumPart> parts(nthreads);
+        std::vector<std::thread> th;
+        auto work = [&](int t) {
+            enumerate_range(P, c, u, int(int64_t(ns0) * t / nthreads), int(int64_t(ns0) * (t + 1) / nthreads), parts[t]);
+        };
+        for (int t = 1; t < nthreads; ++t) th.emplace_back(work, t);
+        work(0);
+        for (auto& x : th) x.join();
+        for (auto& p : parts) {
+            c.tuples.insert(c.tuples.end(), p.tuples.begin(), p.tuples.end());
+            c.tumk.insert(c.tumk.end(), p.tumk.begin(), p.tumk.end());
+            c.n_prefilter += p.n_pre;
+            c.n_det += p.n_det;
         }
     }
 }
@@ -877,7 +904,7 @@ static int dp54(const Problem& P, double* y_io, double t0, double tf, double den
 }
 
 // ------------------------------------------------------------ construction
-static Problem build(const tb_problem_desc* d, bool enumerate_tuples) {
+static Problem build(const tb_problem_desc* d, bool enumerate_tuples, int nthreads) {
     Problem P;
     P.region = d->region;
     for (int i = 0; i < d->n_meshes; ++i) P.meshes.push_back(make_mesh(d->region, d->meshes[i]));
@@ -939,7 +966,7 @@ static Problem build(const tb_problem_desc* d, bool enumerate_tuples) {
             c.tuples.assign(cd.tuples, cd.tuples + size_t(cd.n_tuples) * c.L);
             c.tumk.assign(cd.tuple_umklapp, cd.tuple_umklapp + size_t(cd.n_tuples));
         } else if (enumerate_tuples) {
-            enumerate(P, c);
+            enumerate(P, c, nthreads);
         }
         P.chans.push_back(std::move(c));
     }
@@ -957,9 +984,9 @@ extern "C" {
 
 const char* or_last_error(void) { return g_err.c_str(); }
 
-void* or_create(const tb_problem_desc* desc, int enumerate_tuples) {
+void* or_create(const tb_problem_desc* desc, int enumerate_tuples, int nthreads) {
     try {
-        return new Problem(build(desc, enumerate_tuples != 0));
+        return new Problem(build(desc, enumerate_tuples != 0, nthreads));
     } catch (const std::exception& ex) {
         g_err = ex.what();
         return nullptr;
