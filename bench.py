@@ -38,9 +38,9 @@ T_END = 20.0
 DENSE = T_END / 10.0
 
 
-def workload():
+def workload(n_mesh=N_MESH):
     from tortoise_b200 import workloads as W
-    mat = W.config1(N_MESH)
+    mat = W.config1(n_mesh)
     f0 = W.initial_status(mat, kT=0.1, seed=1).vec
     return mat, f0
 
@@ -309,6 +309,28 @@ def ours(args, world, rank, local, pg):
     eng.close()
 
 
+def rhs_only(args):
+    """Profiling driver: K right-hand-side evaluations (collision + drift +
+    M^-1) of the workload on the device, nothing else (used for the ncu
+    launch list and kernel captures summarised under profiles/)."""
+    import torch
+    from tortoise_b200 import engine as E
+    mat, f0 = workload(args.mesh)
+    layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32}[args.layout]
+    eng = E.Engine(mat, layout=layout, allow_fp32=args.mixed)
+    f = torch.tensor(f0, device="cuda")
+    out = torch.zeros_like(f)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.rhs_only):
+        eng.rhs_device(f.data_ptr(), out.data_ptr())
+    eng.synchronize()
+    dt = time.perf_counter() - t0
+    print(json.dumps({"rhs_only": args.rhs_only, "mesh": args.mesh, "layouts": [eng.channel_info(c)["layout"]
+                      for c in range(len(mat.channels))], "seconds": dt}), flush=True)
+    eng.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -318,7 +340,12 @@ def main():
     ap.add_argument("--layout", default="auto", choices=["auto", "mc64", "t64", "t32"])
     ap.add_argument("--mixed", action="store_true", help="allow FP32 moment storage (FP64 accumulate)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--rhs-only", type=int, default=0, help="profiling driver: K RHS evaluations only")
+    ap.add_argument("--mesh", type=int, default=N_MESH, help="sections per side (profiling driver only)")
     args = ap.parse_args()
+    if args.rhs_only:
+        rhs_only(args)
+        return
     world, rank, local, pg = dist_setup(args)
     try:
         if args.impl == "reference":
