@@ -231,6 +231,24 @@ void* tb_get_stream(tb_handle* h);
  * callers that compose their own right-hand side. */
 int tb_collision_accumulate(tb_handle* h, int ch, const double* f, double* acc);
 
+/* The error norm of ONE band (what Band::relativeError computes for one
+ * population) for callers that cannot call cudaMalloc when they need it -- a
+ * host application whose device memory is fully reserved by its own pool
+ * allocator, or code that must not risk the implicit device synchronisation of
+ * cudaMalloc/cudaFree inside its own asynchronous work.  It needs no handle and
+ * allocates nothing: err, pop (n_elements*3 doubles each, linear-form layout)
+ * and result (one double) are device memory supplied by the caller, and the
+ * per-block partial sums live in a fixed 64 KiB device array of the library
+ * (held on every device that loads the library until the process exits).
+ * Limit: n_elements <= 1,048,576 (TB_ERR_CAPACITY beyond).  The first call on
+ * a device looks up that array's device address, so make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race.
+ * Launches on `stream` (a cudaStream_t, NULL = default stream) and does not
+ * synchronise.  No counterpart in the reference. */
+int tb_band_relative_error_noalloc(const double* err, const double* pop, int64_t n_elements, double elem_volume,
+                                   double statistics, double rel_tol, double abs_tol, double penalisation,
+                                   double* result, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -22,6 +22,7 @@ SOURCES = {
     "tb_drift.cu": [],
     "tb_dp45.cu": [],
     "tb_tensor.cu": [],
+    "tb_static_scratch.cu": [],
 }
 
 
