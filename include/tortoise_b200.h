@@ -171,6 +171,22 @@ const char* tb_last_error(void);
 int tb_create(tb_handle** h, const tb_problem_desc* desc, const tb_options* opts);
 int tb_destroy(tb_handle* h);
 
+/* Batched ensemble: n_runs independent runs (different initial conditions,
+ * temperatures, coupling constants, meshes ...) in one handle and one state
+ * vector (runs concatenated in order).  Runs whose structure is identical
+ * (region, meshes, dispersions, statistics, channels, Monte-Carlo tables)
+ * share one tuple list and one moment tensor: the collision kernels stream
+ * each tuple tile once and contract it against every such run.  Every run
+ * keeps its own amplitudes, tolerances, constraints, drift, state and, in the
+ * integrator, its own adaptive step size and accept/reject sequence.  Bands
+ * and channels are numbered globally in run order (tb_run_info gives each
+ * run's first band and channel).  No counterpart in the reference (one
+ * Material per process there). */
+int tb_create_batch(tb_handle** h, const tb_problem_desc* const* runs, int n_runs, const tb_options* opts);
+int tb_num_runs(const tb_handle* h);
+int tb_run_info(const tb_handle* h, int run, int64_t* dof_offset, int64_t* ndofs, int32_t* first_band,
+                int32_t* first_channel);
+
 int64_t tb_num_dofs(const tb_handle* h);
 int64_t tb_band_offset(const tb_handle* h, int band);
 int     tb_num_channels(const tb_handle* h);
@@ -193,7 +209,8 @@ int tb_rhs(tb_handle* h, const double* f, double* dfdt, int flags);
  * ScatteringChannel.cpp:651-670), M^-1 included. */
 int tb_channel_propagate(tb_handle* h, int ch, const double* f, double* out, int flags);
 
-/* MaterialStatus::relativeError(err, pop) (MaterialStatus.cpp:189-196). */
+/* MaterialStatus::relativeError(err, pop) (MaterialStatus.cpp:189-196), one
+ * value per run: result[n_runs]. */
 int tb_relative_error(tb_handle* h, const double* err, const double* pop, double* result, int flags);
 
 /* MaterialStatus::applyConstraints for time-independent constraints. */
@@ -204,7 +221,9 @@ int tb_apply_constraints(tb_handle* h, double* f, int flags);
  * Algorithms/DormandPrince54.hpp:479-665) as called by MaterialTimeStatus::
  * propagate (src/Physics/Status/MaterialTimeStatus.cpp:102-137).
  * f_inout: state at t0 on entry, state at the last accepted step on exit.
- * dense_out[max_dense*ndofs], dense_times[max_dense] receive the dense outputs. */
+ * dense_out[max_dense*ndofs], dense_times[max_dense] receive the dense outputs;
+ * for a batch, run r's block (max_dense slots of its own ndofs) follows run
+ * r-1's, and dense_times holds max_dense entries per run. */
 int tb_dp45_integrate(tb_handle* h, double* f_inout, double t0, double t_final, double dense_step,
                       double* dense_out, double* dense_times, int64_t max_dense, tb_dp45_stats* stats,
                       int flags);
@@ -214,7 +233,13 @@ int tb_dp45_integrate(tb_handle* h, double* f_inout, double t0, double t_final, 
  * end.  max_dense == 0 keeps no dense output. */
 int tb_dp45_begin(tb_handle* h, const double* f0, double t0, double t_final, double dense_step, int64_t max_dense,
                   int flags);
+/* Per-run start time, end time and dense step (arrays of n_runs). */
+int tb_dp45_begin_batch(tb_handle* h, const double* f0, const double* t0, const double* t_final,
+                        const double* dense_step, int64_t max_dense, int flags);
+/* Statistics of one run as of the last tb_dp45_poll / tb_dp45_end. */
+int tb_dp45_run_stats(tb_handle* h, int run, tb_dp45_stats* stats);
 int tb_dp45_advance(tb_handle* h, int64_t n_attempts);
+/* stats of run 0; stats->done = 1 once every run is done. */
 int tb_dp45_poll(tb_handle* h, tb_dp45_stats* stats);
 int tb_dp45_end(tb_handle* h, double* f_out, double* dense_out, double* dense_times, int64_t max_dense,
                 tb_dp45_stats* stats, int flags);

@@ -1,0 +1,67 @@
+"""Batched ensembles: one handle, several runs.  Every run of a batch must
+give what it gives alone (RHS to 1e-12; DP45 with its own accept/reject
+sequence and dense outputs to 1e-10), whether it shares structure with other
+runs (shared tuple lists / moment tensors) or not."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from tortoise_b200 import engine as E
+from tortoise_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _runs():
+    """Three e-ph runs of equal structure (4x4) with different coupling and
+    temperature, plus one run of another structure (3x3, two phonon baths)."""
+    mats, states = [], []
+    for k, (amp, kT) in enumerate([(1.0, 0.1), (0.5, 0.05), (2.0, 0.2)]):
+        m = W.build_material(4, ("P", "D"), (0.2,), ee=False, eph=True, field=(0.1, 0.0), rtol=1e-6, atol=1e-9,
+                             eph_amplitude=amp)
+        mats.append(m)
+        states.append(W.initial_status(m, kT=kT, seed=10 + k).vec)
+    m = W.build_material(3, ("P",), (0.15, 0.25), ee=False, eph=True, field=(0.0, 0.05), rtol=1e-6, atol=1e-9,
+                         phonon_bath=True)
+    mats.append(m)
+    states.append(W.initial_status(m, kT=0.1, seed=20).vec)
+    return mats, states
+
+
+@pytest.mark.parametrize("layout", [E.LAYOUT_MC64, E.LAYOUT_T64])
+def test_batch_rhs_equals_individual_runs(gpu_lib, layout):
+    mats, states = _runs()
+    be = E.BatchEngine(mats, layout=layout)
+    got = be.split(be.rhs(np.concatenate(states)))
+    for m, f, g in zip(mats, states, got):
+        ref = E.Engine(m, layout=layout).rhs(f)
+        assert rel_l2(g, ref) < 1e-12
+    # equal-structure runs share one tuple list
+    n0 = be.channel_info(be.chan0[0])["n_tuples"]
+    assert be.channel_info(be.chan0[1])["n_tuples"] == n0
+
+
+def test_batch_amplitude_update(gpu_lib):
+    mats, states = _runs()
+    be = E.BatchEngine(mats, layout=E.LAYOUT_T64)
+    f = np.concatenate(states)
+    base = be.split(be.rhs(f, drift=False))
+    for c in range(len(mats[1].channels)):
+        be.set_amplitude(be.chan0[1] + c, 0.0)
+    after = be.split(be.rhs(f, drift=False))
+    assert np.linalg.norm(after[1]) == 0.0
+    assert rel_l2(after[0], base[0]) < 1e-14 and rel_l2(after[2], base[2]) < 1e-14
+
+
+def test_batch_dp45_equals_individual_runs(gpu_lib):
+    mats, states = _runs()
+    be = E.BatchEngine(mats, layout=E.LAYOUT_MC64)
+    tf = [0.4, 0.3, 0.2, 0.4]
+    res = be.dp45(np.concatenate(states), 0.0, tf, 0.1)
+    for r, (m, f) in enumerate(zip(mats, states)):
+        ref = E.Engine(m, layout=E.LAYOUT_MC64).dp45(f, 0.0, tf[r], 0.1)
+        got = res["runs"][r]
+        assert got["status"] == 0
+        assert [got["attempts"], got["accepted"], got["rejected"]] == [ref["attempts"], ref["accepted"], ref["rejected"]]
+        assert np.allclose(got["dense_t"], ref["dense_t"], rtol=0, atol=1e-14)
+        assert rel_l2(got["dense"], ref["dense"]) < 1e-10

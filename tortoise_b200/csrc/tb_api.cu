@@ -93,12 +93,11 @@ static std::vector<double> coord_function(const HostMesh& m, int dim) {
     return v;
 }
 
-struct Channel {
-    ChanDev dev;
+// A channel structure shared by every run of the same structure: the tuple
+// list, the moment tensor and the Monte-Carlo tables exist once.
+struct GroupChan {
+    ChanDev dev;                  // table pointers of the group's first run
     int L = 0;
-    int band[TB_MAX_LEGS] = {0, 0, 0, 0};
-    double amplitude = 0.0;
-    double amp_full = 0.0;        // amplitude * prod_l (vol_l * 2), in the reference's order
     double* d_umk = nullptr;
     double* d_mc = nullptr;
     double* d_mc_pre = nullptr;
@@ -106,6 +105,25 @@ struct Channel {
     int64_t diag[3] = {0, 0, 0};
     int layout = TB_LAYOUT_MC64;
     MomentTensor tensor;
+    std::vector<int> insts;       // channel instances using it (run order)
+    InstDev* d_insts = nullptr;   // [insts.size()]
+};
+
+// One run's channel (the unit tb_channel_info / tb_set_amplitude address).
+struct ChanInst {
+    int group = 0;
+    int run = 0;
+    int band[TB_MAX_LEGS] = {0, 0, 0, 0};   // global band ids
+    double amplitude = 0.0;
+    InstDev dev{};
+    InstDev* d_single = nullptr;  // this instance alone (single-channel calls)
+    int slot = 0;                 // position inside the group's d_insts
+};
+
+struct RunInfo {
+    int band0 = 0, nbands = 0;
+    int64_t dof_off = 0, ndofs = 0;
+    int chan0 = 0, nchans = 0;
 };
 
 }  // namespace tb
@@ -114,7 +132,7 @@ using namespace tb;
 
 namespace tb {
 int choose_layouts(tb_handle* h);
-int run_rhs_acc(tb_handle* h, const double* d_in, double* d_acc, const int* done, int flags, int only_channel);
+int run_rhs_acc(tb_handle* h, const double* d_in, double* d_acc, const DPCtl* ctl, int flags, int only_inst);
 }  // namespace tb
 
 struct tb_handle {
@@ -123,11 +141,15 @@ struct tb_handle {
     tb_options opts{};
     std::vector<HostMesh> meshes;
     std::vector<HostBand> bands;
+    std::vector<BandDev> banddev;
     std::vector<double*> dev_allocs;
-    BandsDev bandsdev{};
-    std::vector<Channel> chans;
+    std::vector<void*> dev_raw;
+    std::vector<RunInfo> runs;
+    std::vector<GroupChan> groups;
+    std::vector<ChanInst> insts;
+    ElemDev ed{};
+    bool any_drift = false;
     int64_t ndofs = 0;
-    int nblk = 1;
     double* d_f = nullptr;
     double* d_out = nullptr;
     double* d_acc = nullptr;
@@ -136,9 +158,11 @@ struct tb_handle {
     DPBufs dp{};
     bool dp_ready = false;
     int64_t dense_cap_alloc = -1;
+    RunDev* d_runs = nullptr;
+    std::vector<RunDev> hruns;
     cudaGraphExec_t graph = nullptr;
     int graph_flags = -1;
-    DPCtl* h_ctl = nullptr;   // pinned host mirror
+    DPCtl* h_ctl = nullptr;   // pinned host mirror [nruns]
     int dp_flags = 0;
 };
 
@@ -151,6 +175,15 @@ double* dev_alloc(tb_handle* h, size_t n) {
     return p;
 }
 
+template <typename T>
+T* dev_upload_raw(tb_handle* h, const T* src, size_t n) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, sizeof(T) * (n ? n : 1)) != cudaSuccess) return nullptr;
+    h->dev_raw.push_back(p);
+    if (n) cudaMemcpy(p, src, sizeof(T) * n, cudaMemcpyHostToDevice);
+    return static_cast<T*>(p);
+}
+
 double* dev_upload(tb_handle* h, const std::vector<double>& v) {
     double* p = dev_alloc(h, v.size());
     if (p && !v.empty()) cudaMemcpy(p, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice);
@@ -159,7 +192,7 @@ double* dev_upload(tb_handle* h, const std::vector<double>& v) {
 
 int validate(const tb_problem_desc* d) {
     if (!d) { set_error("null problem description"); return TB_ERR_BAD_DESC; }
-    if (d->n_bands <= 0 || d->n_bands > TB_MAX_BANDS) { set_error("n_bands must be 1..8"); return TB_ERR_BAD_DESC; }
+    if (d->n_bands <= 0) { set_error("n_bands must be > 0"); return TB_ERR_BAD_DESC; }
     if (d->n_meshes <= 0) { set_error("n_meshes must be > 0"); return TB_ERR_BAD_DESC; }
     for (int i = 0; i < d->n_meshes; ++i)
         if (d->meshes[i].nsplit[0] <= 0 || d->meshes[i].nsplit[1] <= 0) {
@@ -210,62 +243,136 @@ int validate(const tb_problem_desc* d) {
     return TB_OK;
 }
 
-int build(tb_handle* h, const tb_problem_desc* d) {
-    TB_TRY(validate(d));
-    for (int i = 0; i < d->n_meshes; ++i) h->meshes.push_back(make_mesh(d->region, d->meshes[i]));
-    int64_t off = 0;
-    h->bandsdev.nb = d->n_bands;
-    int maxne = 1;
+// Bytes that decide the structure of a run: region, meshes, band dispersions
+// and statistics, channel definitions, Monte-Carlo tables and supplied tuple
+// lists.  Runs with equal keys share tuple lists and moment tensors;
+// amplitudes, tolerances, constraints, drift and states may differ.
+std::string structure_key(const tb_problem_desc* d) {
+    std::string k;
+    auto put = [&](const void* p, size_t n) { k.append(static_cast<const char*>(p), n); };
+    put(&d->region, sizeof(tb_region));
+    put(&d->n_meshes, sizeof(int32_t));
+    for (int i = 0; i < d->n_meshes; ++i) put(&d->meshes[i], sizeof(tb_mesh_desc));
+    put(&d->n_bands, sizeof(int32_t));
     for (int b = 0; b < d->n_bands; ++b) {
         const tb_band_desc& bd = d->bands[b];
-        const HostMesh& m = h->meshes[bd.mesh];
-        HostBand B;
-        B.mesh = bd.mesh;
-        B.ne = m.ne;
-        B.off = off;
-        B.charge = bd.charge;
-        B.stat = bd.statistics;
-        B.abs_tol = bd.abs_tol;
-        B.rel_tol = bd.rel_tol;
-        B.penal = bd.penalisation;
-        B.constrained = bd.constrained;
-        B.vel[0] = bd.drift_velocity[0];
-        B.vel[1] = bd.drift_velocity[1];
-        B.disp.assign(bd.dispersion, bd.dispersion + size_t(m.ne) * 3);
-        B.kx = coord_function(m, 0);
-        B.ky = coord_function(m, 1);
-        B.minE.resize(m.ne);
-        B.maxE.resize(m.ne);
-        for (int e = 0; e < m.ne; ++e) {
-            const double n0 = B.disp[3 * e], n1 = B.disp[3 * e + 1] + n0, n2 = B.disp[3 * e + 2] + n0;
-            B.minE[e] = std::min(n0, std::min(n1, n2));
-            B.maxE[e] = std::max(n0, std::max(n1, n2));
+        put(&bd.mesh, sizeof(int32_t));
+        put(&bd.statistics, sizeof(double));
+        const tb_mesh_desc& md = d->meshes[bd.mesh];
+        put(bd.dispersion, sizeof(double) * size_t(2 * md.nsplit[0] * md.nsplit[1]) * 3);
+    }
+    put(&d->n_channels, sizeof(int32_t));
+    for (int c = 0; c < d->n_channels; ++c) {
+        const tb_channel_desc& cd = d->channels[c];
+        put(&cd.nlegs, sizeof(int32_t));
+        put(cd.band, sizeof(cd.band));
+        put(cd.dir, sizeof(cd.dir));
+        put(&cd.n_mc, sizeof(int32_t));
+        put(&cd.min_det, sizeof(double));
+        put(&cd.threshold, sizeof(double));
+        put(&cd.n_umklapp, sizeof(int32_t));
+        put(cd.umklapp, sizeof(double) * 2 * size_t(cd.n_umklapp));
+        const int R = 2 * (cd.nlegs - 2) + 1;
+        put(cd.mc_points, sizeof(double) * size_t(cd.n_mc) * R);
+        const double* pre = cd.mc_points_precalc ? cd.mc_points_precalc : cd.mc_points;
+        put(pre, sizeof(double) * size_t(cd.n_mc) * R);
+        put(&cd.n_tuples, sizeof(int64_t));
+        if (cd.n_tuples > 0) {
+            put(cd.tuples, sizeof(int32_t) * size_t(cd.n_tuples) * cd.nlegs);
+            put(cd.tuple_umklapp, sizeof(int32_t) * size_t(cd.n_tuples));
         }
-        if (B.constrained) B.cpop.assign(bd.constrained_population, bd.constrained_population + size_t(m.ne) * 3);
-        off += int64_t(m.ne) * 3;
-        maxne = std::max(maxne, m.ne);
-        h->bands.push_back(std::move(B));
+    }
+    return k;
+}
+
+double amp_full_of(tb_handle* h, const ChanInst& ci, int L, double amplitude) {
+    double af = amplitude;   // constructAmplitude order: amplitude * prod_l (vol_l * 2)
+    for (int l = 0; l < L; ++l) af *= h->meshes[h->bands[ci.band[l]].mesh].vol * 2.0;
+    return af;
+}
+
+int build_runs(tb_handle* h, const tb_problem_desc* const* descs, int nruns) {
+    if (nruns <= 0) { set_error("at least one run is needed"); return TB_ERR_ARG; }
+    for (int r = 0; r < nruns; ++r) TB_TRY(validate(descs[r]));
+    std::vector<std::string> keys(nruns);
+    std::vector<int> group_of_run(nruns, -1), group_first_run;
+    int64_t off = 0;
+    for (int r = 0; r < nruns; ++r) {
+        const tb_problem_desc* d = descs[r];
+        RunInfo ri;
+        ri.band0 = int(h->bands.size());
+        ri.nbands = d->n_bands;
+        ri.dof_off = off;
+        const int mesh0 = int(h->meshes.size());
+        for (int i = 0; i < d->n_meshes; ++i) h->meshes.push_back(make_mesh(d->region, d->meshes[i]));
+        for (int b = 0; b < d->n_bands; ++b) {
+            const tb_band_desc& bd = d->bands[b];
+            const HostMesh& m = h->meshes[mesh0 + bd.mesh];
+            HostBand B;
+            B.mesh = mesh0 + bd.mesh;
+            B.ne = m.ne;
+            B.off = off;
+            B.charge = bd.charge;
+            B.stat = bd.statistics;
+            B.abs_tol = bd.abs_tol;
+            B.rel_tol = bd.rel_tol;
+            B.penal = bd.penalisation;
+            B.constrained = bd.constrained;
+            B.vel[0] = bd.drift_velocity[0];
+            B.vel[1] = bd.drift_velocity[1];
+            B.disp.assign(bd.dispersion, bd.dispersion + size_t(m.ne) * 3);
+            if (B.constrained) B.cpop.assign(bd.constrained_population, bd.constrained_population + size_t(m.ne) * 3);
+            off += int64_t(m.ne) * 3;
+            h->bands.push_back(std::move(B));
+        }
+        ri.ndofs = off - ri.dof_off;
+        ri.chan0 = int(h->insts.size());
+        ri.nchans = d->n_channels;
+        h->runs.push_back(ri);
+        keys[r] = structure_key(d);
+        for (int q = 0; q < int(group_first_run.size()); ++q)
+            if (keys[group_first_run[q]] == keys[r]) { group_of_run[r] = q; break; }
+        if (group_of_run[r] < 0) {
+            group_of_run[r] = int(group_first_run.size());
+            group_first_run.push_back(r);
+        }
+        for (int c = 0; c < d->n_channels; ++c) h->insts.emplace_back();
     }
     h->ndofs = off;
-    h->nblk = (maxne + 255) / 256;
-    h->bandsdev.ndofs = off;
-    // device band tables
-    std::vector<const double*> d_disp(d->n_bands), d_kx(d->n_bands), d_ky(d->n_bands), d_minE(d->n_bands),
-        d_maxE(d->n_bands);
-    for (int b = 0; b < d->n_bands; ++b) {
+    // per-band device tables (every band its own; equal-structure runs read
+    // their group's first-run tables inside the channel kernels)
+    const int nb = int(h->bands.size());
+    std::vector<const double*> d_disp(nb), d_kx(nb), d_ky(nb), d_minE(nb), d_maxE(nb);
+    h->banddev.resize(nb);
+    for (int b = 0; b < nb; ++b) {
         HostBand& B = h->bands[b];
-        d_disp[b] = dev_upload(h, B.disp);
-        d_kx[b] = dev_upload(h, B.kx);
-        d_ky[b] = dev_upload(h, B.ky);
-        d_minE[b] = dev_upload(h, B.minE);
-        d_maxE[b] = dev_upload(h, B.maxE);
-        const double* d_cpop = B.constrained ? dev_upload(h, B.cpop) : nullptr;
-        if (!d_disp[b] || !d_kx[b] || !d_ky[b] || !d_minE[b] || !d_maxE[b] || (B.constrained && !d_cpop)) {
-            set_error("band table allocation failed");
-            return TB_ERR_OOM;
-        }
-        BandDev& bd = h->bandsdev.b[b];
         const HostMesh& m = h->meshes[B.mesh];
+        const int r = int(std::upper_bound(h->runs.begin(), h->runs.end(), b,
+                                           [](int x, const RunInfo& ri) { return x < ri.band0; }) - h->runs.begin()) - 1;
+        const bool first_of_group = group_first_run[group_of_run[r]] == r;
+        if (first_of_group) {
+            B.kx = coord_function(m, 0);
+            B.ky = coord_function(m, 1);
+            B.minE.resize(m.ne);
+            B.maxE.resize(m.ne);
+            for (int e = 0; e < m.ne; ++e) {
+                const double n0 = B.disp[3 * e], n1 = B.disp[3 * e + 1] + n0, n2 = B.disp[3 * e + 2] + n0;
+                B.minE[e] = std::min(n0, std::min(n1, n2));
+                B.maxE[e] = std::max(n0, std::max(n1, n2));
+            }
+            d_disp[b] = dev_upload(h, B.disp);
+            d_kx[b] = dev_upload(h, B.kx);
+            d_ky[b] = dev_upload(h, B.ky);
+            d_minE[b] = dev_upload(h, B.minE);
+            d_maxE[b] = dev_upload(h, B.maxE);
+            if (!d_disp[b] || !d_kx[b] || !d_ky[b] || !d_minE[b] || !d_maxE[b]) {
+                set_error("band table allocation failed");
+                return TB_ERR_OOM;
+            }
+        }
+        const double* d_cpop = B.constrained ? dev_upload(h, B.cpop) : nullptr;
+        if (B.constrained && !d_cpop) { set_error("band table allocation failed"); return TB_ERR_OOM; }
+        BandDev& bd = h->banddev[b];
         bd.mesh.nx = m.nx; bd.mesh.ny = m.ny; bd.mesh.ne = m.ne;
         for (int i = 0; i < 2; ++i)
             for (int j = 0; j < 2; ++j) bd.mesh.dG[i][j] = m.dG[i][j];
@@ -284,76 +391,143 @@ int build(tb_handle* h, const tb_problem_desc* d) {
         bd.cpop = d_cpop;
         bd.vel[0] = B.vel[0];
         bd.vel[1] = B.vel[1];
+        if (B.vel[0] != 0.0 || B.vel[1] != 0.0) h->any_drift = true;
+    }
+    // element blocks
+    std::vector<int> blk_first(nb + 1, 0), blk_band, band_run(nb);
+    for (int b = 0; b < nb; ++b) {
+        const int nblk = (h->bands[b].ne + 255) / 256;
+        blk_first[b + 1] = blk_first[b] + nblk;
+        for (int k = 0; k < nblk; ++k) blk_band.push_back(b);
+    }
+    for (int r = 0; r < nruns; ++r)
+        for (int b = h->runs[r].band0; b < h->runs[r].band0 + h->runs[r].nbands; ++b) band_run[b] = r;
+    h->ed.bands = dev_upload_raw(h, h->banddev.data(), h->banddev.size());
+    h->ed.band_run = dev_upload_raw(h, band_run.data(), band_run.size());
+    h->ed.blk_band = dev_upload_raw(h, blk_band.data(), blk_band.size());
+    h->ed.blk_first = dev_upload_raw(h, blk_first.data(), blk_first.size());
+    h->ed.nb = nb;
+    h->ed.nblk = blk_first[nb];
+    h->ed.ndofs = h->ndofs;
+    if (!h->ed.bands || !h->ed.band_run || !h->ed.blk_band || !h->ed.blk_first) {
+        set_error("element table allocation failed");
+        return TB_ERR_OOM;
+    }
+    h->hruns.resize(nruns);
+    for (int r = 0; r < nruns; ++r) {
+        RunDev& rd = h->hruns[r];
+        rd.band0 = h->runs[r].band0;
+        rd.nbands = h->runs[r].nbands;
+        rd.blk0 = blk_first[rd.band0];
+        rd.blk1 = blk_first[rd.band0 + rd.nbands];
+        rd.dof_off = h->runs[r].dof_off;
+        rd.ndofs = h->runs[r].ndofs;
+        rd.dense_off = 0;
+        rd.dense_t_off = 0;
     }
     // state scratch
     h->d_f = dev_alloc(h, size_t(h->ndofs));
     h->d_out = dev_alloc(h, size_t(h->ndofs));
     h->d_acc = dev_alloc(h, size_t(h->ndofs));
-    h->d_part = dev_alloc(h, size_t(2 * TB_MAX_BANDS * h->nblk + 8));
+    h->d_part = dev_alloc(h, size_t(2 * h->ed.nblk + 8));
     if (!h->d_f || !h->d_out || !h->d_acc || !h->d_part) { set_error("state allocation failed"); return TB_ERR_OOM; }
     TB_CUDA(cudaMemsetAsync(h->d_acc, 0, sizeof(double) * size_t(h->ndofs), h->stream));
-    // channels
-    h->chans.resize(d->n_channels);
-    for (int ci = 0; ci < d->n_channels; ++ci) {
-        const tb_channel_desc& cd = d->channels[ci];
-        Channel& C = h->chans[ci];
-        C.L = cd.nlegs;
-        C.amplitude = cd.amplitude;
-        ChanDev& c = C.dev;
-        c.L = cd.nlegs;
-        c.nmc = cd.n_mc;
-        c.R = 2 * (cd.nlegs - 2) + 1;
-        c.n_umk = cd.n_umklapp;
-        double av = 1.0;
-        for (int l = 0; l < C.L; ++l) {
-            C.band[l] = cd.band[l];
-            const HostBand& B = h->bands[cd.band[l]];
-            LegDev& lg = c.leg[l];
-            lg.disp = d_disp[cd.band[l]];
-            lg.kx = d_kx[cd.band[l]];
-            lg.ky = d_ky[cd.band[l]];
-            lg.foff = B.off;
-            lg.dir = double(cd.dir[l]);
-            lg.stat = B.stat;
-            lg.ne = B.ne;
-            av *= h->meshes[B.mesh].vol * 2.0;
-        }
-        c.amp_vol = av;
-        double af = C.amplitude;
-        for (int l = 0; l < C.L; ++l) af *= h->meshes[h->bands[cd.band[l]].mesh].vol * 2.0;
-        C.amp_full = af;
-        c.fact = 1.0;
-        for (int i = 0; i < C.L - 2; ++i) c.fact *= 2.0;
-        c.min_det = cd.min_det;
-        c.threshold = cd.threshold;
-        for (int i = 0; i < 4; ++i) c.gvec[i] = d->region.gvec[i];
-        C.d_umk = dev_upload(h, std::vector<double>(cd.umklapp, cd.umklapp + 2 * size_t(cd.n_umklapp)));
-        C.d_mc = dev_upload(h, std::vector<double>(cd.mc_points, cd.mc_points + size_t(cd.n_mc) * c.R));
-        const double* pre = cd.mc_points_precalc ? cd.mc_points_precalc : cd.mc_points;
-        C.d_mc_pre = dev_upload(h, std::vector<double>(pre, pre + size_t(cd.n_mc) * c.R));
-        if (!C.d_umk || !C.d_mc || !C.d_mc_pre) { set_error("channel table allocation failed"); return TB_ERR_OOM; }
-        c.umk = C.d_umk;
-        c.mc = C.d_mc;
-        if (cd.n_tuples > 0) {
-            TB_TRY(C.tup.reserve(C.L, cd.n_tuples, h->stream));
-            std::vector<int32_t> soa(size_t(C.L + 1) * size_t(cd.n_tuples));
-            for (int64_t i = 0; i < cd.n_tuples; ++i) {
-                for (int l = 0; l < C.L; ++l) soa[size_t(l) * cd.n_tuples + i] = cd.tuples[i * C.L + l];
-                soa[size_t(C.L) * cd.n_tuples + i] = cd.tuple_umklapp[i];
+    // channel groups and instances
+    std::vector<int> group_chan0(group_first_run.size(), -1);
+    for (int r = 0; r < nruns; ++r) {
+        const tb_problem_desc* d = descs[r];
+        const int g = group_of_run[r];
+        const RunInfo& ri = h->runs[r];
+        if (group_first_run[g] == r) {
+            group_chan0[g] = int(h->groups.size());
+            for (int ci = 0; ci < d->n_channels; ++ci) {
+                const tb_channel_desc& cd = d->channels[ci];
+                h->groups.emplace_back();
+                GroupChan& G = h->groups.back();
+                G.L = cd.nlegs;
+                ChanDev& c = G.dev;
+                c.L = cd.nlegs;
+                c.nmc = cd.n_mc;
+                c.R = 2 * (cd.nlegs - 2) + 1;
+                c.n_umk = cd.n_umklapp;
+                double av = 1.0;
+                for (int l = 0; l < G.L; ++l) {
+                    const int gb = ri.band0 + cd.band[l];
+                    const HostBand& B = h->bands[gb];
+                    LegDev& lg = c.leg[l];
+                    lg.disp = d_disp[gb];
+                    lg.kx = d_kx[gb];
+                    lg.ky = d_ky[gb];
+                    lg.foff = B.off;
+                    lg.dir = double(cd.dir[l]);
+                    lg.stat = B.stat;
+                    lg.ne = B.ne;
+                    av *= h->meshes[B.mesh].vol * 2.0;
+                }
+                c.amp_vol = av;
+                c.fact = 1.0;
+                for (int i = 0; i < G.L - 2; ++i) c.fact *= 2.0;
+                c.min_det = cd.min_det;
+                c.threshold = cd.threshold;
+                for (int i = 0; i < 4; ++i) c.gvec[i] = d->region.gvec[i];
+                G.d_umk = dev_upload(h, std::vector<double>(cd.umklapp, cd.umklapp + 2 * size_t(cd.n_umklapp)));
+                G.d_mc = dev_upload(h, std::vector<double>(cd.mc_points, cd.mc_points + size_t(cd.n_mc) * c.R));
+                const double* pre = cd.mc_points_precalc ? cd.mc_points_precalc : cd.mc_points;
+                G.d_mc_pre = dev_upload(h, std::vector<double>(pre, pre + size_t(cd.n_mc) * c.R));
+                if (!G.d_umk || !G.d_mc || !G.d_mc_pre) { set_error("channel table allocation failed"); return TB_ERR_OOM; }
+                c.umk = G.d_umk;
+                c.mc = G.d_mc;
+                if (cd.n_tuples > 0) {
+                    TB_TRY(G.tup.reserve(G.L, cd.n_tuples, h->stream));
+                    std::vector<int32_t> soa(size_t(G.L + 1) * size_t(cd.n_tuples));
+                    for (int64_t i = 0; i < cd.n_tuples; ++i) {
+                        for (int l = 0; l < G.L; ++l) soa[size_t(l) * cd.n_tuples + i] = cd.tuples[i * G.L + l];
+                        soa[size_t(G.L) * cd.n_tuples + i] = cd.tuple_umklapp[i];
+                    }
+                    TB_CUDA(cudaMemcpy(G.tup.d, soa.data(), sizeof(int32_t) * soa.size(), cudaMemcpyHostToDevice));
+                    G.tup.n = cd.n_tuples;
+                    G.diag[0] = G.diag[1] = G.diag[2] = -1;
+                } else {
+                    int legband[TB_MAX_LEGS];
+                    const double* mins[TB_MAX_LEGS];
+                    const double* maxs[TB_MAX_LEGS];
+                    for (int l = 0; l < G.L; ++l) {
+                        legband[l] = ri.band0 + cd.band[l];
+                        mins[l] = d_minE[legband[l]];
+                        maxs[l] = d_maxE[legband[l]];
+                    }
+                    TB_TRY(enumerate_channel(c, h->meshes.data(), h->bands.data(), legband, G.d_mc_pre, mins, maxs,
+                                             h->stream, G.tup, G.diag));
+                }
             }
-            TB_CUDA(cudaMemcpy(C.tup.d, soa.data(), sizeof(int32_t) * soa.size(), cudaMemcpyHostToDevice));
-            C.tup.n = cd.n_tuples;
-            C.diag[0] = C.diag[1] = C.diag[2] = -1;
-        } else {
-            int legband[TB_MAX_LEGS];
-            const double* mins[TB_MAX_LEGS];
-            const double* maxs[TB_MAX_LEGS];
-            for (int l = 0; l < C.L; ++l) { legband[l] = cd.band[l]; mins[l] = d_minE[cd.band[l]]; maxs[l] = d_maxE[cd.band[l]]; }
-            TB_TRY(enumerate_channel(c, h->meshes.data(), h->bands.data(), legband, C.d_mc_pre, mins, maxs, h->stream,
-                                     C.tup, C.diag));
+        }
+        for (int ci = 0; ci < d->n_channels; ++ci) {
+            const tb_channel_desc& cd = d->channels[ci];
+            const int id = ri.chan0 + ci;
+            ChanInst& I = h->insts[id];
+            I.group = group_chan0[g] + ci;
+            I.run = r;
+            for (int l = 0; l < cd.nlegs; ++l) I.band[l] = ri.band0 + cd.band[l];
+            I.amplitude = cd.amplitude;
+            I.dev.run = r;
+            for (int l = 0; l < TB_MAX_LEGS; ++l) I.dev.foff[l] = (l < cd.nlegs) ? h->bands[I.band[l]].off : 0;
+            I.dev.amplitude = cd.amplitude;
+            I.dev.amp_full = amp_full_of(h, I, cd.nlegs, cd.amplitude);
+            GroupChan& G = h->groups[I.group];
+            I.slot = int(G.insts.size());
+            G.insts.push_back(id);
         }
     }
-    // layouts (and moment tensors)
+    for (auto& G : h->groups) {
+        std::vector<InstDev> v;
+        for (int id : G.insts) v.push_back(h->insts[id].dev);
+        G.d_insts = dev_upload_raw(h, v.data(), v.size());
+        if (!G.d_insts) { set_error("instance table allocation failed"); return TB_ERR_OOM; }
+    }
+    for (auto& I : h->insts) {
+        I.d_single = dev_upload_raw(h, &I.dev, 1);
+        if (!I.d_single) { set_error("instance table allocation failed"); return TB_ERR_OOM; }
+    }
     TB_TRY(choose_layouts(h));
     TB_CUDA(cudaStreamSynchronize(h->stream));
     return TB_OK;
@@ -363,48 +537,57 @@ int build(tb_handle* h, const tb_problem_desc* d) {
 
 // The RHS accumulation (pre-M^-1) of the input state into acc (which must be zero).
 namespace tb {
-int run_rhs_acc(tb_handle* h, const double* d_in, double* d_acc, const int* done, int flags, int only_channel) {
+int run_rhs_acc(tb_handle* h, const double* d_in, double* d_acc, const DPCtl* ctl, int flags, int only_inst) {
     if (!(flags & TB_NO_COLLISIONS)) {
-        for (size_t ci = 0; ci < h->chans.size(); ++ci) {
-            if (only_channel >= 0 && int(ci) != only_channel) continue;
-            Channel& C = h->chans[ci];
-            if (C.amplitude == 0.0 || C.tup.n == 0) continue;
-            if (C.layout == TB_LAYOUT_MC64) {
-                TB_TRY(launch_collision_mc(C.dev, C.amp_full, C.tup.d, C.tup.cap, C.tup.n, d_in, d_acc, done,
+        for (size_t gi = 0; gi < h->groups.size(); ++gi) {
+            GroupChan& G = h->groups[gi];
+            if (G.tup.n == 0) continue;
+            const InstDev* insts = G.d_insts;
+            int n_insts = int(G.insts.size());
+            if (only_inst >= 0) {
+                if (h->insts[only_inst].group != int(gi)) continue;
+                insts = h->insts[only_inst].d_single;
+                n_insts = 1;
+            } else {
+                bool any = false;
+                for (int id : G.insts) any |= h->insts[id].amplitude != 0.0;
+                if (!any) continue;
+            }
+            if (G.layout == TB_LAYOUT_MC64) {
+                TB_TRY(launch_collision_mc(G.dev, insts, n_insts, G.tup.d, G.tup.cap, G.tup.n, d_in, d_acc, ctl,
                                            h->stream, 148 * 32));
             } else {
-                TB_TRY(launch_collision_tensor(C.dev, C.amplitude, C.tensor, C.tup.d, C.tup.cap, C.tup.n, d_in, d_acc,
-                                               done, h->stream));
+                TB_TRY(launch_collision_tensor(G.dev, insts, n_insts, G.tensor, G.tup.d, G.tup.cap, G.tup.n, d_in,
+                                               d_acc, ctl, h->stream));
             }
         }
     }
-    if (!(flags & TB_NO_DRIFT) && only_channel < 0) TB_TRY(launch_drift(h->bandsdev, d_in, d_acc, done, h->stream));
+    if (!(flags & TB_NO_DRIFT) && only_inst < 0 && h->any_drift) TB_TRY(launch_drift(h->ed, d_in, d_acc, ctl, h->stream));
     return TB_OK;
 }
 
 int choose_layouts(tb_handle* h) {
-    // Budget for precomputed tensors
     size_t freeb = 0, totalb = 0;
     cudaMemGetInfo(&freeb, &totalb);
     int64_t budget = h->opts.tensor_budget_bytes > 0 ? h->opts.tensor_budget_bytes : int64_t(double(freeb) * 0.6);
-    for (auto& C : h->chans) {
+    for (auto& G : h->groups) {
         int want = h->opts.layout;
         if (want == TB_LAYOUT_AUTO) {
             // L = 3 and L = 2 tensors are cheaper per tuple than the Monte-Carlo
             // evaluation (HBM-bound contraction vs FP64-bound quadrature);
             // for L = 4 the 405-moment tensor costs more bytes than the
             // quadrature costs FP64 cycles on B200.
-            if (C.L <= 3) want = h->opts.allow_fp32 ? TB_LAYOUT_T32 : TB_LAYOUT_T64;
+            if (G.L <= 3) want = h->opts.allow_fp32 ? TB_LAYOUT_T32 : TB_LAYOUT_T64;
             else want = TB_LAYOUT_MC64;
         }
         if (want == TB_LAYOUT_T32 || want == TB_LAYOUT_T64) {
-            const int64_t bytes = tensor_bytes(C.L, want == TB_LAYOUT_T32, C.tup.n);
-            if (C.tup.n == 0 || bytes > budget) want = TB_LAYOUT_MC64;
+            const int64_t bytes = tensor_bytes(G.L, want == TB_LAYOUT_T32, G.tup.n);
+            if (G.tup.n == 0 || bytes > budget) want = TB_LAYOUT_MC64;
             else budget -= bytes;
         }
-        C.layout = want;
-        if (want != TB_LAYOUT_MC64) TB_TRY(build_tensor(C.dev, C.tup.d, C.tup.cap, C.tup.n, want == TB_LAYOUT_T32,
-                                                        C.tensor, h->stream));
+        G.layout = want;
+        if (want != TB_LAYOUT_MC64)
+            TB_TRY(build_tensor(G.dev, G.tup.d, G.tup.cap, G.tup.n, want == TB_LAYOUT_T32, G.tensor, h->stream));
     }
     return TB_OK;
 }
@@ -414,6 +597,7 @@ int choose_layouts(tb_handle* h) {
 namespace {
 
 int dp_alloc(tb_handle* h, int64_t max_dense) {
+    const int nruns = int(h->runs.size());
     if (!h->dp_ready) {
         DPBufs& B = h->dp;
         const size_t n = size_t(h->ndofs);
@@ -422,13 +606,17 @@ int dp_alloc(tb_handle* h, int64_t max_dense) {
         B.y5 = dev_alloc(h, n);
         for (int i = 0; i < 7; ++i) B.k[i] = dev_alloc(h, n);
         B.acc = h->d_acc;
-        B.part = dev_alloc(h, size_t(2 * TB_MAX_BANDS * h->nblk + 8));
-        B.nblk = h->nblk;
+        B.part = dev_alloc(h, size_t(2 * h->ed.nblk + 8));
+        B.nblk = h->ed.nblk;
+        B.nruns = nruns;
         DPCtl* c = nullptr;
-        if (cudaMalloc(&c, sizeof(DPCtl)) != cudaSuccess) { set_error("controller allocation failed"); return TB_ERR_OOM; }
+        if (cudaMalloc(&c, sizeof(DPCtl) * nruns) != cudaSuccess) { set_error("controller allocation failed"); return TB_ERR_OOM; }
         B.ctl = c;
-        h->dev_allocs.push_back(reinterpret_cast<double*>(c));
-        if (cudaMallocHost(&h->h_ctl, sizeof(DPCtl)) != cudaSuccess) { set_error("pinned allocation failed"); return TB_ERR_OOM; }
+        h->dev_raw.push_back(c);
+        if (cudaMallocHost(&h->h_ctl, sizeof(DPCtl) * nruns) != cudaSuccess) {
+            set_error("pinned allocation failed");
+            return TB_ERR_OOM;
+        }
         for (int i = 0; i < 7; ++i)
             if (!B.k[i]) { set_error("stage allocation failed"); return TB_ERR_OOM; }
         if (!B.y || !B.tmp || !B.y5 || !B.part) { set_error("stage allocation failed"); return TB_ERR_OOM; }
@@ -436,17 +624,31 @@ int dp_alloc(tb_handle* h, int64_t max_dense) {
         B.dense_t = nullptr;
         h->dp_ready = true;
     }
-    if (max_dense > h->dense_cap_alloc) {
+    if (max_dense > h->dense_cap_alloc || !h->d_runs) {
         // (re)allocate the dense buffers; invalidates the captured graph
         DPBufs& B = h->dp;
         if (B.dense) { cudaFree(B.dense); B.dense = nullptr; }
         if (B.dense_t) { cudaFree(B.dense_t); B.dense_t = nullptr; }
         const int64_t cap = std::max<int64_t>(max_dense, 1);
-        if (cudaMalloc(&B.dense, sizeof(double) * size_t(cap) * size_t(h->ndofs)) != cudaSuccess ||
-            cudaMalloc(&B.dense_t, sizeof(double) * size_t(cap)) != cudaSuccess) {
+        int64_t doff = 0, toff = 0;
+        for (int r = 0; r < nruns; ++r) {
+            h->hruns[r].dense_off = doff;
+            h->hruns[r].dense_t_off = toff;
+            doff += cap * h->hruns[r].ndofs;
+            toff += cap;
+        }
+        if (cudaMalloc(&B.dense, sizeof(double) * size_t(doff)) != cudaSuccess ||
+            cudaMalloc(&B.dense_t, sizeof(double) * size_t(toff)) != cudaSuccess) {
             set_error("dense output allocation failed");
             return TB_ERR_OOM;
         }
+        if (!h->d_runs) {
+            h->d_runs = dev_upload_raw(h, h->hruns.data(), h->hruns.size());
+            if (!h->d_runs) { set_error("run table allocation failed"); return TB_ERR_OOM; }
+        } else {
+            TB_CUDA(cudaMemcpy(h->d_runs, h->hruns.data(), sizeof(RunDev) * h->hruns.size(), cudaMemcpyHostToDevice));
+        }
+        B.runs = h->d_runs;
         h->dense_cap_alloc = cap;
         if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
     }
@@ -455,16 +657,15 @@ int dp_alloc(tb_handle* h, int64_t max_dense) {
 
 int record_attempt(tb_handle* h, int flags) {
     const DPBufs& B = h->dp;
-    const int* done = &B.ctl->done;
-    TB_TRY(launch_stage(h->bandsdev, B, 0, h->stream));
+    TB_TRY(launch_stage(h->ed, B, 0, h->stream));
     for (int s = 1; s <= 5; ++s) {
-        TB_TRY(run_rhs_acc(h, B.tmp, B.acc, done, flags, -1));
-        TB_TRY(launch_stage(h->bandsdev, B, s, h->stream));
+        TB_TRY(run_rhs_acc(h, B.tmp, B.acc, B.ctl, flags, -1));
+        TB_TRY(launch_stage(h->ed, B, s, h->stream));
     }
-    TB_TRY(run_rhs_acc(h, B.y5, B.acc, done, flags, -1));
-    TB_TRY(launch_stage(h->bandsdev, B, 6, h->stream));
-    TB_TRY(launch_controller(h->bandsdev, B, h->stream));
-    TB_TRY(launch_dense_commit(h->bandsdev, B, h->stream));
+    TB_TRY(run_rhs_acc(h, B.y5, B.acc, B.ctl, flags, -1));
+    TB_TRY(launch_stage(h->ed, B, 6, h->stream));
+    TB_TRY(launch_controller(h->ed, B, h->stream));
+    TB_TRY(launch_dense_commit(h->ed, B, h->stream));
     return TB_OK;
 }
 
@@ -505,8 +706,8 @@ extern "C" {
 
 const char* tb_last_error(void) { return tb::get_error(); }
 
-int tb_create(tb_handle** out, const tb_problem_desc* desc, const tb_options* opts) {
-    if (!out) { set_error("null handle pointer"); return TB_ERR_ARG; }
+int tb_create_batch(tb_handle** out, const tb_problem_desc* const* runs, int n_runs, const tb_options* opts) {
+    if (!out || !runs) { set_error("null argument"); return TB_ERR_ARG; }
     *out = nullptr;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -520,10 +721,15 @@ int tb_create(tb_handle** out, const tb_problem_desc* desc, const tb_options* op
     h->device = h->opts.device;
     TB_CUDA(cudaSetDevice(h->device));
     TB_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-    int rc = build(h.get(), desc);
+    int rc = build_runs(h.get(), runs, n_runs);
     if (rc != TB_OK) { tb_destroy(h.release()); return rc; }
     *out = h.release();
     return TB_OK;
+}
+
+int tb_create(tb_handle** out, const tb_problem_desc* desc, const tb_options* opts) {
+    const tb_problem_desc* one[1] = {desc};
+    return tb_create_batch(out, one, 1, opts);
 }
 
 int tb_destroy(tb_handle* h) {
@@ -531,8 +737,9 @@ int tb_destroy(tb_handle* h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->graph) cudaGraphExecDestroy(h->graph);
-    for (auto& C : h->chans) { C.tup.release(); C.tensor.release(); }
+    for (auto& G : h->groups) { G.tup.release(); G.tensor.release(); }
     for (double* p : h->dev_allocs) cudaFree(p);
+    for (void* p : h->dev_raw) cudaFree(p);
     if (h->dp.dense) cudaFree(h->dp.dense);
     if (h->dp.dense_t) cudaFree(h->dp.dense_t);
     if (h->h_ctl) cudaFreeHost(h->h_ctl);
@@ -548,49 +755,68 @@ int64_t tb_band_offset(const tb_handle* h, int band) {
     return h->bands[band].off;
 }
 
-int tb_num_channels(const tb_handle* h) { return h ? int(h->chans.size()) : -1; }
+int tb_num_runs(const tb_handle* h) { return h ? int(h->runs.size()) : -1; }
+
+int tb_run_info(const tb_handle* h, int run, int64_t* dof_offset, int64_t* ndofs, int32_t* first_band,
+                int32_t* first_channel) {
+    if (!h || run < 0 || run >= int(h->runs.size())) { set_error("run index out of range"); return TB_ERR_ARG; }
+    const RunInfo& r = h->runs[run];
+    if (dof_offset) *dof_offset = r.dof_off;
+    if (ndofs) *ndofs = r.ndofs;
+    if (first_band) *first_band = r.band0;
+    if (first_channel) *first_channel = r.chan0;
+    return TB_OK;
+}
+
+int tb_num_channels(const tb_handle* h) { return h ? int(h->insts.size()) : -1; }
 
 int tb_channel_info(const tb_handle* h, int ch, int64_t* n_tuples, int64_t* n_prefilter, int64_t* n_det,
                     int32_t* layout) {
-    if (!h || ch < 0 || ch >= int(h->chans.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
-    const Channel& C = h->chans[ch];
-    if (n_tuples) *n_tuples = C.tup.n;
-    if (n_prefilter) *n_prefilter = C.diag[0];
-    if (n_det) *n_det = C.diag[1];
-    if (layout) *layout = C.layout;
+    if (!h || ch < 0 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
+    const GroupChan& G = h->groups[h->insts[ch].group];
+    if (n_tuples) *n_tuples = G.tup.n;
+    if (n_prefilter) *n_prefilter = G.diag[0];
+    if (n_det) *n_det = G.diag[1];
+    if (layout) *layout = G.layout;
     return TB_OK;
 }
 
 int tb_get_tuples(const tb_handle* h, int ch, int32_t* ids, int32_t* umk) {
-    if (!h || ch < 0 || ch >= int(h->chans.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
-    const Channel& C = h->chans[ch];
-    const int64_t n = C.tup.n;
+    if (!h || ch < 0 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
+    const GroupChan& G = h->groups[h->insts[ch].group];
+    const int64_t n = G.tup.n;
     if (n == 0) return TB_OK;
-    std::vector<int32_t> soa(size_t(C.L + 1) * size_t(n));
+    std::vector<int32_t> soa(size_t(G.L + 1) * size_t(n));
     cudaSetDevice(h->device);
-    for (int r = 0; r <= C.L; ++r)
-        TB_CUDA(cudaMemcpy(soa.data() + size_t(r) * n, C.tup.d + size_t(r) * C.tup.cap, sizeof(int32_t) * size_t(n),
+    for (int r = 0; r <= G.L; ++r)
+        TB_CUDA(cudaMemcpy(soa.data() + size_t(r) * n, G.tup.d + size_t(r) * G.tup.cap, sizeof(int32_t) * size_t(n),
                            cudaMemcpyDeviceToHost));
     for (int64_t i = 0; i < n; ++i) {
         if (ids)
-            for (int l = 0; l < C.L; ++l) ids[i * C.L + l] = soa[size_t(l) * n + i];
-        if (umk) umk[i] = soa[size_t(C.L) * n + i];
+            for (int l = 0; l < G.L; ++l) ids[i * G.L + l] = soa[size_t(l) * n + i];
+        if (umk) umk[i] = soa[size_t(G.L) * n + i];
     }
     return TB_OK;
 }
 
 int tb_set_amplitude(tb_handle* h, int ch, double amplitude) {
-    if (!h || ch < 0 || ch >= int(h->chans.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
-    Channel& C = h->chans[ch];
-    C.amplitude = amplitude;
-    double af = amplitude;
-    for (int l = 0; l < C.L; ++l) af *= h->meshes[h->bands[C.band[l]].mesh].vol * 2.0;
-    C.amp_full = af;
-    if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }  // amplitudes are baked into the graph
+    if (!h || ch < 0 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
+    TB_CUDA(cudaSetDevice(h->device));
+    ChanInst& I = h->insts[ch];
+    GroupChan& G = h->groups[I.group];
+    I.amplitude = amplitude;
+    I.dev.amplitude = amplitude;
+    I.dev.amp_full = amp_full_of(h, I, G.L, amplitude);
+    // the kernels read instances from device memory, so a captured graph
+    // sees the new value at its next launch
+    TB_CUDA(cudaStreamSynchronize(h->stream));
+    TB_CUDA(cudaMemcpy(G.d_insts + I.slot, &I.dev, sizeof(InstDev), cudaMemcpyHostToDevice));
+    TB_CUDA(cudaMemcpy(I.d_single, &I.dev, sizeof(InstDev), cudaMemcpyHostToDevice));
+    if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }  // channel skip set changes
     return TB_OK;
 }
 
-static int rhs_common(tb_handle* h, const double* f, double* out, int flags, int only_channel) {
+static int rhs_common(tb_handle* h, const double* f, double* out, int flags, int only_inst) {
     if (!h || !f || !out) { set_error("null argument"); return TB_ERR_ARG; }
     TB_CUDA(cudaSetDevice(h->device));
     const size_t bytes = sizeof(double) * size_t(h->ndofs);
@@ -602,8 +828,8 @@ static int rhs_common(tb_handle* h, const double* f, double* out, int flags, int
         d_res = h->d_out;
     }
     TB_CUDA(cudaMemsetAsync(h->d_acc, 0, bytes, h->stream));
-    TB_TRY(run_rhs_acc(h, d_in, h->d_acc, nullptr, flags, only_channel));
-    TB_TRY(launch_inverse_mass(h->bandsdev, h->d_acc, d_res, h->stream));
+    TB_TRY(run_rhs_acc(h, d_in, h->d_acc, nullptr, flags, only_inst));
+    TB_TRY(launch_inverse_mass(h->ed, h->d_acc, d_res, h->stream));
     TB_CUDA(cudaMemsetAsync(h->d_acc, 0, bytes, h->stream));
     if (flags & TB_PTR_HOST) {
         TB_CUDA(cudaMemcpyAsync(out, h->d_out, bytes, cudaMemcpyDeviceToHost, h->stream));
@@ -615,7 +841,7 @@ static int rhs_common(tb_handle* h, const double* f, double* out, int flags, int
 int tb_rhs(tb_handle* h, const double* f, double* dfdt, int flags) { return rhs_common(h, f, dfdt, flags, -1); }
 
 int tb_channel_propagate(tb_handle* h, int ch, const double* f, double* out, int flags) {
-    if (!h || ch < 0 || ch >= int(h->chans.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
+    if (!h || ch < 0 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
     return rhs_common(h, f, out, flags | TB_NO_DRIFT, ch);
 }
 
@@ -630,19 +856,25 @@ int tb_relative_error(tb_handle* h, const double* err, const double* pop, double
         de = h->d_f;
         dp = h->d_out;
     }
-    TB_TRY(launch_error_norm(h->bandsdev, de, dp, h->d_part, h->nblk, h->stream));
-    std::vector<double> part(size_t(2 * h->bandsdev.nb * h->nblk));
+    TB_TRY(launch_error_norm(h->ed, de, dp, h->d_part, h->stream));
+    const int nblk = h->ed.nblk;
+    std::vector<double> part(size_t(2 * nblk));
     TB_CUDA(cudaMemcpyAsync(part.data(), h->d_part, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, h->stream));
     TB_CUDA(cudaStreamSynchronize(h->stream));
-    double errNorm = 0.0;
-    for (int b = 0; b < h->bandsdev.nb; ++b) {
-        const BandDev& bd = h->bandsdev.b[b];
-        double sr = 0.0, sp = 0.0;
-        for (int k = 0; k < h->nblk; ++k) { sr += part[size_t(2 * b) * h->nblk + k]; sp += part[size_t(2 * b + 1) * h->nblk + k]; }
-        const double be = std::sqrt((bd.mesh.vol * sr + bd.penal * (bd.mesh.vol * sp)) / (double(bd.ne) * bd.mesh.vol));
-        if (be >= errNorm) errNorm = be;
+    std::vector<int> first(h->bands.size() + 1, 0);
+    for (size_t b = 0; b < h->bands.size(); ++b) first[b + 1] = first[b] + (h->bands[b].ne + 255) / 256;
+    for (size_t r = 0; r < h->runs.size(); ++r) {
+        double errNorm = 0.0;
+        for (int b = h->runs[r].band0; b < h->runs[r].band0 + h->runs[r].nbands; ++b) {
+            const BandDev& bd = h->banddev[b];
+            double sr = 0.0, sp = 0.0;
+            for (int k = first[b]; k < first[b + 1]; ++k) { sr += part[size_t(k)]; sp += part[size_t(nblk + k)]; }
+            const double be =
+                std::sqrt((bd.mesh.vol * sr + bd.penal * (bd.mesh.vol * sp)) / (double(bd.ne) * bd.mesh.vol));
+            if (be >= errNorm) errNorm = be;
+        }
+        result[r] = errNorm;
     }
-    *result = errNorm;
     return TB_OK;
 }
 
@@ -652,19 +884,21 @@ int tb_apply_constraints(tb_handle* h, double* f, int flags) {
     const size_t bytes = sizeof(double) * size_t(h->ndofs);
     if (flags & TB_PTR_HOST) {
         TB_CUDA(cudaMemcpyAsync(h->d_f, f, bytes, cudaMemcpyHostToDevice, h->stream));
-        TB_TRY(launch_enforce(h->bandsdev, h->d_f, h->d_f, h->stream));
+        TB_TRY(launch_enforce(h->ed, h->d_f, h->d_f, h->stream));
         TB_CUDA(cudaMemcpyAsync(f, h->d_f, bytes, cudaMemcpyDeviceToHost, h->stream));
         TB_CUDA(cudaStreamSynchronize(h->stream));
     } else {
-        TB_TRY(launch_enforce(h->bandsdev, f, f, h->stream));
+        TB_TRY(launch_enforce(h->ed, f, f, h->stream));
     }
     return TB_OK;
 }
 
-int tb_dp45_begin(tb_handle* h, const double* f0, double t0, double t_final, double dense_step, int64_t max_dense,
-                  int flags) {
-    if (!h || !f0) { set_error("null argument"); return TB_ERR_ARG; }
-    if (!(dense_step > 0.0)) { set_error("dense_step must be > 0"); return TB_ERR_ARG; }
+int tb_dp45_begin_batch(tb_handle* h, const double* f0, const double* t0, const double* t_final,
+                        const double* dense_step, int64_t max_dense, int flags) {
+    if (!h || !f0 || !t0 || !t_final || !dense_step) { set_error("null argument"); return TB_ERR_ARG; }
+    const int nruns = int(h->runs.size());
+    for (int r = 0; r < nruns; ++r)
+        if (!(dense_step[r] > 0.0)) { set_error("dense_step must be > 0"); return TB_ERR_ARG; }
     TB_CUDA(cudaSetDevice(h->device));
     TB_TRY(dp_alloc(h, max_dense));
     const int rflags = flags & (TB_NO_DRIFT | TB_NO_COLLISIONS);
@@ -673,28 +907,38 @@ int tb_dp45_begin(tb_handle* h, const double* f0, double t0, double t_final, dou
     DPBufs& B = h->dp;
     TB_CUDA(cudaMemcpyAsync(B.y, f0, bytes, (flags & TB_PTR_HOST) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
                             h->stream));
-    DPCtl c;
-    std::memset(&c, 0, sizeof(c));
-    c.t = t0;
-    c.tf = t_final;
-    c.dense_step = dense_step;
-    c.dense_time = t0 + dense_step;
-    c.min_step = dense_step / 10000.;
-    c.olderror = 1.0;
-    c.dt = dense_step;
-    c.dt = std::min(c.dt, (c.t + c.dt) - c.t);   // timeStepVetoer with no time-dependent constraints
-    c.dense_cap = max_dense;
-    c.rhs_evals = 1;
-    c.done = (t0 < t_final) ? 0 : 1;
-    *h->h_ctl = c;
-    TB_CUDA(cudaMemcpyAsync(B.ctl, h->h_ctl, sizeof(DPCtl), cudaMemcpyHostToDevice, h->stream));
+    TB_CUDA(cudaStreamSynchronize(h->stream));   // the pinned mirror is rewritten below
+    for (int r = 0; r < nruns; ++r) {
+        DPCtl& c = h->h_ctl[r];
+        std::memset(&c, 0, sizeof(c));
+        c.t = t0[r];
+        c.tf = t_final[r];
+        c.dense_step = dense_step[r];
+        c.dense_time = t0[r] + dense_step[r];
+        c.min_step = dense_step[r] / 10000.;
+        c.olderror = 1.0;
+        c.dt = dense_step[r];
+        c.dt = std::min(c.dt, (c.t + c.dt) - c.t);   // timeStepVetoer with no time-dependent constraints
+        c.dense_cap = max_dense;
+        c.rhs_evals = 1;
+        c.done = (t0[r] < t_final[r]) ? 0 : 1;
+    }
+    TB_CUDA(cudaMemcpyAsync(B.ctl, h->h_ctl, sizeof(DPCtl) * nruns, cudaMemcpyHostToDevice, h->stream));
     // k1 = timeOp(t0, enforceValue(t0, y0))
-    TB_TRY(launch_enforce(h->bandsdev, B.y, B.tmp, h->stream));
+    TB_TRY(launch_enforce(h->ed, B.y, B.tmp, h->stream));
     TB_CUDA(cudaMemsetAsync(B.acc, 0, bytes, h->stream));
     TB_TRY(run_rhs_acc(h, B.tmp, B.acc, nullptr, rflags, -1));
-    TB_TRY(launch_k1(h->bandsdev, B, h->stream));
+    TB_TRY(launch_k1(h->ed, B, h->stream));
     TB_TRY(ensure_graph(h, rflags));
     return TB_OK;
+}
+
+int tb_dp45_begin(tb_handle* h, const double* f0, double t0, double t_final, double dense_step, int64_t max_dense,
+                  int flags) {
+    if (!h) { set_error("null handle"); return TB_ERR_ARG; }
+    const size_t nr = h->runs.size();
+    std::vector<double> a(nr, t0), b(nr, t_final), c(nr, dense_step);
+    return tb_dp45_begin_batch(h, f0, a.data(), b.data(), c.data(), max_dense, flags);
 }
 
 int tb_dp45_advance(tb_handle* h, int64_t n_attempts) {
@@ -704,15 +948,32 @@ int tb_dp45_advance(tb_handle* h, int64_t n_attempts) {
     return TB_OK;
 }
 
-int tb_dp45_poll(tb_handle* h, tb_dp45_stats* st) {
+static int poll_all(tb_handle* h) {
     if (!h || !h->dp_ready) { set_error("tb_dp45_begin was not called"); return TB_ERR_ARG; }
     TB_CUDA(cudaSetDevice(h->device));
-    TB_CUDA(cudaMemcpyAsync(h->h_ctl, h->dp.ctl, sizeof(DPCtl), cudaMemcpyDeviceToHost, h->stream));
+    TB_CUDA(cudaMemcpyAsync(h->h_ctl, h->dp.ctl, sizeof(DPCtl) * h->runs.size(), cudaMemcpyDeviceToHost, h->stream));
     TB_CUDA(cudaStreamSynchronize(h->stream));
-    fill_stats(*h->h_ctl, st);
     int tflag = 0;
     TB_TRY(tensor_error_flag(&tflag));
-    if (tflag && st) { st->status = TB_ERR_TIMEOUT; st->done = 1; }
+    if (tflag)
+        for (size_t r = 0; r < h->runs.size(); ++r) { h->h_ctl[r].status = TB_ERR_TIMEOUT; h->h_ctl[r].done = 1; }
+    return TB_OK;
+}
+
+int tb_dp45_poll(tb_handle* h, tb_dp45_stats* st) {
+    TB_TRY(poll_all(h));
+    fill_stats(h->h_ctl[0], st);
+    if (st) {
+        int all_done = 1;
+        for (size_t r = 0; r < h->runs.size(); ++r) all_done &= h->h_ctl[r].done ? 1 : 0;
+        st->done = all_done;
+    }
+    return TB_OK;
+}
+
+int tb_dp45_run_stats(tb_handle* h, int run, tb_dp45_stats* st) {
+    if (!h || !h->dp_ready || run < 0 || run >= int(h->runs.size())) { set_error("bad run index"); return TB_ERR_ARG; }
+    fill_stats(h->h_ctl[run], st);
     return TB_OK;
 }
 
@@ -723,12 +984,26 @@ int tb_dp45_end(tb_handle* h, double* f_out, double* dense_out, double* dense_ti
     const size_t bytes = sizeof(double) * size_t(h->ndofs);
     const cudaMemcpyKind kind = (flags & TB_PTR_HOST) ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     if (f_out) TB_CUDA(cudaMemcpyAsync(f_out, h->dp.y, bytes, kind, h->stream));
-    const int64_t nd = std::min<int64_t>(std::min<int64_t>(s.n_dense, max_dense), h->dense_cap_alloc);
-    if (nd > 0 && dense_out) TB_CUDA(cudaMemcpyAsync(dense_out, h->dp.dense, bytes * size_t(nd), kind, h->stream));
-    if (nd > 0 && dense_times) TB_CUDA(cudaMemcpyAsync(dense_times, h->dp.dense_t, sizeof(double) * size_t(nd), kind, h->stream));
+    // dense outputs: run r's block holds max_dense slots of its own ndofs
+    int64_t uoff = 0, utoff = 0;
+    for (size_t r = 0; r < h->runs.size(); ++r) {
+        const RunDev& rd = h->hruns[r];
+        const int64_t nd = std::min<int64_t>(std::min<int64_t>(h->h_ctl[r].n_dense, max_dense), h->dense_cap_alloc);
+        if (nd > 0 && dense_out)
+            TB_CUDA(cudaMemcpyAsync(dense_out + uoff, h->dp.dense + rd.dense_off, sizeof(double) * size_t(nd * rd.ndofs),
+                                    kind, h->stream));
+        if (nd > 0 && dense_times)
+            TB_CUDA(cudaMemcpyAsync(dense_times + utoff, h->dp.dense_t + rd.dense_t_off, sizeof(double) * size_t(nd),
+                                    kind, h->stream));
+        uoff += max_dense * rd.ndofs;
+        utoff += max_dense;
+    }
     TB_CUDA(cudaStreamSynchronize(h->stream));
     if (st) *st = s;
-    return s.status;
+    int worst = TB_OK;
+    for (size_t r = 0; r < h->runs.size(); ++r)
+        if (h->h_ctl[r].status != TB_OK) { worst = h->h_ctl[r].status; break; }
+    return worst;
 }
 
 int tb_dp45_integrate(tb_handle* h, double* f_inout, double t0, double t_final, double dense_step, double* dense_out,
@@ -756,7 +1031,7 @@ void* tb_get_stream(tb_handle* h) { return h ? (void*)h->stream : nullptr; }
 
 int tb_collision_accumulate(tb_handle* h, int ch, const double* f, double* acc) {
     if (!h || !f || !acc) { set_error("null argument"); return TB_ERR_ARG; }
-    if (ch < -1 || ch >= int(h->chans.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
+    if (ch < -1 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
     TB_CUDA(cudaSetDevice(h->device));
     return run_rhs_acc(h, f, acc, nullptr, TB_NO_DRIFT, ch);
 }

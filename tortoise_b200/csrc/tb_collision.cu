@@ -13,16 +13,17 @@
 //   * the 3L results are scattered with FP64 atomics (RED) into the pre-M^-1
 //     accumulator, which stays L2-resident.
 // The kernel is FP64-FMA bound (about 55 FP64 operations per MC point for L=4).
+#include "tb_dp45.cuh"
 #include "tb_geom.cuh"
 #include "tb_kernels.cuh"
 
 namespace tb {
 
 template <int L>
-__global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, double amp_full, const int32_t* __restrict__ tup,
-                                                      int64_t stride, int64_t n, const double* __restrict__ f,
-                                                      double* __restrict__ acc, const int* __restrict__ done) {
-    if (done && *done) return;
+__global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* __restrict__ insts, int n_insts,
+                                                      const int32_t* __restrict__ tup, int64_t stride, int64_t n,
+                                                      const double* __restrict__ f, double* __restrict__ acc,
+                                                      const DPCtl* __restrict__ ctl) {
     extern __shared__ double s_mc[];
     constexpr int R = 2 * (L - 2) + 1;
     for (int i = threadIdx.x; i < c.nmc * R; i += blockDim.x) s_mc[i] = c.mc[i];
@@ -65,89 +66,94 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, double amp_full
                 mg[r] = 32.0 * 1.1102230246251565e-16 * (sc + fabs(a0[r]) + sg);
             }
         }
-        // commonLinForm0 (A, direct) and commonLinForm1 (B, time reversed),
-        // ScatteringChannel.cpp:633-641
-        double A[L][3], B[L][3];
-#pragma unroll
-        for (int l = 0; l < L; ++l) {
-            const double d = c.leg[l].dir, s = c.leg[l].stat;
-            const double* fe = f + c.leg[l].foff + 3 * (int64_t)e[l];
-            const double ka = (l == 0 ? -1.0 : 1.0) * 0.5;
-            const double ca = (1. - d) * s + (1. + d);
-            const double cb = (1. + d) * s + (1. - d);
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const double unit = (j == 0) ? 1.0 : 0.0;
-                const double fj = __ldg(fe + j);
-                A[l][j] = ka * ((1. - d) * unit + ca * fj);
-                B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
-            }
-        }
-        double s0 = 0.0, sx[L], sy[L];
-#pragma unroll
-        for (int l = 0; l < L; ++l) { sx[l] = 0.0; sy[l] = 0.0; }
-        for (int m = 0; m < c.nmc; ++m) {
-            const double* q = s_mc + m * R;
-            double qv[R];
-#pragma unroll
-            for (int j = 0; j < R; ++j) qv[j] = q[j];
-            double al[3];
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                double t = a0[r];
-#pragma unroll
-                for (int j = 0; j < R; ++j) t = fma(G[r][j], qv[j], t);
-                al[r] = t;
-            }
-            const double kp0 = qv[R - 1];
-            const double tiny = 8.0 * 1.1102230246251565e-16;
-            const bool near = (fabs(al[0]) <= mg[0]) || (fabs(al[1]) <= mg[1]) || (fabs(al[2]) <= mg[2]) ||
-                              (fabs(kp0 + al[0] - 1.0) <= mg[0] + tiny * (2.0 + fabs(al[0]))) ||
-                              (fabs(al[1] + al[2] - 1.0) <= mg[1] + mg[2] + tiny * (1.0 + fabs(al[1]) + fabs(al[2])));
-            if (near) exact_alpha<L>(g, Ci, qv, al);
-            const bool th = theta_of(kp0, al);
-            double px[L], py[L];
-#pragma unroll
-            for (int l = 0; l < L - 2; ++l) { px[l] = qv[2 * l]; py[l] = qv[2 * l + 1]; }
-            px[L - 2] = kp0; py[L - 2] = al[0];
-            px[L - 1] = al[1]; py[L - 1] = al[2];
-            double pa = 1.0, pb = 1.0;
-#pragma unroll
+        for (int k = 0; k < n_insts; ++k) {
+            const InstDev in = insts[k];
+            if (in.amp_full == 0.0) continue;
+            if (ctl && ctl[in.run].done) continue;
+            // commonLinForm0 (A, direct) and commonLinForm1 (B, time reversed),
+            // ScatteringChannel.cpp:633-641
+            double A[L][3], B[L][3];
+    #pragma unroll
             for (int l = 0; l < L; ++l) {
-                pa *= (A[l][1] * px[l] + A[l][2] * py[l]) + A[l][0];
-                pb *= (B[l][1] * px[l] + B[l][2] * py[l]) + B[l][0];
+                const double d = c.leg[l].dir, s = c.leg[l].stat;
+                const double* fe = f + in.foff[l] + 3 * (int64_t)e[l];
+                const double ka = (l == 0 ? -1.0 : 1.0) * 0.5;
+                const double ca = (1. - d) * s + (1. + d);
+                const double cb = (1. + d) * s + (1. - d);
+    #pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const double unit = (j == 0) ? 1.0 : 0.0;
+                    const double fj = __ldg(fe + j);
+                    A[l][j] = ka * ((1. - d) * unit + ca * fj);
+                    B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
+                }
             }
-            const double common = (pa + pb) * (th ? 1.0 : 0.0);
-            s0 += common;
-#pragma unroll
+            double s0 = 0.0, sx[L], sy[L];
+    #pragma unroll
+            for (int l = 0; l < L; ++l) { sx[l] = 0.0; sy[l] = 0.0; }
+            for (int m = 0; m < c.nmc; ++m) {
+                const double* q = s_mc + m * R;
+                double qv[R];
+    #pragma unroll
+                for (int j = 0; j < R; ++j) qv[j] = q[j];
+                double al[3];
+    #pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    double t = a0[r];
+    #pragma unroll
+                    for (int j = 0; j < R; ++j) t = fma(G[r][j], qv[j], t);
+                    al[r] = t;
+                }
+                const double kp0 = qv[R - 1];
+                const double tiny = 8.0 * 1.1102230246251565e-16;
+                const bool near = (fabs(al[0]) <= mg[0]) || (fabs(al[1]) <= mg[1]) || (fabs(al[2]) <= mg[2]) ||
+                                  (fabs(kp0 + al[0] - 1.0) <= mg[0] + tiny * (2.0 + fabs(al[0]))) ||
+                                  (fabs(al[1] + al[2] - 1.0) <= mg[1] + mg[2] + tiny * (1.0 + fabs(al[1]) + fabs(al[2])));
+                if (near) exact_alpha<L>(g, Ci, qv, al);
+                const bool th = theta_of(kp0, al);
+                double px[L], py[L];
+    #pragma unroll
+                for (int l = 0; l < L - 2; ++l) { px[l] = qv[2 * l]; py[l] = qv[2 * l + 1]; }
+                px[L - 2] = kp0; py[L - 2] = al[0];
+                px[L - 1] = al[1]; py[L - 1] = al[2];
+                double pa = 1.0, pb = 1.0;
+    #pragma unroll
+                for (int l = 0; l < L; ++l) {
+                    pa *= (A[l][1] * px[l] + A[l][2] * py[l]) + A[l][0];
+                    pb *= (B[l][1] * px[l] + B[l][2] * py[l]) + B[l][0];
+                }
+                const double common = (pa + pb) * (th ? 1.0 : 0.0);
+                s0 += common;
+    #pragma unroll
+                for (int l = 0; l < L; ++l) {
+                    sx[l] = fma(px[l], common, sx[l]);
+                    sy[l] = fma(py[l], common, sy[l]);
+                }
+            }
+            const double scale = 1.0 / (inv_fact_nmc * fabs(g.det));
+    #pragma unroll
             for (int l = 0; l < L; ++l) {
-                sx[l] = fma(px[l], common, sx[l]);
-                sy[l] = fma(py[l], common, sy[l]);
+                const double d = c.leg[l].dir;
+                double* o = acc + in.foff[l] + 3 * (int64_t)e[l];
+                atomicAdd(o + 0, d * ((scale * s0) * in.amp_full));
+                atomicAdd(o + 1, d * ((scale * sx[l]) * in.amp_full));
+                atomicAdd(o + 2, d * ((scale * sy[l]) * in.amp_full));
             }
-        }
-        const double scale = 1.0 / (inv_fact_nmc * fabs(g.det));
-#pragma unroll
-        for (int l = 0; l < L; ++l) {
-            const double d = c.leg[l].dir;
-            double* o = acc + c.leg[l].foff + 3 * (int64_t)e[l];
-            atomicAdd(o + 0, d * ((scale * s0) * amp_full));
-            atomicAdd(o + 1, d * ((scale * sx[l]) * amp_full));
-            atomicAdd(o + 2, d * ((scale * sy[l]) * amp_full));
         }
     }
 }
 
-int launch_collision_mc(const ChanDev& c, double amp_full, const int32_t* tup, int64_t stride, int64_t n,
-                        const double* f, double* acc, const int* done, cudaStream_t s, int grid_hint) {
-    if (n <= 0) return TB_OK;
+int launch_collision_mc(const ChanDev& c, const InstDev* insts, int n_insts, const int32_t* tup, int64_t stride,
+                        int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s, int grid_hint) {
+    if (n <= 0 || n_insts <= 0) return TB_OK;
     const int threads = 256;
     int64_t blocks = (n + threads - 1) / threads;
     if (grid_hint > 0 && blocks > grid_hint) blocks = grid_hint;
     const size_t smem = sizeof(double) * size_t(c.nmc) * c.R;
     switch (c.L) {
-        case 2: k_collision_mc<2><<<unsigned(blocks), threads, smem, s>>>(c, amp_full, tup, stride, n, f, acc, done); break;
-        case 3: k_collision_mc<3><<<unsigned(blocks), threads, smem, s>>>(c, amp_full, tup, stride, n, f, acc, done); break;
-        case 4: k_collision_mc<4><<<unsigned(blocks), threads, smem, s>>>(c, amp_full, tup, stride, n, f, acc, done); break;
+        case 2: k_collision_mc<2><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, acc, ctl); break;
+        case 3: k_collision_mc<3><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, acc, ctl); break;
+        case 4: k_collision_mc<4><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, acc, ctl); break;
         default: set_error("nlegs must be 2..4"); return TB_ERR_ARG;
     }
     TB_CUDA(cudaGetLastError());
@@ -155,25 +161,20 @@ int launch_collision_mc(const ChanDev& c, double amp_full, const int32_t* tup, i
 }
 
 // ------------------------------------------------------------ inverse mass
-__global__ void k_inverse_mass(BandsDev bands, const double* __restrict__ acc, double* __restrict__ out) {
-    for (int b = 0; b < bands.nb; ++b) {
-        const BandDev& bd = bands.b[b];
-        for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < bd.ne; e += gridDim.x * blockDim.x) {
-            const double* a = acc + bd.off + 3 * (int64_t)e;
-            double* o = out + bd.off + 3 * (int64_t)e;
-            const double x = a[0], y = a[1], z = a[2];
+__global__ void k_inverse_mass(ElemDev ed, const double* __restrict__ acc, double* __restrict__ out) {
+    const int band = ed.blk_band[blockIdx.x];
+    const BandDev& bd = ed.bands[band];
+    const int e = (blockIdx.x - ed.blk_first[band]) * blockDim.x + threadIdx.x;
+    if (e >= bd.ne) return;
+    const double* a = acc + bd.off + 3 * (int64_t)e;
+    double* o = out + bd.off + 3 * (int64_t)e;
+    const double x = a[0], y = a[1], z = a[2];
 #pragma unroll
-            for (int j = 0; j < 3; ++j) o[j] = x * bd.mesh.Minv[0][j] + y * bd.mesh.Minv[1][j] + z * bd.mesh.Minv[2][j];
-        }
-    }
+    for (int j = 0; j < 3; ++j) o[j] = x * bd.mesh.Minv[0][j] + y * bd.mesh.Minv[1][j] + z * bd.mesh.Minv[2][j];
 }
 
-int launch_inverse_mass(const BandsDev& bands, const double* acc, double* out, cudaStream_t s) {
-    int maxne = 1;
-    for (int b = 0; b < bands.nb; ++b) maxne = bands.b[b].ne > maxne ? bands.b[b].ne : maxne;
-    const int threads = 256;
-    const int blocks = (maxne + threads - 1) / threads;
-    k_inverse_mass<<<blocks, threads, 0, s>>>(bands, acc, out);
+int launch_inverse_mass(const ElemDev& ed, const double* acc, double* out, cudaStream_t s) {
+    k_inverse_mass<<<ed.nblk, 256, 0, s>>>(ed, acc, out);
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }

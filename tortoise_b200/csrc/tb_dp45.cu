@@ -44,114 +44,116 @@ __device__ __forceinline__ void enforce3(const BandDev& bd, int e, double v[3]) 
     }
 }
 
-// Element-wise stage kernel (see tb_dp45.cuh for the meaning of s).
+// Element-wise stage kernel (see tb_dp45.cuh for the meaning of s).  One
+// block covers 256 elements of one band, so every block belongs to one run.
 template <int S>
-__global__ void __launch_bounds__(256) k_stage(BandsDev bands, DPBufs B) {
+__global__ void __launch_bounds__(256) k_stage(ElemDev ed, DPBufs B) {
     __shared__ double sh[8];
-    const DPCtl* ctl = B.ctl;
-    if (ctl->done) return;
-    const double dt = ctl->dt;
-    for (int bi = 0; bi < bands.nb; ++bi) {
-        const BandDev& bd = bands.b[bi];
-        double srel = 0.0, spen = 0.0;
-        const int e = blockIdx.x * blockDim.x + threadIdx.x;
-        if (e < bd.ne) {
-            const int64_t o = bd.off + 3 * (int64_t)e;
-            if (S >= 1) {
-                // k_{S+1} = acc * M^-1, acc = 0
-                const double x = B.acc[o], y = B.acc[o + 1], z = B.acc[o + 2];
-                double* kk = B.k[S];
+    const int band = ed.blk_band[blockIdx.x];
+    const DPCtl& ctl = B.ctl[ed.band_run[band]];
+    if (ctl.done) return;
+    const double dt = ctl.dt;
+    const BandDev& bd = ed.bands[band];
+    double srel = 0.0, spen = 0.0;
+    const int e = (blockIdx.x - ed.blk_first[band]) * blockDim.x + threadIdx.x;
+    if (e < bd.ne) {
+        const int64_t o = bd.off + 3 * (int64_t)e;
+        if (S >= 1) {
+            // k_{S+1} = acc * M^-1, acc = 0
+            const double x = B.acc[o], y = B.acc[o + 1], z = B.acc[o + 2];
+            double* kk = B.k[S];
 #pragma unroll
-                for (int j = 0; j < 3; ++j) kk[o + j] = x * bd.mesh.Minv[0][j] + y * bd.mesh.Minv[1][j] + z * bd.mesh.Minv[2][j];
-                B.acc[o] = 0.0; B.acc[o + 1] = 0.0; B.acc[o + 2] = 0.0;
-            }
-            double v[3];
-            if (S <= 4) {
-                // input of k_{S+2}: y + sum_{j<=S} (a_{S+1,j} dt) k_{j+1}
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    double t = B.y[o + c];
-#pragma unroll
-                    for (int j = 0; j <= S; ++j) t = t + (c_A[S + 1][j] * dt) * B.k[j][o + c];
-                    v[c] = t;
-                }
-                enforce3(bd, e, v);
-#pragma unroll
-                for (int c = 0; c < 3; ++c) B.tmp[o + c] = v[c];
-            } else if (S == 5) {
-                // y5 = y + (dt b1) k1 + (dt b3) k3 + (dt b4) k4 + (dt b5) k5 + (dt b6) k6
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    double t = B.y[o + c];
-                    t = t + (dt * c_b[0]) * B.k[0][o + c];
-                    t = t + (dt * c_b[2]) * B.k[2][o + c];
-                    t = t + (dt * c_b[3]) * B.k[3][o + c];
-                    t = t + (dt * c_b[4]) * B.k[4][o + c];
-                    t = t + (dt * c_b[5]) * B.k[5][o + c];
-                    v[c] = t;
-                }
-                enforce3(bd, e, v);
-#pragma unroll
-                for (int c = 0; c < 3; ++c) B.y5[o + c] = v[c];
-            } else {
-                // y4 and the error
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    double t = B.y[o + c];
-                    t = t + (dt * c_bh[0]) * B.k[0][o + c];
-                    t = t + (dt * c_bh[2]) * B.k[2][o + c];
-                    t = t + (dt * c_bh[3]) * B.k[3][o + c];
-                    t = t + (dt * c_bh[4]) * B.k[4][o + c];
-                    t = t + (dt * c_bh[5]) * B.k[5][o + c];
-                    t = t + (dt * c_bh[6]) * B.k[6][o + c];
-                    v[c] = t;
-                }
-                enforce3(bd, e, v);
-                double err[3], p5[3];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) { p5[c] = B.y5[o + c]; err[c] = p5[c] - v[c]; }
-                elem_rel_err(bd, err, p5, srel, spen);
-            }
+            for (int j = 0; j < 3; ++j) kk[o + j] = x * bd.mesh.Minv[0][j] + y * bd.mesh.Minv[1][j] + z * bd.mesh.Minv[2][j];
+            B.acc[o] = 0.0; B.acc[o + 1] = 0.0; B.acc[o + 2] = 0.0;
         }
-        if (S == 6) {
-            const double r = block_sum<256>(srel, sh);
-            const double p = block_sum<256>(spen, sh);
-            if (threadIdx.x == 0) {
-                B.part[(2 * bi) * B.nblk + blockIdx.x] = r;
-                B.part[(2 * bi + 1) * B.nblk + blockIdx.x] = p;
+        double v[3];
+        if (S <= 4) {
+            // input of k_{S+2}: y + sum_{j<=S} (a_{S+1,j} dt) k_{j+1}
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                double t = B.y[o + c];
+#pragma unroll
+                for (int j = 0; j <= S; ++j) t = t + (c_A[S + 1][j] * dt) * B.k[j][o + c];
+                v[c] = t;
             }
+            enforce3(bd, e, v);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) B.tmp[o + c] = v[c];
+        } else if (S == 5) {
+            // y5 = y + (dt b1) k1 + (dt b3) k3 + (dt b4) k4 + (dt b5) k5 + (dt b6) k6
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                double t = B.y[o + c];
+                t = t + (dt * c_b[0]) * B.k[0][o + c];
+                t = t + (dt * c_b[2]) * B.k[2][o + c];
+                t = t + (dt * c_b[3]) * B.k[3][o + c];
+                t = t + (dt * c_b[4]) * B.k[4][o + c];
+                t = t + (dt * c_b[5]) * B.k[5][o + c];
+                v[c] = t;
+            }
+            enforce3(bd, e, v);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) B.y5[o + c] = v[c];
+        } else {
+            // y4 and the error
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                double t = B.y[o + c];
+                t = t + (dt * c_bh[0]) * B.k[0][o + c];
+                t = t + (dt * c_bh[2]) * B.k[2][o + c];
+                t = t + (dt * c_bh[3]) * B.k[3][o + c];
+                t = t + (dt * c_bh[4]) * B.k[4][o + c];
+                t = t + (dt * c_bh[5]) * B.k[5][o + c];
+                t = t + (dt * c_bh[6]) * B.k[6][o + c];
+                v[c] = t;
+            }
+            enforce3(bd, e, v);
+            double err[3], p5[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) { p5[c] = B.y5[o + c]; err[c] = p5[c] - v[c]; }
+            elem_rel_err(bd, err, p5, srel, spen);
+        }
+    }
+    if (S == 6) {
+        const double r = block_sum<256>(srel, sh);
+        const double p = block_sum<256>(spen, sh);
+        if (threadIdx.x == 0) {
+            B.part[blockIdx.x] = r;
+            B.part[B.nblk + blockIdx.x] = p;
         }
     }
 }
 
-int launch_stage(const BandsDev& bands, const DPBufs& B, int s, cudaStream_t st) {
+int launch_stage(const ElemDev& ed, const DPBufs& B, int s, cudaStream_t st) {
     switch (s) {
-        case 0: k_stage<0><<<B.nblk, 256, 0, st>>>(bands, B); break;
-        case 1: k_stage<1><<<B.nblk, 256, 0, st>>>(bands, B); break;
-        case 2: k_stage<2><<<B.nblk, 256, 0, st>>>(bands, B); break;
-        case 3: k_stage<3><<<B.nblk, 256, 0, st>>>(bands, B); break;
-        case 4: k_stage<4><<<B.nblk, 256, 0, st>>>(bands, B); break;
-        case 5: k_stage<5><<<B.nblk, 256, 0, st>>>(bands, B); break;
-        default: k_stage<6><<<B.nblk, 256, 0, st>>>(bands, B); break;
+        case 0: k_stage<0><<<ed.nblk, 256, 0, st>>>(ed, B); break;
+        case 1: k_stage<1><<<ed.nblk, 256, 0, st>>>(ed, B); break;
+        case 2: k_stage<2><<<ed.nblk, 256, 0, st>>>(ed, B); break;
+        case 3: k_stage<3><<<ed.nblk, 256, 0, st>>>(ed, B); break;
+        case 4: k_stage<4><<<ed.nblk, 256, 0, st>>>(ed, B); break;
+        case 5: k_stage<5><<<ed.nblk, 256, 0, st>>>(ed, B); break;
+        default: k_stage<6><<<ed.nblk, 256, 0, st>>>(ed, B); break;
     }
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }
 
-// Single-thread controller: DormandPrince54.hpp:580-661.
-__global__ void k_controller(BandsDev bands, DPBufs B) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    DPCtl* c = B.ctl;
+// Controller, one thread per run: DormandPrince54.hpp:580-661.
+__global__ void k_controller(ElemDev ed, DPBufs B) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= B.nruns) return;
+    DPCtl* c = B.ctl + r;
+    const RunDev& run = B.runs[r];
     if (c->done) { c->skip = 1; return; }
     c->skip = 0;
     c->attempts += 1;
     c->rhs_evals += 6;
     double errNorm = 0.0;
     bool nonfinite = false;
-    for (int bi = 0; bi < bands.nb; ++bi) {
-        const BandDev& bd = bands.b[bi];
+    for (int bi = run.band0; bi < run.band0 + run.nbands; ++bi) {
+        const BandDev& bd = ed.bands[bi];
         double sr = 0.0, sp = 0.0;
-        for (int k = 0; k < B.nblk; ++k) { sr += B.part[(2 * bi) * B.nblk + k]; sp += B.part[(2 * bi + 1) * B.nblk + k]; }
+        for (int k = ed.blk_first[bi]; k < ed.blk_first[bi + 1]; ++k) { sr += B.part[k]; sp += B.part[B.nblk + k]; }
         const double ir = bd.mesh.vol * sr, ip = bd.mesh.vol * sp;
         const double be = sqrt((ir + bd.penal * ip) / (double(bd.ne) * bd.mesh.vol));
         if (!isfinite(be)) nonfinite = true;
@@ -212,141 +214,137 @@ __global__ void k_controller(BandsDev bands, DPBufs B) {
     if (c->max_attempts > 0 && c->attempts >= c->max_attempts) c->done = 1;
 }
 
-int launch_controller(const BandsDev& bands, const DPBufs& B, cudaStream_t st) {
-    k_controller<<<1, 32, 0, st>>>(bands, B);
+int launch_controller(const ElemDev& ed, const DPBufs& B, cudaStream_t st) {
+    k_controller<<<(B.nruns + 127) / 128, 128, 0, st>>>(ed, B);
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }
 
 // Dense output (DormandPrince54.hpp:598-611) followed by the FSAL commit
-// y <- y5, k1 <- k7 of an accepted attempt.  The dense outputs use the
-// pre-commit y and the time-base of the step: s = (denseTime - t_old)/dt_old,
-// which the controller stored.
-__global__ void __launch_bounds__(256) k_dense_commit(BandsDev bands, DPBufs B) {
-    const DPCtl* c = B.ctl;
+// y <- y5, k1 <- k7 of an accepted attempt, per run.  The dense outputs use
+// the pre-commit y and the attempt's own dt (step_dt).
+__global__ void __launch_bounds__(256) k_dense_commit(ElemDev ed, DPBufs B) {
+    const int band = ed.blk_band[blockIdx.x];
+    const int r = ed.band_run[band];
+    const DPCtl* c = B.ctl + r;
     if (c->skip || !c->acc_now) return;
-    for (int bi = 0; bi < bands.nb; ++bi) {
-        const BandDev& bd = bands.b[bi];
-        const int e = blockIdx.x * blockDim.x + threadIdx.x;
-        if (e >= bd.ne) continue;
-        const int64_t o = bd.off + 3 * (int64_t)e;
-        const long long base = c->n_dense;
-        for (int k = 0; k < c->n_now; ++k) {
-            const long long slot = base + k;
-            if (slot >= c->dense_cap) break;
-            const double s = c->dense_s[k];
-            const double dt = c->step_dt;
-            const double bt1 = -(435. * s * s * s - 1184. * s * s + 1098. * s - 384.) / (384.);
-            const double bt3 = 500. * s * (6. * s * s - 14. * s + 9.) / (1113.);
-            const double bt4 = -125. * s * (9. * s * s - 16. * s + 6.) / (192.);
-            const double bt5 = 729. * s * (35. * s * s - 64. * s + 26.) / (6784.);
-            const double bt6 = -11. * s * (3. * s - 2.) * (5. * s - 6.) / (84.);
-            const double bt7 = s * (s - 1.) * (5. * s - 3.) / (2.);
-            double v[3];
-#pragma unroll
-            for (int cc = 0; cc < 3; ++cc) {
-                double t = B.y[o + cc];
-                t = t + (s * dt * bt1) * B.k[0][o + cc];
-                t = t + (s * dt * bt3) * B.k[2][o + cc];
-                t = t + (s * dt * bt4) * B.k[3][o + cc];
-                t = t + (s * dt * bt5) * B.k[4][o + cc];
-                t = t + (s * dt * bt6) * B.k[5][o + cc];
-                t = t + (s * dt * bt7) * B.k[6][o + cc];
-                v[cc] = t;
-            }
-            enforce3(bd, e, v);
-            double* out = B.dense + slot * bands.ndofs + o;
-            out[0] = v[0]; out[1] = v[1]; out[2] = v[2];
-        }
+    const BandDev& bd = ed.bands[band];
+    const int e = (blockIdx.x - ed.blk_first[band]) * blockDim.x + threadIdx.x;
+    if (e >= bd.ne) return;
+    const RunDev& run = B.runs[r];
+    const int64_t o = bd.off + 3 * (int64_t)e;
+    const long long base = c->n_dense;
+    const double dt = c->step_dt;
+    for (int k = 0; k < c->n_now; ++k) {
+        const long long slot = base + k;
+        if (slot >= c->dense_cap) break;
+        const double s = c->dense_s[k];
+        const double bt1 = -(435. * s * s * s - 1184. * s * s + 1098. * s - 384.) / (384.);
+        const double bt3 = 500. * s * (6. * s * s - 14. * s + 9.) / (1113.);
+        const double bt4 = -125. * s * (9. * s * s - 16. * s + 6.) / (192.);
+        const double bt5 = 729. * s * (35. * s * s - 64. * s + 26.) / (6784.);
+        const double bt6 = -11. * s * (3. * s - 2.) * (5. * s - 6.) / (84.);
+        const double bt7 = s * (s - 1.) * (5. * s - 3.) / (2.);
+        double v[3];
 #pragma unroll
         for (int cc = 0; cc < 3; ++cc) {
-            B.y[o + cc] = B.y5[o + cc];
-            B.k[0][o + cc] = B.k[6][o + cc];
+            double t = B.y[o + cc];
+            t = t + (s * dt * bt1) * B.k[0][o + cc];
+            t = t + (s * dt * bt3) * B.k[2][o + cc];
+            t = t + (s * dt * bt4) * B.k[3][o + cc];
+            t = t + (s * dt * bt5) * B.k[4][o + cc];
+            t = t + (s * dt * bt6) * B.k[5][o + cc];
+            t = t + (s * dt * bt7) * B.k[6][o + cc];
+            v[cc] = t;
         }
+        enforce3(bd, e, v);
+        double* out = B.dense + run.dense_off + slot * run.ndofs + (o - run.dof_off);
+        out[0] = v[0]; out[1] = v[1]; out[2] = v[2];
+    }
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) {
+        B.y[o + cc] = B.y5[o + cc];
+        B.k[0][o + cc] = B.k[6][o + cc];
     }
 }
 
 __global__ void k_dense_count(DPBufs B) {
-    DPCtl* c = B.ctl;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= B.nruns) return;
+    DPCtl* c = B.ctl + r;
     if (c->skip || !c->acc_now) return;
+    const RunDev& run = B.runs[r];
     for (int k = 0; k < c->n_now; ++k) {
         const long long slot = c->n_dense + k;
-        if (slot < c->dense_cap) B.dense_t[slot] = c->dense_t[k];
+        if (slot < c->dense_cap) B.dense_t[run.dense_t_off + slot] = c->dense_t[k];
     }
     c->n_dense += c->n_now;
-    if (c->n_dense > c->dense_cap) { c->status = TB_ERR_CAPACITY; c->done = 1; }
+    if (c->dense_cap > 0 && c->n_dense > c->dense_cap) { c->status = TB_ERR_CAPACITY; c->done = 1; }
 }
 
-int launch_dense_commit(const BandsDev& bands, const DPBufs& B, cudaStream_t st) {
-    k_dense_commit<<<B.nblk, 256, 0, st>>>(bands, B);
+int launch_dense_commit(const ElemDev& ed, const DPBufs& B, cudaStream_t st) {
+    k_dense_commit<<<ed.nblk, 256, 0, st>>>(ed, B);
     TB_CUDA(cudaGetLastError());
-    k_dense_count<<<1, 1, 0, st>>>(B);
+    k_dense_count<<<(B.nruns + 127) / 128, 128, 0, st>>>(B);
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }
 
-__global__ void k_first(BandsDev bands, DPBufs B) {
-    for (int bi = 0; bi < bands.nb; ++bi) {
-        const BandDev& bd = bands.b[bi];
-        const int e = blockIdx.x * blockDim.x + threadIdx.x;
-        if (e >= bd.ne) continue;
-        const int64_t o = bd.off + 3 * (int64_t)e;
-        const double x = B.acc[o], y = B.acc[o + 1], z = B.acc[o + 2];
+__global__ void k_first(ElemDev ed, DPBufs B) {
+    const int band = ed.blk_band[blockIdx.x];
+    const BandDev& bd = ed.bands[band];
+    const int e = (blockIdx.x - ed.blk_first[band]) * blockDim.x + threadIdx.x;
+    if (e >= bd.ne) return;
+    const int64_t o = bd.off + 3 * (int64_t)e;
+    const double x = B.acc[o], y = B.acc[o + 1], z = B.acc[o + 2];
 #pragma unroll
-        for (int j = 0; j < 3; ++j) B.k[0][o + j] = x * bd.mesh.Minv[0][j] + y * bd.mesh.Minv[1][j] + z * bd.mesh.Minv[2][j];
-        B.acc[o] = 0.0; B.acc[o + 1] = 0.0; B.acc[o + 2] = 0.0;
-    }
+    for (int j = 0; j < 3; ++j) B.k[0][o + j] = x * bd.mesh.Minv[0][j] + y * bd.mesh.Minv[1][j] + z * bd.mesh.Minv[2][j];
+    B.acc[o] = 0.0; B.acc[o + 1] = 0.0; B.acc[o + 2] = 0.0;
 }
 
-int launch_k1(const BandsDev& bands, const DPBufs& B, cudaStream_t st) {
-    k_first<<<B.nblk, 256, 0, st>>>(bands, B);
+int launch_k1(const ElemDev& ed, const DPBufs& B, cudaStream_t st) {
+    k_first<<<ed.nblk, 256, 0, st>>>(ed, B);
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }
 
-__global__ void k_enforce(BandsDev bands, const double* src, double* dst) {
-    for (int bi = 0; bi < bands.nb; ++bi) {
-        const BandDev& bd = bands.b[bi];
-        for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < bd.ne; e += gridDim.x * blockDim.x) {
-            const int64_t o = bd.off + 3 * (int64_t)e;
-            double v[3] = {src[o], src[o + 1], src[o + 2]};
-            enforce3(bd, e, v);
-            dst[o] = v[0]; dst[o + 1] = v[1]; dst[o + 2] = v[2];
-        }
-    }
+__global__ void k_enforce(ElemDev ed, const double* src, double* dst) {
+    const int band = ed.blk_band[blockIdx.x];
+    const BandDev& bd = ed.bands[band];
+    const int e = (blockIdx.x - ed.blk_first[band]) * blockDim.x + threadIdx.x;
+    if (e >= bd.ne) return;
+    const int64_t o = bd.off + 3 * (int64_t)e;
+    double v[3] = {src[o], src[o + 1], src[o + 2]};
+    enforce3(bd, e, v);
+    dst[o] = v[0]; dst[o + 1] = v[1]; dst[o + 2] = v[2];
 }
 
-int launch_enforce(const BandsDev& bands, const double* src, double* dst, cudaStream_t st) {
-    int maxne = 1;
-    for (int b = 0; b < bands.nb; ++b) maxne = bands.b[b].ne > maxne ? bands.b[b].ne : maxne;
-    k_enforce<<<(maxne + 255) / 256, 256, 0, st>>>(bands, src, dst);
+int launch_enforce(const ElemDev& ed, const double* src, double* dst, cudaStream_t st) {
+    k_enforce<<<ed.nblk, 256, 0, st>>>(ed, src, dst);
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }
 
-__global__ void __launch_bounds__(256) k_error_norm(BandsDev bands, const double* err, const double* pop, double* part,
-                                                    int nblk) {
+__global__ void __launch_bounds__(256) k_error_norm(ElemDev ed, const double* err, const double* pop, double* part) {
     __shared__ double sh[8];
-    for (int bi = 0; bi < bands.nb; ++bi) {
-        const BandDev& bd = bands.b[bi];
-        double r = 0.0, p = 0.0;
-        const int e = blockIdx.x * blockDim.x + threadIdx.x;
-        if (e < bd.ne) {
-            const int64_t o = bd.off + 3 * (int64_t)e;
-            elem_rel_err(bd, err + o, pop + o, r, p);
-        }
-        const double rs = block_sum<256>(r, sh);
-        const double ps = block_sum<256>(p, sh);
-        if (threadIdx.x == 0) {
-            part[(2 * bi) * nblk + blockIdx.x] = rs;
-            part[(2 * bi + 1) * nblk + blockIdx.x] = ps;
-        }
+    const int band = ed.blk_band[blockIdx.x];
+    const BandDev& bd = ed.bands[band];
+    double r = 0.0, p = 0.0;
+    const int e = (blockIdx.x - ed.blk_first[band]) * blockDim.x + threadIdx.x;
+    if (e < bd.ne) {
+        const int64_t o = bd.off + 3 * (int64_t)e;
+        elem_rel_err(bd, err + o, pop + o, r, p);
+    }
+    const double rs = block_sum<256>(r, sh);
+    const double ps = block_sum<256>(p, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = rs;
+        part[ed.nblk + blockIdx.x] = ps;
     }
 }
 
-int launch_error_norm(const BandsDev& bands, const double* err, const double* pop, double* part, int nblk,
-                      cudaStream_t st) {
-    k_error_norm<<<nblk, 256, 0, st>>>(bands, err, pop, part, nblk);
+int launch_error_norm(const ElemDev& ed, const double* err, const double* pop, double* part, cudaStream_t st) {
+    k_error_norm<<<ed.nblk, 256, 0, st>>>(ed, err, pop, part);
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }

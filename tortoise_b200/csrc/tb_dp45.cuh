@@ -26,17 +26,28 @@ struct DPCtl {
     long long max_attempts;  // 0 = unbounded
 };
 
+// Per-run layout inside the concatenated state of a batch.
+struct RunDev {
+    int band0, nbands;      // global band range of the run
+    int blk0, blk1;         // element-block range of its bands
+    int64_t dof_off, ndofs; // state slice
+    int64_t dense_off;      // offset (doubles) of its dense-output block
+    int64_t dense_t_off;    // offset of its dense-time block
+};
+
 struct DPBufs {
-    double* y;       // current state
+    double* y;       // current state (all runs)
     double* tmp;     // stage input
     double* y5;      // 5th-order solution (stage-7 input)
     double* k[7];    // stages k1..k7
     double* acc;     // pre-M^-1 RHS accumulator (zero between evaluations)
-    double* part;    // [2 * nb * nblk] error-norm partial sums
-    int nblk;        // blocks of the element-wise kernels
-    double* dense;   // [dense_cap * ndofs]
-    double* dense_t; // [dense_cap]
-    DPCtl* ctl;
+    double* part;    // [2 * nblk] error-norm partial sums per element block
+    int nblk;
+    int nruns;
+    const RunDev* runs;   // [nruns]
+    double* dense;   // per-run dense blocks [slot][ndofs_run]
+    double* dense_t; // per-run dense times [slot]
+    DPCtl* ctl;      // [nruns]
 };
 
 // Stage kernel s (0..6) of one attempt:
@@ -45,15 +56,15 @@ struct DPBufs {
 //   5     :  k6 = acc M^-1, acc = 0, y5 = enforce(y + sum_j b_j dt k_j)
 //   6     :  k7 = acc M^-1, acc = 0, err = y5 - enforce(y + sum_j bh_j dt k_j) and
 //            the per-band error-norm partials.
-int launch_stage(const BandsDev& bands, const DPBufs& B, int s, cudaStream_t st);
-int launch_controller(const BandsDev& bands, const DPBufs& B, cudaStream_t st);
-int launch_dense_commit(const BandsDev& bands, const DPBufs& B, cudaStream_t st);
+int launch_stage(const ElemDev& ed, const DPBufs& B, int s, cudaStream_t st);
+int launch_controller(const ElemDev& ed, const DPBufs& B, cudaStream_t st);
+int launch_dense_commit(const ElemDev& ed, const DPBufs& B, cudaStream_t st);
 // k1 = M^-1 acc, acc = 0 (first evaluation of an integration).
-int launch_k1(const BandsDev& bands, const DPBufs& B, cudaStream_t st);
+int launch_k1(const ElemDev& ed, const DPBufs& B, cudaStream_t st);
 // dst = enforce(src)  (applyConstraints)
-int launch_enforce(const BandsDev& bands, const double* src, double* dst, cudaStream_t st);
-// Band::relativeError partial sums for arbitrary err/pop (diagnostics, tests).
-int launch_error_norm(const BandsDev& bands, const double* err, const double* pop, double* part, int nblk,
-                      cudaStream_t st);
+int launch_enforce(const ElemDev& ed, const double* src, double* dst, cudaStream_t st);
+// Band::relativeError partial sums per element block for arbitrary err/pop:
+// part[blk] (relative term), part[nblk + blk] (penalisation term).
+int launch_error_norm(const ElemDev& ed, const double* err, const double* pop, double* part, cudaStream_t st);
 
 }  // namespace tb

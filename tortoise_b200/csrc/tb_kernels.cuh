@@ -5,28 +5,43 @@
 
 namespace tb {
 
-#define TB_MAX_BANDS 8
+struct DPCtl;
 
-struct BandsDev {
-    int nb;
-    int64_t ndofs;
-    BandDev b[TB_MAX_BANDS];
+// One run's use of a shared channel: where its bands live in the global
+// state and its coupling constant.  Runs with identical structure share the
+// channel's tuple list (and moment tensor); each run is one instance.
+struct InstDev {
+    int64_t foff[TB_MAX_LEGS];  // band offsets of the run's legs in the state
+    double amp_full;            // amplitude * prod_l (vol_l * 2)  (Monte-Carlo path)
+    double amplitude;           // amplitude                     (moment-tensor path)
+    int run;
+    int pad;
 };
 
-// Layout of the per-tuple moment tensor used by the precomputed-tensor
-// contraction (see tb_tensor.cu).
-enum TensorPrec { TENSOR_NONE = 0, TENSOR_F64 = 1, TENSOR_F32 = 2 };
+// Element-wise work over every band of every run.  Blocks of 256 elements;
+// block b belongs to band blk_band[b] and covers elements
+// (b - blk_first[band]) * 256 + [0, 256).
+struct ElemDev {
+    const BandDev* bands;       // [nb]
+    const int* band_run;        // [nb]
+    const int* blk_band;        // [nblk]
+    const int* blk_first;       // [nb + 1]
+    int nb;
+    int nblk;
+    int64_t ndofs;
+};
 
-// Collision contribution of one channel (before M^-1), added into acc:
-// Monte-Carlo quadrature evaluated per tuple (scatteringIntegrationTypeB).
-int launch_collision_mc(const ChanDev& c, double amp_full, const int32_t* tup, int64_t stride, int64_t n,
-                        const double* f, double* acc, const int* done, cudaStream_t s, int grid_hint);
+// Collision contribution of one channel for every instance in `insts`
+// (before M^-1), added into acc.  ctl (per run, may be null) lets finished
+// runs skip their work inside a batched integration.
+int launch_collision_mc(const ChanDev& c, const InstDev* insts, int n_insts, const int32_t* tup, int64_t stride,
+                        int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s, int grid_hint);
 
 // Vlasov drift (volume minus upwind surface term, before M^-1) of every band
 // with a nonzero drift velocity, added into acc.
-int launch_drift(const BandsDev& bands, const double* f, double* acc, const int* done, cudaStream_t s);
+int launch_drift(const ElemDev& ed, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s);
 
 // out = acc * M^-1 per element (Function::applyInverseMass).
-int launch_inverse_mass(const BandsDev& bands, const double* acc, double* out, cudaStream_t s);
+int launch_inverse_mass(const ElemDev& ed, const double* acc, double* out, cudaStream_t s);
 
 }  // namespace tb

@@ -23,6 +23,7 @@
 // each thread reads its tuple's moments bank-conflict free.  FP32 storage
 // halves the bytes; products and accumulation stay FP64, and the
 // gain-minus-loss vector v = ka + kb is formed in FP64 from f.
+#include "tb_dp45.cuh"
 #include "tb_geom.cuh"
 #include "tb_tensor.cuh"
 
@@ -190,17 +191,25 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 }
 
 template <int L, typename T, int TT, int STAGES>
-__global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, double amplitude, const T* __restrict__ mom,
-                                                         int64_t ntiles, const int32_t* __restrict__ tup,
-                                                         int64_t stride, int64_t n, const double* __restrict__ f,
-                                                         double* __restrict__ acc, const int* __restrict__ done,
-                                                         int* __restrict__ err_flag) {
+__global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, const InstDev* __restrict__ insts, int n_insts,
+                                                         const T* __restrict__ mom, int64_t ntiles,
+                                                         const int32_t* __restrict__ tup, int64_t stride, int64_t n,
+                                                         const double* __restrict__ f, double* __restrict__ acc,
+                                                         const DPCtl* __restrict__ ctl, int* __restrict__ err_flag) {
     constexpr int K = TDim<L>::K, KM = TDim<L>::KM, NMOM = TDim<L>::NMOM;
     constexpr uint32_t TILE_BYTES = uint32_t(NMOM) * TT * sizeof(T);
     extern __shared__ __align__(128) unsigned char smem_raw[];
     T* stage_buf = reinterpret_cast<T*>(smem_raw);
     __shared__ __align__(8) uint64_t bars[STAGES];
-    if (done && *done) return;
+    {
+        // every instance finished or switched off: nothing to stream
+        bool any = false;
+        for (int k = 0; k < n_insts; ++k) {
+            const InstDev in = insts[k];
+            any |= (in.amplitude != 0.0) && !(ctl && ctl[in.run].done);
+        }
+        if (!any) return;
+    }
     const int tid = threadIdx.x;
     if (tid == 0) {
         for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
@@ -237,70 +246,74 @@ __global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, double ampli
             int e[L];
 #pragma unroll
             for (int l = 0; l < L; ++l) e[l] = __ldg(tup + l * stride + i);
-            // gain (B) / loss (A) forms, ScatteringChannel.cpp:633-641
-            double A[L][3], B[L][3];
+            for (int k = 0; k < n_insts; ++k) {
+                const InstDev in = insts[k];
+                if (in.amplitude == 0.0 || (ctl && ctl[in.run].done)) continue;
+                // gain (B) / loss (A) forms, ScatteringChannel.cpp:633-641
+                double A[L][3], B[L][3];
 #pragma unroll
-            for (int l = 0; l < L; ++l) {
-                const double d = c.leg[l].dir, st = c.leg[l].stat;
-                const double* fe = f + c.leg[l].foff + 3 * (int64_t)e[l];
-                const double ka = (l == 0 ? -1.0 : 1.0) * 0.5;
-                const double ca = (1. - d) * st + (1. + d);
-                const double cb = (1. + d) * st + (1. - d);
+                for (int l = 0; l < L; ++l) {
+                    const double d = c.leg[l].dir, st = c.leg[l].stat;
+                    const double* fe = f + in.foff[l] + 3 * (int64_t)e[l];
+                    const double ka = (l == 0 ? -1.0 : 1.0) * 0.5;
+                    const double ca = (1. - d) * st + (1. + d);
+                    const double cb = (1. + d) * st + (1. - d);
 #pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    const double unit = (j == 0) ? 1.0 : 0.0;
-                    const double fj = __ldg(fe + j);
-                    A[l][j] = ka * ((1. - d) * unit + ca * fj);
-                    B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
+                    for (int j = 0; j < 3; ++j) {
+                        const double unit = (j == 0) ? 1.0 : 0.0;
+                        const double fj = __ldg(fe + j);
+                        A[l][j] = ka * ((1. - d) * unit + ca * fj);
+                        B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
+                    }
                 }
-            }
-            // v = kron(A) + kron(B), leg 0 most significant
-            double v[K];
+                // v = kron(A) + kron(B), leg 0 most significant
+                double v[K];
 #pragma unroll
-            for (int j = 0; j < K; ++j) {
-                int r = j;
-                double pa = 1.0, pb = 1.0;
+                for (int j = 0; j < K; ++j) {
+                    int r = j;
+                    double pa = 1.0, pb = 1.0;
 #pragma unroll
-                for (int l = L - 1; l >= 0; --l) {
-                    const int Jl = r % 3;
-                    r /= 3;
-                    pa *= A[l][Jl];
-                    pb *= B[l][Jl];
+                    for (int l = L - 1; l >= 0; --l) {
+                        const int Jl = r % 3;
+                        r /= 3;
+                        pa *= A[l][Jl];
+                        pb *= B[l][Jl];
+                    }
+                    v[j] = pa + pb;
                 }
-                v[j] = pa + pb;
-            }
-            double r0 = 0.0;
+                double r0 = 0.0;
 #pragma unroll
-            for (int j = 0; j < K; ++j) r0 = fma(double(sm[j * TT + tid]), v[j], r0);
+                for (int j = 0; j < K; ++j) r0 = fma(double(sm[j * TT + tid]), v[j], r0);
 #pragma unroll
-            for (int lam = 0; lam < L; ++lam) {
-                int sstep = 1;
+                for (int lam = 0; lam < L; ++lam) {
+                    int sstep = 1;
 #pragma unroll
-                for (int l = L - 1; l > lam; --l) sstep *= 3;
-                double r1 = 0.0, r2 = 0.0;
+                    for (int l = L - 1; l > lam; --l) sstep *= 3;
+                    double r1 = 0.0, r2 = 0.0;
 #pragma unroll
-                for (int km = 0; km < KM; ++km) {
-                    // J with J_lam = 0 whose other legs enumerate km in leg order
-                    int hi = km / sstep, lo = km % sstep;
-                    const int j0 = hi * 3 * sstep + lo;
-                    const int j1 = j0 + sstep, j2 = j0 + 2 * sstep;
-                    const double qxx = double(sm[(K + (lam * 3 + 0) * KM + km) * TT + tid]);
-                    const double qxy = double(sm[(K + (lam * 3 + 1) * KM + km) * TT + tid]);
-                    const double qyy = double(sm[(K + (lam * 3 + 2) * KM + km) * TT + tid]);
-                    const double s1 = double(sm[j1 * TT + tid]);
-                    const double s2 = double(sm[j2 * TT + tid]);
-                    r1 = fma(s1, v[j0], r1);
-                    r1 = fma(qxx, v[j1], r1);
-                    r1 = fma(qxy, v[j2], r1);
-                    r2 = fma(s2, v[j0], r2);
-                    r2 = fma(qxy, v[j1], r2);
-                    r2 = fma(qyy, v[j2], r2);
+                    for (int km = 0; km < KM; ++km) {
+                        // J with J_lam = 0 whose other legs enumerate km in leg order
+                        int hi = km / sstep, lo = km % sstep;
+                        const int j0 = hi * 3 * sstep + lo;
+                        const int j1 = j0 + sstep, j2 = j0 + 2 * sstep;
+                        const double qxx = double(sm[(K + (lam * 3 + 0) * KM + km) * TT + tid]);
+                        const double qxy = double(sm[(K + (lam * 3 + 1) * KM + km) * TT + tid]);
+                        const double qyy = double(sm[(K + (lam * 3 + 2) * KM + km) * TT + tid]);
+                        const double s1 = double(sm[j1 * TT + tid]);
+                        const double s2 = double(sm[j2 * TT + tid]);
+                        r1 = fma(s1, v[j0], r1);
+                        r1 = fma(qxx, v[j1], r1);
+                        r1 = fma(qxy, v[j2], r1);
+                        r2 = fma(s2, v[j0], r2);
+                        r2 = fma(qxy, v[j1], r2);
+                        r2 = fma(qyy, v[j2], r2);
+                    }
+                    const double d = c.leg[lam].dir;
+                    double* o = acc + in.foff[lam] + 3 * (int64_t)e[lam];
+                    atomicAdd(o + 0, d * (r0 * in.amplitude));
+                    atomicAdd(o + 1, d * (r1 * in.amplitude));
+                    atomicAdd(o + 2, d * (r2 * in.amplitude));
                 }
-                const double d = c.leg[lam].dir;
-                double* o = acc + c.leg[lam].foff + 3 * (int64_t)e[lam];
-                atomicAdd(o + 0, d * (r0 * amplitude));
-                atomicAdd(o + 1, d * (r1 * amplitude));
-                atomicAdd(o + 2, d * (r2 * amplitude));
             }
         }
         __syncthreads();   // every thread is done with stage s
@@ -356,8 +369,8 @@ int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n
 static int* g_err_flag = nullptr;
 
 template <int L, bool F32>
-static int launch_t(const ChanDev& c, double amplitude, const MomentTensor& T, const int32_t* tup, int64_t stride,
-                    int64_t n, const double* f, double* acc, const int* done, cudaStream_t s) {
+static int launch_t(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T, const int32_t* tup,
+                    int64_t stride, int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s) {
     using E = typename std::conditional<F32, float, double>::type;
     constexpr int TT = TTile<L, F32>::TT;
     constexpr int STAGES = 2;
@@ -382,22 +395,22 @@ static int launch_t(const ChanDev& c, double amplitude, const MomentTensor& T, c
     if (grid > T.ntiles) grid = T.ntiles;
     if (grid < 1) return TB_OK;
     k_collision_tensor<L, E, TT, STAGES><<<unsigned(grid), TT, smem, s>>>(
-        c, amplitude, reinterpret_cast<const E*>(T.d), T.ntiles, tup, stride, n, f, acc, done, g_err_flag);
+        c, insts, n_insts, reinterpret_cast<const E*>(T.d), T.ntiles, tup, stride, n, f, acc, ctl, g_err_flag);
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }
 
-int launch_collision_tensor(const ChanDev& c, double amplitude, const MomentTensor& T, const int32_t* tup,
-                            int64_t stride, int64_t n, const double* f, double* acc, const int* done,
-                            cudaStream_t s) {
-    if (n <= 0) return TB_OK;
+int launch_collision_tensor(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T,
+                            const int32_t* tup, int64_t stride, int64_t n, const double* f, double* acc,
+                            const DPCtl* ctl, cudaStream_t s) {
+    if (n <= 0 || n_insts <= 0) return TB_OK;
     switch (c.L * 2 + (T.fp32 ? 1 : 0)) {
-        case 4: return launch_t<2, false>(c, amplitude, T, tup, stride, n, f, acc, done, s);
-        case 5: return launch_t<2, true>(c, amplitude, T, tup, stride, n, f, acc, done, s);
-        case 6: return launch_t<3, false>(c, amplitude, T, tup, stride, n, f, acc, done, s);
-        case 7: return launch_t<3, true>(c, amplitude, T, tup, stride, n, f, acc, done, s);
-        case 8: return launch_t<4, false>(c, amplitude, T, tup, stride, n, f, acc, done, s);
-        case 9: return launch_t<4, true>(c, amplitude, T, tup, stride, n, f, acc, done, s);
+        case 4: return launch_t<2, false>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
+        case 5: return launch_t<2, true>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
+        case 6: return launch_t<3, false>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
+        case 7: return launch_t<3, true>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
+        case 8: return launch_t<4, false>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
+        case 9: return launch_t<4, true>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
     }
     set_error("nlegs must be 2..4");
     return TB_ERR_ARG;

@@ -1,7 +1,7 @@
 // tb_tensor.cuh -- precomputed moment tensors of the collision operator.
 #pragma once
 
-#include "tb_common.cuh"
+#include "tb_kernels.cuh"
 
 namespace tb {
 
@@ -17,8 +17,9 @@ struct MomentTensor {
 int64_t tensor_bytes(int L, bool fp32, int64_t n_tuples);
 int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, bool fp32, MomentTensor& T,
                  cudaStream_t s);
-int launch_collision_tensor(const ChanDev& c, double amplitude, const MomentTensor& T, const int32_t* tup,
-                            int64_t stride, int64_t n, const double* f, double* acc, const int* done, cudaStream_t s);
+int launch_collision_tensor(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T,
+                            const int32_t* tup, int64_t stride, int64_t n, const double* f, double* acc,
+                            const DPCtl* ctl, cudaStream_t s);
 
 // 1 once a bulk-copy wait of the contraction kernel ran out (then TB_ERR_TIMEOUT)
 int tensor_error_flag(int* value);

@@ -75,6 +75,12 @@ def lib():
         L.tb_get_stream.restype = vp
         L.tb_get_stream.argtypes = [vp]
         L.tb_collision_accumulate.argtypes = [vp, C.c_int, vp, vp]
+        L.tb_create_batch.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int, C.POINTER(Options)]
+        L.tb_num_runs.argtypes = [vp]
+        L.tb_run_info.argtypes = [vp, C.c_int, C.POINTER(i64), C.POINTER(i64), C.POINTER(C.c_int32),
+                                  C.POINTER(C.c_int32)]
+        L.tb_dp45_begin_batch.argtypes = [vp, vp, dp, dp, dp, i64, C.c_int]
+        L.tb_dp45_run_stats.argtypes = [vp, C.c_int, C.POINTER(DP45Stats)]
         _lib = L
     return _lib
 
@@ -147,9 +153,10 @@ class Engine:
     def relative_error(self, err, pop):
         err = np.ascontiguousarray(err, dtype=np.float64)
         pop = np.ascontiguousarray(pop, dtype=np.float64)
-        r = C.c_double()
-        _check(lib().tb_relative_error(self.h, _hp(err), _hp(pop), C.byref(r), PTR_HOST), "tb_relative_error")
-        return r.value
+        r = np.zeros(max(1, lib().tb_num_runs(self.h)))
+        _check(lib().tb_relative_error(self.h, _hp(err), _hp(pop), r.ctypes.data_as(C.POINTER(C.c_double)),
+                                       PTR_HOST), "tb_relative_error")
+        return float(r[0]) if r.size == 1 else r
 
     def apply_constraints(self, f):
         f = np.ascontiguousarray(f, dtype=np.float64).copy()
@@ -196,3 +203,77 @@ class Engine:
 
     def synchronize(self):
         _check(lib().tb_synchronize(self.h), "tb_synchronize")
+
+
+class BatchEngine(Engine):
+    """Several independent runs (Materials) in one device handle
+    (tb_create_batch).  Runs with identical structure share tuple lists and
+    moment tensors; each keeps its own amplitudes, tolerances, state and step
+    size.  Channels and bands are numbered globally in run order."""
+
+    def __init__(self, materials, layout=LAYOUT_AUTO, allow_fp32=False, device=0, tensor_budget_bytes=0):
+        self.materials = list(materials)
+        self.material = self.materials[0]
+        self.packs = [m.pack() for m in self.materials]
+        arr = (C.c_void_p * len(self.packs))(*[C.addressof(p.desc) for p in self.packs])
+        opts = Options(device, layout, 1 if allow_fp32 else 0, tensor_budget_bytes, 0)
+        h = C.c_void_p()
+        _check(lib().tb_create_batch(C.byref(h), arr, len(self.packs), C.byref(opts)), "tb_create_batch")
+        self.h = h
+        self.ndofs = lib().tb_num_dofs(h)
+        self.nruns = len(self.packs)
+        self.slices, self.chan0 = [], []
+        for r in range(self.nruns):
+            off, n = C.c_int64(), C.c_int64()
+            b0, c0 = C.c_int32(), C.c_int32()
+            _check(lib().tb_run_info(h, r, C.byref(off), C.byref(n), C.byref(b0), C.byref(c0)), "tb_run_info")
+            self.slices.append(slice(off.value, off.value + n.value))
+            self.chan0.append(c0.value)
+
+    def tuples(self, ch):
+        r = max(i for i in range(self.nruns) if self.chan0[i] <= ch)
+        info = self.channel_info(ch)
+        L = self.materials[r].channels[ch - self.chan0[r]].nlegs
+        ids = np.zeros((info["n_tuples"], L), dtype=np.int32)
+        umk = np.zeros(info["n_tuples"], dtype=np.int32)
+        _check(lib().tb_get_tuples(self.h, ch, ids.ctypes.data_as(C.POINTER(C.c_int32)),
+                                   umk.ctypes.data_as(C.POINTER(C.c_int32))), "tb_get_tuples")
+        return ids, umk
+
+    def split(self, vec):
+        return [np.asarray(vec)[s] for s in self.slices]
+
+    def dp45(self, y0, t0, tf, dense, max_dense=None, drift=True):
+        """Integrates every run; t0, tf, dense may be scalars or per-run lists."""
+        y = np.ascontiguousarray(y0, dtype=np.float64).copy()
+        as_arr = lambda x: np.ascontiguousarray(np.broadcast_to(np.asarray(x, dtype=np.float64), (self.nruns,)))
+        t0a, tfa, da = as_arr(t0), as_arr(tf), as_arr(dense)
+        if max_dense is None:
+            max_dense = int(np.ceil(np.max((tfa - t0a) / da))) + 2
+        flags = PTR_HOST | (0 if drift else NO_DRIFT)
+        dp = C.POINTER(C.c_double)
+        _check(lib().tb_dp45_begin_batch(self.h, _hp(y), t0a.ctypes.data_as(dp), tfa.ctypes.data_as(dp),
+                                         da.ctypes.data_as(dp), max_dense, flags), "tb_dp45_begin_batch")
+        batch = 4
+        while True:
+            self.dp45_advance(batch)
+            if self.dp45_poll()["done"]:
+                break
+            batch = min(64, batch * 2)
+        sizes = [s.stop - s.start for s in self.slices]
+        dout = np.zeros(max_dense * sum(sizes))
+        dts = np.zeros(max_dense * self.nruns)
+        st = DP45Stats()
+        rc = lib().tb_dp45_end(self.h, _hp(y), _hp(dout), _hp(dts), max_dense, C.byref(st), PTR_HOST)
+        runs, off = [], 0
+        for r in range(self.nruns):
+            rs = DP45Stats()
+            _check(lib().tb_dp45_run_stats(self.h, r, C.byref(rs)), "tb_dp45_run_stats")
+            d = rs.as_dict()
+            nd = min(rs.n_dense, max_dense)
+            d["dense"] = dout[off:off + max_dense * sizes[r]].reshape(max_dense, sizes[r])[:nd]
+            d["dense_t"] = dts[r * max_dense:r * max_dense + nd]
+            d["y"] = y[self.slices[r]]
+            runs.append(d)
+            off += max_dense * sizes[r]
+        return {"rc": rc, "y": y, "runs": runs}
