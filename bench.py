@@ -309,6 +309,57 @@ def ours(args, world, rank, local, pg):
     eng.close()
 
 
+def batched(args):
+    """Batched ensemble (configs[2] shape): args.batch runs in one handle,
+    DP45 attempts of all runs per graph launch; value = run-attempts/s."""
+    import torch
+    from tortoise_b200 import engine as E
+    from tortoise_b200 import workloads as W
+    mats, states = W.config2_runs(args.batch)
+    layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32}[args.layout]
+    t0 = time.perf_counter()
+    be = E.BatchEngine(mats, layout=layout, allow_fp32=args.mixed)
+    t_setup = time.perf_counter() - t0
+    f0 = np.concatenate(states)
+    stream = torch.cuda.ExternalStream(be.stream_ptr())
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # collision phase alone
+    f = torch.tensor(f0, device="cuda")
+    acc = torch.zeros_like(f)
+    be.collision_accumulate(f.data_ptr(), acc.data_ptr())
+    be.synchronize()
+    ev0.record(stream)
+    for _ in range(5):
+        be.collision_accumulate(f.data_ptr(), acc.data_ptr())
+    ev1.record(stream)
+    ev1.synchronize()
+    t_coll = ev0.elapsed_time(ev1) * 1e-3 / 5
+    be.dp45_begin(f0, 0.0, 1.0e9, DENSE, 0)
+    be.dp45_advance(args.warmup)
+    be.synchronize()
+    with ClockSampler(0) as clk:
+        ev0.record(stream)
+        be.dp45_advance(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+    t = ev0.elapsed_time(ev1) * 1e-3
+    Ns = sorted({m.bands[0].mesh.nsplit[0] for m in mats})
+    groups = {}
+    for m in mats:
+        groups[m.bands[0].mesh.nsplit[0]] = groups.get(m.bands[0].mesh.nsplit[0], 0) + 1
+    uniq = {}
+    for r, m in enumerate(mats):
+        N = m.bands[0].mesh.nsplit[0]
+        if N not in uniq:
+            uniq[N] = sum(be.channel_info(be.chan0[r] + c)["n_tuples"] for c in range(len(m.channels)))
+    print(json.dumps({"batched": True, "runs": args.batch, "mixed": args.mixed, "steps": args.steps,
+                      "run_attempts_per_s": args.batch * args.steps / t, "ms_per_attempt": 1e3 * t / args.steps,
+                      "collision_ms": 1e3 * t_coll, "setup_s": t_setup, "runs_per_N": groups,
+                      "tuples_per_structure": uniq, "dofs": be.ndofs,
+                      "layouts": sorted({be.channel_info(c)["layout"] for c in range(be.channel_count())}),
+                      "clocks": clk.summary()}), flush=True)
+
+
 def rhs_only(args):
     """Profiling driver: K right-hand-side evaluations (collision + drift +
     M^-1) of the workload on the device, nothing else (used for the ncu
@@ -342,9 +393,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--rhs-only", type=int, default=0, help="profiling driver: K RHS evaluations only")
     ap.add_argument("--mesh", type=int, default=N_MESH, help="sections per side (profiling driver only)")
+    ap.add_argument("--batch", type=int, default=0, help="batched ensemble of this many runs (configs[2] shape)")
     args = ap.parse_args()
     if args.rhs_only:
         rhs_only(args)
+        return
+    if args.batch:
+        batched(args)
         return
     world, rank, local, pg = dist_setup(args)
     try:

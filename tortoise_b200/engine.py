@@ -194,6 +194,9 @@ class Engine:
         _check(lib().tb_dp45_poll(self.h, C.byref(st)), "tb_dp45_poll")
         return st.as_dict()
 
+    def channel_count(self):
+        return lib().tb_num_channels(self.h)
+
     def stream_ptr(self):
         return lib().tb_get_stream(self.h)
 

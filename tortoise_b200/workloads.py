@@ -94,3 +94,23 @@ def config3(N=32, ee=False, **kw):
 
 def config4(N=128, ee=False, **kw):
     return build_material(N, ("P", "D", "H"), (0.15, 0.25), ee=ee, eph=True, rtol=1e-8, atol=1e-9, **kw)
+
+
+def config2_runs(n_runs=256, seed=2024, Ns=(16, 24, 32, 48, 64), ee=False, **kw):
+    """Batched ensemble: per run N uniform in Ns, kT uniform in [0.03, 0.2],
+    coupling constants uniform in [0.5, 2.0] and a seeded bump; bands, phonon,
+    field and tolerances as config1.  All runs use the same Monte-Carlo seed,
+    so runs of equal N have identical structure (shared tuple lists and
+    moment tensors).  Returns (materials, initial state vectors)."""
+    rng = np.random.default_rng(seed)
+    mats, states = [], []
+    for r in range(n_runs):
+        N = int(rng.choice(Ns))
+        kT = float(rng.uniform(0.03, 0.2))
+        amp_eph = float(rng.uniform(0.5, 2.0))
+        amp_ee = float(rng.uniform(0.5, 2.0))
+        m = build_material(N, ("P", "D"), (0.2,), ee=ee, eph=True, field=(0.1, 0.0), rtol=1e-8, atol=1e-9,
+                           eph_amplitude=amp_eph, ee_amplitude=amp_ee, **kw)
+        mats.append(m)
+        states.append(initial_status(m, kT=kT, seed=int(rng.integers(1 << 30))).vec)
+    return mats, states
