@@ -16,6 +16,7 @@
 #include "tb_dp45.cuh"
 #include "tb_geom.cuh"
 #include "tb_kernels.cuh"
+#include "tb_scatter.cuh"
 
 namespace tb {
 
@@ -29,14 +30,18 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* 
     for (int i = threadIdx.x; i < c.nmc * R; i += blockDim.x) s_mc[i] = c.mc[i];
     __syncthreads();
     const double inv_fact_nmc = c.fact * double(c.nmc);
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    // warp-uniform loop: every lane of a warp shares `base`, so the warp
+    // scatter below can reduce across lanes
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        bool valid = i < n;
         int e[L];
 #pragma unroll
-        for (int l = 0; l < L; ++l) e[l] = __ldg(tup + l * stride + i);
-        const int u = __ldg(tup + L * stride + i);
+        for (int l = 0; l < L; ++l) e[l] = valid ? __ldg(tup + l * stride + i) : 0;
+        const int u = valid ? __ldg(tup + L * stride + i) : 0;
         TupleGeom<L> g;
         tuple_geometry<L>(c, e, u, g);
-        if (fabs(g.det) < c.min_det) continue;
+        if (!(fabs(g.det) >= c.min_det)) valid = false;   // also NaN-safe for padding lanes
         double Ci[3][3];
         dc_inverse<L>(g, Ci);
         // alpha = -Ci (DF q - N) = G q + alpha0 (fast path, FMA).  The
@@ -70,6 +75,7 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* 
             const InstDev in = insts[k];
             if (in.amp_full == 0.0) continue;
             if (ctl && ctl[in.run].done) continue;
+            if (!__any_sync(0xffffffffu, valid)) continue;
             // commonLinForm0 (A, direct) and commonLinForm1 (B, time reversed),
             // ScatteringChannel.cpp:633-641
             double A[L][3], B[L][3];

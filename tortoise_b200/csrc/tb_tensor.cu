@@ -25,6 +25,7 @@
 // gain-minus-loss vector v = ka + kb is formed in FP64 from f.
 #include "tb_dp45.cuh"
 #include "tb_geom.cuh"
+#include "tb_scatter.cuh"
 #include "tb_tensor.cuh"
 
 namespace tb {
@@ -242,10 +243,13 @@ __global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, const InstDe
         }
         const T* sm = stage_buf + (size_t)s * NMOM * TT;
         const int64_t i = tile * TT + tid;
-        if (i < n) {
+        {
+            // every lane runs the instance loop (padding lanes contribute zero
+            // moments and no atomics) so that the warp scatter can reduce
+            const bool valid = i < n;
             int e[L];
 #pragma unroll
-            for (int l = 0; l < L; ++l) e[l] = __ldg(tup + l * stride + i);
+            for (int l = 0; l < L; ++l) e[l] = valid ? __ldg(tup + l * stride + i) : 0;
             for (int k = 0; k < n_insts; ++k) {
                 const InstDev in = insts[k];
                 if (in.amplitude == 0.0 || (ctl && ctl[in.run].done)) continue;
@@ -309,10 +313,16 @@ __global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, const InstDe
                         r2 = fma(qyy, v[j2], r2);
                     }
                     const double d = c.leg[lam].dir;
-                    double* o = acc + in.foff[lam] + 3 * (int64_t)e[lam];
-                    atomicAdd(o + 0, d * (r0 * in.amplitude));
-                    atomicAdd(o + 1, d * (r1 * in.amplitude));
-                    atomicAdd(o + 2, d * (r2 * in.amplitude));
+                    const int64_t key = in.foff[lam] + 3 * (int64_t)e[lam];
+                    if (lam < L - 1) {
+                        warp_scatter3(valid ? key : -1, acc + key, d * (r0 * in.amplitude), d * (r1 * in.amplitude),
+                                      d * (r2 * in.amplitude));
+                    } else if (valid) {
+                        double* o = acc + key;
+                        atomicAdd(o + 0, d * (r0 * in.amplitude));
+                        atomicAdd(o + 1, d * (r1 * in.amplitude));
+                        atomicAdd(o + 2, d * (r2 * in.amplitude));
+                    }
                 }
             }
         }
