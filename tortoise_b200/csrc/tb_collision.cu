@@ -79,14 +79,14 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* 
             // commonLinForm0 (A, direct) and commonLinForm1 (B, time reversed),
             // ScatteringChannel.cpp:633-641
             double A[L][3], B[L][3];
-    #pragma unroll
+#pragma unroll
             for (int l = 0; l < L; ++l) {
                 const double d = c.leg[l].dir, s = c.leg[l].stat;
                 const double* fe = f + in.foff[l] + 3 * (int64_t)e[l];
                 const double ka = (l == 0 ? -1.0 : 1.0) * 0.5;
                 const double ca = (1. - d) * s + (1. + d);
                 const double cb = (1. + d) * s + (1. - d);
-    #pragma unroll
+#pragma unroll
                 for (int j = 0; j < 3; ++j) {
                     const double unit = (j == 0) ? 1.0 : 0.0;
                     const double fj = __ldg(fe + j);
@@ -95,18 +95,18 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* 
                 }
             }
             double s0 = 0.0, sx[L], sy[L];
-    #pragma unroll
+#pragma unroll
             for (int l = 0; l < L; ++l) { sx[l] = 0.0; sy[l] = 0.0; }
             for (int m = 0; m < c.nmc; ++m) {
                 const double* q = s_mc + m * R;
                 double qv[R];
-    #pragma unroll
+#pragma unroll
                 for (int j = 0; j < R; ++j) qv[j] = q[j];
                 double al[3];
-    #pragma unroll
+#pragma unroll
                 for (int r = 0; r < 3; ++r) {
                     double t = a0[r];
-    #pragma unroll
+#pragma unroll
                     for (int j = 0; j < R; ++j) t = fma(G[r][j], qv[j], t);
                     al[r] = t;
                 }
@@ -118,32 +118,38 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* 
                 if (near) exact_alpha<L>(g, Ci, qv, al);
                 const bool th = theta_of(kp0, al);
                 double px[L], py[L];
-    #pragma unroll
+#pragma unroll
                 for (int l = 0; l < L - 2; ++l) { px[l] = qv[2 * l]; py[l] = qv[2 * l + 1]; }
                 px[L - 2] = kp0; py[L - 2] = al[0];
                 px[L - 1] = al[1]; py[L - 1] = al[2];
                 double pa = 1.0, pb = 1.0;
-    #pragma unroll
+#pragma unroll
                 for (int l = 0; l < L; ++l) {
                     pa *= (A[l][1] * px[l] + A[l][2] * py[l]) + A[l][0];
                     pb *= (B[l][1] * px[l] + B[l][2] * py[l]) + B[l][0];
                 }
                 const double common = (pa + pb) * (th ? 1.0 : 0.0);
                 s0 += common;
-    #pragma unroll
+#pragma unroll
                 for (int l = 0; l < L; ++l) {
                     sx[l] = fma(px[l], common, sx[l]);
                     sy[l] = fma(py[l], common, sy[l]);
                 }
             }
-            const double scale = 1.0 / (inv_fact_nmc * fabs(g.det));
-    #pragma unroll
+            const double scale = valid ? 1.0 / (inv_fact_nmc * fabs(g.det)) : 0.0;
+#pragma unroll
             for (int l = 0; l < L; ++l) {
                 const double d = c.leg[l].dir;
-                double* o = acc + in.foff[l] + 3 * (int64_t)e[l];
-                atomicAdd(o + 0, d * ((scale * s0) * in.amp_full));
-                atomicAdd(o + 1, d * ((scale * sx[l]) * in.amp_full));
-                atomicAdd(o + 2, d * ((scale * sy[l]) * in.amp_full));
+                const int64_t key = in.foff[l] + 3 * (int64_t)e[l];
+                if (l < L - 1) {
+                    warp_scatter3(valid ? key : -1, acc + key, d * ((scale * s0) * in.amp_full),
+                                  d * ((scale * sx[l]) * in.amp_full), d * ((scale * sy[l]) * in.amp_full));
+                } else if (valid) {
+                    double* o = acc + key;
+                    atomicAdd(o + 0, d * ((scale * s0) * in.amp_full));
+                    atomicAdd(o + 1, d * ((scale * sx[l]) * in.amp_full));
+                    atomicAdd(o + 2, d * ((scale * sy[l]) * in.amp_full));
+                }
             }
         }
     }
