@@ -256,6 +256,63 @@ void* tb_get_stream(tb_handle* h);
  * callers that compose their own right-hand side. */
 int tb_collision_accumulate(tb_handle* h, int ch, const double* f, double* acc);
 
+/* ---------------------------------------------------------------- adjoint
+ * No counterpart in the reference, which has no derivatives.  The right-hand
+ * side is F(f) = M^-1 (sum_c amplitude_c C_c(f) + V f) (ScatteringChannel::
+ * propagate and Vlasov::propagate followed by Function::applyInverseMass).
+ * grad_amp arrays have tb_num_channels(h) entries in channel order and are
+ * HOST memory whatever the flags say. */
+
+typedef struct tb_adjoint_stats {
+    double  t_obs;            /* time of the observable (the last dense output)   */
+    double  dense_s;          /* its fraction inside the step that produced it    */
+    int64_t steps;            /* accepted steps up to and including that step     */
+    int64_t attempts;         /* forward attempts (accepted + rejected)           */
+    int64_t checkpoints;      /* states stored by the forward sweep               */
+    int64_t rhs_evals;        /* right-hand sides: forward + recomputation        */
+    int64_t vjp_evals;        /* transposed right-hand sides of the reverse sweep */
+    int32_t status;
+    int32_t checkpoint_every;
+} tb_adjoint_stats;
+
+/* grad_f = (dF/df)^T theta at f, grad_amp[c] = <theta, dF/d amplitude_c>.
+ * flags: TB_PTR_HOST for f, theta, grad_f; TB_NO_DRIFT; TB_NO_COLLISIONS. */
+int tb_adjoint_rhs_vjp(tb_handle* h, const double* f, const double* theta, double* grad_f, double* grad_amp,
+                       int flags);
+
+/* Forward sweep of a differentiable integration (single-run handles): the
+ * same adaptive integration as tb_dp45_integrate from t0 to t1 with dense
+ * step dense_step, which also logs every accepted step (t, dt) and stores
+ * f after every `checkpoint_every`-th accepted step in device memory.
+ * max_steps bounds the accepted steps (TB_ERR_CAPACITY beyond); the
+ * checkpoints take (max_steps / checkpoint_every + 2) * ndofs doubles.
+ * f_obs (may be NULL) receives f at the last dense output time. */
+int tb_adjoint_forward(tb_handle* h, const double* f0, double t0, double t1, double dense_step,
+                       int checkpoint_every, int64_t max_steps, double* f_obs, tb_adjoint_stats* st, int flags);
+
+/* Reverse sweep for the observable J = <lambda_T, f(t_obs)>: grad_f0 = dJ/df0
+ * and grad_amp[c] = dJ/d amplitude_c of the step sequence the forward sweep
+ * chose (step sizes frozen; their dependence on f is not differentiated).
+ * Recomputes each segment of checkpoint_every steps from its checkpoint. */
+int tb_adjoint_backward(tb_handle* h, const double* lambda_T, double* grad_f0, double* grad_amp,
+                        tb_adjoint_stats* st, int flags);
+
+/* tb_adjoint_forward followed by tb_adjoint_backward. */
+int tb_adjoint_integrate(tb_handle* h, const double* f0, double t0, double t1, double dense_step,
+                         int checkpoint_every, int64_t max_steps, const double* lambda_T, double* f_obs,
+                         double* grad_f0, double* grad_amp, tb_adjoint_stats* st, int flags);
+
+/* The frozen step sizes of the last forward sweep (up to cap of them), their
+ * count and the dense fraction of the observable's step. */
+int tb_adjoint_steps(tb_handle* h, double* dts, int64_t cap, int64_t* n_steps, double* dense_s);
+
+/* Fixed-step Dormand-Prince: n_steps steps of sizes dts (HOST array) from f0,
+ * then the dense output at fraction dense_s of the last step, into f_out.
+ * The same arithmetic as the adaptive integration's accepted steps; replays
+ * a logged step sequence (the map tb_adjoint_backward differentiates). */
+int tb_dp45_replay(tb_handle* h, const double* f0, const double* dts, int64_t n_steps, double dense_s,
+                   double* f_out, int flags);
+
 /* The error norm of ONE band (what Band::relativeError computes for one
  * population) for callers that cannot call cudaMalloc when they need it -- a
  * host application whose device memory is fully reserved by its own pool

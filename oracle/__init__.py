@@ -54,6 +54,7 @@ def lib():
         L.or_dp45.restype = C.c_int
         L.or_dp45.argtypes = [vp, dp, C.c_double, C.c_double, C.c_double, dp, dp, C.c_int,
                               C.POINTER(C.c_int), C.c_int, C.c_int, i64, C.POINTER(i64), dp]
+        L.or_dp45_replay.argtypes = [vp, dp, dp, i64, C.c_double, dp, C.c_int, C.c_int]
         _lib = L
     return _lib
 
@@ -173,6 +174,15 @@ class Oracle:
         return {"rc": rc, "y": y, "dense": dout[:n], "dense_t": dt_[:n], "n_dense": nd.value,
                 "attempts": st[0], "accepted": st[1], "rejected": st[2], "rhs_evals": st[3],
                 "t": ds[0], "dt": ds[1], "last_err": ds[2]}
+
+    def dp45_replay(self, y0, dts, dense_s, drift=True):
+        """Fixed-step Dormand-Prince over dts, then the dense output at dense_s."""
+        y0 = np.ascontiguousarray(y0, dtype=np.float64)
+        dts = np.ascontiguousarray(dts, dtype=np.float64)
+        out = np.empty(self.ndofs)
+        lib().or_dp45_replay(self.h, _dp(y0), _dp(dts), len(dts), float(dense_s), _dp(out), self.nthreads,
+                             1 if drift else 0)
+        return out
 
 
 def scalar_example(t0=0.0, y0=0.0, tf=10.0, dense=1.0, max_dense=64):

@@ -893,6 +893,59 @@ static int dp54_core(int64_t n, double* y_io, double t0, double tf, double dense
     return notfailed ? 0 : TB_ERR_DT_UNDERFLOW;
 }
 
+// Fixed-step replay of accepted Dormand-Prince steps: the step arithmetic of
+// dp54_core above with the step sizes given, then the dense output at
+// fraction dense_s of the last step (DormandPrince54.hpp:598-611).  The
+// reference has no such entry point; it is the map whose derivative the
+// library's discrete adjoint computes (step sizes frozen).
+template <class RHS, class ENF>
+static void dp54_replay_core(int64_t n, const double* y0, const double* dts, int64_t n_steps, double s,
+                             double* out, RHS f_rhs, ENF enforce) {
+    const double a21 = 1. / 5., a31 = 3. / 40., a32 = 9. / 40., a41 = 44. / 45., a42 = -56. / 15., a43 = 32. / 9.,
+                 a51 = 19372. / 6561., a52 = -25360. / 2187., a53 = 64448. / 6561., a54 = -212. / 729.,
+                 a61 = 9017. / 3168., a62 = -355. / 33., a63 = 46732. / 5247., a64 = 49. / 176.,
+                 a65 = -5103. / 18656.;
+    const double b1 = 35. / 384., b3 = 500. / 1113., b4 = 125. / 192., b5 = -2187. / 6784., b6 = 11. / 84.;
+    std::vector<double> y(y0, y0 + n), k1(n), k2(n), k3(n), k4(n), k5(n), k6(n), k7(n), y5(n), tmp(n);
+    enforce(y.data());
+    f_rhs(y.data(), k1.data());
+    for (int64_t st = 0; st < n_steps; ++st) {
+        const double dt = dts[st];
+        for (int64_t i = 0; i < n; ++i) tmp[i] = y[i] + (a21 * dt) * k1[i];
+        enforce(tmp.data()); f_rhs(tmp.data(), k2.data());
+        for (int64_t i = 0; i < n; ++i) tmp[i] = y[i] + (a31 * dt) * k1[i] + (a32 * dt) * k2[i];
+        enforce(tmp.data()); f_rhs(tmp.data(), k3.data());
+        for (int64_t i = 0; i < n; ++i) tmp[i] = y[i] + (a41 * dt) * k1[i] + (a42 * dt) * k2[i] + (a43 * dt) * k3[i];
+        enforce(tmp.data()); f_rhs(tmp.data(), k4.data());
+        for (int64_t i = 0; i < n; ++i)
+            tmp[i] = y[i] + (a51 * dt) * k1[i] + (a52 * dt) * k2[i] + (a53 * dt) * k3[i] + (a54 * dt) * k4[i];
+        enforce(tmp.data()); f_rhs(tmp.data(), k5.data());
+        for (int64_t i = 0; i < n; ++i)
+            tmp[i] = y[i] + (a61 * dt) * k1[i] + (a62 * dt) * k2[i] + (a63 * dt) * k3[i] + (a64 * dt) * k4[i] +
+                     (a65 * dt) * k5[i];
+        enforce(tmp.data()); f_rhs(tmp.data(), k6.data());
+        for (int64_t i = 0; i < n; ++i)
+            y5[i] = y[i] + (dt * b1) * k1[i] + (dt * b3) * k3[i] + (dt * b4) * k4[i] + (dt * b5) * k5[i] +
+                    (dt * b6) * k6[i];
+        enforce(y5.data());
+        f_rhs(y5.data(), k7.data());
+        if (st + 1 == n_steps) {
+            const double bt1 = -(435. * s * s * s - 1184. * s * s + 1098. * s - 384.) / (384.);
+            const double bt3 = 500. * s * (6. * s * s - 14. * s + 9.) / (1113.);
+            const double bt4 = -125. * s * (9. * s * s - 16. * s + 6.) / (192.);
+            const double bt5 = 729. * s * (35. * s * s - 64. * s + 26.) / (6784.);
+            const double bt6 = -11. * s * (3. * s - 2.) * (5. * s - 6.) / (84.);
+            const double bt7 = s * (s - 1.) * (5. * s - 3.) / (2.);
+            for (int64_t i = 0; i < n; ++i)
+                out[i] = y[i] + (s * dt * bt1) * k1[i] + (s * dt * bt3) * k3[i] + (s * dt * bt4) * k4[i] +
+                         (s * dt * bt5) * k5[i] + (s * dt * bt6) * k6[i] + (s * dt * bt7) * k7[i];
+            enforce(out);
+        }
+        y.swap(y5);
+        k1.swap(k7);
+    }
+}
+
 static int dp54(const Problem& P, double* y_io, double t0, double tf, double dense, double* dense_out,
                 double* dense_t, int max_dense, int* n_dense, int nthreads, bool drift, int64_t max_attempts,
                 DPStats& st) {
@@ -1079,6 +1132,15 @@ int or_dp45(void* h, double* y, double t0, double tf, double dense, double* dens
     stats[0] = st.attempts; stats[1] = st.accepted; stats[2] = st.rejected; stats[3] = st.rhs_evals;
     dstats[0] = st.t; dstats[1] = st.dt; dstats[2] = st.last_err;
     return rc;
+}
+
+void or_dp45_replay(void* h, const double* y0, const double* dts, int64_t n_steps, double dense_s, double* out,
+                    int nthreads, int drift) {
+    const Problem& P = *static_cast<Problem*>(h);
+    dp54_replay_core(
+        P.ndofs, y0, dts, n_steps, dense_s, out,
+        [&](const double* in, double* o) { rhs(P, in, o, nthreads, drift != 0); },
+        [&](double* v) { apply_constraints(P, v); });
 }
 
 // The scalar example of the reference's DP54 documentation

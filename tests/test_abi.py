@@ -43,7 +43,8 @@ int main(void) {
          sizeof(tb_channel_desc), sizeof(tb_problem_desc));
   printf("%zu %zu %zu\n", offsetof(tb_channel_desc, umklapp), offsetof(tb_channel_desc, n_tuples),
          offsetof(tb_band_desc, drift_velocity));
-  printf("%zu %zu\n", sizeof(tb_options), sizeof(tb_dp45_stats));
+  printf("%zu %zu %zu %zu\n", sizeof(tb_options), sizeof(tb_dp45_stats), sizeof(tb_adjoint_stats),
+         offsetof(tb_adjoint_stats, status));
   return 0;
 }
 ''')
@@ -54,7 +55,8 @@ int main(void) {
     want = [C.sizeof(abi.TbRegion), C.sizeof(abi.TbMeshDesc), C.sizeof(abi.TbBandDesc),
             C.sizeof(abi.TbChannelDesc), C.sizeof(abi.TbProblemDesc),
             abi.TbChannelDesc.umklapp.offset, abi.TbChannelDesc.n_tuples.offset,
-            abi.TbBandDesc.drift_velocity.offset, C.sizeof(engine.Options), C.sizeof(engine.DP45Stats)]
+            abi.TbBandDesc.drift_velocity.offset, C.sizeof(engine.Options), C.sizeof(engine.DP45Stats),
+            C.sizeof(engine.AdjointStats), engine.AdjointStats.status.offset]
     assert got == want
 
 

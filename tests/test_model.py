@@ -44,3 +44,37 @@ def test_mc_points_in_reference_simplex():
     c = mat.channels[0]
     assert c.mc_points.shape == (50, 5) and c.mc_points_precalc.shape == (50, 5)
     assert not np.array_equal(c.mc_points, c.mc_points_precalc)
+
+
+def test_observable_weights_against_the_oracle_integral():
+    """J = w . f of tortoise_b200.adjoint equals the oracle's mass-matrix
+    integral of f times the weight function (1, E, or dE/dk)."""
+    import oracle
+    from tortoise_b200 import adjoint as A
+    from tortoise_b200 import workloads as W
+    mat = W.build_material(4, ("P", "D"), (0.2,), ee=False, eph=True)
+    f = W.initial_status(mat, kT=0.1, seed=2).vec
+    o = oracle.Oracle(mat, enumerate_tuples=False)
+    offs, _ = mat.band_offsets()
+    for b, band in enumerate(mat.bands):
+        n = band.mesh.ne * 3
+        fb = f[offs[b]:offs[b] + n]
+        one = np.tile([1.0, 0.0, 0.0], band.mesh.ne)
+        assert abs(A.observable_weights(mat, b, "density") @ f - o.integrate(b, fb, one)) < 1e-14
+        want = o.integrate(b, fb, band.dispersion_coeffs)
+        assert abs(A.observable_weights(mat, b, "energy") @ f - want) <= 1e-13 * abs(want)
+
+
+def test_current_weights_of_a_linear_dispersion():
+    """For E = a kx + b ky the band velocity is (a, b) on every element, so
+    the current of f = 1 is (a, b) times the k-space area."""
+    from tortoise_b200 import adjoint as A
+    from tortoise_b200.model import FERMION, Material, Mesh, Region
+    region = Region((-1.0, -1.0), ((2.0, 0.0), (0.0, 2.0)))
+    mesh = Mesh(region, (0.0, 0.0), (1.0, 1.0), (5, 3))
+    mat = Material("lin", region)
+    mat.addBand("el:L", -1.0, FERMION, mesh, lambda kx, ky: 0.7 * kx - 0.2 * ky)
+    f = np.tile([1.0, 0.0, 0.0], mesh.ne)
+    jx = A.observable_weights(mat, 0, "current", 0) @ f
+    jy = A.observable_weights(mat, 0, "current", 1) @ f
+    assert abs(jx - 0.7 * 4.0) < 1e-12 and abs(jy + 0.2 * 4.0) < 1e-12

@@ -23,6 +23,8 @@ SOURCES = {
     "tb_dp45.cu": [],
     "tb_tensor.cu": [],
     "tb_static_scratch.cu": [],
+    "tb_vjp.cu": [],
+    "tb_adjoint.cu": [],
 }
 
 

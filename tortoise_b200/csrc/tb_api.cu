@@ -14,10 +14,7 @@
 #include <string>
 #include <vector>
 
-#include "tb_dp45.cuh"
-#include "tb_enumerate.cuh"
-#include "tb_kernels.cuh"
-#include "tb_tensor.cuh"
+#include "tb_handle.cuh"
 
 namespace tb {
 
@@ -93,80 +90,15 @@ static std::vector<double> coord_function(const HostMesh& m, int dim) {
     return v;
 }
 
-// A channel structure shared by every run of the same structure: the tuple
-// list, the moment tensor and the Monte-Carlo tables exist once.
-struct GroupChan {
-    ChanDev dev;                  // table pointers of the group's first run
-    int L = 0;
-    double* d_umk = nullptr;
-    double* d_mc = nullptr;
-    double* d_mc_pre = nullptr;
-    DeviceTuples tup;
-    int64_t diag[3] = {0, 0, 0};
-    int layout = TB_LAYOUT_MC64;
-    MomentTensor tensor;
-    std::vector<int> insts;       // channel instances using it (run order)
-    InstDev* d_insts = nullptr;   // [insts.size()]
-};
-
-// One run's channel (the unit tb_channel_info / tb_set_amplitude address).
-struct ChanInst {
-    int group = 0;
-    int run = 0;
-    int band[TB_MAX_LEGS] = {0, 0, 0, 0};   // global band ids
-    double amplitude = 0.0;
-    InstDev dev{};
-    InstDev* d_single = nullptr;  // this instance alone (single-channel calls)
-    int slot = 0;                 // position inside the group's d_insts
-};
-
-struct RunInfo {
-    int band0 = 0, nbands = 0;
-    int64_t dof_off = 0, ndofs = 0;
-    int chan0 = 0, nchans = 0;
-};
-
 }  // namespace tb
 
 using namespace tb;
 
 namespace tb {
 int choose_layouts(tb_handle* h);
-int run_rhs_acc(tb_handle* h, const double* d_in, double* d_acc, const DPCtl* ctl, int flags, int only_inst);
 }  // namespace tb
 
-struct tb_handle {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    tb_options opts{};
-    std::vector<HostMesh> meshes;
-    std::vector<HostBand> bands;
-    std::vector<BandDev> banddev;
-    std::vector<double*> dev_allocs;
-    std::vector<void*> dev_raw;
-    std::vector<RunInfo> runs;
-    std::vector<GroupChan> groups;
-    std::vector<ChanInst> insts;
-    ElemDev ed{};
-    bool any_drift = false;
-    int64_t ndofs = 0;
-    double* d_f = nullptr;
-    double* d_out = nullptr;
-    double* d_acc = nullptr;
-    double* d_part = nullptr;
-    // DP45
-    DPBufs dp{};
-    bool dp_ready = false;
-    int64_t dense_cap_alloc = -1;
-    RunDev* d_runs = nullptr;
-    std::vector<RunDev> hruns;
-    cudaGraphExec_t graph = nullptr;
-    int graph_flags = -1;
-    DPCtl* h_ctl = nullptr;   // pinned host mirror [nruns]
-    int dp_flags = 0;
-};
-
-namespace {
+namespace tb {
 
 double* dev_alloc(tb_handle* h, size_t n) {
     double* p = nullptr;
@@ -533,7 +465,7 @@ int build_runs(tb_handle* h, const tb_problem_desc* const* descs, int nruns) {
     return TB_OK;
 }
 
-}  // namespace
+}  // namespace tb
 
 // The RHS accumulation (pre-M^-1) of the input state into acc (which must be zero).
 namespace tb {
@@ -594,7 +526,7 @@ int choose_layouts(tb_handle* h) {
 }  // namespace tb
 
 // ---------------------------------------------------------------- DP45 glue
-namespace {
+namespace tb {
 
 int dp_alloc(tb_handle* h, int64_t max_dense) {
     const int nruns = int(h->runs.size());
@@ -699,7 +631,7 @@ void fill_stats(const DPCtl& c, tb_dp45_stats* st) {
     st->done = c.done;
 }
 
-}  // namespace
+}  // namespace tb
 
 // ====================================================================== C API
 extern "C" {
@@ -737,6 +669,7 @@ int tb_destroy(tb_handle* h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->graph) cudaGraphExecDestroy(h->graph);
+    adjoint_release(h);
     for (auto& G : h->groups) { G.tup.release(); G.tensor.release(); }
     for (double* p : h->dev_allocs) cudaFree(p);
     for (void* p : h->dev_raw) cudaFree(p);
@@ -893,8 +826,16 @@ int tb_apply_constraints(tb_handle* h, double* f, int flags) {
     return TB_OK;
 }
 
-int tb_dp45_begin_batch(tb_handle* h, const double* f0, const double* t0, const double* t_final,
-                        const double* dense_step, int64_t max_dense, int flags) {
+}  // extern "C"
+
+namespace tb {
+
+// Start a (batched) integration.  `hooks` carries the adjoint recording
+// buffers (step log, checkpoints) or is null for a plain integration; the
+// captured attempt graph holds the DPBufs by value, so a change of hooks
+// re-captures it.
+int dp_begin(tb_handle* h, const double* f0, const double* t0, const double* t_final, const double* dense_step,
+             int64_t max_dense, int flags, const DPBufs* hooks) {
     if (!h || !f0 || !t0 || !t_final || !dense_step) { set_error("null argument"); return TB_ERR_ARG; }
     const int nruns = int(h->runs.size());
     for (int r = 0; r < nruns; ++r)
@@ -905,6 +846,19 @@ int tb_dp45_begin_batch(tb_handle* h, const double* f0, const double* t0, const 
     h->dp_flags = flags;
     const size_t bytes = sizeof(double) * size_t(h->ndofs);
     DPBufs& B = h->dp;
+    {
+        const DPBufs none{};
+        const DPBufs& hk = hooks ? *hooks : none;
+        if (B.step_log != hk.step_log || B.log_cap != hk.log_cap || B.ckpt != hk.ckpt ||
+            B.ckpt_every != hk.ckpt_every || B.ckpt_cap != hk.ckpt_cap) {
+            B.step_log = hk.step_log;
+            B.log_cap = hk.log_cap;
+            B.ckpt = hk.ckpt;
+            B.ckpt_every = hk.ckpt_every;
+            B.ckpt_cap = hk.ckpt_cap;
+            if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+        }
+    }
     TB_CUDA(cudaMemcpyAsync(B.y, f0, bytes, (flags & TB_PTR_HOST) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
                             h->stream));
     TB_CUDA(cudaStreamSynchronize(h->stream));   // the pinned mirror is rewritten below
@@ -922,6 +876,7 @@ int tb_dp45_begin_batch(tb_handle* h, const double* f0, const double* t0, const 
         c.dense_cap = max_dense;
         c.rhs_evals = 1;
         c.done = (t0[r] < t_final[r]) ? 0 : 1;
+        c.last_dense_step = -1;
     }
     TB_CUDA(cudaMemcpyAsync(B.ctl, h->h_ctl, sizeof(DPCtl) * nruns, cudaMemcpyHostToDevice, h->stream));
     // k1 = timeOp(t0, enforceValue(t0, y0))
@@ -929,8 +884,18 @@ int tb_dp45_begin_batch(tb_handle* h, const double* f0, const double* t0, const 
     TB_CUDA(cudaMemsetAsync(B.acc, 0, bytes, h->stream));
     TB_TRY(run_rhs_acc(h, B.tmp, B.acc, nullptr, rflags, -1));
     TB_TRY(launch_k1(h->ed, B, h->stream));
+    if (B.ckpt) TB_CUDA(cudaMemcpyAsync(B.ckpt, B.tmp, bytes, cudaMemcpyDeviceToDevice, h->stream));
     TB_TRY(ensure_graph(h, rflags));
     return TB_OK;
+}
+
+}  // namespace tb
+
+extern "C" {
+
+int tb_dp45_begin_batch(tb_handle* h, const double* f0, const double* t0, const double* t_final,
+                        const double* dense_step, int64_t max_dense, int flags) {
+    return dp_begin(h, f0, t0, t_final, dense_step, max_dense, flags, nullptr);
 }
 
 int tb_dp45_begin(tb_handle* h, const double* f0, double t0, double t_final, double dense_step, int64_t max_dense,

@@ -186,6 +186,20 @@ __global__ void k_controller(ElemDev ed, DPBufs B) {
         if (k > TB_MAX_DENSE_PER_STEP) { c->status = TB_ERR_CAPACITY; k = TB_MAX_DENSE_PER_STEP; }
         c->n_now = k;
         c->dense_time = dtime;
+        if (k > 0) {
+            c->last_dense_step = c->accepted;
+            c->last_dense_s = c->dense_s[(k < TB_MAX_DENSE_PER_STEP ? k : TB_MAX_DENSE_PER_STEP) - 1];
+        }
+        if (B.step_log) {
+            if (c->accepted < B.log_cap) {
+                B.step_log[2 * c->accepted] = t;
+                B.step_log[2 * c->accepted + 1] = dt;
+            } else {
+                c->status = TB_ERR_CAPACITY;
+            }
+            const long long na = c->accepted + 1;
+            if (B.ckpt && na % B.ckpt_every == 0 && na / B.ckpt_every >= B.ckpt_cap) c->status = TB_ERR_CAPACITY;
+        }
         t += dt;
         double scale;
         if (errNorm == 0.) scale = maxscale;
@@ -265,6 +279,14 @@ __global__ void __launch_bounds__(256) k_dense_commit(ElemDev ed, DPBufs B) {
     for (int cc = 0; cc < 3; ++cc) {
         B.y[o + cc] = B.y5[o + cc];
         B.k[0][o + cc] = B.k[6][o + cc];
+    }
+    if (B.ckpt && c->accepted % B.ckpt_every == 0) {
+        // c->accepted already counts this step
+        const long long slot = c->accepted / B.ckpt_every;
+        if (slot < B.ckpt_cap) {
+            double* ck = B.ckpt + slot * run.ndofs + (o - run.dof_off);
+            ck[0] = B.y5[o]; ck[1] = B.y5[o + 1]; ck[2] = B.y5[o + 2];
+        }
     }
 }
 

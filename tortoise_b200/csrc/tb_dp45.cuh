@@ -24,6 +24,8 @@ struct DPCtl {
     double dense_s[TB_MAX_DENSE_PER_STEP];
     double dense_t[TB_MAX_DENSE_PER_STEP];
     long long max_attempts;  // 0 = unbounded
+    long long last_dense_step;  // index (among accepted steps) of the step that made the last dense output
+    double last_dense_s;        // its dense-output fraction s in (0, 1.0001]
 };
 
 // Per-run layout inside the concatenated state of a batch.
@@ -48,6 +50,14 @@ struct DPBufs {
     double* dense;   // per-run dense blocks [slot][ndofs_run]
     double* dense_t; // per-run dense times [slot]
     DPCtl* ctl;      // [nruns]
+    // adjoint recording (single run; null in a plain integration):
+    // step_log[2 n], step_log[2 n + 1] = t, dt of accepted step n;
+    // ckpt[c] = y after accepted step c * ckpt_every (ckpt[0] = enforced y0)
+    double* step_log;
+    long long log_cap;
+    double* ckpt;
+    long long ckpt_every;
+    long long ckpt_cap;
 };
 
 // Stage kernel s (0..6) of one attempt:

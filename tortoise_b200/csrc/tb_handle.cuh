@@ -1,0 +1,98 @@
+// tb_handle.cuh -- the library handle and the host-side helpers shared by
+// the C ABI (tb_api.cu) and the adjoint driver (tb_adjoint.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "tb_dp45.cuh"
+#include "tb_enumerate.cuh"
+#include "tb_kernels.cuh"
+#include "tb_tensor.cuh"
+
+namespace tb {
+
+// A channel structure shared by every run of the same structure: the tuple
+// list, the moment tensor and the Monte-Carlo tables exist once.
+struct GroupChan {
+    ChanDev dev;                  // table pointers of the group's first run
+    int L = 0;
+    double* d_umk = nullptr;
+    double* d_mc = nullptr;
+    double* d_mc_pre = nullptr;
+    DeviceTuples tup;
+    int64_t diag[3] = {0, 0, 0};
+    int layout = TB_LAYOUT_MC64;
+    MomentTensor tensor;
+    std::vector<int> insts;       // channel instances using it (run order)
+    InstDev* d_insts = nullptr;   // [insts.size()]
+};
+
+// One run's channel (the unit tb_channel_info / tb_set_amplitude address).
+struct ChanInst {
+    int group = 0;
+    int run = 0;
+    int band[TB_MAX_LEGS] = {0, 0, 0, 0};   // global band ids
+    double amplitude = 0.0;
+    InstDev dev{};
+    InstDev* d_single = nullptr;  // this instance alone (single-channel calls)
+    int slot = 0;                 // position inside the group's d_insts
+};
+
+struct RunInfo {
+    int band0 = 0, nbands = 0;
+    int64_t dof_off = 0, ndofs = 0;
+    int chan0 = 0, nchans = 0;
+};
+
+struct AdjointState;
+
+}  // namespace tb
+
+struct tb_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    tb_options opts{};
+    std::vector<tb::HostMesh> meshes;
+    std::vector<tb::HostBand> bands;
+    std::vector<tb::BandDev> banddev;
+    std::vector<double*> dev_allocs;
+    std::vector<void*> dev_raw;
+    std::vector<tb::RunInfo> runs;
+    std::vector<tb::GroupChan> groups;
+    std::vector<tb::ChanInst> insts;
+    tb::ElemDev ed{};
+    bool any_drift = false;
+    int64_t ndofs = 0;
+    double* d_f = nullptr;
+    double* d_out = nullptr;
+    double* d_acc = nullptr;
+    double* d_part = nullptr;
+    // DP45
+    tb::DPBufs dp{};
+    bool dp_ready = false;
+    int64_t dense_cap_alloc = -1;
+    tb::RunDev* d_runs = nullptr;
+    std::vector<tb::RunDev> hruns;
+    cudaGraphExec_t graph = nullptr;
+    int graph_flags = -1;
+    tb::DPCtl* h_ctl = nullptr;   // pinned host mirror [nruns]
+    int dp_flags = 0;
+    // adjoint (tb_adjoint.cu)
+    tb::AdjointState* adj = nullptr;
+};
+
+
+namespace tb {
+
+double* dev_alloc(tb_handle* h, size_t n);
+int run_rhs_acc(tb_handle* h, const double* d_in, double* d_acc, const DPCtl* ctl, int flags, int only_inst);
+int dp_alloc(tb_handle* h, int64_t max_dense);
+int ensure_graph(tb_handle* h, int flags);
+int dp_begin(tb_handle* h, const double* f0, const double* t0, const double* t_final, const double* dense_step,
+             int64_t max_dense, int flags, const DPBufs* hooks);
+void adjoint_release(tb_handle* h);
+
+}  // namespace tb

@@ -1,0 +1,405 @@
+// tb_vjp.cu -- vector-Jacobian products of the right-hand side
+// F(f) = M^-1 (C(f) + V f)  (collision operator C, Vlasov drift V).
+//
+// No counterpart in the reference (it has no derivatives); these are the
+// exact transposes of the forward kernels in tb_collision.cu, tb_tensor.cu,
+// tb_drift.cu and of applyInverseMass:
+//   u        = M^-T theta                      (per element)
+//   grad_f  += C'(f)^T u  + V^T u
+//   grad_amp[c] = <u, C_c(f)> / amplitude_c    (C_c is linear in its amplitude)
+// Each leg factor of a tuple is affine in its element's 3 coefficients of f
+// (ScatteringChannel.cpp:633-641), so the derivative of the product of L
+// factors is the sum over legs of (other legs' factors) x (that leg's slope).
+#include "tb_dp45.cuh"
+#include "tb_geom.cuh"
+#include "tb_tensor.cuh"
+#include "tb_vjp.cuh"
+
+namespace tb {
+
+template <int L> struct VDim {
+    static constexpr int K = (L == 2) ? 9 : (L == 3) ? 27 : 81;
+    static constexpr int KM = K / 3;
+    static constexpr int NMOM = K * (1 + L);
+};
+
+__device__ __forceinline__ void block_atomic_sum(double v, double* dst) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(dst, v);
+}
+
+// ---------------------------------------------------------------- M^-T
+__global__ void k_minv_t(ElemDev ed, const double* __restrict__ theta, double* __restrict__ u) {
+    const int band = ed.blk_band[blockIdx.x];
+    const BandDev& bd = ed.bands[band];
+    const int e = (blockIdx.x - ed.blk_first[band]) * blockDim.x + threadIdx.x;
+    if (e >= bd.ne) return;
+    const int64_t o = bd.off + 3 * (int64_t)e;
+    const double t0 = theta[o], t1 = theta[o + 1], t2 = theta[o + 2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) u[o + i] = bd.mesh.Minv[i][0] * t0 + bd.mesh.Minv[i][1] * t1 + bd.mesh.Minv[i][2] * t2;
+}
+
+// Zero the constrained bands (the projection of MaterialStatus::applyConstraints).
+__global__ void k_project(ElemDev ed, double* __restrict__ v) {
+    const int band = ed.blk_band[blockIdx.x];
+    const BandDev& bd = ed.bands[band];
+    if (!bd.constrained) return;
+    const int e = (blockIdx.x - ed.blk_first[band]) * blockDim.x + threadIdx.x;
+    if (e >= bd.ne) return;
+    const int64_t o = bd.off + 3 * (int64_t)e;
+    v[o] = 0.0; v[o + 1] = 0.0; v[o + 2] = 0.0;
+}
+
+int launch_minv_t(const ElemDev& ed, const double* theta, double* u, cudaStream_t s) {
+    k_minv_t<<<ed.nblk, 256, 0, s>>>(ed, theta, u);
+    TB_CUDA(cudaGetLastError());
+    return TB_OK;
+}
+
+int launch_project(const ElemDev& ed, double* v, cudaStream_t s) {
+    k_project<<<ed.nblk, 256, 0, s>>>(ed, v);
+    TB_CUDA(cudaGetLastError());
+    return TB_OK;
+}
+
+// ----------------------------------------------------------- forms of f
+template <int L>
+__device__ __forceinline__ void leg_forms(const ChanDev& c, const InstDev& in, const double* f, const int (&e)[L],
+                                          double (&A)[L][3], double (&B)[L][3], double (&sa)[L], double (&sb)[L]) {
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+        const double d = c.leg[l].dir, s = c.leg[l].stat;
+        const double* fe = f + in.foff[l] + 3 * (int64_t)e[l];
+        const double ka = (l == 0 ? -1.0 : 1.0) * 0.5;
+        const double ca = (1. - d) * s + (1. + d);
+        const double cb = (1. + d) * s + (1. - d);
+        sa[l] = ka * ca;    // dA[l][j] / df_j
+        sb[l] = 0.5 * cb;   // dB[l][j] / df_j
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const double unit = (j == 0) ? 1.0 : 0.0;
+            const double fj = __ldg(fe + j);
+            A[l][j] = ka * ((1. - d) * unit + ca * fj);
+            B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
+        }
+    }
+}
+
+// --------------------------------------------- collision VJP, Monte-Carlo
+template <int L>
+__global__ void __launch_bounds__(128) k_vjp_mc(ChanDev c, const InstDev* __restrict__ insts, int n_insts,
+                                                const int32_t* __restrict__ tup, int64_t stride, int64_t n,
+                                                const double* __restrict__ f, const double* __restrict__ u,
+                                                double* __restrict__ grad_f, double* __restrict__ grad_amp) {
+    extern __shared__ double s_mc[];
+    constexpr int R = 2 * (L - 2) + 1;
+    for (int i = threadIdx.x; i < c.nmc * R; i += blockDim.x) s_mc[i] = c.mc[i];
+    __syncthreads();
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        bool valid = i < n;
+        int e[L];
+#pragma unroll
+        for (int l = 0; l < L; ++l) e[l] = valid ? __ldg(tup + l * stride + i) : 0;
+        const int uu = valid ? __ldg(tup + L * stride + i) : 0;
+        TupleGeom<L> g;
+        tuple_geometry<L>(c, e, uu, g);
+        if (!(fabs(g.det) >= c.min_det)) valid = false;
+        double Ci[3][3];
+        dc_inverse<L>(g, Ci);
+        const double scale = valid ? 1.0 / (c.fact * double(c.nmc) * fabs(g.det)) : 0.0;
+        for (int k = 0; k < n_insts; ++k) {
+            const InstDev in = insts[k];
+            double A[L][3], B[L][3], sa[L], sb[L];
+            leg_forms<L>(c, in, f, e, A, B, sa, sb);
+            double ul[L][3];
+#pragma unroll
+            for (int l = 0; l < L; ++l)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) ul[l][j] = c.leg[l].dir * __ldg(u + in.foff[l] + 3 * (int64_t)e[l] + j);
+            double gA[L][3], gB[L][3], gamp = 0.0;
+#pragma unroll
+            for (int l = 0; l < L; ++l)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) { gA[l][j] = 0.0; gB[l][j] = 0.0; }
+            if (valid) {
+                for (int m = 0; m < c.nmc; ++m) {
+                    const double* qv = s_mc + m * R;
+                    double p[L][2];
+                    if (!mc_point_exact<L>(g, Ci, qv, p)) continue;
+                    double av[L], bv[L];
+#pragma unroll
+                    for (int l = 0; l < L; ++l) {
+                        av[l] = (A[l][1] * p[l][0] + A[l][2] * p[l][1]) + A[l][0];
+                        bv[l] = (B[l][1] * p[l][0] + B[l][2] * p[l][1]) + B[l][0];
+                    }
+                    double om = 0.0;   // sum over legs of dir * (u . test functions)
+#pragma unroll
+                    for (int l = 0; l < L; ++l) om += ul[l][0] + ul[l][1] * p[l][0] + ul[l][2] * p[l][1];
+                    double pa = 1.0, pb = 1.0;
+#pragma unroll
+                    for (int l = 0; l < L; ++l) { pa *= av[l]; pb *= bv[l]; }
+                    gamp += om * (pa + pb);
+#pragma unroll
+                    for (int mm = 0; mm < L; ++mm) {
+                        double ra = om, rb = om;
+#pragma unroll
+                        for (int l = 0; l < L; ++l)
+                            if (l != mm) { ra *= av[l]; rb *= bv[l]; }
+                        gA[mm][0] += ra; gA[mm][1] += ra * p[mm][0]; gA[mm][2] += ra * p[mm][1];
+                        gB[mm][0] += rb; gB[mm][1] += rb * p[mm][0]; gB[mm][2] += rb * p[mm][1];
+                    }
+                }
+            }
+            if (valid) {
+                const double sc = scale * in.amp_full;
+#pragma unroll
+                for (int l = 0; l < L; ++l) {
+                    double* o = grad_f + in.foff[l] + 3 * (int64_t)e[l];
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) atomicAdd(o + j, sc * (sa[l] * gA[l][j] + sb[l] * gB[l][j]));
+                }
+            }
+            block_atomic_sum(valid ? scale * c.amp_vol * gamp : 0.0, grad_amp + k);
+        }
+    }
+}
+
+// --------------------------------------------- collision VJP, moment tensor
+template <int L, typename T>
+__global__ void __launch_bounds__(128) k_vjp_tensor(ChanDev c, const InstDev* __restrict__ insts, int n_insts,
+                                                    const T* __restrict__ mom, int TT, const int32_t* __restrict__ tup,
+                                                    int64_t stride, int64_t n, const double* __restrict__ f,
+                                                    const double* __restrict__ u, double* __restrict__ grad_f,
+                                                    double* __restrict__ grad_amp) {
+    constexpr int K = VDim<L>::K, KM = VDim<L>::KM, NMOM = VDim<L>::NMOM;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        const bool valid = i < n;
+        int e[L];
+#pragma unroll
+        for (int l = 0; l < L; ++l) e[l] = valid ? __ldg(tup + l * stride + i) : 0;
+        const T* mt = mom + (i / TT) * (int64_t)NMOM * TT + (i % TT);
+        for (int k = 0; k < n_insts; ++k) {
+            const InstDev in = insts[k];
+            double A[L][3], B[L][3], sa[L], sb[L];
+            leg_forms<L>(c, in, f, e, A, B, sa, sb);
+            // w[J] = sum_{lam, beta} dir_lam u[e_lam, beta] W[lam, beta][J]
+            double w[K];
+#pragma unroll
+            for (int j = 0; j < K; ++j) w[j] = 0.0;
+            if (valid) {
+                double usum0 = 0.0;
+#pragma unroll
+                for (int lam = 0; lam < L; ++lam) usum0 += c.leg[lam].dir * __ldg(u + in.foff[lam] + 3 * (int64_t)e[lam]);
+#pragma unroll
+                for (int j = 0; j < K; ++j) w[j] = usum0 * double(mt[(int64_t)j * TT]);
+#pragma unroll
+                for (int lam = 0; lam < L; ++lam) {
+                    const double d = c.leg[lam].dir;
+                    const double u1 = d * __ldg(u + in.foff[lam] + 3 * (int64_t)e[lam] + 1);
+                    const double u2 = d * __ldg(u + in.foff[lam] + 3 * (int64_t)e[lam] + 2);
+                    int sstep = 1;
+#pragma unroll
+                    for (int l = L - 1; l > lam; --l) sstep *= 3;
+#pragma unroll
+                    for (int km = 0; km < KM; ++km) {
+                        const int hi = km / sstep, lo = km % sstep;
+                        const int j0 = hi * 3 * sstep + lo, j1 = j0 + sstep, j2 = j0 + 2 * sstep;
+                        const double qxx = double(mt[(int64_t)(K + (lam * 3 + 0) * KM + km) * TT]);
+                        const double qxy = double(mt[(int64_t)(K + (lam * 3 + 1) * KM + km) * TT]);
+                        const double qyy = double(mt[(int64_t)(K + (lam * 3 + 2) * KM + km) * TT]);
+                        const double s1 = double(mt[(int64_t)j1 * TT]);
+                        const double s2 = double(mt[(int64_t)j2 * TT]);
+                        w[j0] += u1 * s1 + u2 * s2;
+                        w[j1] += u1 * qxx + u2 * qxy;
+                        w[j2] += u1 * qxy + u2 * qyy;
+                    }
+                }
+            }
+            // d/dA[m][j] of sum_J w[J] prod_l A[l][J_l]; the same for B
+            double gA[L][3], gB[L][3], gamp = 0.0;
+#pragma unroll
+            for (int l = 0; l < L; ++l)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) { gA[l][j] = 0.0; gB[l][j] = 0.0; }
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                int J[L];
+                int r = j;
+#pragma unroll
+                for (int l = L - 1; l >= 0; --l) { J[l] = r % 3; r /= 3; }
+                double pa = 1.0, pb = 1.0;
+#pragma unroll
+                for (int l = 0; l < L; ++l) { pa *= A[l][J[l]]; pb *= B[l][J[l]]; }
+                gamp += w[j] * (pa + pb);
+#pragma unroll
+                for (int mm = 0; mm < L; ++mm) {
+                    double ra = w[j], rb = w[j];
+#pragma unroll
+                    for (int l = 0; l < L; ++l)
+                        if (l != mm) { ra *= A[l][J[l]]; rb *= B[l][J[l]]; }
+                    gA[mm][J[mm]] += ra;
+                    gB[mm][J[mm]] += rb;
+                }
+            }
+            if (valid) {
+#pragma unroll
+                for (int l = 0; l < L; ++l) {
+                    double* o = grad_f + in.foff[l] + 3 * (int64_t)e[l];
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) atomicAdd(o + j, in.amplitude * (sa[l] * gA[l][j] + sb[l] * gB[l][j]));
+                }
+            }
+            block_atomic_sum(valid ? gamp : 0.0, grad_amp + k);
+        }
+    }
+}
+
+int launch_collision_vjp(const ChanDev& c, const InstDev* insts, int n_insts, int layout, const MomentTensor& T,
+                         const int32_t* tup, int64_t stride, int64_t n, const double* f, const double* u,
+                         double* grad_f, double* grad_amp, cudaStream_t s) {
+    if (n <= 0 || n_insts <= 0) return TB_OK;
+    const int threads = 128;
+    int64_t blocks = (n + threads - 1) / threads;
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    if (layout == TB_LAYOUT_MC64) {
+        const size_t smem = sizeof(double) * size_t(c.nmc) * c.R;
+        switch (c.L) {
+            case 2: k_vjp_mc<2><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, u, grad_f, grad_amp); break;
+            case 3: k_vjp_mc<3><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, u, grad_f, grad_amp); break;
+            default: k_vjp_mc<4><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, u, grad_f, grad_amp); break;
+        }
+    } else {
+        const int TT = (c.L == 4) ? 32 : (T.fp32 ? 128 : 64);
+        switch (c.L * 2 + (T.fp32 ? 1 : 0)) {
+            case 4: k_vjp_tensor<2, double><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, (const double*)T.d, TT, tup, stride, n, f, u, grad_f, grad_amp); break;
+            case 5: k_vjp_tensor<2, float><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, (const float*)T.d, TT, tup, stride, n, f, u, grad_f, grad_amp); break;
+            case 6: k_vjp_tensor<3, double><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, (const double*)T.d, TT, tup, stride, n, f, u, grad_f, grad_amp); break;
+            case 7: k_vjp_tensor<3, float><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, (const float*)T.d, TT, tup, stride, n, f, u, grad_f, grad_amp); break;
+            case 8: k_vjp_tensor<4, double><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, (const double*)T.d, TT, tup, stride, n, f, u, grad_f, grad_amp); break;
+            default: k_vjp_tensor<4, float><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, (const float*)T.d, TT, tup, stride, n, f, u, grad_f, grad_amp); break;
+        }
+    }
+    TB_CUDA(cudaGetLastError());
+    return TB_OK;
+}
+
+// ---------------------------------------------------------- drift VJP
+// Transpose of k_drift: the volume term couples an element to itself, the
+// upwind surface term couples the element to the face neighbour it reads.
+__device__ __forceinline__ int adj_el(int nx, int nt, int e, int face) {
+    if (e & 1) {
+        if (face == 0) return (e + 2 * nx - 1 + nt) % nt;
+        if (face == 1) return e - 1;
+        return ((e - 1) % (2 * nx) == 0) ? e + 2 * nx - 3 : e - 3;
+    } else {
+        if (face == 0) return ((e + 2) % (2 * nx) == 0) ? e - 2 * nx + 3 : e + 3;
+        if (face == 1) return e + 1;
+        return (e - 2 * nx + 1 + nt) % nt;
+    }
+}
+
+__device__ __forceinline__ void normal_of(const MeshDev& m, int e, int face, double n[2]) {
+    const double d00 = m.dG[0][0], d01 = m.dG[0][1], d10 = m.dG[1][0], d11 = m.dG[1][1];
+    double v0, v1, sgn;
+    if (e & 1) {
+        if (face == 0) { v0 = d10; v1 = -d00; sgn = (v0 * d01 + v1 * d11 > 0.) ? 1. : -1.; }
+        else if (face == 1) { v0 = d11 + d10; v1 = -d01 - d00; sgn = (v0 * d00 + v1 * d10 > 0.) ? 1. : -1.; }
+        else { v0 = d11; v1 = -d01; sgn = (v0 * d00 + v1 * d10 > 0.) ? -1. : 1.; }
+    } else {
+        if (face == 0) { v0 = d11; v1 = -d01; sgn = (v0 * d00 + v1 * d10 > 0.) ? 1. : -1.; }
+        else if (face == 1) { v0 = d11 + d10; v1 = -d01 - d00; sgn = (v0 * d00 + v1 * d10 > 0.) ? -1. : 1.; }
+        else { v0 = d10; v1 = -d00; sgn = (v0 * d01 + v1 * d11 > 0.) ? -1. : 1.; }
+    }
+    const double nn = sqrt(v0 * v0 + v1 * v1);
+    n[0] = v0 / nn * sgn;
+    n[1] = v1 / nn * sgn;
+}
+
+__device__ __forceinline__ double area_of(const MeshDev& m, int e, int face) {
+    const double d00 = m.dG[0][0], d01 = m.dG[0][1], d10 = m.dG[1][0], d11 = m.dG[1][1];
+    const int ff = (e & 1) ? face : 2 - face;
+    if (ff == 0) return sqrt(d00 * d00 + d10 * d10);
+    if (ff == 1) return sqrt((d00 + d01) * (d00 + d01) + (d10 + d11) * (d10 + d11));
+    return sqrt(d01 * d01 + d11 * d11);
+}
+
+__device__ __forceinline__ void side_pt(int side, int q, double& x, double& y) {
+    const double g = q ? TB_GP1_1 : TB_GP1_0;
+    if (side == 0) { x = 1. - g; y = g; }
+    else if (side == 1) { x = 0.; y = g; }
+    else { x = g; y = 0.; }
+}
+
+__global__ void __launch_bounds__(256) k_drift_vjp(ElemDev ed, const double* __restrict__ u, double* __restrict__ grad_f) {
+    const int band = ed.blk_band[blockIdx.x];
+    const BandDev& bd = ed.bands[band];
+    const double vel0 = bd.vel[0], vel1 = bd.vel[1];
+    if (vel0 == 0.0 && vel1 == 0.0) return;
+    const int e = (blockIdx.x - ed.blk_first[band]) * blockDim.x + threadIdx.x;
+    if (e >= bd.ne) return;
+    const MeshDev m = bd.mesh;
+    const int nt = m.ne;
+    const double* ub = u + bd.off;
+    double* gb = grad_f + bd.off;
+    const double ue[3] = {ub[3 * e], ub[3 * e + 1], ub[3 * e + 2]};
+    // volume: out[e,b] += vol * (v0 dx_b + v1 dy_b) * sum_q w_q f_e(q)
+    const int s = e / 2, par = e & 1;
+    const double sx = double(s % m.nx), sy = double(s / m.nx);
+    double vx[3], vy[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double ox = (k == 0) ? 0.0 : (par ? (k == 1 ? 0.0 : 1.0) : 1.0);
+        const double oy = (k == 0) ? 0.0 : (par ? 1.0 : (k == 1 ? 0.0 : 1.0));
+        const double px = sx + ox, py = sy + oy;
+        vx[k] = m.rel_origin[0] + (m.dG[0][0] * px + m.dG[0][1] * py);
+        vy[k] = m.rel_origin[1] + (m.dG[1][0] * px + m.dG[1][1] * py);
+    }
+    const double v0X = vx[0], v0Y = vy[0], v1X = vx[1], v1Y = vy[1], v2X = vx[2], v2Y = vy[2];
+    const double denx = v0Y * (v1X - v2X) + v1Y * (v2X - v0X) + v2Y * (v0X - v1X);
+    const double deny = v0X * (v1Y - v2Y) + v1X * (v2Y - v0Y) + v2X * (v0Y - v1Y);
+    const double dx[3] = {0.0, (v0Y - v2Y) / denx, -(v0Y - v1Y) / denx};
+    const double dy[3] = {0.0, (v0X - v2X) / deny, -(v0X - v1X) / deny};
+    double coef = 0.0;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) coef += ue[b] * (m.vol * vel0 * dx[b] + m.vol * vel1 * dy[b]);
+    // d/dc_j of sum_q w f(q) with f(q) = c0 + c1 x_q + c2 y_q
+    const double w = TB_GW2, ga = TB_GP2_A, gbb = TB_GP2_B;
+    atomicAdd(gb + 3 * e + 0, coef * (3.0 * w));
+    atomicAdd(gb + 3 * e + 1, coef * (w * (ga + gbb + ga)));
+    atomicAdd(gb + 3 * e + 2, coef * (w * (ga + ga + gbb)));
+    // surface: out[e,b] -= s * area * sum_q 0.5 phi_b(pt(side,q)) f_ei(pt(si,q))
+#pragma unroll
+    for (int side = 0; side < 3; ++side) {
+        double n[2];
+        normal_of(m, e, side, n);
+        const double sv = vel0 * n[0] + vel1 * n[1];
+        int ei, si;
+        if (sv > 0.) { ei = e; si = side; }
+        else { ei = adj_el(m.nx, nt, e, side); si = 2 - side; }
+        const double area = area_of(m, e, side);
+        double g3[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            double bx, by, xi, yi;
+            side_pt(side, q, bx, by);
+            side_pt(si, q, xi, yi);
+            const double phiu = ue[0] + ue[1] * bx + ue[2] * by;
+            const double wq = -sv * area * 0.5 * phiu;
+            g3[0] += wq; g3[1] += wq * xi; g3[2] += wq * yi;
+        }
+#pragma unroll
+        for (int j = 0; j < 3; ++j) atomicAdd(gb + 3 * ei + j, g3[j]);
+    }
+}
+
+int launch_drift_vjp(const ElemDev& ed, const double* u, double* grad_f, cudaStream_t s) {
+    k_drift_vjp<<<ed.nblk, 256, 0, s>>>(ed, u, grad_f);
+    TB_CUDA(cudaGetLastError());
+    return TB_OK;
+}
+
+}  // namespace tb

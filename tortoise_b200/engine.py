@@ -42,6 +42,15 @@ class DP45Stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class AdjointStats(C.Structure):
+    _fields_ = [("t_obs", C.c_double), ("dense_s", C.c_double), ("steps", C.c_int64),
+                ("attempts", C.c_int64), ("checkpoints", C.c_int64), ("rhs_evals", C.c_int64),
+                ("vjp_evals", C.c_int64), ("status", C.c_int32), ("checkpoint_every", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def lib():
     """Loads the in-tree CUDA library (raises if it was not built)."""
     global _lib
@@ -81,6 +90,14 @@ def lib():
                                   C.POINTER(C.c_int32)]
         L.tb_dp45_begin_batch.argtypes = [vp, vp, dp, dp, dp, i64, C.c_int]
         L.tb_dp45_run_stats.argtypes = [vp, C.c_int, C.POINTER(DP45Stats)]
+        L.tb_adjoint_rhs_vjp.argtypes = [vp, vp, vp, vp, dp, C.c_int]
+        L.tb_adjoint_forward.argtypes = [vp, vp, C.c_double, C.c_double, C.c_double, C.c_int, i64, vp,
+                                         C.POINTER(AdjointStats), C.c_int]
+        L.tb_adjoint_backward.argtypes = [vp, vp, vp, dp, C.POINTER(AdjointStats), C.c_int]
+        L.tb_adjoint_integrate.argtypes = [vp, vp, C.c_double, C.c_double, C.c_double, C.c_int, i64, vp, vp, vp,
+                                           dp, C.POINTER(AdjointStats), C.c_int]
+        L.tb_adjoint_steps.argtypes = [vp, dp, i64, C.POINTER(i64), dp]
+        L.tb_dp45_replay.argtypes = [vp, vp, dp, i64, C.c_double, vp, C.c_int]
         _lib = L
     return _lib
 
@@ -206,6 +223,56 @@ class Engine:
 
     def synchronize(self):
         _check(lib().tb_synchronize(self.h), "tb_synchronize")
+
+    # -- adjoint -------------------------------------------------------------
+    def rhs_vjp(self, f, theta, drift=True, collisions=True):
+        """(dF/df)^T theta and dF/d amplitude_c . theta per channel (host arrays)."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        g = np.empty(self.ndofs)
+        ga = np.zeros(max(1, self.channel_count()))
+        flags = PTR_HOST | (0 if drift else NO_DRIFT) | (0 if collisions else NO_COLLISIONS)
+        _check(lib().tb_adjoint_rhs_vjp(self.h, _hp(f), _hp(theta), _hp(g), ga.ctypes.data_as(C.POINTER(C.c_double)),
+                                        flags), "tb_adjoint_rhs_vjp")
+        return g, ga[:self.channel_count()]
+
+    def adjoint_forward(self, y0, t0, tf, dense, checkpoint_every=16, max_steps=16384, drift=True):
+        """Differentiable forward sweep; returns f at the last dense output and stats."""
+        y0 = np.ascontiguousarray(y0, dtype=np.float64)
+        fo = np.empty(self.ndofs)
+        st = AdjointStats()
+        flags = PTR_HOST | (0 if drift else NO_DRIFT)
+        _check(lib().tb_adjoint_forward(self.h, _hp(y0), t0, tf, dense, int(checkpoint_every), int(max_steps),
+                                        _hp(fo), C.byref(st), flags), "tb_adjoint_forward")
+        return fo, st.as_dict()
+
+    def adjoint_backward(self, lam):
+        """Gradients of <lam, f(t_obs)> wrt f0 and the channel amplitudes."""
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        g = np.empty(self.ndofs)
+        ga = np.zeros(max(1, self.channel_count()))
+        st = AdjointStats()
+        _check(lib().tb_adjoint_backward(self.h, _hp(lam), _hp(g), ga.ctypes.data_as(C.POINTER(C.c_double)),
+                                         C.byref(st), PTR_HOST), "tb_adjoint_backward")
+        return g, ga[:self.channel_count()], st.as_dict()
+
+    def adjoint_steps(self):
+        n, s = C.c_int64(), C.c_double()
+        _check(lib().tb_adjoint_steps(self.h, None, 0, C.byref(n), C.byref(s)), "tb_adjoint_steps")
+        dts = np.zeros(max(1, n.value))
+        _check(lib().tb_adjoint_steps(self.h, dts.ctypes.data_as(C.POINTER(C.c_double)), n.value, C.byref(n),
+                                      C.byref(s)), "tb_adjoint_steps")
+        return dts[:n.value], s.value
+
+    def dp45_replay(self, y0, dts, dense_s, drift=True):
+        """Fixed-step Dormand-Prince over dts, then the dense output at dense_s."""
+        y0 = np.ascontiguousarray(y0, dtype=np.float64)
+        dts = np.ascontiguousarray(dts, dtype=np.float64)
+        out = np.empty(self.ndofs)
+        flags = PTR_HOST | (0 if drift else NO_DRIFT)
+        _check(lib().tb_dp45_replay(self.h, _hp(y0), dts.ctypes.data_as(C.POINTER(C.c_double)), len(dts),
+                                    float(dense_s), _hp(out), flags), "tb_dp45_replay")
+        return out
 
 
 class BatchEngine(Engine):
