@@ -25,6 +25,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -40,7 +41,7 @@ DENSE = T_END / 10.0
 
 def workload(n_mesh=N_MESH):
     from tortoise_b200 import workloads as W
-    mat = W.config1(n_mesh)
+    mat = W.two_band_eph_drift(n_mesh)
     f0 = W.initial_status(mat, kT=0.1, seed=1).vec
     return mat, f0
 
@@ -59,7 +60,7 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "bench_clocks_%d.csv" % os.getpid())
+        self.path = os.path.join(os.environ.get("TB_CLOCKS_DIR", tempfile.gettempdir()), "bench_clocks_%d.csv" % os.getpid())
 
     def __enter__(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
@@ -310,12 +311,13 @@ def ours(args, world, rank, local, pg):
 
 
 def batched(args):
-    """Batched ensemble (configs[2] shape): args.batch runs in one handle,
-    DP45 attempts of all runs per graph launch; value = run-attempts/s."""
+    """Batched ensemble (ensemble_runs: N in {16..64}, per-run kT and
+    couplings): args.batch runs in one handle, DP45 attempts of all runs per
+    graph launch; value = run-attempts/s."""
     import torch
     from tortoise_b200 import engine as E
     from tortoise_b200 import workloads as W
-    mats, states = W.config2_runs(args.batch)
+    mats, states = W.ensemble_runs(args.batch)
     layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32}[args.layout]
     t0 = time.perf_counter()
     be = E.BatchEngine(mats, layout=layout, allow_fp32=args.mixed)
@@ -352,12 +354,84 @@ def batched(args):
         N = m.bands[0].mesh.nsplit[0]
         if N not in uniq:
             uniq[N] = sum(be.channel_info(be.chan0[r] + c)["n_tuples"] for c in range(len(m.channels)))
+    layouts = sorted({be.channel_info(c)["layout"] for c in range(be.channel_count())})
+    be.close()
+    # The same run-attempts done one run at a time on the plain single-run
+    # FP64 path (one handle per structure; runs of equal N cost the same).
+    seq = {}
+    for N in Ns:
+        r = next(i for i, m in enumerate(mats) if m.bands[0].mesh.nsplit[0] == N)
+        eng = E.Engine(mats[r], layout=E.LAYOUT_AUTO, allow_fp32=False)
+        s1 = torch.cuda.ExternalStream(eng.stream_ptr())
+        eng.dp45_begin(states[r], 0.0, 1.0e9, DENSE, 0)
+        eng.dp45_advance(args.warmup)
+        eng.synchronize()
+        ev0.record(s1)
+        eng.dp45_advance(args.steps)
+        ev1.record(s1)
+        ev1.synchronize()
+        seq[N] = ev0.elapsed_time(ev1) * 1e-3 / args.steps
+        eng.close()
+    t_seq = sum(groups[N] * seq[N] for N in Ns)   # one attempt of every run
     print(json.dumps({"batched": True, "runs": args.batch, "mixed": args.mixed, "steps": args.steps,
                       "run_attempts_per_s": args.batch * args.steps / t, "ms_per_attempt": 1e3 * t / args.steps,
                       "collision_ms": 1e3 * t_coll, "setup_s": t_setup, "runs_per_N": groups,
-                      "tuples_per_structure": uniq, "dofs": be.ndofs,
-                      "layouts": sorted({be.channel_info(c)["layout"] for c in range(be.channel_count())}),
+                      "tuples_per_structure": uniq, "dofs": be.ndofs, "layouts": layouts,
+                      "sequential_fp64_ms_per_attempt_by_N": {N: 1e3 * seq[N] for N in Ns},
+                      "sequential_fp64_run_attempts_per_s": args.batch / t_seq,
+                      "speedup_vs_sequential_fp64": (args.batch * args.steps / t) / (args.batch / t_seq),
                       "clocks": clk.summary()}), flush=True)
+
+
+def adjoint(args):
+    """Gradient of the band-2 (Dirac cone) energy at t = 5 of the 32x32
+    two-band e-ph + drift workload with respect to every initial coefficient
+    and the channel couplings: forward sweep with a checkpoint every 16
+    accepted steps, reverse sweep with per-segment recomputation.  Reports the
+    time of both sweeps and central differences (h = 1e-6) of the replayed
+    step sequence in args.adjoint seeded directions plus the e-ph coupling."""
+    from tortoise_b200 import adjoint as A
+    from tortoise_b200 import engine as E
+    from tortoise_b200 import workloads as W
+    mat = W.two_band_eph_drift(32)
+    f0 = W.initial_status(mat, kT=0.1, seed=0).vec
+    layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32}[args.layout]
+    eng = E.Engine(mat, layout=layout, allow_fp32=args.mixed)
+    w = A.observable_weights(mat, 1, "energy")
+    amps = np.array([c.amplitude for c in mat.channels])
+    tf, tb = [], []
+    for _ in range(3):
+        eng.synchronize()
+        t0 = time.perf_counter()
+        fo, st = eng.adjoint_forward(f0, 0.0, 5.0, 0.5, checkpoint_every=16, max_steps=100000)
+        t1 = time.perf_counter()
+        g, ga, bst = eng.adjoint_backward(w)
+        t2 = time.perf_counter()
+        tf.append(t1 - t0)
+        tb.append(t2 - t1)
+    dts, s = eng.adjoint_steps()
+    J = lambda f: float(w @ eng.dp45_replay(f, dts, s))
+    rng = np.random.default_rng(1234)
+    h, errs = 1e-6, []
+    for _ in range(args.adjoint):
+        d = rng.standard_normal(eng.ndofs)
+        fd = (J(f0 + h * d) - J(f0 - h * d)) / (2 * h)
+        errs.append(abs(fd - float(g @ d)) / abs(float(g @ d)))
+    vals = []
+    for sg in (1, -1):
+        A.set_amplitudes(eng, amps * (1 + sg * h))
+        vals.append(J(f0))
+    A.set_amplitudes(eng, amps)
+    fd_c, ad_c = (vals[0] - vals[1]) / (2 * h), float(amps @ ga)
+    print(json.dumps({"adjoint": True, "workload": "2-band e-ph + drift, 32x32 mesh, t 0 -> 5, dense 0.5",
+                      "observable": "energy of band 2 (Dirac cone) at t = 5", "dofs": eng.ndofs,
+                      "accepted_steps": bst["steps"], "attempts": bst["attempts"], "checkpoint_every": 16,
+                      "checkpoints": bst["checkpoints"], "rhs_evals": bst["rhs_evals"], "vjp_evals": bst["vjp_evals"],
+                      "forward_s": min(tf), "backward_s": min(tb), "backward_over_forward": min(tb) / min(tf),
+                      "fd_directions": args.adjoint, "fd_max_rel_err": max(errs) if errs else None,
+                      "fd_coupling_rel_err": abs(fd_c - ad_c) / abs(ad_c), "layouts": sorted(
+                          {eng.channel_info(c)["layout"] for c in range(eng.channel_count())})}), flush=True)
+    eng.close()
 
 
 def rhs_only(args):
@@ -393,8 +467,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--rhs-only", type=int, default=0, help="profiling driver: K RHS evaluations only")
     ap.add_argument("--mesh", type=int, default=N_MESH, help="sections per side (profiling driver only)")
-    ap.add_argument("--batch", type=int, default=0, help="batched ensemble of this many runs (configs[2] shape)")
+    ap.add_argument("--batch", type=int, default=0, help="batched ensemble of this many runs (per-run N, kT, couplings)")
+    ap.add_argument("--adjoint", type=int, default=-1,
+                    help="adjoint gradient of the 32x32 workload, checked in this many FD directions")
     args = ap.parse_args()
+    if args.adjoint >= 0:
+        adjoint(args)
+        return
     if args.rhs_only:
         rhs_only(args)
         return

@@ -30,8 +30,8 @@ def tuple_hash(ids, umk):
 def cases():
     """name -> (material builder, state seed, kT)."""
     return {
-        "ee_n3": (lambda: W.config0(3), 1, 0.1),
-        "ee_n4": (lambda: W.config0(4), 2, 0.1),
+        "ee_n3": (lambda: W.parabolic_ee(3), 1, 0.1),
+        "ee_n4": (lambda: W.parabolic_ee(4), 2, 0.1),
         "ee2_n3": (lambda: W.build_material(3, ("P", "D"), (), ee=True, eph=False, rtol=1e-6, atol=1e-9), 3, 0.1),
         "eph_n4": (lambda: W.build_material(4, ("P", "D"), (0.2,), ee=False, eph=True, field=(0.1, 0.0),
                                             rtol=1e-6, atol=1e-9), 4, 0.1),

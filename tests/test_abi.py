@@ -67,7 +67,7 @@ def test_create_without_device_fails_cleanly():
     if torch.cuda.is_available():
         pytest.skip("device present")
     from tortoise_b200 import workloads as W
-    mat = W.config0(3)
+    mat = W.parabolic_ee(3)
     with pytest.raises(engine.TortoiseError) as ei:
         engine.Engine(mat)
     assert ei.value.rc == 7

@@ -40,7 +40,7 @@ def test_mc_points_in_reference_simplex():
     rng = np.random.default_rng(0)
     p = random_points_reference(rng, 2, 1000)
     assert (p >= 0).all() and (p.sum(axis=1) <= 1.0).all()
-    mat = W.config0(3)
+    mat = W.parabolic_ee(3)
     c = mat.channels[0]
     assert c.mc_points.shape == (50, 5) and c.mc_points_precalc.shape == (50, 5)
     assert not np.array_equal(c.mc_points, c.mc_points_precalc)

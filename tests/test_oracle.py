@@ -11,7 +11,7 @@ from tests.golden.make_golden import cases, tuple_hash
 
 
 def test_mass_matrix_identities():
-    mat = W.config0(4)
+    mat = W.parabolic_ee(4)
     o = oracle.Oracle(mat)
     M, Mi = o.mass_matrix(0)
     vol = mat.bands[0].mesh.elemVolume
@@ -62,7 +62,7 @@ def test_equilibrium_is_nearly_stationary():
     the mesh resolves kT and shrinks under refinement."""
     ratios = []
     for N in (4, 6):
-        mat = W.config0(N)
+        mat = W.parabolic_ee(N)
         o = oracle.Oracle(mat)
         eq = W.initial_status(mat, kT=3.0, seed=0, bump_amplitude=0.0).vec
         neq = W.initial_status(mat, kT=3.0, seed=0, bump_amplitude=0.3).vec
@@ -119,7 +119,7 @@ def test_tuples_are_valid_and_ordered():
 
 def test_single_tuple_partition_additivity():
     """propagate over a tuple range is additive (the TBB reduction split)."""
-    mat = W.config0(4)
+    mat = W.parabolic_ee(4)
     o = oracle.Oracle(mat)
     f0 = W.initial_status(mat, seed=2).vec
     n = o.num_tuples(0)

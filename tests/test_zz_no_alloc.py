@@ -31,7 +31,7 @@ def _bind(lib):
 def test_noalloc_error_norm_matches_existing_entry_point(gpu_lib, n):
     import torch
     fn = _bind(gpu_lib)
-    mat = W.config0(n)
+    mat = W.parabolic_ee(n)
     band = mat.bands[0]
     band.penalisationUnphysicalPopulation = 0.5
     eng = E.Engine(mat)

@@ -41,7 +41,7 @@ template <int L, bool F32> struct TTile {
     static constexpr int TT = (L == 4) ? 32 : (F32 ? 128 : 64);
 };
 
-static int tile_tuples(int L, bool fp32) {
+int tile_tuples(int L, bool fp32) {
     if (L == 4) return 32;
     return fp32 ? 128 : 64;
 }

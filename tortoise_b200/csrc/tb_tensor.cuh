@@ -15,6 +15,8 @@ struct MomentTensor {
 };
 
 int64_t tensor_bytes(int L, bool fp32, int64_t n_tuples);
+// tuples per tile of the tile-major moment layout
+int tile_tuples(int L, bool fp32);
 int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, bool fp32, MomentTensor& T,
                  cudaStream_t s);
 int launch_collision_tensor(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T,

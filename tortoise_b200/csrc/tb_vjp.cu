@@ -273,7 +273,7 @@ int launch_collision_vjp(const ChanDev& c, const InstDev* insts, int n_insts, in
             default: k_vjp_mc<4><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, u, grad_f, grad_amp); break;
         }
     } else {
-        const int TT = (c.L == 4) ? 32 : (T.fp32 ? 128 : 64);
+        const int TT = tile_tuples(c.L, T.fp32);
         switch (c.L * 2 + (T.fp32 ? 1 : 0)) {
             case 4: k_vjp_tensor<2, double><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, (const double*)T.d, TT, tup, stride, n, f, u, grad_f, grad_amp); break;
             case 5: k_vjp_tensor<2, float><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, (const float*)T.d, TT, tup, stride, n, f, u, grad_f, grad_amp); break;

@@ -76,32 +76,32 @@ def initial_status(mat, kT=0.1, mu=0.3, kT_phonon=0.05, seed=0, bump_amplitude=0
     return st
 
 
-# Shapes of the benchmark configurations (sizes; see DESIGN.md for scope).
-def config0(N=16, **kw):
+# The benchmark workloads, named by what they hold.
+def parabolic_ee(N=16, **kw):
     """One parabolic band, e-e constant matrix element, rtol 1e-6 / atol 1e-9."""
     return build_material(N, ("P",), (), ee=True, eph=False, rtol=1e-6, atol=1e-9, **kw)
 
 
-def config1(N=64, ee=False, **kw):
+def two_band_eph_drift(N=64, ee=False, **kw):
     """Parabola + Dirac cone, optical phonon hw=0.2 (Bose kT=0.05), field (0.1,0),
-    rtol 1e-8.  e-e is off by default at N=64 (tuple counts)."""
+    rtol 1e-8.  e-e is off by default: at N=64 its tuple lists (~1e11 per
+    channel) exceed device memory; at N=32 an adjoint needs ~1200 e-e
+    evaluations of ~2e9 tuples."""
     return build_material(N, ("P", "D"), (0.2,), ee=ee, eph=True, field=(0.1, 0.0), rtol=1e-8, atol=1e-9, **kw)
 
 
-def config3(N=32, ee=False, **kw):
-    return build_material(N, ("P", "D"), (0.2,), ee=ee, eph=True, field=(0.1, 0.0), rtol=1e-8, atol=1e-9, **kw)
-
-
-def config4(N=128, ee=False, **kw):
+def three_band_two_phonon(N=128, ee=False, **kw):
+    """Parabola, Dirac cone and heavy hole with two phonon branches (0.15, 0.25)."""
     return build_material(N, ("P", "D", "H"), (0.15, 0.25), ee=ee, eph=True, rtol=1e-8, atol=1e-9, **kw)
 
 
-def config2_runs(n_runs=256, seed=2024, Ns=(16, 24, 32, 48, 64), ee=False, **kw):
+def ensemble_runs(n_runs=256, seed=2024, Ns=(16, 24, 32, 48, 64), ee=False, **kw):
     """Batched ensemble: per run N uniform in Ns, kT uniform in [0.03, 0.2],
     coupling constants uniform in [0.5, 2.0] and a seeded bump; bands, phonon,
-    field and tolerances as config1.  All runs use the same Monte-Carlo seed,
-    so runs of equal N have identical structure (shared tuple lists and
-    moment tensors).  Returns (materials, initial state vectors)."""
+    field and tolerances as two_band_eph_drift.  All runs use the same
+    Monte-Carlo seed, so runs of equal N have identical structure (shared
+    tuple lists and moment tensors).  Returns (materials, initial state
+    vectors)."""
     rng = np.random.default_rng(seed)
     mats, states = [], []
     for r in range(n_runs):
