@@ -186,14 +186,27 @@ def reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def moment_bytes(L, layout):
+    """Bytes of one tuple's stored moments: 3^L (1 + L) moments as FP64 (t64),
+    FP32 (t32) or the upper 40 bits of FP64 (t40: a 4-byte word plus one
+    byte, bytes packed four per word)."""
+    nm = {2: 27, 3: 108, 4: 405}[L]
+    return {"t64": 8 * nm, "t32": 4 * nm, "t40": 4 * (nm + (nm + 3) // 4)}.get(layout, 0)
+
+
+def mixed_flag(args):
+    return {None: 0, "t32": 1, "t40": 2}[args.mixed]
+
+
 def ours(args, world, rank, local, pg):
     import torch
     from tortoise_b200 import engine as E
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     mat, f0 = workload()
-    layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32}[args.layout]
-    eng = E.Engine(mat, layout=layout, allow_fp32=args.mixed, device=local)
+    layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32,
+              "t40": E.LAYOUT_T40}[args.layout]
+    eng = E.Engine(mat, layout=layout, allow_fp32=mixed_flag(args), device=local)
     nch = len(mat.channels)
     infos = [eng.channel_info(c) for c in range(nch)]
     ntup = sum(i["n_tuples"] for i in infos)
@@ -214,12 +227,10 @@ def ours(args, world, rank, local, pg):
     ev1.record(stream)
     ev1.synchronize()
     t_coll = ev0.elapsed_time(ev1) * 1e-3 / reps
-    nmom = {2: 27, 3: 108, 4: 405}
     bytes_coll = 0
     for c, inf in zip(mat.channels, infos):
         L, n = c.nlegs, inf["n_tuples"]
-        if inf["layout"] in ("t64", "t32"):
-            bytes_coll += n * nmom[L] * (4 if inf["layout"] == "t32" else 8)
+        bytes_coll += n * moment_bytes(L, inf["layout"])
         bytes_coll += n * 4 * (L + 1)
     bytes_coll += eng.ndofs * 8 * 3   # f read once, accumulator read + written once
     hbm, peak_kind = peaks()
@@ -280,12 +291,13 @@ def ours(args, world, rank, local, pg):
     tp = os.path.join(ROOT, "profiles", "collision_traffic.json")
     if os.path.exists(tp):
         d = json.load(open(tp))
-        key = "t32" if args.mixed else "t64"
+        key = infos[0]["layout"]
         if key in d and d[key].get("bytes_per_tuple"):
             traffic = d[key]["bytes_per_tuple"] * ntup
     line = {"metric": METRIC, "value": value, "unit": "DP45 steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if not args.mixed else "f32-storage/f64-accumulate",
+            "scaling": "weak", "vs_baseline": None, "dtype": {None: "f64", "t32": "f32-storage/f64-accumulate",
+                      "t40": "fp64-upper-40-bit-storage/f64-accumulate"}[args.mixed],
             "data": "synthetic (seeded PCG64 bump on Fermi-Dirac, Bose phonons)",
             "config": {"workload": "2-band e-ph + drift, 64x64 mesh (8192 triangles/band), NMC=50, rtol 1e-8",
                        "tuples": ntup, "channels": nch, "layouts": [i["layout"] for i in infos],
@@ -318,9 +330,10 @@ def batched(args):
     from tortoise_b200 import engine as E
     from tortoise_b200 import workloads as W
     mats, states = W.ensemble_runs(args.batch)
-    layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32}[args.layout]
+    layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32,
+              "t40": E.LAYOUT_T40}[args.layout]
     t0 = time.perf_counter()
-    be = E.BatchEngine(mats, layout=layout, allow_fp32=args.mixed)
+    be = E.BatchEngine(mats, layout=layout, allow_fp32=mixed_flag(args))
     t_setup = time.perf_counter() - t0
     f0 = np.concatenate(states)
     stream = torch.cuda.ExternalStream(be.stream_ptr())
@@ -395,8 +408,9 @@ def adjoint(args):
     from tortoise_b200 import workloads as W
     mat = W.two_band_eph_drift(32)
     f0 = W.initial_status(mat, kT=0.1, seed=0).vec
-    layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32}[args.layout]
-    eng = E.Engine(mat, layout=layout, allow_fp32=args.mixed)
+    layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32,
+              "t40": E.LAYOUT_T40}[args.layout]
+    eng = E.Engine(mat, layout=layout, allow_fp32=mixed_flag(args))
     w = A.observable_weights(mat, 1, "energy")
     amps = np.array([c.amplitude for c in mat.channels])
     tf, tb = [], []
@@ -441,8 +455,9 @@ def rhs_only(args):
     import torch
     from tortoise_b200 import engine as E
     mat, f0 = workload(args.mesh)
-    layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32}[args.layout]
-    eng = E.Engine(mat, layout=layout, allow_fp32=args.mixed)
+    layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32,
+              "t40": E.LAYOUT_T40}[args.layout]
+    eng = E.Engine(mat, layout=layout, allow_fp32=mixed_flag(args))
     f = torch.tensor(f0, device="cuda")
     out = torch.zeros_like(f)
     torch.cuda.synchronize()
@@ -462,8 +477,9 @@ def main():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--layout", default="auto", choices=["auto", "mc64", "t64", "t32"])
-    ap.add_argument("--mixed", action="store_true", help="allow FP32 moment storage (FP64 accumulate)")
+    ap.add_argument("--layout", default="auto", choices=["auto", "mc64", "t64", "t32", "t40"])
+    ap.add_argument("--mixed", nargs="?", const="t40", default=None, choices=["t32", "t40"],
+                    help="reduced-precision moment storage: t40 (upper 40 bits of FP64, default) or t32 (FP32)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--rhs-only", type=int, default=0, help="profiling driver: K RHS evaluations only")
     ap.add_argument("--mesh", type=int, default=N_MESH, help="sections per side (profiling driver only)")

@@ -38,12 +38,12 @@ def _dir_err(fd, ad, scale):
     return abs(fd - ad) / max(abs(ad), 1e-3 * scale)
 
 
-@pytest.mark.parametrize("layout", [E.LAYOUT_MC64, E.LAYOUT_T64, E.LAYOUT_T32])
+@pytest.mark.parametrize("layout", [E.LAYOUT_MC64, E.LAYOUT_T64, E.LAYOUT_T32, E.LAYOUT_T40])
 @pytest.mark.parametrize("bath", [False, True])
 def test_rhs_vjp_is_the_transpose(gpu_lib, layout, bath):
     mat = _mat(4, ee=True, bath=bath)
     f = W.initial_status(mat, kT=0.1, seed=11).vec
-    eng = E.Engine(mat, layout=layout, allow_fp32=(layout == E.LAYOUT_T32))
+    eng = E.Engine(mat, layout=layout)
     rng = np.random.default_rng(7)
     n = eng.ndofs
     for drift in (True, False):

@@ -65,3 +65,34 @@ def test_batch_dp45_equals_individual_runs(gpu_lib):
         assert [got["attempts"], got["accepted"], got["rejected"]] == [ref["attempts"], ref["accepted"], ref["rejected"]]
         assert np.allclose(got["dense_t"], ref["dense_t"], rtol=0, atol=1e-14)
         assert rel_l2(got["dense"], ref["dense"]) < 1e-10
+
+
+def test_mixed_precision_trajectory_within_1e8(gpu_lib):
+    """Mixed-precision moment storage (FP64 products, accumulation,
+    gain - loss, error norm, controller) against the FP64 path on the two-band
+    e-ph + drift workload at 16x16, rtol 1e-8, to t = 1, every dense output:
+    40-bit storage (T40: upper 40 bits of FP64, 2^-29) within 5e-9 relative L2
+    (measured ~1e-9), plain FP32 storage (T32) within 3e-8 (measured ~1e-8).
+    A batch of three runs of that structure in T40 gives every run's FP64
+    trajectory to 5e-9 as well."""
+    mats, states = [], []
+    for k, (amp, kT) in enumerate([(1.0, 0.1), (0.6, 0.05), (1.7, 0.2)]):
+        m = W.two_band_eph_drift(16, eph_amplitude=amp)
+        mats.append(m)
+        states.append(W.initial_status(m, kT=kT, seed=40 + k).vec)
+    r64 = E.Engine(mats[0], layout=E.LAYOUT_T64).dp45(states[0], 0.0, 1.0, 0.25)
+    r40 = E.Engine(mats[0], layout=E.LAYOUT_T40).dp45(states[0], 0.0, 1.0, 0.25)
+    r32 = E.Engine(mats[0], layout=E.LAYOUT_T32).dp45(states[0], 0.0, 1.0, 0.25)
+    assert r64["status"] == 0 and r40["status"] == 0 and r32["status"] == 0
+    e40 = [rel_l2(a, b) for a, b in zip(r40["dense"], r64["dense"])]
+    e32 = [rel_l2(a, b) for a, b in zip(r32["dense"], r64["dense"])]
+    assert len(e40) == 4 and max(e40) < 5e-9, e40
+    assert max(e32) < 3e-8, e32
+    be = E.BatchEngine(mats, layout=E.LAYOUT_AUTO, allow_fp32=2)
+    assert {be.channel_info(c)["layout"] for c in range(be.channel_count())} == {"t40"}
+    res = be.dp45(np.concatenate(states), 0.0, 1.0, 0.25)
+    for r, (m, f) in enumerate(zip(mats, states)):
+        ref = E.Engine(m, layout=E.LAYOUT_T64).dp45(f, 0.0, 1.0, 0.25)
+        got = res["runs"][r]
+        assert got["status"] == 0
+        assert max(rel_l2(a, b) for a, b in zip(got["dense"], ref["dense"])) < 5e-9

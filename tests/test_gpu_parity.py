@@ -171,3 +171,19 @@ def test_tensor_layout_fp32_error_bound(gpu_lib, name):
     mat, f0 = _setup(name)
     eng = E.Engine(mat, layout=E.LAYOUT_T32, allow_fp32=True)
     assert rel_l2(eng.rhs(f0, drift=False), g["rhs_nodrift"]) < 1e-6
+
+
+@pytest.mark.parametrize("name", ["eph_n4", "ee_n3", "ee2_n3", "eph_bath_n4"])
+def test_tensor_layout_40bit_error_bound(gpu_lib, name):
+    """Moments stored as the upper 40 bits of FP64 (sign, exponent, 28
+    mantissa bits, rounded: 2^-29 relative), rebuilt into FP64 registers:
+    every channel and the RHS within 2e-8 relative L2 of the FP64 oracle
+    (FP32 storage gives ~1.2e-7; 40 bits are 32x finer)."""
+    g = golden(name)
+    mat, f0 = _setup(name)
+    eng = E.Engine(mat, layout=E.LAYOUT_T40)
+    for ch in range(len(mat.channels)):
+        if eng.channel_info(ch)["n_tuples"] > 0:
+            assert eng.channel_info(ch)["layout"] == "t40"
+        assert rel_l2(eng.channel_propagate(ch, f0), g["ch%d_prop" % ch]) < 2e-8
+    assert rel_l2(eng.rhs(f0, drift=False), g["rhs_nodrift"]) < 2e-8

@@ -509,17 +509,20 @@ int choose_layouts(tb_handle* h) {
             // evaluation (HBM-bound contraction vs FP64-bound quadrature);
             // for L = 4 the 405-moment tensor costs more bytes than the
             // quadrature costs FP64 cycles on B200.
-            if (G.L <= 3) want = h->opts.allow_fp32 ? TB_LAYOUT_T32 : TB_LAYOUT_T64;
+            // allow_fp32 = 1: FP32 moments; 2: 40-bit (truncated FP64) moments
+            if (G.L <= 3)
+                want = h->opts.allow_fp32 == 1 ? TB_LAYOUT_T32 : h->opts.allow_fp32 == 2 ? TB_LAYOUT_T40 : TB_LAYOUT_T64;
             else want = TB_LAYOUT_MC64;
         }
-        if (want == TB_LAYOUT_T32 || want == TB_LAYOUT_T64) {
-            const int64_t bytes = tensor_bytes(G.L, want == TB_LAYOUT_T32, G.tup.n);
+        const int kind = (want == TB_LAYOUT_T32) ? TK_F32 : (want == TB_LAYOUT_T40) ? TK_F40 : TK_F64;
+        if (want == TB_LAYOUT_T32 || want == TB_LAYOUT_T64 || want == TB_LAYOUT_T40) {
+            const int64_t bytes = tensor_bytes(G.L, kind, G.tup.n);
             if (G.tup.n == 0 || bytes > budget) want = TB_LAYOUT_MC64;
             else budget -= bytes;
         }
         G.layout = want;
         if (want != TB_LAYOUT_MC64)
-            TB_TRY(build_tensor(G.dev, G.tup.d, G.tup.cap, G.tup.n, want == TB_LAYOUT_T32, G.tensor, h->stream));
+            TB_TRY(build_tensor(G.dev, G.tup.d, G.tup.cap, G.tup.n, kind, G.tensor, h->stream));
     }
     return TB_OK;
 }
@@ -650,6 +653,11 @@ int tb_create_batch(tb_handle** out, const tb_problem_desc* const* runs, int n_r
     std::unique_ptr<tb_handle> h(new tb_handle());
     if (opts) h->opts = *opts;
     else { h->opts.layout = TB_LAYOUT_AUTO; h->opts.allow_fp32 = 0; }
+    if (h->opts.layout < TB_LAYOUT_AUTO || h->opts.layout > TB_LAYOUT_T40 || h->opts.allow_fp32 < 0 ||
+        h->opts.allow_fp32 > 2) {
+        set_error("tb_options: layout must be 0..4 and allow_fp32 0..2");
+        return TB_ERR_ARG;
+    }
     h->device = h->opts.device;
     TB_CUDA(cudaSetDevice(h->device));
     TB_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));

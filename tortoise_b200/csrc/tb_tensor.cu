@@ -20,9 +20,22 @@
 // Storage is tile-major: a tile of TT tuples is one contiguous block
 // [nmom][TT], so the contraction kernel streams whole tiles into shared memory
 // with one 1-D bulk TMA copy (cp.async.bulk + mbarrier, double buffered) and
-// each thread reads its tuple's moments bank-conflict free.  FP32 storage
-// halves the bytes; products and accumulation stay FP64, and the
-// gain-minus-loss vector v = ka + kb is formed in FP64 from f.
+// each thread reads its tuple's moments bank-conflict free.  Three storage
+// kinds:
+//   TK_F64    FP64 moments;
+//   TK_F32    FP32 moments (2^-24 relative rounding each), half the bytes;
+//   TK_F40    the upper 40 bits of each FP64 moment (sign, exponent and 28
+//             mantissa bits, rounded to nearest: 2^-29 relative), 5 bytes per
+//             moment: a row of the upper 32-bit words, then rows that pack
+//             the next byte of four consecutive moments into one word.  A
+//             moment is rebuilt as an FP64 register pair (upper word, byte
+//             << 24) with one byte permute: no conversion instruction.
+// Products and accumulation are FP64 for every kind; the gain-minus-loss
+// vector v = ka + kb is formed in FP64 from f.
+#include <cuda_bf16.h>
+
+#include <type_traits>
+
 #include "tb_dp45.cuh"
 #include "tb_geom.cuh"
 #include "tb_scatter.cuh"
@@ -36,22 +49,29 @@ template <int L> struct TDim {
     static constexpr int NMOM = K * (1 + L);
 };
 
-template <int L, bool F32> struct TTile {
+template <int L, int KIND> struct TTile {
     // tuples per tile: keeps one stage at <= ~56 KB of shared memory
-    static constexpr int TT = (L == 4) ? 32 : (F32 ? 128 : 64);
+    static constexpr int TT = (L == 4) ? 32 : (KIND == TK_F32) ? 128 : (KIND == TK_F40 && L == 2) ? 128 : 64;
 };
-
-int tile_tuples(int L, bool fp32) {
-    if (L == 4) return 32;
-    return fp32 ? 128 : 64;
-}
 
 static int nmom_of(int L) { return (L == 2 ? 9 : L == 3 ? 27 : 81) * (1 + L); }
 
-int64_t tensor_bytes(int L, bool fp32, int64_t n) {
-    const int64_t TT = tile_tuples(L, fp32);
+int tile_tuples(int L, int kind) {
+    if (L == 4) return 32;
+    if (kind == TK_F32 || (kind == TK_F40 && L == 2)) return 128;
+    return 64;
+}
+
+// bytes of one tuple's moments in a tile
+static int64_t tuple_bytes(int L, int kind) {
+    const int64_t nm = nmom_of(L);
+    return kind == TK_F64 ? 8 * nm : kind == TK_F32 ? 4 * nm : 4 * (nm + (nm + 3) / 4);
+}
+
+int64_t tensor_bytes(int L, int kind, int64_t n) {
+    const int64_t TT = tile_tuples(L, kind);
     const int64_t ntiles = (n + TT - 1) / TT;
-    return ntiles * TT * nmom_of(L) * (fp32 ? 4 : 8);
+    return ntiles * TT * tuple_bytes(L, kind);
 }
 
 void MomentTensor::release() {
@@ -63,9 +83,9 @@ void MomentTensor::release() {
 // ------------------------------------------------------------ precompute
 // One warp per tuple; every lane recomputes the MC point (cheap) and owns a
 // strided subset of the moments.
-template <int L, typename T>
+template <int L, int KIND>
 __global__ void __launch_bounds__(256) k_build_moments(ChanDev c, const int32_t* __restrict__ tup, int64_t stride,
-                                                       int64_t n, T* __restrict__ out, int TT) {
+                                                       int64_t n, void* __restrict__ out, int TT) {
     extern __shared__ double s_mc[];
     constexpr int R = 2 * (L - 2) + 1;
     constexpr int K = TDim<L>::K, KM = TDim<L>::KM, NMOM = TDim<L>::NMOM;
@@ -150,10 +170,30 @@ __global__ void __launch_bounds__(256) k_build_moments(ChanDev c, const int32_t*
             norm = c.amp_vol / (c.fact * double(c.nmc) * fabs(g.det));
         }
         const int64_t tile = i / TT, pos = i % TT;
-        T* base = out + tile * (int64_t)NMOM * TT + pos;
+        if (KIND == TK_F64) {
+            double* base = static_cast<double*>(out) + tile * (int64_t)NMOM * TT + pos;
 #pragma unroll
-        for (int q = 0; q < PER; ++q)
-            if (own[q]) base[(int64_t)(lane + 32 * q) * TT] = T(acc[q] * norm);
+            for (int q = 0; q < PER; ++q)
+                if (own[q]) base[(int64_t)(lane + 32 * q) * TT] = acc[q] * norm;
+        } else if (KIND == TK_F32) {
+            float* base = static_cast<float*>(out) + tile * (int64_t)NMOM * TT + pos;
+#pragma unroll
+            for (int q = 0; q < PER; ++q)
+                if (own[q]) base[(int64_t)(lane + 32 * q) * TT] = float(acc[q] * norm);
+        } else {
+            // upper 40 bits of the FP64 pattern, rounded to nearest on bit 23
+            constexpr int NB = (NMOM + 3) / 4;   // rows of packed bytes
+            uint32_t* hi = static_cast<uint32_t*>(out) + tile * (int64_t)(NMOM + NB) * TT;
+            uint8_t* lo = reinterpret_cast<uint8_t*>(hi + (int64_t)NMOM * TT);
+#pragma unroll
+            for (int q = 0; q < PER; ++q)
+                if (own[q]) {
+                    const int k = lane + 32 * q;
+                    const unsigned long long b = (unsigned long long)__double_as_longlong(acc[q] * norm) + 0x800000ull;
+                    hi[(int64_t)k * TT + pos] = uint32_t(b >> 32);
+                    lo[4 * ((int64_t)(k >> 2) * TT + pos) + (k & 3)] = uint8_t(b >> 24);
+                }
+        }
     }
 }
 
@@ -191,16 +231,136 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                  : "memory");
 }
 
-template <int L, typename T, int TT, int STAGES>
+// Moment j of this thread's tuple in a staged tile, as FP64.
+template <int KIND, int NMOM, int TT>
+__device__ __forceinline__ double tile_moment(const unsigned char* __restrict__ tile, int tid, int j) {
+    if constexpr (KIND == TK_F64) {
+        return reinterpret_cast<const double*>(tile)[j * TT + tid];
+    } else if constexpr (KIND == TK_F32) {
+        return double(reinterpret_cast<const float*>(tile)[j * TT + tid]);
+    } else {
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(tile);
+        const uint32_t hi = w[j * TT + tid];
+        const uint32_t lw = w[(NMOM + (j >> 2)) * TT + tid];
+        // byte j % 4 of lw into the top byte of the low word, zeros below
+        const uint32_t lo = __byte_perm(lw, 0u, 0x0444u | (uint32_t(j & 3) << 12));
+        return __hiloint2double(int(hi), int(lo));
+    }
+}
+
+// Contraction of one tuple (this thread's) for NI = 1 or 2 instances of
+// the channel; every moment is read from shared memory once and used by all
+// NI instances.  Results are scattered into acc (legs 0 .. L-2 through the
+// warp-segmented reduction, so all 32 lanes must call this together).
+template <int L, int KIND, int TT, int NI>
+__device__ __forceinline__ void contract_tuple(const ChanDev& c, const InstDev (&in)[NI], const int (&e)[L], bool valid,
+                                               const unsigned char* __restrict__ tile, int tid,
+                                               const double* __restrict__ f, double* __restrict__ acc) {
+    constexpr int K = TDim<L>::K, KM = TDim<L>::KM, NMOM = TDim<L>::NMOM;
+    auto M = [&](int j) { return tile_moment<KIND, NMOM, TT>(tile, tid, j); };
+    // v = kron(A) + kron(B) per instance, leg 0 most significant; gain (B) /
+    // loss (A) forms of ScatteringChannel.cpp:633-641
+    double v[NI][K];
+#pragma unroll
+    for (int q = 0; q < NI; ++q) {
+        double A[L][3], B[L][3];
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            const double d = c.leg[l].dir, st = c.leg[l].stat;
+            const double* fe = f + in[q].foff[l] + 3 * (int64_t)e[l];
+            const double ka = (l == 0 ? -1.0 : 1.0) * 0.5;
+            const double ca = (1. - d) * st + (1. + d);
+            const double cb = (1. + d) * st + (1. - d);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const double unit = (j == 0) ? 1.0 : 0.0;
+                const double fj = __ldg(fe + j);
+                A[l][j] = ka * ((1. - d) * unit + ca * fj);
+                B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            int r = j;
+            double pa = 1.0, pb = 1.0;
+#pragma unroll
+            for (int l = L - 1; l >= 0; --l) {
+                const int Jl = r % 3;
+                r /= 3;
+                pa *= A[l][Jl];
+                pb *= B[l][Jl];
+            }
+            v[q][j] = pa + pb;
+        }
+    }
+    double r0[NI];
+#pragma unroll
+    for (int q = 0; q < NI; ++q) r0[q] = 0.0;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const double w = M(j);
+#pragma unroll
+        for (int q = 0; q < NI; ++q) r0[q] = fma(w, v[q][j], r0[q]);
+    }
+#pragma unroll
+    for (int lam = 0; lam < L; ++lam) {
+        int sstep = 1;
+#pragma unroll
+        for (int l = L - 1; l > lam; --l) sstep *= 3;
+        double r1[NI], r2[NI];
+#pragma unroll
+        for (int q = 0; q < NI; ++q) { r1[q] = 0.0; r2[q] = 0.0; }
+#pragma unroll
+        for (int km = 0; km < KM; ++km) {
+            // J with J_lam = 0 whose other legs enumerate km in leg order
+            const int hi = km / sstep, lo = km % sstep;
+            const int j0 = hi * 3 * sstep + lo;
+            const int j1 = j0 + sstep, j2 = j0 + 2 * sstep;
+            const int qa = K + (lam * 3 + 0) * KM + km;
+            const double qxx = M(qa), qxy = M(qa + KM), qyy = M(qa + 2 * KM);
+            const double s1 = M(j1), s2 = M(j2);
+#pragma unroll
+            for (int q = 0; q < NI; ++q) {
+                r1[q] = fma(s1, v[q][j0], r1[q]);
+                r1[q] = fma(qxx, v[q][j1], r1[q]);
+                r1[q] = fma(qxy, v[q][j2], r1[q]);
+                r2[q] = fma(s2, v[q][j0], r2[q]);
+                r2[q] = fma(qxy, v[q][j1], r2[q]);
+                r2[q] = fma(qyy, v[q][j2], r2[q]);
+            }
+        }
+        const double d = c.leg[lam].dir;
+#pragma unroll
+        for (int q = 0; q < NI; ++q) {
+            const double amp = in[q].amplitude;
+            const int64_t key = in[q].foff[lam] + 3 * (int64_t)e[lam];
+            if (lam < L - 1) {
+                warp_scatter3(valid ? key : -1, acc + key, d * (r0[q] * amp), d * (r1[q] * amp), d * (r2[q] * amp));
+            } else if (valid) {
+                double* o = acc + key;
+                atomicAdd(o + 0, d * (r0[q] * amp));
+                atomicAdd(o + 1, d * (r1[q] * amp));
+                atomicAdd(o + 2, d * (r2[q] * amp));
+            }
+        }
+    }
+}
+
+// bytes of one tuple's moments (compile-time twin of tuple_bytes)
+template <int L, int KIND> struct TBytes {
+    static constexpr int NM = TDim<L>::NMOM;
+    static constexpr int B = KIND == TK_F64 ? 8 * NM : KIND == TK_F32 ? 4 * NM : 4 * (NM + (NM + 3) / 4);
+};
+
+template <int L, int KIND, int TT, int STAGES, bool PAIR>
 __global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, const InstDev* __restrict__ insts, int n_insts,
-                                                         const T* __restrict__ mom, int64_t ntiles,
+                                                         const unsigned char* __restrict__ mom, int64_t ntiles,
                                                          const int32_t* __restrict__ tup, int64_t stride, int64_t n,
                                                          const double* __restrict__ f, double* __restrict__ acc,
                                                          const DPCtl* __restrict__ ctl, int* __restrict__ err_flag) {
-    constexpr int K = TDim<L>::K, KM = TDim<L>::KM, NMOM = TDim<L>::NMOM;
-    constexpr uint32_t TILE_BYTES = uint32_t(NMOM) * TT * sizeof(T);
+    constexpr uint32_t TILE_BYTES = uint32_t(TBytes<L, KIND>::B) * TT;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    T* stage_buf = reinterpret_cast<T*>(smem_raw);
+    unsigned char* stage_buf = smem_raw;
     __shared__ __align__(8) uint64_t bars[STAGES];
     {
         // every instance finished or switched off: nothing to stream
@@ -222,7 +382,7 @@ __global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, const InstDe
             const int64_t tile = blockIdx.x + (int64_t)s * gridDim.x;
             if (tile < ntiles) {
                 mbar_expect_tx_arrive(&bars[s], TILE_BYTES);
-                bulk_g2s(stage_buf + (size_t)s * NMOM * TT, mom + tile * (int64_t)NMOM * TT, TILE_BYTES, &bars[s]);
+                bulk_g2s(stage_buf + (size_t)s * TILE_BYTES, mom + tile * (int64_t)TILE_BYTES, TILE_BYTES, &bars[s]);
             }
         }
     }
@@ -241,7 +401,7 @@ __global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, const InstDe
             }
             return;
         }
-        const T* sm = stage_buf + (size_t)s * NMOM * TT;
+        const unsigned char* sm = stage_buf + (size_t)s * TILE_BYTES;
         const int64_t i = tile * TT + tid;
         {
             // every lane runs the instance loop (padding lanes contribute zero
@@ -250,79 +410,23 @@ __global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, const InstDe
             int e[L];
 #pragma unroll
             for (int l = 0; l < L; ++l) e[l] = valid ? __ldg(tup + l * stride + i) : 0;
-            for (int k = 0; k < n_insts; ++k) {
-                const InstDev in = insts[k];
-                if (in.amplitude == 0.0 || (ctl && ctl[in.run].done)) continue;
-                // gain (B) / loss (A) forms, ScatteringChannel.cpp:633-641
-                double A[L][3], B[L][3];
-#pragma unroll
-                for (int l = 0; l < L; ++l) {
-                    const double d = c.leg[l].dir, st = c.leg[l].stat;
-                    const double* fe = f + in.foff[l] + 3 * (int64_t)e[l];
-                    const double ka = (l == 0 ? -1.0 : 1.0) * 0.5;
-                    const double ca = (1. - d) * st + (1. + d);
-                    const double cb = (1. + d) * st + (1. - d);
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) {
-                        const double unit = (j == 0) ? 1.0 : 0.0;
-                        const double fj = __ldg(fe + j);
-                        A[l][j] = ka * ((1. - d) * unit + ca * fj);
-                        B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
-                    }
-                }
-                // v = kron(A) + kron(B), leg 0 most significant
-                double v[K];
-#pragma unroll
-                for (int j = 0; j < K; ++j) {
-                    int r = j;
-                    double pa = 1.0, pb = 1.0;
-#pragma unroll
-                    for (int l = L - 1; l >= 0; --l) {
-                        const int Jl = r % 3;
-                        r /= 3;
-                        pa *= A[l][Jl];
-                        pb *= B[l][Jl];
-                    }
-                    v[j] = pa + pb;
-                }
-                double r0 = 0.0;
-#pragma unroll
-                for (int j = 0; j < K; ++j) r0 = fma(double(sm[j * TT + tid]), v[j], r0);
-#pragma unroll
-                for (int lam = 0; lam < L; ++lam) {
-                    int sstep = 1;
-#pragma unroll
-                    for (int l = L - 1; l > lam; --l) sstep *= 3;
-                    double r1 = 0.0, r2 = 0.0;
-#pragma unroll
-                    for (int km = 0; km < KM; ++km) {
-                        // J with J_lam = 0 whose other legs enumerate km in leg order
-                        int hi = km / sstep, lo = km % sstep;
-                        const int j0 = hi * 3 * sstep + lo;
-                        const int j1 = j0 + sstep, j2 = j0 + 2 * sstep;
-                        const double qxx = double(sm[(K + (lam * 3 + 0) * KM + km) * TT + tid]);
-                        const double qxy = double(sm[(K + (lam * 3 + 1) * KM + km) * TT + tid]);
-                        const double qyy = double(sm[(K + (lam * 3 + 2) * KM + km) * TT + tid]);
-                        const double s1 = double(sm[j1 * TT + tid]);
-                        const double s2 = double(sm[j2 * TT + tid]);
-                        r1 = fma(s1, v[j0], r1);
-                        r1 = fma(qxx, v[j1], r1);
-                        r1 = fma(qxy, v[j2], r1);
-                        r2 = fma(s2, v[j0], r2);
-                        r2 = fma(qxy, v[j1], r2);
-                        r2 = fma(qyy, v[j2], r2);
-                    }
-                    const double d = c.leg[lam].dir;
-                    const int64_t key = in.foff[lam] + 3 * (int64_t)e[lam];
-                    if (lam < L - 1) {
-                        warp_scatter3(valid ? key : -1, acc + key, d * (r0 * in.amplitude), d * (r1 * in.amplitude),
-                                      d * (r2 * in.amplitude));
-                    } else if (valid) {
-                        double* o = acc + key;
-                        atomicAdd(o + 0, d * (r0 * in.amplitude));
-                        atomicAdd(o + 1, d * (r1 * in.amplitude));
-                        atomicAdd(o + 2, d * (r2 * in.amplitude));
-                    }
+            // instances in pairs: each moment read from shared memory (and
+            // widened to FP64) serves two runs' contractions
+            auto active = [&](const InstDev& q) { return q.amplitude != 0.0 && !(ctl && ctl[q.run].done); };
+            int k = 0;
+            while (k < n_insts) {
+                const InstDev a = insts[k];
+                if (!active(a)) { ++k; continue; }
+                int k2 = k + 1;
+                while (k2 < n_insts && !active(insts[k2])) ++k2;
+                if (PAIR && k2 < n_insts) {
+                    const InstDev pair[2] = {a, insts[k2]};
+                    contract_tuple<L, KIND, TT, 2>(c, pair, e, valid, sm, tid, f, acc);
+                    k = k2 + 1;
+                } else {
+                    const InstDev one[1] = {a};
+                    contract_tuple<L, KIND, TT, 1>(c, one, e, valid, sm, tid, f, acc);
+                    k = PAIR ? k2 : k + 1;
                 }
             }
         }
@@ -331,18 +435,17 @@ __global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, const InstDe
             const int64_t next = tile + (int64_t)STAGES * gridDim.x;
             if (next < ntiles) {
                 mbar_expect_tx_arrive(&bars[s], TILE_BYTES);
-                bulk_g2s(stage_buf + (size_t)s * NMOM * TT, mom + next * (int64_t)NMOM * TT, TILE_BYTES, &bars[s]);
+                bulk_g2s(stage_buf + (size_t)s * TILE_BYTES, mom + next * (int64_t)TILE_BYTES, TILE_BYTES, &bars[s]);
             }
         }
     }
 }
 
-template <int L, bool F32>
+template <int L, int KIND>
 static int build_t(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, MomentTensor& T, cudaStream_t s) {
-    using E = typename std::conditional<F32, float, double>::type;
-    constexpr int TT = TTile<L, F32>::TT;
+    constexpr int TT = TTile<L, KIND>::TT;
     const int64_t ntiles = (n + TT - 1) / TT;
-    const size_t bytes = size_t(ntiles) * TT * TDim<L>::NMOM * sizeof(E);
+    const size_t bytes = size_t(tensor_bytes(L, KIND, n));
     T.release();
     if (cudaMalloc(&T.d, bytes) != cudaSuccess) {
         T.d = nullptr;
@@ -353,24 +456,27 @@ static int build_t(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t
     const size_t smem = sizeof(double) * size_t(c.nmc) * c.R;
     int64_t blocks = (n * 32 + 255) / 256;
     if (blocks > 148 * 64) blocks = 148 * 64;
-    k_build_moments<L, E><<<unsigned(blocks), 256, smem, s>>>(c, tup, stride, n, reinterpret_cast<E*>(T.d), TT);
+    k_build_moments<L, KIND><<<unsigned(blocks), 256, smem, s>>>(c, tup, stride, n, T.d, TT);
     TB_CUDA(cudaGetLastError());
     T.n = n;
     T.ntiles = ntiles;
     T.nmom = TDim<L>::NMOM;
-    T.fp32 = F32;
+    T.kind = KIND;
     return TB_OK;
 }
 
-int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, bool fp32, MomentTensor& T,
+int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, int kind, MomentTensor& T,
                  cudaStream_t s) {
-    switch (c.L * 2 + (fp32 ? 1 : 0)) {
-        case 4: return build_t<2, false>(c, tup, stride, n, T, s);
-        case 5: return build_t<2, true>(c, tup, stride, n, T, s);
-        case 6: return build_t<3, false>(c, tup, stride, n, T, s);
-        case 7: return build_t<3, true>(c, tup, stride, n, T, s);
-        case 8: return build_t<4, false>(c, tup, stride, n, T, s);
-        case 9: return build_t<4, true>(c, tup, stride, n, T, s);
+    switch (c.L * 3 + kind) {
+        case 6: return build_t<2, TK_F64>(c, tup, stride, n, T, s);
+        case 7: return build_t<2, TK_F32>(c, tup, stride, n, T, s);
+        case 8: return build_t<2, TK_F40>(c, tup, stride, n, T, s);
+        case 9: return build_t<3, TK_F64>(c, tup, stride, n, T, s);
+        case 10: return build_t<3, TK_F32>(c, tup, stride, n, T, s);
+        case 11: return build_t<3, TK_F40>(c, tup, stride, n, T, s);
+        case 12: return build_t<4, TK_F64>(c, tup, stride, n, T, s);
+        case 13: return build_t<4, TK_F32>(c, tup, stride, n, T, s);
+        case 14: return build_t<4, TK_F40>(c, tup, stride, n, T, s);
     }
     set_error("nlegs must be 2..4");
     return TB_ERR_ARG;
@@ -378,17 +484,24 @@ int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n
 
 static int* g_err_flag = nullptr;
 
-template <int L, bool F32>
+template <int L, int KIND>
 static int launch_t(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T, const int32_t* tup,
                     int64_t stride, int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s) {
-    using E = typename std::conditional<F32, float, double>::type;
-    constexpr int TT = TTile<L, F32>::TT;
+
+    constexpr int TT = TTile<L, KIND>::TT;
     constexpr int STAGES = 2;
-    const size_t smem = size_t(STAGES) * TDim<L>::NMOM * TT * sizeof(E);
+    // the instance-pair path (one moment read for two runs) only where a
+    // group has several instances; it needs more registers, and four-leg
+    // pairs would spill
+    auto kern = (L <= 3 && n_insts > 1) ? k_collision_tensor<L, KIND, TT, STAGES, (L <= 3)>
+                                        : k_collision_tensor<L, KIND, TT, STAGES, false>;
+    const size_t smem = size_t(STAGES) * TT * tuple_bytes(L, KIND);
     static bool attr = false;
     if (!attr) {
-        TB_CUDA(cudaFuncSetAttribute(k_collision_tensor<L, E, TT, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int(smem)));
+        TB_CUDA(cudaFuncSetAttribute(k_collision_tensor<L, KIND, TT, STAGES, (L <= 3)>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        TB_CUDA(cudaFuncSetAttribute(k_collision_tensor<L, KIND, TT, STAGES, false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
         attr = true;
     }
     if (!g_err_flag) {
@@ -399,13 +512,13 @@ static int launch_t(const ChanDev& c, const InstDev* insts, int n_insts, const M
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_collision_tensor<L, E, TT, STAGES>, TT, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TT, smem);
     if (per_sm < 1) per_sm = 1;
     int64_t grid = int64_t(nsm) * per_sm;
     if (grid > T.ntiles) grid = T.ntiles;
     if (grid < 1) return TB_OK;
-    k_collision_tensor<L, E, TT, STAGES><<<unsigned(grid), TT, smem, s>>>(
-        c, insts, n_insts, reinterpret_cast<const E*>(T.d), T.ntiles, tup, stride, n, f, acc, ctl, g_err_flag);
+    kern<<<unsigned(grid), TT, smem, s>>>(c, insts, n_insts, static_cast<const unsigned char*>(T.d), T.ntiles, tup, stride, n,
+                                          f, acc, ctl, g_err_flag);
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }
@@ -414,13 +527,16 @@ int launch_collision_tensor(const ChanDev& c, const InstDev* insts, int n_insts,
                             const int32_t* tup, int64_t stride, int64_t n, const double* f, double* acc,
                             const DPCtl* ctl, cudaStream_t s) {
     if (n <= 0 || n_insts <= 0) return TB_OK;
-    switch (c.L * 2 + (T.fp32 ? 1 : 0)) {
-        case 4: return launch_t<2, false>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
-        case 5: return launch_t<2, true>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
-        case 6: return launch_t<3, false>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
-        case 7: return launch_t<3, true>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
-        case 8: return launch_t<4, false>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
-        case 9: return launch_t<4, true>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
+    switch (c.L * 3 + T.kind) {
+        case 6: return launch_t<2, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
+        case 7: return launch_t<2, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
+        case 8: return launch_t<2, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
+        case 9: return launch_t<3, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
+        case 10: return launch_t<3, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
+        case 11: return launch_t<3, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
+        case 12: return launch_t<4, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
+        case 13: return launch_t<4, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
+        case 14: return launch_t<4, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
     }
     set_error("nlegs must be 2..4");
     return TB_ERR_ARG;

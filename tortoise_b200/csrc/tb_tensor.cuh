@@ -5,19 +5,22 @@
 
 namespace tb {
 
+// storage kinds of the moments (see tb_tensor.cu)
+enum { TK_F64 = 0, TK_F32 = 1, TK_F40 = 2 };
+
 struct MomentTensor {
     void* d = nullptr;        // moments, tile-major (see tb_tensor.cu)
     int64_t n = 0;            // tuples
     int64_t ntiles = 0;
     int nmom = 0;             // moments per tuple
-    bool fp32 = false;
+    int kind = TK_F64;
     void release();
 };
 
-int64_t tensor_bytes(int L, bool fp32, int64_t n_tuples);
+int64_t tensor_bytes(int L, int kind, int64_t n_tuples);
 // tuples per tile of the tile-major moment layout
-int tile_tuples(int L, bool fp32);
-int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, bool fp32, MomentTensor& T,
+int tile_tuples(int L, int kind);
+int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, int kind, MomentTensor& T,
                  cudaStream_t s);
 int launch_collision_tensor(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T,
                             const int32_t* tup, int64_t stride, int64_t n, const double* f, double* acc,

@@ -168,9 +168,9 @@ __global__ void __launch_bounds__(128) k_vjp_mc(ChanDev c, const InstDev* __rest
 }
 
 // --------------------------------------------- collision VJP, moment tensor
-template <int L, typename T>
+template <int L, int KIND>
 __global__ void __launch_bounds__(128) k_vjp_tensor(ChanDev c, const InstDev* __restrict__ insts, int n_insts,
-                                                    const T* __restrict__ mom, int TT, const int32_t* __restrict__ tup,
+                                                    const void* __restrict__ mom, int TT, const int32_t* __restrict__ tup,
                                                     int64_t stride, int64_t n, const double* __restrict__ f,
                                                     const double* __restrict__ u, double* __restrict__ grad_f,
                                                     double* __restrict__ grad_amp) {
@@ -181,7 +181,24 @@ __global__ void __launch_bounds__(128) k_vjp_tensor(ChanDev c, const InstDev* __
         int e[L];
 #pragma unroll
         for (int l = 0; l < L; ++l) e[l] = valid ? __ldg(tup + l * stride + i) : 0;
-        const T* mt = mom + (i / TT) * (int64_t)NMOM * TT + (i % TT);
+        // moment j of tuple i: tile-major rows of TT tuples (FP64, FP32, or
+        // the upper 40 bits of FP64 as a word row plus packed byte rows)
+        constexpr int NB = (KIND == TK_F40) ? (NMOM + 3) / 4 : 0;
+        constexpr int ROWB = (KIND == TK_F64) ? 8 : 4;
+        const unsigned char* tb = static_cast<const unsigned char*>(mom) + (i / TT) * (int64_t)(NMOM + NB) * TT * ROWB;
+        const int64_t pos = i % TT;
+        auto M = [&](int j) -> double {
+            if constexpr (KIND == TK_F64) {
+                return reinterpret_cast<const double*>(tb)[(int64_t)j * TT + pos];
+            } else if constexpr (KIND == TK_F32) {
+                return double(reinterpret_cast<const float*>(tb)[(int64_t)j * TT + pos]);
+            } else {
+                const uint32_t* w = reinterpret_cast<const uint32_t*>(tb);
+                const uint32_t lw = w[(int64_t)(NMOM + (j >> 2)) * TT + pos];
+                return __hiloint2double(int(w[(int64_t)j * TT + pos]),
+                                        int(__byte_perm(lw, 0u, 0x0444u | (uint32_t(j & 3) << 12))));
+            }
+        };
         for (int k = 0; k < n_insts; ++k) {
             const InstDev in = insts[k];
             double A[L][3], B[L][3], sa[L], sb[L];
@@ -195,7 +212,7 @@ __global__ void __launch_bounds__(128) k_vjp_tensor(ChanDev c, const InstDev* __
 #pragma unroll
                 for (int lam = 0; lam < L; ++lam) usum0 += c.leg[lam].dir * __ldg(u + in.foff[lam] + 3 * (int64_t)e[lam]);
 #pragma unroll
-                for (int j = 0; j < K; ++j) w[j] = usum0 * double(mt[(int64_t)j * TT]);
+                for (int j = 0; j < K; ++j) w[j] = usum0 * M(j);
 #pragma unroll
                 for (int lam = 0; lam < L; ++lam) {
                     const double d = c.leg[lam].dir;
@@ -208,11 +225,11 @@ __global__ void __launch_bounds__(128) k_vjp_tensor(ChanDev c, const InstDev* __
                     for (int km = 0; km < KM; ++km) {
                         const int hi = km / sstep, lo = km % sstep;
                         const int j0 = hi * 3 * sstep + lo, j1 = j0 + sstep, j2 = j0 + 2 * sstep;
-                        const double qxx = double(mt[(int64_t)(K + (lam * 3 + 0) * KM + km) * TT]);
-                        const double qxy = double(mt[(int64_t)(K + (lam * 3 + 1) * KM + km) * TT]);
-                        const double qyy = double(mt[(int64_t)(K + (lam * 3 + 2) * KM + km) * TT]);
-                        const double s1 = double(mt[(int64_t)j1 * TT]);
-                        const double s2 = double(mt[(int64_t)j2 * TT]);
+                        const double qxx = M(K + (lam * 3 + 0) * KM + km);
+                        const double qxy = M(K + (lam * 3 + 1) * KM + km);
+                        const double qyy = M(K + (lam * 3 + 2) * KM + km);
+                        const double s1 = M(j1);
+                        const double s2 = M(j2);
                         w[j0] += u1 * s1 + u2 * s2;
                         w[j1] += u1 * qxx + u2 * qxy;
                         w[j2] += u1 * qxy + u2 * qyy;
@@ -273,15 +290,21 @@ int launch_collision_vjp(const ChanDev& c, const InstDev* insts, int n_insts, in
             default: k_vjp_mc<4><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, u, grad_f, grad_amp); break;
         }
     } else {
-        const int TT = tile_tuples(c.L, T.fp32);
-        switch (c.L * 2 + (T.fp32 ? 1 : 0)) {
-            case 4: k_vjp_tensor<2, double><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, (const double*)T.d, TT, tup, stride, n, f, u, grad_f, grad_amp); break;
-            case 5: k_vjp_tensor<2, float><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, (const float*)T.d, TT, tup, stride, n, f, u, grad_f, grad_amp); break;
-            case 6: k_vjp_tensor<3, double><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, (const double*)T.d, TT, tup, stride, n, f, u, grad_f, grad_amp); break;
-            case 7: k_vjp_tensor<3, float><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, (const float*)T.d, TT, tup, stride, n, f, u, grad_f, grad_amp); break;
-            case 8: k_vjp_tensor<4, double><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, (const double*)T.d, TT, tup, stride, n, f, u, grad_f, grad_amp); break;
-            default: k_vjp_tensor<4, float><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, (const float*)T.d, TT, tup, stride, n, f, u, grad_f, grad_amp); break;
+        const int TT = tile_tuples(c.L, T.kind);
+#define TB_VJP_T(LL, KK) k_vjp_tensor<LL, KK><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, T.d, TT, tup, \
+                                                                                 stride, n, f, u, grad_f, grad_amp)
+        switch (c.L * 3 + T.kind) {
+            case 6: TB_VJP_T(2, TK_F64); break;
+            case 7: TB_VJP_T(2, TK_F32); break;
+            case 8: TB_VJP_T(2, TK_F40); break;
+            case 9: TB_VJP_T(3, TK_F64); break;
+            case 10: TB_VJP_T(3, TK_F32); break;
+            case 11: TB_VJP_T(3, TK_F40); break;
+            case 12: TB_VJP_T(4, TK_F64); break;
+            case 13: TB_VJP_T(4, TK_F32); break;
+            default: TB_VJP_T(4, TK_F40); break;
         }
+#undef TB_VJP_T
     }
     TB_CUDA(cudaGetLastError());
     return TB_OK;

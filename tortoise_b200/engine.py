@@ -13,8 +13,8 @@ from .abi import STATUS_NAMES
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libtortoise_b200.so")
 
-LAYOUT_AUTO, LAYOUT_MC64, LAYOUT_T64, LAYOUT_T32 = 0, 1, 2, 3
-LAYOUT_NAMES = {1: "mc64", 2: "t64", 3: "t32"}
+LAYOUT_AUTO, LAYOUT_MC64, LAYOUT_T64, LAYOUT_T32, LAYOUT_T40 = 0, 1, 2, 3, 4
+LAYOUT_NAMES = {1: "mc64", 2: "t64", 3: "t32", 4: "t40"}
 PTR_HOST, NO_DRIFT, NO_COLLISIONS = 1, 2, 4
 
 _lib = None
@@ -117,7 +117,7 @@ class Engine:
     def __init__(self, material, layout=LAYOUT_AUTO, allow_fp32=False, device=0, tensor_budget_bytes=0):
         self.material = material
         self.packed = material.pack()
-        opts = Options(device, layout, 1 if allow_fp32 else 0, tensor_budget_bytes, 0)
+        opts = Options(device, layout, int(allow_fp32), tensor_budget_bytes, 0)
         h = C.c_void_p()
         _check(lib().tb_create(C.byref(h), C.addressof(self.packed.desc), C.byref(opts)), "tb_create")
         self.h = h
@@ -286,7 +286,7 @@ class BatchEngine(Engine):
         self.material = self.materials[0]
         self.packs = [m.pack() for m in self.materials]
         arr = (C.c_void_p * len(self.packs))(*[C.addressof(p.desc) for p in self.packs])
-        opts = Options(device, layout, 1 if allow_fp32 else 0, tensor_budget_bytes, 0)
+        opts = Options(device, layout, int(allow_fp32), tensor_budget_bytes, 0)
         h = C.c_void_p()
         _check(lib().tb_create_batch(C.byref(h), arr, len(self.packs), C.byref(opts)), "tb_create_batch")
         self.h = h
