@@ -257,6 +257,16 @@ void* tb_get_stream(tb_handle* h);
  * callers that compose their own right-hand side. */
 int tb_collision_accumulate(tb_handle* h, int ch, const double* f, double* acc);
 
+/* Out-scattering rates, state-shaped, M^-1 applied (replaces
+ * ScatteringChannel::scatteringRates(status, which), src/Physics/Scattering/
+ * ScatteringChannel.cpp:544-612, and MaterialStatus::scatteringRates,
+ * src/Physics/Status/MaterialStatus.cpp:170-187): for every selected leg the
+ * forms of that leg become the constant in / out unit forms and its block,
+ * with the opposite sign of propagate, lands in the leg's band.
+ * ch = -1: every channel (channels with zero amplitude contribute nothing);
+ * leg = -1: every leg.  rates is overwritten.  flags: TB_PTR_HOST. */
+int tb_scattering_rates(tb_handle* h, int ch, int leg, const double* f, double* rates, int flags);
+
 /* ---------------------------------------------------------------- adjoint
  * No counterpart in the reference, which has no derivatives.  The right-hand
  * side is F(f) = M^-1 (sum_c amplitude_c C_c(f) + V f) (ScatteringChannel::

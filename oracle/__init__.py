@@ -55,6 +55,7 @@ def lib():
         L.or_dp45.argtypes = [vp, dp, C.c_double, C.c_double, C.c_double, dp, dp, C.c_int,
                               C.POINTER(C.c_int), C.c_int, C.c_int, i64, C.POINTER(i64), dp]
         L.or_dp45_replay.argtypes = [vp, dp, dp, i64, C.c_double, dp, C.c_int, C.c_int]
+        L.or_scattering_rates.argtypes = [vp, C.c_int, C.c_int, dp, dp, C.c_int]
         _lib = L
     return _lib
 
@@ -182,6 +183,13 @@ class Oracle:
         out = np.empty(self.ndofs)
         lib().or_dp45_replay(self.h, _dp(y0), _dp(dts), len(dts), float(dense_s), _dp(out), self.nthreads,
                              1 if drift else 0)
+        return out
+
+    def scattering_rates(self, f, ch=-1, which=-1):
+        """Out-scattering rates (M^-1 applied), state-shaped; see or_scattering_rates."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        out = np.empty(self.ndofs)
+        lib().or_scattering_rates(self.h, int(ch), int(which), _dp(f), _dp(out), self.nthreads)
         return out
 
 

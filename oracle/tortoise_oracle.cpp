@@ -458,8 +458,12 @@ static void enumerate(const Problem& P, Channel& c, int nthreads) {
 // ----------------------------------------------------------------- propagate
 // singleScatteringPropagator (array overload), ScatteringChannel.cpp:618-650,
 // with scatteringIntegrationTypeB, IntegratorCore.hpp:260-357.
+// which < 0: singleScatteringPropagator (ScatteringChannel.cpp:618-650).
+// which = leg: singleScatteringRate (ScatteringChannel.cpp:544-581): the forms
+// of that leg become the constant in / out unit forms and only its block is
+// kept, subtracted with the leg's direction.
 static void single_propagator(const Problem& P, const Channel& c, const double* f, const int32_t* e, int umk,
-                              double* out) {
+                              double* out, int which = -1) {
     const int L = c.L;
     Geom g;
     build_geom(P, c, e, umk, g);
@@ -477,8 +481,13 @@ static void single_propagator(const Problem& P, const Channel& c, const double* 
         const double cb = (1. + d) * s + (1. - d);
         for (int j = 0; j < 3; ++j) {
             const double unit = (j == 0) ? 1.0 : 0.0;
-            A[l][j] = ka * ((1. - d) * unit + ca * fe[j]);
-            B[l][j] = 0.5 * ((1. + d) * unit + cb * fe[j]);
+            if (l == which) {   // ScatteringChannel.cpp:562-564
+                A[l][j] = (l == 0 ? -1.0 : 1.0) * ca * unit;
+                B[l][j] = cb * unit;
+            } else {
+                A[l][j] = ka * ((1. - d) * unit + ca * fe[j]);
+                B[l][j] = 0.5 * ((1. + d) * unit + cb * fe[j]);
+            }
         }
     }
     const int R = 2 * (L - 2) + 1;
@@ -501,9 +510,13 @@ static void single_propagator(const Problem& P, const Channel& c, const double* 
     const double scale = 1.0 / (factorial_norm(L) * double(c.nmc) * std::fabs(g.det));
     const double amp = full_amplitude(P, c, c.amplitude);
     for (int l = 0; l < L; ++l) {
+        if (which >= 0 && l != which) continue;
         double* o = out + P.off[c.band[l]] + 3 * size_t(e[l]);
         const double d = double(c.dir[l]);
-        for (int j = 0; j < 3; ++j) o[j] += d * ((scale * acc[l][j]) * amp);
+        for (int j = 0; j < 3; ++j) {
+            if (which >= 0) o[j] -= d * ((scale * acc[l][j]) * amp);
+            else o[j] += d * ((scale * acc[l][j]) * amp);
+        }
     }
 }
 
@@ -511,14 +524,14 @@ static void single_propagator(const Problem& P, const Channel& c, const double* 
 // reduction over tuple ranges with one private accumulator per task
 // (TBB parallel_reduce there, std::thread here), then applyInverseMass.
 static void channel_propagate_range(const Problem& P, const Channel& c, const double* f, double* out,
-                                    int64_t t0, int64_t t1, int nthreads, bool inverse_mass) {
+                                    int64_t t0, int64_t t1, int nthreads, bool inverse_mass, int which = -1) {
     const int64_t n = t1 - t0;
     nthreads = std::max(1, std::min<int>(nthreads, int(std::max<int64_t>(1, n / 64))));
     std::vector<std::vector<double>> part(nthreads, std::vector<double>(size_t(P.ndofs), 0.0));
     auto work = [&](int t) {
         int64_t a = t0 + n * t / nthreads, b = t0 + n * (t + 1) / nthreads;
         for (int64_t i = a; i < b; ++i)
-            single_propagator(P, c, f, &c.tuples[size_t(i) * c.L], c.tumk[size_t(i)], part[t].data());
+            single_propagator(P, c, f, &c.tuples[size_t(i) * c.L], c.tumk[size_t(i)], part[t].data(), which);
     };
     std::vector<std::thread> th;
     for (int t = 1; t < nthreads; ++t) th.emplace_back(work, t);
@@ -1132,6 +1145,26 @@ int or_dp45(void* h, double* y, double t0, double tf, double dense, double* dens
     stats[0] = st.attempts; stats[1] = st.accepted; stats[2] = st.rejected; stats[3] = st.rhs_evals;
     dstats[0] = st.t; dstats[1] = st.dt; dstats[2] = st.last_err;
     return rc;
+}
+
+// ScatteringChannel::scatteringRates(status, which) (ScatteringChannel.cpp:582-603)
+// summed over the legs of one channel (ch >= 0, which < 0), one leg (which >=
+// 0) or, with ch < 0, every channel with a nonzero amplitude and every leg
+// (MaterialStatus::scatteringRates, MaterialStatus.cpp:170-187).  Each leg's
+// rate lands in its own band; out (the whole state) is overwritten, M^-1
+// applied.
+void or_scattering_rates(void* h, int ch, int which, const double* f, double* out, int nthreads) {
+    const Problem& P = *static_cast<Problem*>(h);
+    std::fill(out, out + P.ndofs, 0.0);
+    for (size_t ci = 0; ci < P.chans.size(); ++ci) {
+        const Channel& c = P.chans[ci];
+        if (ch >= 0 && int(ci) != ch) continue;
+        if (ch < 0 && c.amplitude == 0.0) continue;
+        for (int l = 0; l < c.L; ++l) {
+            if (which >= 0 && l != which) continue;
+            channel_propagate_range(P, c, f, out, 0, int64_t(c.tumk.size()), nthreads, true, l);
+        }
+    }
 }
 
 void or_dp45_replay(void* h, const double* y0, const double* dts, int64_t n_steps, double dense_s, double* out,

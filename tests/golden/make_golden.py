@@ -57,6 +57,9 @@ def make(name):
         out["ch%d_prop" % ch] = o.channel_propagate(ch, f0)
     out["rhs"] = o.rhs(f0, drift=True)
     out["rhs_nodrift"] = o.rhs(f0, drift=False)
+    out["rates"] = o.scattering_rates(f0)   # MaterialStatus::scatteringRates
+    for ch in range(len(mat.channels)):
+        out["ch%d_rates" % ch] = o.scattering_rates(f0, ch)
     rng = np.random.default_rng(seed + 100)
     err = 1e-7 * rng.standard_normal(f0.size)
     out["err"] = err

@@ -187,3 +187,49 @@ def test_tensor_layout_40bit_error_bound(gpu_lib, name):
             assert eng.channel_info(ch)["layout"] == "t40"
         assert rel_l2(eng.channel_propagate(ch, f0), g["ch%d_prop" % ch]) < 2e-8
     assert rel_l2(eng.rhs(f0, drift=False), g["rhs_nodrift"]) < 2e-8
+
+
+@pytest.mark.parametrize("layout,tol", [(E.LAYOUT_MC64, 1e-12), (E.LAYOUT_T64, 1e-12), (E.LAYOUT_T40, 2e-8),
+                                        (E.LAYOUT_T32, 1e-6)])
+@pytest.mark.parametrize("name", CASES)
+def test_scattering_rates_parity(gpu_lib, name, layout, tol):
+    """tb_scattering_rates (ScatteringChannel::scatteringRates /
+    MaterialStatus::scatteringRates) against the oracle's golden rates, per
+    channel and for the whole status; FP64 layouts to 1e-12, reduced-precision
+    storage to its stated bound."""
+    g = golden(name)
+    mat, f0 = _setup(name)
+    eng = E.Engine(mat, layout=layout)
+    assert rel_l2(eng.scattering_rates(f0), g["rates"]) < tol
+    for ch in range(len(mat.channels)):
+        ref = g["ch%d_rates" % ch]
+        got = eng.scattering_rates(f0, ch)
+        if np.linalg.norm(ref) == 0.0:
+            assert np.linalg.norm(got) == 0.0
+        else:
+            assert rel_l2(got, ref) < tol
+
+
+def test_scattering_rates_per_leg_and_errors(gpu_lib):
+    """Single legs against the live oracle, the reference-shaped Material API,
+    and argument checks."""
+    mat, f0 = _setup("eph_n4")
+    o = oracle.Oracle(mat)
+    eng = mat.engine()
+    for ch, c in enumerate(mat.channels):
+        for leg in range(c.nlegs):
+            assert rel_l2(eng.scattering_rates(f0, ch, leg), o.scattering_rates(f0, ch, leg)) < 1e-12
+    from tortoise_b200.model import IN, OUT, MaterialStatus
+    st = MaterialStatus(mat, f0)
+    offs, _ = mat.band_offsets()
+    b = mat.id("el:P")
+    want = sum(o.scattering_rates(f0, ch, leg) for ch, c in enumerate(mat.channels)
+               if mat.band_names[c.legBandNumber[0]] in ("el:P", "el:D")
+               for leg in range(c.nlegs) if c.legBandNumber[leg] == b)
+    got = mat.scatteringRates(["el:*", "pn:*", "el:*"], [IN, IN, OUT], st, "el:P")
+    assert rel_l2(got, want[offs[b]:offs[b] + got.size]) < 1e-12
+    assert rel_l2(st.scatteringRates().vec, o.scattering_rates(f0)) < 1e-12
+    with pytest.raises(E.TortoiseError):
+        eng.scattering_rates(f0, len(mat.channels), -1)
+    with pytest.raises(E.TortoiseError):
+        eng.scattering_rates(f0, 0, 3)

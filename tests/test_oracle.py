@@ -127,3 +127,33 @@ def test_single_tuple_partition_additivity():
     a = o.channel_propagate(0, f0, 0, n // 3)
     b = o.channel_propagate(0, f0, n // 3, n)
     assert rel_l2(a + b, full) < 1e-13
+
+
+def test_scattering_rates_are_twice_the_affine_slope():
+    """The oracle's ScatteringChannel::scatteringRates (ScatteringChannel.cpp:
+    544-612) against its propagate: each leg's gain / loss forms are affine in
+    that leg's coefficients with half the slope of the rate's unit forms, so
+    for a leg whose band no other leg of the channel uses, the rate equals -2
+    times the change of the channel's output on that band when c0 of every
+    element of the band rises by 1 (exact up to rounding)."""
+    import oracle
+    mat = W.build_material(4, ("P", "D"), (0.2,), ee=False, eph=True, field=(0.1, 0.0))
+    f = W.initial_status(mat, kT=0.1, seed=4).vec
+    o = oracle.Oracle(mat)
+    offs, n = mat.band_offsets()
+    checked = 0
+    for ch, c in enumerate(mat.channels):
+        for leg, b in enumerate(c.legBandNumber):
+            if list(c.legBandNumber).count(b) != 1:
+                continue
+            sl = slice(offs[b], offs[b] + mat.bands[b].mesh.ne * 3)
+            u = np.zeros(n)
+            u[sl][0::3] = 1.0
+            slope = o.channel_propagate(ch, f + u)[sl] - o.channel_propagate(ch, f)[sl]
+            rate = o.scattering_rates(f, ch, leg)[sl]
+            assert np.linalg.norm(rate + 2.0 * slope) <= 1e-12 * np.linalg.norm(rate)
+            checked += 1
+    assert checked >= 6
+    # the whole-status sum is the sum over channels and legs
+    tot = sum(o.scattering_rates(f, ch) for ch in range(len(mat.channels)))
+    assert np.allclose(o.scattering_rates(f), tot, rtol=1e-13, atol=0)

@@ -781,6 +781,52 @@ static int rhs_common(tb_handle* h, const double* f, double* out, int flags, int
 
 int tb_rhs(tb_handle* h, const double* f, double* dfdt, int flags) { return rhs_common(h, f, dfdt, flags, -1); }
 
+int tb_scattering_rates(tb_handle* h, int ch, int leg, const double* f, double* rates, int flags) {
+    if (!h || !f || !rates) { set_error("null argument"); return TB_ERR_ARG; }
+    if (ch < -1 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
+    if (leg < -1 || leg >= TB_MAX_LEGS || (ch >= 0 && leg >= h->groups[h->insts[ch].group].L)) {
+        set_error("leg index out of range");
+        return TB_ERR_ARG;
+    }
+    TB_CUDA(cudaSetDevice(h->device));
+    const size_t bytes = sizeof(double) * size_t(h->ndofs);
+    const double* d_in = f;
+    double* d_res = rates;
+    if (flags & TB_PTR_HOST) {
+        TB_CUDA(cudaMemcpyAsync(h->d_f, f, bytes, cudaMemcpyHostToDevice, h->stream));
+        d_in = h->d_f;
+        d_res = h->d_out;
+    }
+    TB_CUDA(cudaMemsetAsync(h->d_acc, 0, bytes, h->stream));
+    for (size_t gi = 0; gi < h->groups.size(); ++gi) {
+        GroupChan& G = h->groups[gi];
+        if (G.tup.n == 0) continue;
+        const InstDev* insts = G.d_insts;
+        int n_insts = int(G.insts.size());
+        if (ch >= 0) {
+            if (h->insts[ch].group != int(gi)) continue;
+            insts = h->insts[ch].d_single;
+            n_insts = 1;
+        }
+        for (int l = 0; l < G.L; ++l) {
+            if (leg >= 0 && l != leg) continue;
+            if (G.layout == TB_LAYOUT_MC64)
+                TB_TRY(launch_collision_mc(G.dev, insts, n_insts, G.tup.d, G.tup.cap, G.tup.n, d_in, h->d_acc, nullptr,
+                                           h->stream, 148 * 32, l));
+            else
+                TB_TRY(launch_collision_tensor(G.dev, insts, n_insts, G.tensor, G.tup.d, G.tup.cap, G.tup.n, d_in,
+                                               h->d_acc, nullptr, h->stream, l));
+        }
+    }
+    TB_TRY(launch_inverse_mass(h->ed, h->d_acc, d_res, h->stream));
+    TB_CUDA(cudaMemsetAsync(h->d_acc, 0, bytes, h->stream));
+    if (flags & TB_PTR_HOST) {
+        TB_CUDA(cudaMemcpyAsync(rates, h->d_out, bytes, cudaMemcpyDeviceToHost, h->stream));
+        TB_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    return TB_OK;
+}
+
 int tb_channel_propagate(tb_handle* h, int ch, const double* f, double* out, int flags) {
     if (!h || ch < 0 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
     return rhs_common(h, f, out, flags | TB_NO_DRIFT, ch);

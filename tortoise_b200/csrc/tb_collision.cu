@@ -24,7 +24,7 @@ template <int L>
 __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* __restrict__ insts, int n_insts,
                                                       const int32_t* __restrict__ tup, int64_t stride, int64_t n,
                                                       const double* __restrict__ f, double* __restrict__ acc,
-                                                      const DPCtl* __restrict__ ctl) {
+                                                      const DPCtl* __restrict__ ctl, int rate_leg) {
     extern __shared__ double s_mc[];
     constexpr int R = 2 * (L - 2) + 1;
     for (int i = threadIdx.x; i < c.nmc * R; i += blockDim.x) s_mc[i] = c.mc[i];
@@ -93,6 +93,12 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* 
                     A[l][j] = ka * ((1. - d) * unit + ca * fj);
                     B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
                 }
+                if (l == rate_leg) {
+                    // scattering rate of this leg: constant in / out unit forms
+                    // (ScatteringChannel.cpp:562-564)
+                    A[l][0] = (l == 0 ? -1.0 : 1.0) * ca; A[l][1] = 0.0; A[l][2] = 0.0;
+                    B[l][0] = cb; B[l][1] = 0.0; B[l][2] = 0.0;
+                }
             }
             double s0 = 0.0, sx[L], sy[L];
 #pragma unroll
@@ -139,7 +145,8 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* 
             const double scale = valid ? 1.0 / (inv_fact_nmc * fabs(g.det)) : 0.0;
 #pragma unroll
             for (int l = 0; l < L; ++l) {
-                const double d = c.leg[l].dir;
+                if (rate_leg >= 0 && l != rate_leg) continue;   // uniform: the rate keeps one leg
+                const double d = rate_leg >= 0 ? -c.leg[l].dir : c.leg[l].dir;
                 const int64_t key = in.foff[l] + 3 * (int64_t)e[l];
                 if (l < L - 1) {
                     warp_scatter3(valid ? key : -1, acc + key, d * ((scale * s0) * in.amp_full),
@@ -156,16 +163,17 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* 
 }
 
 int launch_collision_mc(const ChanDev& c, const InstDev* insts, int n_insts, const int32_t* tup, int64_t stride,
-                        int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s, int grid_hint) {
+                        int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s, int grid_hint,
+                        int rate_leg) {
     if (n <= 0 || n_insts <= 0) return TB_OK;
     const int threads = 256;
     int64_t blocks = (n + threads - 1) / threads;
     if (grid_hint > 0 && blocks > grid_hint) blocks = grid_hint;
     const size_t smem = sizeof(double) * size_t(c.nmc) * c.R;
     switch (c.L) {
-        case 2: k_collision_mc<2><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, acc, ctl); break;
-        case 3: k_collision_mc<3><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, acc, ctl); break;
-        case 4: k_collision_mc<4><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, acc, ctl); break;
+        case 2: k_collision_mc<2><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, acc, ctl, rate_leg); break;
+        case 3: k_collision_mc<3><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, acc, ctl, rate_leg); break;
+        case 4: k_collision_mc<4><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, acc, ctl, rate_leg); break;
         default: set_error("nlegs must be 2..4"); return TB_ERR_ARG;
     }
     TB_CUDA(cudaGetLastError());

@@ -255,7 +255,7 @@ __device__ __forceinline__ double tile_moment(const unsigned char* __restrict__ 
 template <int L, int KIND, int TT, int NI>
 __device__ __forceinline__ void contract_tuple(const ChanDev& c, const InstDev (&in)[NI], const int (&e)[L], bool valid,
                                                const unsigned char* __restrict__ tile, int tid,
-                                               const double* __restrict__ f, double* __restrict__ acc) {
+                                               const double* __restrict__ f, double* __restrict__ acc, int rate_leg) {
     constexpr int K = TDim<L>::K, KM = TDim<L>::KM, NMOM = TDim<L>::NMOM;
     auto M = [&](int j) { return tile_moment<KIND, NMOM, TT>(tile, tid, j); };
     // v = kron(A) + kron(B) per instance, leg 0 most significant; gain (B) /
@@ -277,6 +277,12 @@ __device__ __forceinline__ void contract_tuple(const ChanDev& c, const InstDev (
                 const double fj = __ldg(fe + j);
                 A[l][j] = ka * ((1. - d) * unit + ca * fj);
                 B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
+            }
+            if (l == rate_leg) {
+                // scattering rate of this leg: constant in / out unit forms
+                // (ScatteringChannel.cpp:562-564)
+                A[l][0] = (l == 0 ? -1.0 : 1.0) * ca; A[l][1] = 0.0; A[l][2] = 0.0;
+                B[l][0] = cb; B[l][1] = 0.0; B[l][2] = 0.0;
             }
         }
 #pragma unroll
@@ -304,6 +310,7 @@ __device__ __forceinline__ void contract_tuple(const ChanDev& c, const InstDev (
     }
 #pragma unroll
     for (int lam = 0; lam < L; ++lam) {
+        if (rate_leg >= 0 && lam != rate_leg) continue;   // uniform: the rate keeps one leg
         int sstep = 1;
 #pragma unroll
         for (int l = L - 1; l > lam; --l) sstep *= 3;
@@ -329,7 +336,7 @@ __device__ __forceinline__ void contract_tuple(const ChanDev& c, const InstDev (
                 r2[q] = fma(qyy, v[q][j2], r2[q]);
             }
         }
-        const double d = c.leg[lam].dir;
+        const double d = rate_leg >= 0 ? -c.leg[lam].dir : c.leg[lam].dir;
 #pragma unroll
         for (int q = 0; q < NI; ++q) {
             const double amp = in[q].amplitude;
@@ -357,7 +364,8 @@ __global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, const InstDe
                                                          const unsigned char* __restrict__ mom, int64_t ntiles,
                                                          const int32_t* __restrict__ tup, int64_t stride, int64_t n,
                                                          const double* __restrict__ f, double* __restrict__ acc,
-                                                         const DPCtl* __restrict__ ctl, int* __restrict__ err_flag) {
+                                                         const DPCtl* __restrict__ ctl, int* __restrict__ err_flag,
+                                                         int rate_leg) {
     constexpr uint32_t TILE_BYTES = uint32_t(TBytes<L, KIND>::B) * TT;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char* stage_buf = smem_raw;
@@ -421,11 +429,11 @@ __global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, const InstDe
                 while (k2 < n_insts && !active(insts[k2])) ++k2;
                 if (PAIR && k2 < n_insts) {
                     const InstDev pair[2] = {a, insts[k2]};
-                    contract_tuple<L, KIND, TT, 2>(c, pair, e, valid, sm, tid, f, acc);
+                    contract_tuple<L, KIND, TT, 2>(c, pair, e, valid, sm, tid, f, acc, rate_leg);
                     k = k2 + 1;
                 } else {
                     const InstDev one[1] = {a};
-                    contract_tuple<L, KIND, TT, 1>(c, one, e, valid, sm, tid, f, acc);
+                    contract_tuple<L, KIND, TT, 1>(c, one, e, valid, sm, tid, f, acc, rate_leg);
                     k = PAIR ? k2 : k + 1;
                 }
             }
@@ -486,7 +494,8 @@ static int* g_err_flag = nullptr;
 
 template <int L, int KIND>
 static int launch_t(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T, const int32_t* tup,
-                    int64_t stride, int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s) {
+                    int64_t stride, int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s,
+                    int rate_leg) {
 
     constexpr int TT = TTile<L, KIND>::TT;
     constexpr int STAGES = 2;
@@ -518,25 +527,25 @@ static int launch_t(const ChanDev& c, const InstDev* insts, int n_insts, const M
     if (grid > T.ntiles) grid = T.ntiles;
     if (grid < 1) return TB_OK;
     kern<<<unsigned(grid), TT, smem, s>>>(c, insts, n_insts, static_cast<const unsigned char*>(T.d), T.ntiles, tup, stride, n,
-                                          f, acc, ctl, g_err_flag);
+                                          f, acc, ctl, g_err_flag, rate_leg);
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }
 
 int launch_collision_tensor(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T,
                             const int32_t* tup, int64_t stride, int64_t n, const double* f, double* acc,
-                            const DPCtl* ctl, cudaStream_t s) {
+                            const DPCtl* ctl, cudaStream_t s, int rate_leg) {
     if (n <= 0 || n_insts <= 0) return TB_OK;
     switch (c.L * 3 + T.kind) {
-        case 6: return launch_t<2, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
-        case 7: return launch_t<2, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
-        case 8: return launch_t<2, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
-        case 9: return launch_t<3, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
-        case 10: return launch_t<3, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
-        case 11: return launch_t<3, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
-        case 12: return launch_t<4, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
-        case 13: return launch_t<4, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
-        case 14: return launch_t<4, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
+        case 6: return launch_t<2, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 7: return launch_t<2, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 8: return launch_t<2, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 9: return launch_t<3, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 10: return launch_t<3, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 11: return launch_t<3, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 12: return launch_t<4, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 13: return launch_t<4, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 14: return launch_t<4, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
     }
     set_error("nlegs must be 2..4");
     return TB_ERR_ARG;

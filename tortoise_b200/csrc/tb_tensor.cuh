@@ -22,9 +22,10 @@ int64_t tensor_bytes(int L, int kind, int64_t n_tuples);
 int tile_tuples(int L, int kind);
 int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, int kind, MomentTensor& T,
                  cudaStream_t s);
+// rate_leg >= 0: scattering rate of that leg instead (see launch_collision_mc)
 int launch_collision_tensor(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T,
                             const int32_t* tup, int64_t stride, int64_t n, const double* f, double* acc,
-                            const DPCtl* ctl, cudaStream_t s);
+                            const DPCtl* ctl, cudaStream_t s, int rate_leg = -1);
 
 // 1 once a bulk-copy wait of the contraction kernel ran out (then TB_ERR_TIMEOUT)
 int tensor_error_flag(int* value);

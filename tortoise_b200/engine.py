@@ -84,6 +84,7 @@ def lib():
         L.tb_get_stream.restype = vp
         L.tb_get_stream.argtypes = [vp]
         L.tb_collision_accumulate.argtypes = [vp, C.c_int, vp, vp]
+        L.tb_scattering_rates.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_int]
         L.tb_create_batch.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int, C.POINTER(Options)]
         L.tb_num_runs.argtypes = [vp]
         L.tb_run_info.argtypes = [vp, C.c_int, C.POINTER(i64), C.POINTER(i64), C.POINTER(C.c_int32),
@@ -165,6 +166,13 @@ class Engine:
         f = np.ascontiguousarray(f, dtype=np.float64)
         out = np.empty(self.ndofs)
         _check(lib().tb_channel_propagate(self.h, ch, _hp(f), _hp(out), PTR_HOST), "tb_channel_propagate")
+        return out
+
+    def scattering_rates(self, f, ch=-1, leg=-1):
+        """Out-scattering rates (MaterialStatus::scatteringRates for ch = leg = -1)."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        out = np.empty(self.ndofs)
+        _check(lib().tb_scattering_rates(self.h, int(ch), int(leg), _hp(f), _hp(out), PTR_HOST), "tb_scattering_rates")
         return out
 
     def relative_error(self, err, pop):

@@ -277,6 +277,42 @@ class Material:
             added.append(c)
         return added
 
+    # -- analysis (Material.cpp:396-410) -----------------------------------
+    def scatteringChannelMatchList(self, band_names_wildcards, directions):
+        """Channels whose ordered legs match the wildcards and directions
+        exactly (Material.cpp:124-162)."""
+        L = len(band_names_wildcards)
+        out = []
+        for i, c in enumerate(self.channels):
+            if c.nlegs != L or list(c.legDirection) != list(directions):
+                continue
+            if all(match_string(w, self.band_names[b]) for w, b in zip(band_names_wildcards, c.legBandNumber)):
+                out.append(i)
+        return out
+
+    def scatteringRates(self, band_names_wildcards, directions, status, bandName):
+        """Material::scatteringRates<L> (Material.cpp:396-402): out-scattering
+        rates of band bandName from the matching channels, on the GPU."""
+        eng = self.engine()
+        b = self.id(bandName)
+        offs, _ = self.band_offsets()
+        out = np.zeros(self.bands[b].mesh.ne * 3)
+        for ch in self.scatteringChannelMatchList(band_names_wildcards, directions):
+            for leg, lb in enumerate(self.channels[ch].legBandNumber):
+                if lb == b:
+                    out += eng.scattering_rates(status.vec, ch, leg)[offs[b]:offs[b] + out.size]
+        return out
+
+    def selectivePropagation(self, band_names_wildcards, directions, status, bandName):
+        """Material::selectivePropagation<L> (Material.cpp:404-410)."""
+        eng = self.engine()
+        tot = np.zeros(status.vec.size)
+        for ch in self.scatteringChannelMatchList(band_names_wildcards, directions):
+            tot += eng.channel_propagate(ch, status.vec)
+        b = self.id(bandName)
+        offs, _ = self.band_offsets()
+        return tot[offs[b]:offs[b] + self.bands[b].mesh.ne * 3]
+
     # -- packing ---------------------------------------------------------
     def pack(self):
         return PackedProblem(self.region, self.meshes, self.bands, self.channels)
@@ -334,6 +370,11 @@ class MaterialStatus:
 
     def relativeError(self, population):
         return self.material.engine().relative_error(self.vec, population.vec)
+
+    def scatteringRates(self):
+        """MaterialStatus::scatteringRates (MaterialStatus.cpp:170-187): the
+        out-scattering rate of every band from every channel, on the GPU."""
+        return MaterialStatus(self.material, self.material.engine().scattering_rates(self.vec))
 
 
 class MaterialTimeStatus:
