@@ -317,23 +317,31 @@ def ours(args, world, rank, local, pg):
     clk_s = clk.summary()
     if clk_s:
         line["clocks"] = clk_s
+    if rank == 0 and world == 1 and not args.no_extras and args.mixed is None:
+        # the north-star comparison beside the FP64 headline: mixed-precision
+        # storage on this workload, and the batched ensemble against
+        # sequential single-run FP64
+        line["mixed"] = mixed_measure(eng, mat, f0, args.steps, args.warmup, dev)
+        eng.close()
+        line["batched"] = batched_measure(256, 10, 3, "t40")
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()
 
 
-def batched(args):
+def batched_measure(n_runs, steps, warmup, mixed, layout_name="auto"):
     """Batched ensemble (ensemble_runs: N in {16..64}, per-run kT and
-    couplings): args.batch runs in one handle, DP45 attempts of all runs per
-    graph launch; value = run-attempts/s."""
+    couplings): n_runs runs in one handle, DP45 attempts of all runs per
+    graph launch; value = run-attempts/s.  Baseline: the same run-attempts on
+    the plain single-run FP64 path, one run at a time."""
     import torch
     from tortoise_b200 import engine as E
     from tortoise_b200 import workloads as W
-    mats, states = W.ensemble_runs(args.batch)
+    mats, states = W.ensemble_runs(n_runs)
     layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32,
-              "t40": E.LAYOUT_T40}[args.layout]
+              "t40": E.LAYOUT_T40}[layout_name]
     t0 = time.perf_counter()
-    be = E.BatchEngine(mats, layout=layout, allow_fp32=mixed_flag(args))
+    be = E.BatchEngine(mats, layout=layout, allow_fp32={None: 0, "t32": 1, "t40": 2}[mixed])
     t_setup = time.perf_counter() - t0
     f0 = np.concatenate(states)
     stream = torch.cuda.ExternalStream(be.stream_ptr())
@@ -350,11 +358,11 @@ def batched(args):
     ev1.synchronize()
     t_coll = ev0.elapsed_time(ev1) * 1e-3 / 5
     be.dp45_begin(f0, 0.0, 1.0e9, DENSE, 0)
-    be.dp45_advance(args.warmup)
+    be.dp45_advance(warmup)
     be.synchronize()
     with ClockSampler(0) as clk:
         ev0.record(stream)
-        be.dp45_advance(args.steps)
+        be.dp45_advance(steps)
         ev1.record(stream)
         ev1.synchronize()
     t = ev0.elapsed_time(ev1) * 1e-3
@@ -368,7 +376,9 @@ def batched(args):
         if N not in uniq:
             uniq[N] = sum(be.channel_info(be.chan0[r] + c)["n_tuples"] for c in range(len(m.channels)))
     layouts = sorted({be.channel_info(c)["layout"] for c in range(be.channel_count())})
+    ndofs = be.ndofs
     be.close()
+    del f, acc
     # The same run-attempts done one run at a time on the plain single-run
     # FP64 path (one handle per structure; runs of equal N cost the same).
     seq = {}
@@ -377,23 +387,71 @@ def batched(args):
         eng = E.Engine(mats[r], layout=E.LAYOUT_AUTO, allow_fp32=False)
         s1 = torch.cuda.ExternalStream(eng.stream_ptr())
         eng.dp45_begin(states[r], 0.0, 1.0e9, DENSE, 0)
-        eng.dp45_advance(args.warmup)
+        eng.dp45_advance(warmup)
         eng.synchronize()
         ev0.record(s1)
-        eng.dp45_advance(args.steps)
+        eng.dp45_advance(steps)
         ev1.record(s1)
         ev1.synchronize()
-        seq[N] = ev0.elapsed_time(ev1) * 1e-3 / args.steps
+        seq[N] = ev0.elapsed_time(ev1) * 1e-3 / steps
         eng.close()
     t_seq = sum(groups[N] * seq[N] for N in Ns)   # one attempt of every run
-    print(json.dumps({"batched": True, "runs": args.batch, "mixed": args.mixed, "steps": args.steps,
-                      "run_attempts_per_s": args.batch * args.steps / t, "ms_per_attempt": 1e3 * t / args.steps,
-                      "collision_ms": 1e3 * t_coll, "setup_s": t_setup, "runs_per_N": groups,
-                      "tuples_per_structure": uniq, "dofs": be.ndofs, "layouts": layouts,
-                      "sequential_fp64_ms_per_attempt_by_N": {N: 1e3 * seq[N] for N in Ns},
-                      "sequential_fp64_run_attempts_per_s": args.batch / t_seq,
-                      "speedup_vs_sequential_fp64": (args.batch * args.steps / t) / (args.batch / t_seq),
-                      "clocks": clk.summary()}), flush=True)
+    return {"runs": n_runs, "mixed": mixed, "steps": steps,
+            "run_attempts_per_s": n_runs * steps / t, "ms_per_attempt": 1e3 * t / steps,
+            "collision_ms": 1e3 * t_coll, "setup_s": t_setup, "runs_per_N": groups,
+            "tuples_per_structure": uniq, "dofs": ndofs, "layouts": layouts,
+            "sequential_fp64_ms_per_attempt_by_N": {N: 1e3 * seq[N] for N in Ns},
+            "sequential_fp64_run_attempts_per_s": n_runs / t_seq,
+            "speedup_vs_sequential_fp64": (n_runs * steps / t) / (n_runs / t_seq),
+            "clocks": clk.summary()}
+
+
+def batched(args):
+    d = batched_measure(args.batch, args.steps, args.warmup, args.mixed, args.layout)
+    print(json.dumps(dict({"batched": True}, **d)), flush=True)
+
+
+def mixed_measure(eng64, mat, f0, steps, warmup, dev):
+    """The same workload with 40-bit moment storage: collision GB/s, DP45
+    attempts/s and the error of its dense outputs against the FP64 path's
+    (both integrated to t = 0.2 with dense step 0.05)."""
+    import torch
+    from tortoise_b200 import engine as E
+    eng = E.Engine(mat, layout=E.LAYOUT_AUTO, allow_fp32=2)
+    infos = [eng.channel_info(c) for c in range(len(mat.channels))]
+    stream = torch.cuda.ExternalStream(eng.stream_ptr(), device=dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f = torch.tensor(f0, device=dev)
+    acc = torch.zeros_like(f)
+    for _ in range(3):
+        eng.collision_accumulate(f.data_ptr(), acc.data_ptr())
+    eng.synchronize()
+    ev0.record(stream)
+    for _ in range(20):
+        eng.collision_accumulate(f.data_ptr(), acc.data_ptr())
+    ev1.record(stream)
+    ev1.synchronize()
+    t_coll = ev0.elapsed_time(ev1) * 1e-3 / 20
+    bytes_coll = sum(i["n_tuples"] * (moment_bytes(c.nlegs, i["layout"]) + 4 * (c.nlegs + 1))
+                     for c, i in zip(mat.channels, infos)) + eng.ndofs * 8 * 3
+    eng.dp45_begin(f0, 0.0, 1.0e9, DENSE, 0)
+    eng.dp45_advance(warmup)
+    eng.synchronize()
+    ev0.record(stream)
+    eng.dp45_advance(steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    t = ev0.elapsed_time(ev1) * 1e-3
+    r40 = eng.dp45(f0, 0.0, 0.2, 0.05)
+    r64 = eng64.dp45(f0, 0.0, 0.2, 0.05)
+    err = max(float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(r40["dense"], r64["dense"]))
+    eng.close()
+    hbm, _ = peaks()
+    return {"layouts": [i["layout"] for i in infos], "value": steps / t, "unit": "DP45 steps/s",
+            "collision_gbs": bytes_coll / t_coll / 1e9, "frac": bytes_coll / t_coll / 1e9 / hbm,
+            "seconds_per_launch": t_coll,
+            "error_vs_fp64": err, "error_metric": "max relative L2 over the dense outputs at t = 0.05 .. 0.2",
+            "dtype": "fp64-upper-40-bit-storage/f64-accumulate"}
 
 
 def adjoint(args):
@@ -481,6 +539,7 @@ def main():
     ap.add_argument("--mixed", nargs="?", const="t40", default=None, choices=["t32", "t40"],
                     help="reduced-precision moment storage: t40 (upper 40 bits of FP64, default) or t32 (FP32)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and batched measurements")
     ap.add_argument("--rhs-only", type=int, default=0, help="profiling driver: K RHS evaluations only")
     ap.add_argument("--mesh", type=int, default=N_MESH, help="sections per side (profiling driver only)")
     ap.add_argument("--batch", type=int, default=0, help="batched ensemble of this many runs (per-run N, kT, couplings)")
