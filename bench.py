@@ -206,7 +206,7 @@ def ours(args, world, rank, local, pg):
     mat, f0 = workload()
     layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32,
               "t40": E.LAYOUT_T40}[args.layout]
-    eng = E.Engine(mat, layout=layout, allow_fp32=mixed_flag(args), device=local)
+    eng = E.Engine(mat, layout=layout, allow_fp32=mixed_flag(args), device=local, autotune=not args.no_tune)
     nch = len(mat.channels)
     infos = [eng.channel_info(c) for c in range(nch)]
     ntup = sum(i["n_tuples"] for i in infos)
@@ -301,6 +301,7 @@ def ours(args, world, rank, local, pg):
             "data": "synthetic (seeded PCG64 bump on Fermi-Dirac, Bose phonons)",
             "config": {"workload": "2-band e-ph + drift, 64x64 mesh (8192 triangles/band), NMC=50, rtol 1e-8",
                        "tuples": ntup, "channels": nch, "layouts": [i["layout"] for i in infos],
+                       "schedules": [eng.schedule(c) for c in range(nch)],
                        "dofs": eng.ndofs, "parallelism": "replicas x%d" % world,
                        "l2": "moment tensors (%.1f GB) exceed L2; no flush" % (bytes_coll / 1e9)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -329,7 +330,7 @@ def ours(args, world, rank, local, pg):
     eng.close()
 
 
-def batched_measure(n_runs, steps, warmup, mixed, layout_name="auto"):
+def batched_measure(n_runs, steps, warmup, mixed, layout_name="auto", tune=True):
     """Batched ensemble (ensemble_runs: N in {16..64}, per-run kT and
     couplings): n_runs runs in one handle, DP45 attempts of all runs per
     graph launch; value = run-attempts/s.  Baseline: the same run-attempts on
@@ -341,7 +342,7 @@ def batched_measure(n_runs, steps, warmup, mixed, layout_name="auto"):
     layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32,
               "t40": E.LAYOUT_T40}[layout_name]
     t0 = time.perf_counter()
-    be = E.BatchEngine(mats, layout=layout, allow_fp32={None: 0, "t32": 1, "t40": 2}[mixed])
+    be = E.BatchEngine(mats, layout=layout, allow_fp32={None: 0, "t32": 1, "t40": 2}[mixed], autotune=tune)
     t_setup = time.perf_counter() - t0
     f0 = np.concatenate(states)
     stream = torch.cuda.ExternalStream(be.stream_ptr())
@@ -376,6 +377,7 @@ def batched_measure(n_runs, steps, warmup, mixed, layout_name="auto"):
         if N not in uniq:
             uniq[N] = sum(be.channel_info(be.chan0[r] + c)["n_tuples"] for c in range(len(m.channels)))
     layouts = sorted({be.channel_info(c)["layout"] for c in range(be.channel_count())})
+    scheds = sorted({(s["stages"], s["pair"]) for s in (be.schedule(c) for c in range(be.channel_count()))})
     ndofs = be.ndofs
     be.close()
     del f, acc
@@ -384,7 +386,7 @@ def batched_measure(n_runs, steps, warmup, mixed, layout_name="auto"):
     seq = {}
     for N in Ns:
         r = next(i for i, m in enumerate(mats) if m.bands[0].mesh.nsplit[0] == N)
-        eng = E.Engine(mats[r], layout=E.LAYOUT_AUTO, allow_fp32=False)
+        eng = E.Engine(mats[r], layout=E.LAYOUT_AUTO, allow_fp32=False, autotune=tune)
         s1 = torch.cuda.ExternalStream(eng.stream_ptr())
         eng.dp45_begin(states[r], 0.0, 1.0e9, DENSE, 0)
         eng.dp45_advance(warmup)
@@ -399,7 +401,7 @@ def batched_measure(n_runs, steps, warmup, mixed, layout_name="auto"):
     return {"runs": n_runs, "mixed": mixed, "steps": steps,
             "run_attempts_per_s": n_runs * steps / t, "ms_per_attempt": 1e3 * t / steps,
             "collision_ms": 1e3 * t_coll, "setup_s": t_setup, "runs_per_N": groups,
-            "tuples_per_structure": uniq, "dofs": ndofs, "layouts": layouts,
+            "tuples_per_structure": uniq, "dofs": ndofs, "layouts": layouts, "schedules": scheds,
             "sequential_fp64_ms_per_attempt_by_N": {N: 1e3 * seq[N] for N in Ns},
             "sequential_fp64_run_attempts_per_s": n_runs / t_seq,
             "speedup_vs_sequential_fp64": (n_runs * steps / t) / (n_runs / t_seq),
@@ -407,7 +409,7 @@ def batched_measure(n_runs, steps, warmup, mixed, layout_name="auto"):
 
 
 def batched(args):
-    d = batched_measure(args.batch, args.steps, args.warmup, args.mixed, args.layout)
+    d = batched_measure(args.batch, args.steps, args.warmup, args.mixed, args.layout, not args.no_tune)
     print(json.dumps(dict({"batched": True}, **d)), flush=True)
 
 
@@ -417,7 +419,7 @@ def mixed_measure(eng64, mat, f0, steps, warmup, dev):
     (both integrated to t = 0.2 with dense step 0.05)."""
     import torch
     from tortoise_b200 import engine as E
-    eng = E.Engine(mat, layout=E.LAYOUT_AUTO, allow_fp32=2)
+    eng = E.Engine(mat, layout=E.LAYOUT_AUTO, allow_fp32=2, autotune=True)
     infos = [eng.channel_info(c) for c in range(len(mat.channels))]
     stream = torch.cuda.ExternalStream(eng.stream_ptr(), device=dev)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -540,6 +542,7 @@ def main():
                     help="reduced-precision moment storage: t40 (upper 40 bits of FP64, default) or t32 (FP32)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and batched measurements")
+    ap.add_argument("--no-tune", action="store_true", help="fixed contraction schedule (no autotuner)")
     ap.add_argument("--rhs-only", type=int, default=0, help="profiling driver: K RHS evaluations only")
     ap.add_argument("--mesh", type=int, default=N_MESH, help="sections per side (profiling driver only)")
     ap.add_argument("--batch", type=int, default=0, help="batched ensemble of this many runs (per-run N, kT, couplings)")

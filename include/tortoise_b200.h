@@ -146,6 +146,7 @@ typedef struct tb_options {
     int32_t allow_fp32;           /* AUTO for 2- and 3-leg channels: 0 -> T64, 1 -> T32, 2 -> T40 */
     int64_t tensor_budget_bytes;  /* cap on precomputed-tensor memory (0: 60% free) */
     int32_t verbose;
+    int32_t autotune;             /* 1: time the contraction schedules at creation, keep the fastest */
 } tb_options;
 
 /* Pointer flags */
@@ -256,6 +257,13 @@ void* tb_get_stream(tb_handle* h);
  * all channels with ch = -1.  The bare collision kernels, for timing and for
  * callers that compose their own right-hand side. */
 int tb_collision_accumulate(tb_handle* h, int ch, const double* f, double* acc);
+
+/* Contraction schedule of a channel's moment-tensor group: bulk-copy
+ * pipeline stages (1 or 2), whether two instances share each moment read (1)
+ * and, after tb_options.autotune, the fastest measured launch time in seconds
+ * (0 when not tuned).  Monte-Carlo channels report 0, 0, 0.  No counterpart
+ * in the reference. */
+int tb_channel_schedule(const tb_handle* h, int ch, int32_t* stages, int32_t* pair, double* seconds);
 
 /* Out-scattering rates, state-shaped, M^-1 applied (replaces
  * ScatteringChannel::scatteringRates(status, which), src/Physics/Scattering/

@@ -96,3 +96,20 @@ def test_mixed_precision_trajectory_within_1e8(gpu_lib):
         got = res["runs"][r]
         assert got["status"] == 0
         assert max(rel_l2(a, b) for a, b in zip(got["dense"], ref["dense"])) < 5e-9
+
+
+def test_autotuned_schedule_gives_the_same_operator(gpu_lib):
+    """tb_options.autotune times the contraction schedules (bulk-copy stages
+    1 / 2, instance pairs off / on) and keeps the fastest; the operator must
+    not change (1e-12), and the chosen schedule is reported."""
+    mats, states = _runs()
+    f = np.concatenate(states)
+    for layout in (E.LAYOUT_T64, E.LAYOUT_T40):
+        plain = E.BatchEngine(mats, layout=layout)
+        tuned = E.BatchEngine(mats, layout=layout, autotune=True)
+        assert rel_l2(tuned.rhs(f), plain.rhs(f)) < 1e-12
+        s = tuned.schedule(0)
+        assert s["stages"] in (1, 2) and s["pair"] in (0, 1) and s["tuned_seconds"] > 0.0
+        assert plain.schedule(0)["tuned_seconds"] == 0.0
+    mc = E.BatchEngine(mats, layout=E.LAYOUT_MC64, autotune=True)
+    assert mc.schedule(0) == {"stages": 0, "pair": 0, "tuned_seconds": 0.0}

@@ -96,6 +96,7 @@ using namespace tb;
 
 namespace tb {
 int choose_layouts(tb_handle* h);
+int autotune(tb_handle* h);
 }  // namespace tb
 
 namespace tb {
@@ -461,6 +462,7 @@ int build_runs(tb_handle* h, const tb_problem_desc* const* descs, int nruns) {
         if (!I.d_single) { set_error("instance table allocation failed"); return TB_ERR_OOM; }
     }
     TB_TRY(choose_layouts(h));
+    if (h->opts.autotune) TB_TRY(autotune(h));
     TB_CUDA(cudaStreamSynchronize(h->stream));
     return TB_OK;
 }
@@ -495,6 +497,24 @@ int run_rhs_acc(tb_handle* h, const double* d_in, double* d_acc, const DPCtl* ct
         }
     }
     if (!(flags & TB_NO_DRIFT) && only_inst < 0 && h->any_drift) TB_TRY(launch_drift(h->ed, d_in, d_acc, ctl, h->stream));
+    return TB_OK;
+}
+
+// Times every contraction schedule of every moment-tensor group on a
+// representative state (all coefficients 0.25; the cost does not depend on
+// the values) and keeps the fastest (tune_tensor).  The accumulator is
+// cleared afterwards.
+int autotune(tb_handle* h) {
+    const size_t n = size_t(h->ndofs);
+    std::vector<double> probe(n, 0.25);
+    TB_CUDA(cudaMemcpyAsync(h->d_f, probe.data(), sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    for (auto& G : h->groups) {
+        if (G.layout == TB_LAYOUT_MC64 || G.tup.n == 0) continue;
+        TB_TRY(tune_tensor(G.dev, G.d_insts, int(G.insts.size()), G.tensor, G.tup.d, G.tup.cap, G.tup.n, h->d_f,
+                           h->d_acc, h->stream));
+    }
+    TB_CUDA(cudaMemsetAsync(h->d_acc, 0, sizeof(double) * n, h->stream));
+    TB_CUDA(cudaStreamSynchronize(h->stream));
     return TB_OK;
 }
 
@@ -719,6 +739,16 @@ int tb_channel_info(const tb_handle* h, int ch, int64_t* n_tuples, int64_t* n_pr
     if (n_prefilter) *n_prefilter = G.diag[0];
     if (n_det) *n_det = G.diag[1];
     if (layout) *layout = G.layout;
+    return TB_OK;
+}
+
+int tb_channel_schedule(const tb_handle* h, int ch, int32_t* stages, int32_t* pair, double* seconds) {
+    if (!h || ch < 0 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
+    const GroupChan& G = h->groups[h->insts[ch].group];
+    const bool tensor = G.layout != TB_LAYOUT_MC64;
+    if (stages) *stages = tensor ? G.tensor.stages : 0;
+    if (pair) *pair = (tensor && G.L <= 3 && G.insts.size() > 1) ? G.tensor.pair : 0;
+    if (seconds) *seconds = tensor ? G.tensor.tuned_seconds : 0.0;
     return TB_OK;
 }
 

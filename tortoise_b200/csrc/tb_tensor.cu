@@ -32,8 +32,10 @@
 //             << 24) with one byte permute: no conversion instruction.
 // Products and accumulation are FP64 for every kind; the gain-minus-loss
 // vector v = ka + kb is formed in FP64 from f.
-#include <cuda_bf16.h>
-
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <type_traits>
 
 #include "tb_dp45.cuh"
@@ -492,25 +494,16 @@ int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n
 
 static int* g_err_flag = nullptr;
 
-template <int L, int KIND>
-static int launch_t(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T, const int32_t* tup,
-                    int64_t stride, int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s,
-                    int rate_leg) {
-
+template <int L, int KIND, int STAGES, bool PAIR>
+static int launch_variant(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T,
+                          const int32_t* tup, int64_t stride, int64_t n, const double* f, double* acc,
+                          const DPCtl* ctl, cudaStream_t s, int rate_leg) {
     constexpr int TT = TTile<L, KIND>::TT;
-    constexpr int STAGES = 2;
-    // the instance-pair path (one moment read for two runs) only where a
-    // group has several instances; it needs more registers, and four-leg
-    // pairs would spill
-    auto kern = (L <= 3 && n_insts > 1) ? k_collision_tensor<L, KIND, TT, STAGES, (L <= 3)>
-                                        : k_collision_tensor<L, KIND, TT, STAGES, false>;
+    auto kern = k_collision_tensor<L, KIND, TT, STAGES, PAIR>;
     const size_t smem = size_t(STAGES) * TT * tuple_bytes(L, KIND);
     static bool attr = false;
     if (!attr) {
-        TB_CUDA(cudaFuncSetAttribute(k_collision_tensor<L, KIND, TT, STAGES, (L <= 3)>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-        TB_CUDA(cudaFuncSetAttribute(k_collision_tensor<L, KIND, TT, STAGES, false>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
         attr = true;
     }
     if (!g_err_flag) {
@@ -526,10 +519,26 @@ static int launch_t(const ChanDev& c, const InstDev* insts, int n_insts, const M
     int64_t grid = int64_t(nsm) * per_sm;
     if (grid > T.ntiles) grid = T.ntiles;
     if (grid < 1) return TB_OK;
-    kern<<<unsigned(grid), TT, smem, s>>>(c, insts, n_insts, static_cast<const unsigned char*>(T.d), T.ntiles, tup, stride, n,
-                                          f, acc, ctl, g_err_flag, rate_leg);
+    kern<<<unsigned(grid), TT, smem, s>>>(c, insts, n_insts, static_cast<const unsigned char*>(T.d), T.ntiles, tup,
+                                          stride, n, f, acc, ctl, g_err_flag, rate_leg);
     TB_CUDA(cudaGetLastError());
     return TB_OK;
+}
+
+// The instance-pair path (one moment read for two runs) exists for L <= 3
+// only (four-leg pairs would spill registers) and only matters where a group
+// has several instances; it needs more registers than the single path.
+template <int L, int KIND>
+static int launch_t(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T, const int32_t* tup,
+                    int64_t stride, int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s,
+                    int rate_leg) {
+    const bool pair = (L <= 3) && n_insts > 1 && T.pair;
+    if (T.stages == 1) {
+        return pair ? launch_variant<L, KIND, 1, (L <= 3)>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg)
+                    : launch_variant<L, KIND, 1, false>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+    }
+    return pair ? launch_variant<L, KIND, 2, (L <= 3)>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg)
+                : launch_variant<L, KIND, 2, false>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
 }
 
 int launch_collision_tensor(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T,
@@ -549,6 +558,59 @@ int launch_collision_tensor(const ChanDev& c, const InstDev* insts, int n_insts,
     }
     set_error("nlegs must be 2..4");
     return TB_ERR_ARG;
+}
+
+int tune_tensor(const ChanDev& c, const InstDev* insts, int n_insts, MomentTensor& T, const int32_t* tup,
+                int64_t stride, int64_t n, const double* f, double* acc, cudaStream_t s) {
+    if (n <= 0 || n_insts <= 0 || !T.d) return TB_OK;
+    // tuple counts within a factor 2^(1/8) share a cache entry
+    const int64_t bucket = int64_t(std::llround(std::log2(double(n)) * 8.0));
+    const std::tuple<int, int, int64_t, int> key(c.L, T.kind, bucket, n_insts);
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int64_t, int>, std::tuple<int, int, double>> cache;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) {
+            T.stages = std::get<0>(it->second);
+            T.pair = std::get<1>(it->second);
+            T.tuned_seconds = std::get<2>(it->second);
+            return TB_OK;
+        }
+    }
+    cudaEvent_t e0, e1;
+    TB_CUDA(cudaEventCreate(&e0));
+    TB_CUDA(cudaEventCreate(&e1));
+    double best = 1e300;
+    int bs = T.stages, bp = T.pair;
+    const int pairs_max = (c.L <= 3 && n_insts > 1) ? 1 : 0;
+    int rc = TB_OK;
+    for (int st = 1; st <= 2 && rc == TB_OK; ++st)
+        for (int pr = 0; pr <= pairs_max && rc == TB_OK; ++pr) {
+            T.stages = st;
+            T.pair = pr;
+            rc = launch_collision_tensor(c, insts, n_insts, T, tup, stride, n, f, acc, nullptr, s);   // warm-up
+            if (rc != TB_OK) break;
+            constexpr int REPS = 3;
+            cudaEventRecord(e0, s);
+            for (int r = 0; r < REPS && rc == TB_OK; ++r)
+                rc = launch_collision_tensor(c, insts, n_insts, T, tup, stride, n, f, acc, nullptr, s);
+            cudaEventRecord(e1, s);
+            if (cudaEventSynchronize(e1) != cudaSuccess) { rc = TB_ERR_CUDA; break; }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            const double sec = 1e-3 * double(ms) / REPS;
+            if (sec < best) { best = sec; bs = st; bp = pr; }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    T.stages = bs;
+    T.pair = bp;
+    if (rc != TB_OK) return rc;
+    T.tuned_seconds = best;
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = std::make_tuple(bs, bp, best);
+    return TB_OK;
 }
 
 int tensor_error_flag(int* value) {

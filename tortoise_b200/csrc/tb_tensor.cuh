@@ -14,6 +14,11 @@ struct MomentTensor {
     int64_t ntiles = 0;
     int nmom = 0;             // moments per tuple
     int kind = TK_F64;
+    // contraction schedule (set by tune_tensor): bulk-copy pipeline stages,
+    // and whether groups with several instances contract two per moment read
+    int stages = 2;
+    int pair = 1;
+    double tuned_seconds = 0.0;   // best measured launch time (0: not tuned)
     void release();
 };
 
@@ -26,6 +31,14 @@ int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n
 int launch_collision_tensor(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T,
                             const int32_t* tup, int64_t stride, int64_t n, const double* f, double* acc,
                             const DPCtl* ctl, cudaStream_t s, int rate_leg = -1);
+
+// Autotuner: times the contraction of one group for every schedule
+// (stages 1 / 2, instance pairs off / on where several instances exist) on
+// the device data and keeps the fastest in T.  f is any state of the handle's
+// size; acc is scratch (left dirty).  A process-wide cache keyed by
+// (legs, storage kind, tuple count, instance count) skips repeated timing.
+int tune_tensor(const ChanDev& c, const InstDev* insts, int n_insts, MomentTensor& T, const int32_t* tup,
+                int64_t stride, int64_t n, const double* f, double* acc, cudaStream_t s);
 
 // 1 once a bulk-copy wait of the contraction kernel ran out (then TB_ERR_TIMEOUT)
 int tensor_error_flag(int* value);

@@ -29,7 +29,7 @@ class TortoiseError(RuntimeError):
 
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("layout", C.c_int32), ("allow_fp32", C.c_int32),
-                ("tensor_budget_bytes", C.c_int64), ("verbose", C.c_int32)]
+                ("tensor_budget_bytes", C.c_int64), ("verbose", C.c_int32), ("autotune", C.c_int32)]
 
 
 class DP45Stats(C.Structure):
@@ -85,6 +85,8 @@ def lib():
         L.tb_get_stream.argtypes = [vp]
         L.tb_collision_accumulate.argtypes = [vp, C.c_int, vp, vp]
         L.tb_scattering_rates.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_int]
+        L.tb_channel_schedule.argtypes = [vp, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                          C.POINTER(C.c_double)]
         L.tb_create_batch.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int, C.POINTER(Options)]
         L.tb_num_runs.argtypes = [vp]
         L.tb_run_info.argtypes = [vp, C.c_int, C.POINTER(i64), C.POINTER(i64), C.POINTER(C.c_int32),
@@ -115,10 +117,11 @@ def _hp(a):
 class Engine:
     """One device handle for a Material (tb_create ... tb_destroy)."""
 
-    def __init__(self, material, layout=LAYOUT_AUTO, allow_fp32=False, device=0, tensor_budget_bytes=0):
+    def __init__(self, material, layout=LAYOUT_AUTO, allow_fp32=False, device=0, tensor_budget_bytes=0,
+                 autotune=False):
         self.material = material
         self.packed = material.pack()
-        opts = Options(device, layout, int(allow_fp32), tensor_budget_bytes, 0)
+        opts = Options(device, layout, int(allow_fp32), tensor_budget_bytes, 0, int(autotune))
         h = C.c_void_p()
         _check(lib().tb_create(C.byref(h), C.addressof(self.packed.desc), C.byref(opts)), "tb_create")
         self.h = h
@@ -141,6 +144,11 @@ class Engine:
         lay = C.c_int32()
         _check(lib().tb_channel_info(self.h, ch, C.byref(n), C.byref(p), C.byref(d), C.byref(lay)), "tb_channel_info")
         return {"n_tuples": n.value, "n_prefilter": p.value, "n_det": d.value, "layout": LAYOUT_NAMES.get(lay.value)}
+
+    def schedule(self, ch):
+        st, pr, sec = C.c_int32(), C.c_int32(), C.c_double()
+        _check(lib().tb_channel_schedule(self.h, ch, C.byref(st), C.byref(pr), C.byref(sec)), "tb_channel_schedule")
+        return {"stages": st.value, "pair": pr.value, "tuned_seconds": sec.value}
 
     def tuples(self, ch):
         info = self.channel_info(ch)
@@ -289,12 +297,13 @@ class BatchEngine(Engine):
     moment tensors; each keeps its own amplitudes, tolerances, state and step
     size.  Channels and bands are numbered globally in run order."""
 
-    def __init__(self, materials, layout=LAYOUT_AUTO, allow_fp32=False, device=0, tensor_budget_bytes=0):
+    def __init__(self, materials, layout=LAYOUT_AUTO, allow_fp32=False, device=0, tensor_budget_bytes=0,
+                 autotune=False):
         self.materials = list(materials)
         self.material = self.materials[0]
         self.packs = [m.pack() for m in self.materials]
         arr = (C.c_void_p * len(self.packs))(*[C.addressof(p.desc) for p in self.packs])
-        opts = Options(device, layout, int(allow_fp32), tensor_budget_bytes, 0)
+        opts = Options(device, layout, int(allow_fp32), tensor_budget_bytes, 0, int(autotune))
         h = C.c_void_p()
         _check(lib().tb_create_batch(C.byref(h), arr, len(self.packs), C.byref(opts)), "tb_create_batch")
         self.h = h
