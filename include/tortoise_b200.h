@@ -258,6 +258,20 @@ void* tb_get_stream(tb_handle* h);
  * callers that compose their own right-hand side. */
 int tb_collision_accumulate(tb_handle* h, int ch, const double* f, double* acc);
 
+/* The tuple cache of the reference, byte for byte: what
+ * ScatteringChannel::precalculateIndices writes to and reads from
+ * "<scatteringName>.scattIndices" (src/Physics/Scattering/
+ * ScatteringChannel.cpp:421-458, 516-534): int32 nSecSplits of every leg's
+ * mesh (x, y), uint64 tuple count, then per tuple the legs' element ids and
+ * the umklapp column as int32.  tb_write_scatt_indices saves a channel's
+ * tuple list (enumerated on the device or supplied); tb_read_scatt_indices
+ * reads one for tb_channel_desc.tuples: nsplit (2 * nlegs values, or NULL
+ * to skip the check) must match the header as in the reference; with ids ==
+ * umk == NULL it only returns the count. */
+int tb_write_scatt_indices(const tb_handle* h, int ch, const char* path);
+int tb_read_scatt_indices(const char* path, int nlegs, const int32_t* nsplit, int64_t* n_tuples, int32_t* ids,
+                          int32_t* umk, int64_t capacity);
+
 /* Contraction schedule of a channel's moment-tensor group: bulk-copy
  * pipeline stages (1 or 2), whether two instances share each moment read (1)
  * and, after tb_options.autotune, the fastest measured launch time in seconds

@@ -233,3 +233,32 @@ def test_scattering_rates_per_leg_and_errors(gpu_lib):
         eng.scattering_rates(f0, len(mat.channels), -1)
     with pytest.raises(E.TortoiseError):
         eng.scattering_rates(f0, 0, 3)
+
+
+def test_tuple_cache_round_trip(gpu_lib, tmp_path):
+    """Tuple lists enumerated on the device, written in the reference's
+    .scattIndices format, read back into a fresh material: the second handle
+    skips enumeration and gives the same operator; a channel whose inputs
+    changed (other survival points) is not taken from the cache."""
+    from tortoise_b200.model import read_scatt_indices
+    mat, f0 = _setup("eph_n4")
+    eng = E.Engine(mat, layout=E.LAYOUT_T64)
+    ref = eng.rhs(f0)
+    mat.save_tuple_cache(str(tmp_path), eng)
+    for ch, c in enumerate(mat.channels):
+        path = mat.cache_path(str(tmp_path), ch)
+        ids, umk = eng.tuples(ch)
+        n = ids.shape[0]
+        assert (tmp_path / path.split("/")[-1]).stat().st_size == 8 * c.nlegs + 8 + 4 * n * (c.nlegs + 1)
+        rid, rumk = read_scatt_indices(path, c.nlegs)
+        assert np.array_equal(rid, ids) and np.array_equal(rumk, umk)
+    mat2, _ = _setup("eph_n4")
+    mat2.channels[2].constructMCPoints(seed=999)      # its cached list is stale now
+    loaded = mat2.load_tuple_cache(str(tmp_path))
+    assert loaded == [0, 1, 3]
+    mat2.channels[2].constructMCPoints(seed=mat.channels[2].mc_seed)
+    eng2 = E.Engine(mat2, layout=E.LAYOUT_T64)
+    for ch in (0, 1, 3):
+        assert eng2.channel_info(ch)["n_prefilter"] == -1          # supplied, not enumerated
+    assert eng2.channel_info(2)["n_prefilter"] > 0
+    assert rel_l2(eng2.rhs(f0), ref) < 1e-13

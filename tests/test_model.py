@@ -1,5 +1,6 @@
 """Host-side model: wildcard matching, channel deduplication, mesh geometry."""
 import numpy as np
+import pytest
 
 from tortoise_b200 import IN, OUT, workloads as W
 from tortoise_b200.model import Mesh, Region, match_string, random_points_reference
@@ -78,3 +79,68 @@ def test_current_weights_of_a_linear_dispersion():
     jx = A.observable_weights(mat, 0, "current", 0) @ f
     jy = A.observable_weights(mat, 0, "current", 1) @ f
     assert abs(jx - 0.7 * 4.0) < 1e-12 and abs(jy + 0.2 * 4.0) < 1e-12
+
+
+def test_scatt_indices_reader_follows_the_reference_layout(tmp_path):
+    """A file laid out as ScatteringChannel::precalculateIndices writes it
+    (int32 mesh splits per leg, uint64 count, int32 ids + umklapp per tuple)
+    is read back by the Python reader and by the C ABI (no device needed);
+    other mesh splits are refused, as the reference refuses them."""
+    import ctypes as C
+    import struct
+    from tortoise_b200 import engine
+    from tortoise_b200.model import read_scatt_indices
+    ids = np.array([[1, 2, 3], [4, 5, 6], [7, 8, 9], [10, 11, 12]], dtype=np.int32)
+    umk = np.array([0, 3, 1, 2], dtype=np.int32)
+    path = tmp_path / "[(el:P)(pn:0)]-[(el:P)].scattIndices"
+    with open(path, "wb") as fh:
+        fh.write(struct.pack("<6i", 4, 4, 4, 4, 4, 4))
+        fh.write(struct.pack("<Q", 4))
+        for r, u in zip(ids, umk):
+            fh.write(struct.pack("<4i", *r, u))
+    got_ids, got_umk = read_scatt_indices(str(path), 3, [4] * 6)
+    assert np.array_equal(got_ids, ids) and np.array_equal(got_umk, umk)
+    assert read_scatt_indices(str(path), 3, [8] * 6) == (None, None)
+    L = engine.lib()
+    n = C.c_int64()
+    ns = (C.c_int32 * 6)(*([4] * 6))
+    assert L.tb_read_scatt_indices(str(path).encode(), 3, ns, C.byref(n), None, None, 0) == 0 and n.value == 4
+    cids, cumk = np.zeros(12, dtype=np.int32), np.zeros(4, dtype=np.int32)
+    ip = C.POINTER(C.c_int32)
+    assert L.tb_read_scatt_indices(str(path).encode(), 3, ns, C.byref(n), cids.ctypes.data_as(ip),
+                                   cumk.ctypes.data_as(ip), 4) == 0
+    assert np.array_equal(cids.reshape(4, 3), ids) and np.array_equal(cumk, umk)
+    bad = (C.c_int32 * 6)(*([8] * 6))
+    assert L.tb_read_scatt_indices(str(path).encode(), 3, bad, C.byref(n), None, None, 0) == 1   # TB_ERR_BAD_DESC
+    assert L.tb_read_scatt_indices(str(path).encode(), 3, ns, C.byref(n), cids.ctypes.data_as(ip),
+                                   cumk.ctypes.data_as(ip), 2) == 9                              # TB_ERR_CAPACITY
+
+
+def test_tuple_cache_content_hash():
+    """Equal inputs give equal digests; a changed survival table, threshold or
+    dispersion changes the channel's digest."""
+    a = W.build_material(4, ("P", "D"), (0.2,), ee=False, eph=True)
+    b = W.build_material(4, ("P", "D"), (0.2,), ee=False, eph=True)
+    assert [c.content_hash() for c in a.channels] == [c.content_hash() for c in b.channels]
+    h0 = b.channels[0].content_hash()
+    b.channels[0].constructMCPoints(seed=12345)
+    assert b.channels[0].content_hash() != h0
+    c = W.build_material(4, ("P", "D"), (0.2,), ee=False, eph=True)
+    c.channels[1].scattElemeThreshold *= 2
+    assert c.channels[1].content_hash() != a.channels[1].content_hash()
+    d = W.build_material(4, ("P", "H"), (0.2,), ee=False, eph=True)
+    assert d.channels[3].content_hash() != a.channels[3].content_hash()
+
+
+def test_material_status_save_load(tmp_path):
+    """MaterialStatus::save / load (declared in the reference, defined here):
+    round trip bit-exact; a status of another material is refused."""
+    from tortoise_b200.model import MaterialStatus
+    mat = W.build_material(4, ("P", "D"), (0.2,), ee=False, eph=True)
+    st = W.initial_status(mat, kT=0.1, seed=3)
+    st.save(str(tmp_path / "s.bin"))
+    back = MaterialStatus(mat).load(str(tmp_path / "s.bin"))
+    assert np.array_equal(back.vec, st.vec)
+    other = W.build_material(3, ("P", "D"), (0.2,), ee=False, eph=True)
+    with pytest.raises(ValueError):
+        MaterialStatus(other).load(str(tmp_path / "s.bin"))

@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -768,6 +769,77 @@ int tb_get_tuples(const tb_handle* h, int ch, int32_t* ids, int32_t* umk) {
         if (umk) umk[i] = soa[size_t(G.L) * n + i];
     }
     return TB_OK;
+}
+
+// The reference's tuple cache (ScatteringChannel::precalculateIndices,
+// ScatteringChannel.cpp:421-458 reading, 516-534 writing), native byte order:
+//   int32 nSecSplits[L][2]  (each leg's mesh, x then y)
+//   uint64 number of tuples
+//   per tuple: int32 element id of every leg, int32 umklapp column
+int tb_write_scatt_indices(const tb_handle* h, int ch, const char* path) {
+    if (!h || !path || ch < 0 || ch >= int(h->insts.size())) { set_error("bad argument"); return TB_ERR_ARG; }
+    const ChanInst& I = h->insts[ch];
+    const GroupChan& G = h->groups[I.group];
+    const int L = G.L;
+    const int64_t n = G.tup.n;
+    std::vector<int32_t> ids(size_t(std::max<int64_t>(n, 1)) * L), umk(size_t(std::max<int64_t>(n, 1)));
+    TB_TRY(tb_get_tuples(h, ch, ids.data(), umk.data()));
+    FILE* fp = std::fopen(path, "wb");
+    if (!fp) { set_error(std::string("cannot open ") + path); return TB_ERR_ARG; }
+    bool ok = true;
+    for (int l = 0; l < L; ++l) {
+        const HostMesh& m = h->meshes[h->bands[I.band[l]].mesh];
+        const int32_t ns[2] = {m.nx, m.ny};
+        ok = ok && std::fwrite(ns, sizeof(int32_t), 2, fp) == 2;
+    }
+    const uint64_t total = uint64_t(n);
+    ok = ok && std::fwrite(&total, sizeof(uint64_t), 1, fp) == 1;
+    std::vector<int32_t> rec(size_t(L + 1));
+    for (int64_t i = 0; i < n && ok; ++i) {
+        for (int l = 0; l < L; ++l) rec[size_t(l)] = ids[size_t(i) * L + l];
+        rec[size_t(L)] = umk[size_t(i)];
+        ok = std::fwrite(rec.data(), sizeof(int32_t), size_t(L + 1), fp) == size_t(L + 1);
+    }
+    ok = (std::fclose(fp) == 0) && ok;
+    if (!ok) { set_error(std::string("write failed: ") + path); return TB_ERR_ARG; }
+    return TB_OK;
+}
+
+int tb_read_scatt_indices(const char* path, int nlegs, const int32_t* nsplit, int64_t* n_tuples, int32_t* ids,
+                          int32_t* umk, int64_t capacity) {
+    if (!path || !n_tuples || nlegs < 2 || nlegs > TB_MAX_LEGS) { set_error("bad argument"); return TB_ERR_ARG; }
+    FILE* fp = std::fopen(path, "rb");
+    if (!fp) { set_error(std::string("cannot open ") + path); return TB_ERR_ARG; }
+    int rc = TB_OK;
+    int32_t ns[2 * TB_MAX_LEGS];
+    uint64_t total = 0;
+    if (std::fread(ns, sizeof(int32_t), size_t(2 * nlegs), fp) != size_t(2 * nlegs) ||
+        std::fread(&total, sizeof(uint64_t), 1, fp) != 1) {
+        set_error("truncated tuple cache header");
+        rc = TB_ERR_BAD_DESC;
+    }
+    if (rc == TB_OK && nsplit)
+        for (int k = 0; k < 2 * nlegs; ++k)
+            if (ns[k] != nsplit[k]) { set_error("tuple cache was written for other meshes"); rc = TB_ERR_BAD_DESC; }
+    if (rc == TB_OK) {
+        *n_tuples = int64_t(total);
+        if (ids || umk) {
+            if (int64_t(total) > capacity) { set_error("tuple cache larger than the buffers"); rc = TB_ERR_CAPACITY; }
+            std::vector<int32_t> rec(size_t(nlegs + 1));
+            for (uint64_t i = 0; i < total && rc == TB_OK; ++i) {
+                if (std::fread(rec.data(), sizeof(int32_t), size_t(nlegs + 1), fp) != size_t(nlegs + 1)) {
+                    set_error("truncated tuple cache");
+                    rc = TB_ERR_BAD_DESC;
+                    break;
+                }
+                if (ids)
+                    for (int l = 0; l < nlegs; ++l) ids[i * nlegs + l] = rec[size_t(l)];
+                if (umk) umk[i] = rec[size_t(nlegs)];
+            }
+        }
+    }
+    std::fclose(fp);
+    return rc;
 }
 
 int tb_set_amplitude(tb_handle* h, int ch, double amplitude) {

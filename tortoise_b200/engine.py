@@ -85,6 +85,9 @@ def lib():
         L.tb_get_stream.argtypes = [vp]
         L.tb_collision_accumulate.argtypes = [vp, C.c_int, vp, vp]
         L.tb_scattering_rates.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_int]
+        L.tb_write_scatt_indices.argtypes = [vp, C.c_int, C.c_char_p]
+        L.tb_read_scatt_indices.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                                            C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int64]
         L.tb_channel_schedule.argtypes = [vp, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                           C.POINTER(C.c_double)]
         L.tb_create_batch.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int, C.POINTER(Options)]
@@ -144,6 +147,10 @@ class Engine:
         lay = C.c_int32()
         _check(lib().tb_channel_info(self.h, ch, C.byref(n), C.byref(p), C.byref(d), C.byref(lay)), "tb_channel_info")
         return {"n_tuples": n.value, "n_prefilter": p.value, "n_det": d.value, "layout": LAYOUT_NAMES.get(lay.value)}
+
+    def write_scatt_indices(self, ch, path):
+        """The channel's tuple list in the reference's .scattIndices format."""
+        _check(lib().tb_write_scatt_indices(self.h, ch, os.fsencode(path)), "tb_write_scatt_indices")
 
     def schedule(self, ch):
         st, pr, sec = C.c_int32(), C.c_int32(), C.c_double()

@@ -9,6 +9,10 @@ include/Physics/Status/MaterialStatus.hpp, MaterialTimeStatus.hpp).  They
 hold geometry and parameters only; every propagation goes through the CUDA
 library bound in ``tortoise_b200.engine``.
 """
+import hashlib
+import os
+import struct
+
 import numpy as np
 
 from .abi import BOSON, FERMION, IN, OUT, PackedProblem
@@ -103,6 +107,20 @@ class Mesh:
         return nodal_to_linform(nodal)
 
 
+def read_scatt_indices(path, nlegs, nsplit=None):
+    """A "<scatteringName>.scattIndices" file (ScatteringChannel.cpp:421-458):
+    int32 mesh splits of every leg, uint64 count, then per tuple nlegs int32
+    element ids and an int32 umklapp column.  Returns (ids[n, nlegs],
+    umklapp[n]) or (None, None) when the splits differ from nsplit."""
+    raw = open(path, "rb").read()
+    head = np.frombuffer(raw, dtype="<i4", count=2 * nlegs)
+    if nsplit is not None and list(head) != [int(x) for x in nsplit]:
+        return None, None
+    (n,) = struct.unpack_from("<Q", raw, 8 * nlegs)
+    rec = np.frombuffer(raw, dtype="<i4", count=n * (nlegs + 1), offset=8 * nlegs + 8).reshape(n, nlegs + 1)
+    return np.ascontiguousarray(rec[:, :nlegs]), np.ascontiguousarray(rec[:, nlegs])
+
+
 def nodal_to_linform(nodal):
     nodal = np.asarray(nodal, dtype=np.float64).reshape(-1, 3)
     out = nodal.copy()
@@ -166,6 +184,30 @@ class ScatteringChannel:
         ins = "".join("(" + m.band_names[b] + ")" for b, d in zip(self.legBandNumber, self.legDirection) if d > 0)
         outs = "".join("(" + m.band_names[b] + ")" for b, d in zip(self.legBandNumber, self.legDirection) if d < 0)
         return "[" + ins + "]-[" + outs + "]"
+
+    def content_hash(self):
+        """SHA-256 of every input the tuple list depends on: region, the legs'
+        meshes, dispersions and directions, the umklapp table, the survival
+        points, minimum determinant, threshold and amplitude.  The
+        reference's cache only checks the mesh splits; this digest, kept in
+        a side file, also catches a changed dispersion, table or threshold."""
+        m = self.material
+        h = hashlib.sha256()
+        h.update(np.asarray(m.region.origin, dtype=np.float64).tobytes())
+        h.update(np.asarray(m.region.gvec, dtype=np.float64).tobytes())
+        for b, d in zip(self.legBandNumber, self.legDirection):
+            band = m.bands[b]
+            mesh = band.mesh
+            h.update(struct.pack("<ii", int(mesh.nsplit[0]), int(mesh.nsplit[1])))
+            h.update(np.asarray(mesh.rel_origin, dtype=np.float64).tobytes())
+            h.update(np.asarray(mesh.rel_size, dtype=np.float64).tobytes())
+            h.update(np.ascontiguousarray(band.dispersion_coeffs, dtype=np.float64).tobytes())
+            h.update(struct.pack("<id", int(d), float(band.statistics)))
+        h.update(np.ascontiguousarray(self.umklappUnitVectors, dtype=np.float64).tobytes())
+        h.update(np.ascontiguousarray(self.mc_points_precalc, dtype=np.float64).tobytes())
+        h.update(struct.pack("<ddd", float(self.minimumDeterminant), float(self.scattElemeThreshold),
+                             float(self.amplitude)))
+        return h.hexdigest()
 
     def findUmklappVectors(self, n):
         """All (2n+1)^2 test vectors are kept (ScatteringChannel.cpp:194-215)."""
@@ -324,6 +366,44 @@ class Material:
             off += b.mesh.ne * 3
         return out, off
 
+    # -- tuple cache (ScatteringChannel.cpp:421-458, 516-534) ----------------
+    def cache_path(self, directory, ch):
+        return os.path.join(directory, self.channels[ch].scatteringName() + ".scattIndices")
+
+    def load_tuple_cache(self, directory):
+        """Reads "<scatteringName>.scattIndices" of every channel whose file
+        exists, whose header matches its legs' mesh splits (the reference's
+        test) and whose side file "<...>.sha256" matches content_hash() (a
+        file without a side file, e.g. one the reference wrote, is trusted as
+        the reference trusts it).  Returns the channels loaded."""
+        loaded = []
+        for ch, c in enumerate(self.channels):
+            path = self.cache_path(directory, ch)
+            if not os.path.exists(path):
+                continue
+            side = path + ".sha256"
+            if os.path.exists(side) and open(side).read().strip() != c.content_hash():
+                continue
+            ns = [self.bands[b].mesh.nsplit[k] for b in c.legBandNumber for k in (0, 1)]
+            ids, umk = read_scatt_indices(path, c.nlegs, ns)
+            if ids is None:
+                continue
+            c.tuples, c.tuple_umklapp = ids, umk
+            loaded.append(ch)
+        self._engine = None
+        return loaded
+
+    def save_tuple_cache(self, directory, engine=None):
+        """Writes every channel's tuple list in the reference's format (with
+        the content digest in a side file)."""
+        eng = engine or self.engine()
+        os.makedirs(directory, exist_ok=True)
+        for ch, c in enumerate(self.channels):
+            path = self.cache_path(directory, ch)
+            eng.write_scatt_indices(ch, path)
+            with open(path + ".sha256", "w") as fh:
+                fh.write(c.content_hash() + "\n")
+
     def engine(self, **opts):
         """The CUDA handle for this material (built on first use)."""
         from .engine import Engine
@@ -370,6 +450,37 @@ class MaterialStatus:
 
     def relativeError(self, population):
         return self.material.engine().relative_error(self.vec, population.vec)
+
+    # -- I/O: MaterialStatus::save / load, declared in the reference
+    # (MaterialStatus.hpp:131-132) but never defined there.  File: magic
+    # "TBMS1", band count, then per band its name, element count and the
+    # 3 x elements linear-form coefficients (little-endian FP64).
+    def save(self, fileName):
+        with open(fileName, "wb") as fh:
+            fh.write(b"TBMS1")
+            fh.write(struct.pack("<i", len(self.material.bands)))
+            for b, band in enumerate(self.material.bands):
+                name = band.name.encode()
+                fh.write(struct.pack("<i", len(name)) + name)
+                fh.write(struct.pack("<q", band.mesh.ne))
+                fh.write(np.ascontiguousarray(self[band.name], dtype="<f8").tobytes())
+
+    def load(self, fileName):
+        with open(fileName, "rb") as fh:
+            if fh.read(5) != b"TBMS1":
+                raise ValueError("%s is not a saved MaterialStatus" % fileName)
+            (nb,) = struct.unpack("<i", fh.read(4))
+            if nb != len(self.material.bands):
+                raise ValueError("saved status has %d bands, the material %d" % (nb, len(self.material.bands)))
+            for band in self.material.bands:
+                (ln,) = struct.unpack("<i", fh.read(4))
+                name = fh.read(ln).decode()
+                (ne,) = struct.unpack("<q", fh.read(8))
+                if name != band.name or ne != band.mesh.ne:
+                    raise ValueError("saved band %s (%d elements) does not match %s (%d)"
+                                     % (name, ne, band.name, band.mesh.ne))
+                self[band.name] = np.frombuffer(fh.read(24 * ne), dtype="<f8")
+        return self
 
     def scatteringRates(self):
         """MaterialStatus::scatteringRates (MaterialStatus.cpp:170-187): the
