@@ -20,7 +20,9 @@
 
 namespace tb {
 
-template <int L>
+// RATE: scattering-rate variant (rate_leg >= 0), a separate instantiation so
+// that the propagate path keeps its register allocation.
+template <int L, bool RATE>
 __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* __restrict__ insts, int n_insts,
                                                       const int32_t* __restrict__ tup, int64_t stride, int64_t n,
                                                       const double* __restrict__ f, double* __restrict__ acc,
@@ -93,7 +95,7 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* 
                     A[l][j] = ka * ((1. - d) * unit + ca * fj);
                     B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
                 }
-                if (l == rate_leg) {
+                if (RATE && l == rate_leg) {
                     // scattering rate of this leg: constant in / out unit forms
                     // (ScatteringChannel.cpp:562-564)
                     A[l][0] = (l == 0 ? -1.0 : 1.0) * ca; A[l][1] = 0.0; A[l][2] = 0.0;
@@ -145,8 +147,8 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* 
             const double scale = valid ? 1.0 / (inv_fact_nmc * fabs(g.det)) : 0.0;
 #pragma unroll
             for (int l = 0; l < L; ++l) {
-                if (rate_leg >= 0 && l != rate_leg) continue;   // uniform: the rate keeps one leg
-                const double d = rate_leg >= 0 ? -c.leg[l].dir : c.leg[l].dir;
+                if (RATE && l != rate_leg) continue;   // uniform: the rate keeps one leg
+                const double d = RATE ? -c.leg[l].dir : c.leg[l].dir;
                 const int64_t key = in.foff[l] + 3 * (int64_t)e[l];
                 if (l < L - 1) {
                     warp_scatter3(valid ? key : -1, acc + key, d * ((scale * s0) * in.amp_full),
@@ -170,12 +172,20 @@ int launch_collision_mc(const ChanDev& c, const InstDev* insts, int n_insts, con
     int64_t blocks = (n + threads - 1) / threads;
     if (grid_hint > 0 && blocks > grid_hint) blocks = grid_hint;
     const size_t smem = sizeof(double) * size_t(c.nmc) * c.R;
+#define TB_MC_LAUNCH(LL)                                                                                           \
+    if (rate_leg >= 0)                                                                                             \
+        k_collision_mc<LL, true><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, acc, \
+                                                                          ctl, rate_leg);                          \
+    else                                                                                                           \
+        k_collision_mc<LL, false><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f,     \
+                                                                           acc, ctl, -1);
     switch (c.L) {
-        case 2: k_collision_mc<2><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, acc, ctl, rate_leg); break;
-        case 3: k_collision_mc<3><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, acc, ctl, rate_leg); break;
-        case 4: k_collision_mc<4><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, acc, ctl, rate_leg); break;
+        case 2: TB_MC_LAUNCH(2) break;
+        case 3: TB_MC_LAUNCH(3) break;
+        case 4: TB_MC_LAUNCH(4) break;
         default: set_error("nlegs must be 2..4"); return TB_ERR_ARG;
     }
+#undef TB_MC_LAUNCH
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }

@@ -254,7 +254,7 @@ __device__ __forceinline__ double tile_moment(const unsigned char* __restrict__ 
 // the channel; every moment is read from shared memory once and used by all
 // NI instances.  Results are scattered into acc (legs 0 .. L-2 through the
 // warp-segmented reduction, so all 32 lanes must call this together).
-template <int L, int KIND, int TT, int NI>
+template <int L, int KIND, int TT, int NI, bool RATE>
 __device__ __forceinline__ void contract_tuple(const ChanDev& c, const InstDev (&in)[NI], const int (&e)[L], bool valid,
                                                const unsigned char* __restrict__ tile, int tid,
                                                const double* __restrict__ f, double* __restrict__ acc, int rate_leg) {
@@ -280,7 +280,7 @@ __device__ __forceinline__ void contract_tuple(const ChanDev& c, const InstDev (
                 A[l][j] = ka * ((1. - d) * unit + ca * fj);
                 B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
             }
-            if (l == rate_leg) {
+            if (RATE && l == rate_leg) {
                 // scattering rate of this leg: constant in / out unit forms
                 // (ScatteringChannel.cpp:562-564)
                 A[l][0] = (l == 0 ? -1.0 : 1.0) * ca; A[l][1] = 0.0; A[l][2] = 0.0;
@@ -312,7 +312,7 @@ __device__ __forceinline__ void contract_tuple(const ChanDev& c, const InstDev (
     }
 #pragma unroll
     for (int lam = 0; lam < L; ++lam) {
-        if (rate_leg >= 0 && lam != rate_leg) continue;   // uniform: the rate keeps one leg
+        if (RATE && lam != rate_leg) continue;   // uniform: the rate keeps one leg
         int sstep = 1;
 #pragma unroll
         for (int l = L - 1; l > lam; --l) sstep *= 3;
@@ -338,7 +338,7 @@ __device__ __forceinline__ void contract_tuple(const ChanDev& c, const InstDev (
                 r2[q] = fma(qyy, v[q][j2], r2[q]);
             }
         }
-        const double d = rate_leg >= 0 ? -c.leg[lam].dir : c.leg[lam].dir;
+        const double d = RATE ? -c.leg[lam].dir : c.leg[lam].dir;
 #pragma unroll
         for (int q = 0; q < NI; ++q) {
             const double amp = in[q].amplitude;
@@ -361,7 +361,9 @@ template <int L, int KIND> struct TBytes {
     static constexpr int B = KIND == TK_F64 ? 8 * NM : KIND == TK_F32 ? 4 * NM : 4 * (NM + (NM + 3) / 4);
 };
 
-template <int L, int KIND, int TT, int STAGES, bool PAIR>
+// RATE: scattering-rate variant (rate_leg >= 0), a separate instantiation so
+// that the propagate path keeps all its arrays in registers.
+template <int L, int KIND, int TT, int STAGES, bool PAIR, bool RATE>
 __global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, const InstDev* __restrict__ insts, int n_insts,
                                                          const unsigned char* __restrict__ mom, int64_t ntiles,
                                                          const int32_t* __restrict__ tup, int64_t stride, int64_t n,
@@ -431,11 +433,11 @@ __global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, const InstDe
                 while (k2 < n_insts && !active(insts[k2])) ++k2;
                 if (PAIR && k2 < n_insts) {
                     const InstDev pair[2] = {a, insts[k2]};
-                    contract_tuple<L, KIND, TT, 2>(c, pair, e, valid, sm, tid, f, acc, rate_leg);
+                    contract_tuple<L, KIND, TT, 2, RATE>(c, pair, e, valid, sm, tid, f, acc, rate_leg);
                     k = k2 + 1;
                 } else {
                     const InstDev one[1] = {a};
-                    contract_tuple<L, KIND, TT, 1>(c, one, e, valid, sm, tid, f, acc, rate_leg);
+                    contract_tuple<L, KIND, TT, 1, RATE>(c, one, e, valid, sm, tid, f, acc, rate_leg);
                     k = PAIR ? k2 : k + 1;
                 }
             }
@@ -494,12 +496,12 @@ int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n
 
 static int* g_err_flag = nullptr;
 
-template <int L, int KIND, int STAGES, bool PAIR>
+template <int L, int KIND, int STAGES, bool PAIR, bool RATE = false>
 static int launch_variant(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T,
                           const int32_t* tup, int64_t stride, int64_t n, const double* f, double* acc,
                           const DPCtl* ctl, cudaStream_t s, int rate_leg) {
     constexpr int TT = TTile<L, KIND>::TT;
-    auto kern = k_collision_tensor<L, KIND, TT, STAGES, PAIR>;
+    auto kern = k_collision_tensor<L, KIND, TT, STAGES, PAIR, RATE>;
     const size_t smem = size_t(STAGES) * TT * tuple_bytes(L, KIND);
     static bool attr = false;
     if (!attr) {
@@ -532,6 +534,8 @@ template <int L, int KIND>
 static int launch_t(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T, const int32_t* tup,
                     int64_t stride, int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s,
                     int rate_leg) {
+    if (rate_leg >= 0)   // diagnostic operator: one fixed schedule
+        return launch_variant<L, KIND, 2, false, true>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
     const bool pair = (L <= 3) && n_insts > 1 && T.pair;
     if (T.stages == 1) {
         return pair ? launch_variant<L, KIND, 1, (L <= 3)>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg)
