@@ -12,6 +12,7 @@
 // factors is the sum over legs of (other legs' factors) x (that leg's slope).
 #include "tb_dp45.cuh"
 #include "tb_geom.cuh"
+#include "tb_scatter.cuh"
 #include "tb_tensor.cuh"
 #include "tb_vjp.cuh"
 
@@ -167,6 +168,56 @@ __global__ void __launch_bounds__(128) k_vjp_mc(ChanDev c, const InstDev* __rest
     }
 }
 
+// Gradient of  sum_J w[J] prod_l X[l][J_l]  with respect to every X[m][j]
+// (g[m][j] = sum over J with J_m = j of w[J] prod_{l != m} X[l][J_l]) and the
+// sum itself, by contracting w from the last leg backwards (suffixes S_m over
+// legs 0..m) and multiplying prefixes P_m over legs 0..m-1: 81 FMAs per form
+// for three legs instead of the 324 products of the term-by-term expansion.
+// J is leg-0-most-significant, so the last leg is the fastest digit.
+template <int L>
+__device__ __forceinline__ void leg_grads(const double* __restrict__ w, const double (&X)[L][3], double (&g)[L][3],
+                                          double& total) {
+    constexpr int K = VDim<L>::K;
+    double S[L][K];   // S[m]: 3^(m+1) values (S[L-1] = w)
+    double P[L][K];   // P[m]: 3^m values
+#pragma unroll
+    for (int i = 0; i < K; ++i) S[L - 1][i] = w[i];
+#pragma unroll
+    for (int m = L - 2; m >= 0; --m) {
+        int sz = 3;
+#pragma unroll
+        for (int q = 0; q < m; ++q) sz *= 3;
+#pragma unroll
+        for (int i = 0; i < sz; ++i)
+            S[m][i] = S[m + 1][3 * i] * X[m + 1][0] + S[m + 1][3 * i + 1] * X[m + 1][1] + S[m + 1][3 * i + 2] * X[m + 1][2];
+    }
+    P[0][0] = 1.0;
+#pragma unroll
+    for (int m = 1; m < L; ++m) {
+        int sz = 1;
+#pragma unroll
+        for (int q = 0; q < m - 1; ++q) sz *= 3;
+#pragma unroll
+        for (int i = 0; i < sz; ++i)
+#pragma unroll
+            for (int t = 0; t < 3; ++t) P[m][3 * i + t] = (m == 1) ? X[0][t] : P[m - 1][i] * X[m - 1][t];
+    }
+#pragma unroll
+    for (int m = 0; m < L; ++m) {
+        int sz = 1;
+#pragma unroll
+        for (int q = 0; q < m; ++q) sz *= 3;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double acc = 0.0;
+#pragma unroll
+            for (int i = 0; i < sz; ++i) acc = fma(P[m][i], S[m][3 * i + j], acc);
+            g[m][j] = acc;
+        }
+    }
+    total = X[0][0] * S[0][0] + X[0][1] * S[0][1] + X[0][2] * S[0][2];
+}
+
 // --------------------------------------------- collision VJP, moment tensor
 template <int L, int KIND>
 __global__ void __launch_bounds__(128) k_vjp_tensor(ChanDev c, const InstDev* __restrict__ insts, int n_insts,
@@ -237,37 +288,22 @@ __global__ void __launch_bounds__(128) k_vjp_tensor(ChanDev c, const InstDev* __
                 }
             }
             // d/dA[m][j] of sum_J w[J] prod_l A[l][J_l]; the same for B
-            double gA[L][3], gB[L][3], gamp = 0.0;
+            double gA[L][3], gB[L][3], ta, tb2;
+            leg_grads<L>(w, A, gA, ta);
+            leg_grads<L>(w, B, gB, tb2);
+            const double gamp = ta + tb2;
 #pragma unroll
-            for (int l = 0; l < L; ++l)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) { gA[l][j] = 0.0; gB[l][j] = 0.0; }
-#pragma unroll
-            for (int j = 0; j < K; ++j) {
-                int J[L];
-                int r = j;
-#pragma unroll
-                for (int l = L - 1; l >= 0; --l) { J[l] = r % 3; r /= 3; }
-                double pa = 1.0, pb = 1.0;
-#pragma unroll
-                for (int l = 0; l < L; ++l) { pa *= A[l][J[l]]; pb *= B[l][J[l]]; }
-                gamp += w[j] * (pa + pb);
-#pragma unroll
-                for (int mm = 0; mm < L; ++mm) {
-                    double ra = w[j], rb = w[j];
-#pragma unroll
-                    for (int l = 0; l < L; ++l)
-                        if (l != mm) { ra *= A[l][J[l]]; rb *= B[l][J[l]]; }
-                    gA[mm][J[mm]] += ra;
-                    gB[mm][J[mm]] += rb;
-                }
-            }
-            if (valid) {
-#pragma unroll
-                for (int l = 0; l < L; ++l) {
-                    double* o = grad_f + in.foff[l] + 3 * (int64_t)e[l];
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) atomicAdd(o + j, in.amplitude * (sa[l] * gA[l][j] + sb[l] * gB[l][j]));
+            for (int l = 0; l < L; ++l) {
+                const int64_t key = in.foff[l] + 3 * (int64_t)e[l];
+                const double g0 = in.amplitude * (sa[l] * gA[l][0] + sb[l] * gB[l][0]);
+                const double g1 = in.amplitude * (sa[l] * gA[l][1] + sb[l] * gB[l][1]);
+                const double g2 = in.amplitude * (sa[l] * gA[l][2] + sb[l] * gB[l][2]);
+                if (l < L - 1) {
+                    warp_scatter3(valid ? key : -1, grad_f + (valid ? key : 0), g0, g1, g2);
+                } else if (valid) {
+                    atomicAdd(grad_f + key, g0);
+                    atomicAdd(grad_f + key + 1, g1);
+                    atomicAdd(grad_f + key + 2, g2);
                 }
             }
             block_atomic_sum(valid ? gamp : 0.0, grad_amp + k);
