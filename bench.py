@@ -517,7 +517,7 @@ def rhs_only(args):
     mat, f0 = workload(args.mesh)
     layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32,
               "t40": E.LAYOUT_T40}[args.layout]
-    eng = E.Engine(mat, layout=layout, allow_fp32=mixed_flag(args))
+    eng = E.Engine(mat, layout=layout, allow_fp32=mixed_flag(args), autotune=not args.no_tune)
     f = torch.tensor(f0, device="cuda")
     out = torch.zeros_like(f)
     torch.cuda.synchronize()
@@ -527,7 +527,8 @@ def rhs_only(args):
     eng.synchronize()
     dt = time.perf_counter() - t0
     print(json.dumps({"rhs_only": args.rhs_only, "mesh": args.mesh, "layouts": [eng.channel_info(c)["layout"]
-                      for c in range(len(mat.channels))], "seconds": dt}), flush=True)
+                      for c in range(len(mat.channels))], "schedules": [eng.schedule(c) for c in range(len(mat.channels))],
+                      "seconds": dt}), flush=True)
     eng.close()
 
 
