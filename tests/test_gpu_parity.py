@@ -262,3 +262,35 @@ def test_tuple_cache_round_trip(gpu_lib, tmp_path):
         assert eng2.channel_info(ch)["n_prefilter"] == -1          # supplied, not enumerated
     assert eng2.channel_info(2)["n_prefilter"] > 0
     assert rel_l2(eng2.rhs(f0), ref) < 1e-13
+
+
+@pytest.mark.parametrize("layout,etol", [(E.LAYOUT_MC64, 1e-12), (E.LAYOUT_T64, 1e-12), (E.LAYOUT_T40, 1e-8),
+                                         (E.LAYOUT_T32, 1e-6)])
+@pytest.mark.parametrize("name", CASES)
+def test_device_operator_conserves(gpu_lib, name, layout, etol):
+    """Collision term of the device operator.  Electron number: every channel
+    here pairs each electron in leg with an electron out leg, and the
+    zeroth-moment output of a tuple is one number shared by all its legs, so
+    number is conserved to 1e-12 of the sum of magnitudes for every storage
+    layout.  Energy: the P1 delta makes sum_l dir_l E_l = 0 at every
+    Monte-Carlo point, which the FP64 layouts keep to 1e-12; reduced-precision
+    moments round the moments of that identity one by one, so it holds to
+    their precision (1e-8 for 40-bit, 1e-6 for FP32 storage)."""
+    from tortoise_b200.adjoint import observable_weights
+    mat, f0 = _setup(name)
+    eng = E.Engine(mat, layout=layout)
+    d = eng.rhs(f0, drift=False)
+    tot_n = scale_n = tot_e = scale_e = 0.0
+    for b, band in enumerate(mat.bands):
+        if band.constrained:
+            continue
+        we = observable_weights(mat, b, "energy")
+        tot_e += float(we @ d)
+        scale_e += float(np.abs(we) @ np.abs(d))
+        if band.statistics == -1:
+            wn = observable_weights(mat, b, "density")
+            tot_n += float(wn @ d)
+            scale_n += float(np.abs(wn) @ np.abs(d))
+    assert abs(tot_n) <= 1e-12 * scale_n, (tot_n, scale_n)
+    if not any(b.constrained for b in mat.bands):
+        assert abs(tot_e) <= etol * scale_e, (tot_e, scale_e)
