@@ -147,6 +147,8 @@ typedef struct tb_options {
     int64_t tensor_budget_bytes;  /* cap on precomputed-tensor memory (0: 60% free) */
     int32_t verbose;
     int32_t autotune;             /* 1: time the contraction schedules at creation, keep the fastest */
+    int32_t shard_rank;           /* tuple sharding (tb_shard_connect): this process's part ... */
+    int32_t shard_count;          /* ... of shard_count parts; 0 or 1: no sharding  */
 } tb_options;
 
 /* Pointer flags */
@@ -193,7 +195,8 @@ int64_t tb_num_dofs(const tb_handle* h);
 int64_t tb_band_offset(const tb_handle* h, int band);
 int     tb_num_channels(const tb_handle* h);
 /* tuples kept, tuples passing the element energy window, tuples passing the
- * determinant filter, and the collision layout chosen for the channel. */
+ * determinant filter, and the collision layout chosen for the channel.  On a
+ * sharded handle the tuples kept (and tb_get_tuples) are this handle's part. */
 int tb_channel_info(const tb_handle* h, int ch, int64_t* n_tuples, int64_t* n_prefilter, int64_t* n_det,
                     int32_t* layout);
 /* Copies a channel's tuple list to host memory: ids[n*L] (tuple-major), umk[n]. */
@@ -363,6 +366,49 @@ int tb_dp45_replay(tb_handle* h, const double* f0, const double* dts, int64_t n_
 int tb_band_relative_error_noalloc(const double* err, const double* pop, int64_t n_elements, double elem_volume,
                                    double statistics, double rel_tol, double abs_tol, double penalisation,
                                    double* result, void* stream);
+
+/* ---------------------------------------------- tuple sharding across GPUs
+ * One run split over shard_count processes, one GPU each: the process with
+ * tb_options.shard_rank = r keeps the r-th contiguous part of every channel's
+ * tuple list (tb_shard_range), so every tuple is evaluated by exactly one GPU
+ * -- the work split that the TBB reduce of ScatteringChannel<2,L>::propagate
+ * (src/Physics/Scattering/ScatteringChannel.cpp:651-670) makes across host
+ * threads.  Each process then holds a partial collision accumulator.  Once the
+ * handles are connected (tb_shard_connect), every collision evaluation ends
+ * with one in-place FP64 sum all-reduce (NCCL) of that accumulator, before the
+ * replicated drift term and M^-1: tb_rhs, tb_channel_propagate,
+ * tb_collision_accumulate, tb_scattering_rates, every DP45 stage (inside the
+ * captured attempt graph), the adjoint sweeps (the collision VJP and the
+ * amplitude gradients) and tb_dp45_replay.  The state and the integrator are
+ * replicated: the all-reduced accumulator is the same on every rank, so every
+ * rank takes the same steps.  On a connected handle these calls are
+ * collective: every rank makes the same calls in the same order.  Unconnected,
+ * a sharded handle returns its partial sums (their sum over the ranks is the
+ * full operator).  A sharded handle holds only its part of each tuple list, so
+ * tb_write_scatt_indices refuses it.  NCCL (libnccl.so.2) is loaded on the
+ * first tb_shard_* call that needs it.  No counterpart in the reference (one
+ * process per Material there). */
+#define TB_SHARD_ID_BYTES 128
+
+/* The part [begin, end) of n_tuples tuples that rank `rank` of n_ranks keeps:
+ * contiguous, in list order, boundaries on multiples of 128 tuples (whole
+ * moment-tensor tiles), as even as that allows.  Host arithmetic only. */
+int tb_shard_range(int64_t n_tuples, int rank, int n_ranks, int64_t* begin, int64_t* end);
+
+/* A new communicator id (TB_SHARD_ID_BYTES bytes) into `id`.  One rank makes
+ * it; the caller hands the bytes to the other ranks (a store, a broadcast). */
+int tb_shard_unique_id(void* id);
+
+/* Joins the handle to the communicator `id` as rank shard_rank of
+ * shard_count (the handle's options).  Every rank calls it.  timeout_s bounds
+ * this call and every later wait on the handle's stream: a wait that runs out
+ * aborts the communicator and returns TB_ERR_TIMEOUT, and the handle's
+ * collective calls fail from then on. */
+int tb_shard_connect(tb_handle* h, const void* id, double timeout_s);
+
+/* Channel ch's part on this handle: its first tuple's index in the full list
+ * and the full list's length (begin 0 and the local count when unsharded). */
+int tb_shard_info(const tb_handle* h, int ch, int64_t* begin, int64_t* n_total);
 
 #ifdef __cplusplus
 }

@@ -71,3 +71,23 @@ def test_create_without_device_fails_cleanly():
     with pytest.raises(engine.TortoiseError) as ei:
         engine.Engine(mat)
     assert ei.value.rc == 7
+
+
+def test_shard_ranges_partition_the_tuple_list():
+    """tb_shard_range (host arithmetic): for every rank count the parts are
+    contiguous, cover [0, n), start on 128-tuple boundaries and differ by at
+    most one tile; bad arguments are refused."""
+    from tortoise_b200 import engine as E
+    for n in (0, 5, 128, 1000, 12345, 9_800_000, 2**40 + 77):
+        for R in (1, 2, 3, 4, 7, 8):
+            parts = [E.shard_range(n, r, R) for r in range(R)]
+            assert parts[0][0] == 0 and parts[-1][1] == n
+            for (b, e), (b2, _) in zip(parts, parts[1:]):
+                assert e == b2 and b <= e
+            for b, _ in parts:
+                assert b % 128 == 0 or b == n
+            sizes = [e - b for b, e in parts]
+            assert max(sizes) - min(sizes) <= 128 + (n % 128 if n < 128 * R else 0)
+    for args in ((10, 2, 2), (10, -1, 2), (10, 0, 0), (-1, 0, 1)):
+        with pytest.raises(E.TortoiseError):
+            E.shard_range(*args)

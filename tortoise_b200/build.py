@@ -25,6 +25,7 @@ SOURCES = {
     "tb_static_scratch.cu": [],
     "tb_vjp.cu": [],
     "tb_adjoint.cu": [],
+    "tb_shard.cu": [],
 }
 
 
@@ -45,7 +46,7 @@ def build(verbose=False, extra=()):
             print(" ".join(cmd))
         subprocess.check_call(cmd)
         objs.append(obj)
-    cmd = [nvcc(), *ARCH, "-shared", "-o", OUT, *objs, "-lcudart"]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", OUT, *objs, "-lcudart", "-ldl"]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)

@@ -375,6 +375,7 @@ static int vjp_at(tb_handle* h, const double* Y, int flags) {
             TB_TRY(launch_collision_vjp(G.dev, G.d_insts, int(G.insts.size()), G.layout, G.tensor, G.tup.d, G.tup.cap,
                                         G.tup.n, Y, A->u, A->g, A->gamp + A->gamp_off[gi], h->stream));
         }
+        TB_TRY(shard_allreduce(h, A->g, size_t(h->ndofs)));   // sharded: all ranks' partial VJPs
     }
     if (!(flags & TB_NO_DRIFT) && h->any_drift) TB_TRY(launch_drift_vjp(h->ed, A->u, A->g, h->stream));
     A->vjp_evals += 1;
@@ -383,10 +384,11 @@ static int vjp_at(tb_handle* h, const double* Y, int flags) {
 
 static int copy_gamp_out(tb_handle* h, double* grad_amp) {
     AdjointState* A = h->adj;
+    TB_TRY(shard_allreduce(h, A->gamp, size_t(A->n_slots)));   // sharded: all ranks' partial sums
     std::vector<double> slots(size_t(std::max(A->n_slots, 1)));
     TB_CUDA(cudaMemcpyAsync(slots.data(), A->gamp, sizeof(double) * size_t(A->n_slots), cudaMemcpyDeviceToHost,
                             h->stream));
-    TB_CUDA(cudaStreamSynchronize(h->stream));
+    TB_TRY(stream_wait(h));
     for (size_t c = 0; c < h->insts.size(); ++c) {
         const ChanInst& I = h->insts[c];
         grad_amp[c] = slots[size_t(A->gamp_off[I.group] + I.slot)];
@@ -423,7 +425,7 @@ int tb_adjoint_rhs_vjp(tb_handle* h, const double* f, const double* theta, doubl
     else TB_CUDA(cudaMemcpyAsync(grad_f, A->g, bytes, cudaMemcpyDeviceToDevice, h->stream));
     TB_CUDA(cudaMemsetAsync(A->g, 0, bytes, h->stream));
     if (grad_amp) TB_TRY(copy_gamp_out(h, grad_amp));
-    else TB_CUDA(cudaStreamSynchronize(h->stream));
+    else TB_TRY(stream_wait(h));
     return TB_OK;
 }
 
@@ -461,7 +463,7 @@ int tb_dp45_replay(tb_handle* h, const double* f0, const double* dts, int64_t n_
     }
     TB_CUDA(cudaMemcpyAsync(f_out, A->rtmp, bytes, (flags & TB_PTR_HOST) ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
                             h->stream));
-    TB_CUDA(cudaStreamSynchronize(h->stream));
+    TB_TRY(stream_wait(h));
     return TB_OK;
 }
 
@@ -517,7 +519,7 @@ int tb_adjoint_forward(tb_handle* h, const double* f0, double t0, double t1, dou
     if (f_obs)
         TB_CUDA(cudaMemcpyAsync(f_obs, h->dp.dense + last * h->ndofs, sizeof(double) * size_t(h->ndofs),
                                 (flags & TB_PTR_HOST) ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, h->stream));
-    TB_CUDA(cudaStreamSynchronize(h->stream));
+    TB_TRY(stream_wait(h));
     A->step_dt.resize(size_t(A->n_steps));
     for (int64_t n = 0; n < A->n_steps; ++n) A->step_dt[size_t(n)] = lg[size_t(2 * n + 1)];
     A->have_forward = true;
@@ -612,7 +614,7 @@ int tb_adjoint_backward(tb_handle* h, const double* lambda_T, double* grad_f0, d
         if (flags & TB_PTR_HOST) TB_CUDA(cudaMemcpyAsync(grad_f0, out, bytes, cudaMemcpyDeviceToHost, h->stream));
     }
     if (grad_amp) TB_TRY(copy_gamp_out(h, grad_amp));
-    TB_CUDA(cudaStreamSynchronize(h->stream));
+    TB_TRY(stream_wait(h));
     int tflag = 0;
     TB_TRY(tensor_error_flag(&tflag));
     if (tflag) { set_error("moment-tensor copy wait ran out"); return TB_ERR_TIMEOUT; }

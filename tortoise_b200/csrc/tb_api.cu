@@ -462,6 +462,7 @@ int build_runs(tb_handle* h, const tb_problem_desc* const* descs, int nruns) {
         I.d_single = dev_upload_raw(h, &I.dev, 1);
         if (!I.d_single) { set_error("instance table allocation failed"); return TB_ERR_OOM; }
     }
+    for (auto& G : h->groups) TB_TRY(shard_tuples(h, G));
     TB_TRY(choose_layouts(h));
     if (h->opts.autotune) TB_TRY(autotune(h));
     TB_CUDA(cudaStreamSynchronize(h->stream));
@@ -496,6 +497,9 @@ int run_rhs_acc(tb_handle* h, const double* d_in, double* d_acc, const DPCtl* ct
                                                d_acc, ctl, h->stream));
             }
         }
+        // sharded: the partial collision sums of all ranks, before the
+        // (replicated) drift term
+        TB_TRY(shard_allreduce(h, d_acc, size_t(h->ndofs)));
     }
     if (!(flags & TB_NO_DRIFT) && only_inst < 0 && h->any_drift) TB_TRY(launch_drift(h->ed, d_in, d_acc, ctl, h->stream));
     return TB_OK;
@@ -679,6 +683,11 @@ int tb_create_batch(tb_handle** out, const tb_problem_desc* const* runs, int n_r
         set_error("tb_options: layout must be 0..4 and allow_fp32 0..2");
         return TB_ERR_ARG;
     }
+    if (h->opts.shard_count < 0 || h->opts.shard_rank < 0 ||
+        (h->opts.shard_rank > 0 && h->opts.shard_rank >= h->opts.shard_count)) {
+        set_error("tb_options: need 0 <= shard_rank < shard_count (or both 0)");
+        return TB_ERR_ARG;
+    }
     h->device = h->opts.device;
     TB_CUDA(cudaSetDevice(h->device));
     TB_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
@@ -698,6 +707,7 @@ int tb_destroy(tb_handle* h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->graph) cudaGraphExecDestroy(h->graph);
+    shard_release(h);
     adjoint_release(h);
     for (auto& G : h->groups) { G.tup.release(); G.tensor.release(); }
     for (double* p : h->dev_allocs) cudaFree(p);
@@ -778,6 +788,10 @@ int tb_get_tuples(const tb_handle* h, int ch, int32_t* ids, int32_t* umk) {
 //   per tuple: int32 element id of every leg, int32 umklapp column
 int tb_write_scatt_indices(const tb_handle* h, int ch, const char* path) {
     if (!h || !path || ch < 0 || ch >= int(h->insts.size())) { set_error("bad argument"); return TB_ERR_ARG; }
+    if (h->opts.shard_count > 1) {
+        set_error("a sharded handle holds only its part of the tuple list");
+        return TB_ERR_ARG;
+    }
     const ChanInst& I = h->insts[ch];
     const GroupChan& G = h->groups[I.group];
     const int L = G.L;
@@ -852,7 +866,7 @@ int tb_set_amplitude(tb_handle* h, int ch, double amplitude) {
     I.dev.amp_full = amp_full_of(h, I, G.L, amplitude);
     // the kernels read instances from device memory, so a captured graph
     // sees the new value at its next launch
-    TB_CUDA(cudaStreamSynchronize(h->stream));
+    TB_TRY(stream_wait(h));
     TB_CUDA(cudaMemcpy(G.d_insts + I.slot, &I.dev, sizeof(InstDev), cudaMemcpyHostToDevice));
     TB_CUDA(cudaMemcpy(I.d_single, &I.dev, sizeof(InstDev), cudaMemcpyHostToDevice));
     if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }  // channel skip set changes
@@ -876,7 +890,7 @@ static int rhs_common(tb_handle* h, const double* f, double* out, int flags, int
     TB_CUDA(cudaMemsetAsync(h->d_acc, 0, bytes, h->stream));
     if (flags & TB_PTR_HOST) {
         TB_CUDA(cudaMemcpyAsync(out, h->d_out, bytes, cudaMemcpyDeviceToHost, h->stream));
-        TB_CUDA(cudaStreamSynchronize(h->stream));
+        TB_TRY(stream_wait(h));
     }
     return TB_OK;
 }
@@ -920,11 +934,12 @@ int tb_scattering_rates(tb_handle* h, int ch, int leg, const double* f, double* 
                                                h->d_acc, nullptr, h->stream, l));
         }
     }
+    TB_TRY(shard_allreduce(h, h->d_acc, size_t(h->ndofs)));
     TB_TRY(launch_inverse_mass(h->ed, h->d_acc, d_res, h->stream));
     TB_CUDA(cudaMemsetAsync(h->d_acc, 0, bytes, h->stream));
     if (flags & TB_PTR_HOST) {
         TB_CUDA(cudaMemcpyAsync(rates, h->d_out, bytes, cudaMemcpyDeviceToHost, h->stream));
-        TB_CUDA(cudaStreamSynchronize(h->stream));
+        TB_TRY(stream_wait(h));
     }
     return TB_OK;
 }
@@ -949,7 +964,7 @@ int tb_relative_error(tb_handle* h, const double* err, const double* pop, double
     const int nblk = h->ed.nblk;
     std::vector<double> part(size_t(2 * nblk));
     TB_CUDA(cudaMemcpyAsync(part.data(), h->d_part, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, h->stream));
-    TB_CUDA(cudaStreamSynchronize(h->stream));
+    TB_TRY(stream_wait(h));
     std::vector<int> first(h->bands.size() + 1, 0);
     for (size_t b = 0; b < h->bands.size(); ++b) first[b + 1] = first[b] + (h->bands[b].ne + 255) / 256;
     for (size_t r = 0; r < h->runs.size(); ++r) {
@@ -975,7 +990,7 @@ int tb_apply_constraints(tb_handle* h, double* f, int flags) {
         TB_CUDA(cudaMemcpyAsync(h->d_f, f, bytes, cudaMemcpyHostToDevice, h->stream));
         TB_TRY(launch_enforce(h->ed, h->d_f, h->d_f, h->stream));
         TB_CUDA(cudaMemcpyAsync(f, h->d_f, bytes, cudaMemcpyDeviceToHost, h->stream));
-        TB_CUDA(cudaStreamSynchronize(h->stream));
+        TB_TRY(stream_wait(h));
     } else {
         TB_TRY(launch_enforce(h->ed, f, f, h->stream));
     }
@@ -1017,7 +1032,7 @@ int dp_begin(tb_handle* h, const double* f0, const double* t0, const double* t_f
     }
     TB_CUDA(cudaMemcpyAsync(B.y, f0, bytes, (flags & TB_PTR_HOST) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
                             h->stream));
-    TB_CUDA(cudaStreamSynchronize(h->stream));   // the pinned mirror is rewritten below
+    TB_TRY(stream_wait(h));   // the pinned mirror is rewritten below
     for (int r = 0; r < nruns; ++r) {
         DPCtl& c = h->h_ctl[r];
         std::memset(&c, 0, sizeof(c));
@@ -1073,7 +1088,7 @@ static int poll_all(tb_handle* h) {
     if (!h || !h->dp_ready) { set_error("tb_dp45_begin was not called"); return TB_ERR_ARG; }
     TB_CUDA(cudaSetDevice(h->device));
     TB_CUDA(cudaMemcpyAsync(h->h_ctl, h->dp.ctl, sizeof(DPCtl) * h->runs.size(), cudaMemcpyDeviceToHost, h->stream));
-    TB_CUDA(cudaStreamSynchronize(h->stream));
+    TB_TRY(stream_wait(h));
     int tflag = 0;
     TB_TRY(tensor_error_flag(&tflag));
     if (tflag)
@@ -1119,7 +1134,7 @@ int tb_dp45_end(tb_handle* h, double* f_out, double* dense_out, double* dense_ti
         uoff += max_dense * rd.ndofs;
         utoff += max_dense;
     }
-    TB_CUDA(cudaStreamSynchronize(h->stream));
+    TB_TRY(stream_wait(h));
     if (st) *st = s;
     int worst = TB_OK;
     for (size_t r = 0; r < h->runs.size(); ++r)
@@ -1144,7 +1159,7 @@ int tb_dp45_integrate(tb_handle* h, double* f_inout, double t0, double t_final, 
 
 int tb_synchronize(tb_handle* h) {
     if (!h) return TB_ERR_ARG;
-    TB_CUDA(cudaStreamSynchronize(h->stream));
+    TB_TRY(stream_wait(h));
     return TB_OK;
 }
 

@@ -22,7 +22,9 @@ struct GroupChan {
     double* d_umk = nullptr;
     double* d_mc = nullptr;
     double* d_mc_pre = nullptr;
-    DeviceTuples tup;
+    DeviceTuples tup;             // this handle's part of the list (all of it unless sharded)
+    int64_t shard_begin = 0;      // index of tup's first tuple in the full list
+    int64_t n_total = 0;          // length of the full list
     int64_t diag[3] = {0, 0, 0};
     int layout = TB_LAYOUT_MC64;
     MomentTensor tensor;
@@ -82,6 +84,10 @@ struct tb_handle {
     int dp_flags = 0;
     // adjoint (tb_adjoint.cu)
     tb::AdjointState* adj = nullptr;
+    // tuple sharding (tb_shard.cu): ncclComm_t once connected
+    void* comm = nullptr;
+    double comm_timeout = 60.0;
+    bool comm_failed = false;
 };
 
 
@@ -94,5 +100,12 @@ int ensure_graph(tb_handle* h, int flags);
 int dp_begin(tb_handle* h, const double* f0, const double* t0, const double* t_final, const double* dense_step,
              int64_t max_dense, int flags, const DPBufs* hooks);
 void adjoint_release(tb_handle* h);
+
+// tb_shard.cu
+int64_t shard_begin(int64_t n, int rank, int n_ranks);
+int shard_tuples(tb_handle* h, GroupChan& G);          // keep this rank's part of G's tuple list
+int shard_allreduce(tb_handle* h, double* buf, size_t n);   // in-place sum over the ranks (no-op unconnected)
+int stream_wait(tb_handle* h);                         // stream sync, bounded when connected
+void shard_release(tb_handle* h);
 
 }  // namespace tb

@@ -29,7 +29,8 @@ class TortoiseError(RuntimeError):
 
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("layout", C.c_int32), ("allow_fp32", C.c_int32),
-                ("tensor_budget_bytes", C.c_int64), ("verbose", C.c_int32), ("autotune", C.c_int32)]
+                ("tensor_budget_bytes", C.c_int64), ("verbose", C.c_int32), ("autotune", C.c_int32),
+                ("shard_rank", C.c_int32), ("shard_count", C.c_int32)]
 
 
 class DP45Stats(C.Structure):
@@ -104,6 +105,10 @@ def lib():
                                            dp, C.POINTER(AdjointStats), C.c_int]
         L.tb_adjoint_steps.argtypes = [vp, dp, i64, C.POINTER(i64), dp]
         L.tb_dp45_replay.argtypes = [vp, vp, dp, i64, C.c_double, vp, C.c_int]
+        L.tb_shard_range.argtypes = [i64, C.c_int, C.c_int, C.POINTER(i64), C.POINTER(i64)]
+        L.tb_shard_unique_id.argtypes = [C.c_char_p]
+        L.tb_shard_connect.argtypes = [vp, C.c_char_p, C.c_double]
+        L.tb_shard_info.argtypes = [vp, C.c_int, C.POINTER(i64), C.POINTER(i64)]
         _lib = L
     return _lib
 
@@ -117,14 +122,43 @@ def _hp(a):
     return C.c_void_p(a.ctypes.data)
 
 
+SHARD_ID_BYTES = 128
+
+
+def shard_range(n_tuples, rank, n_ranks):
+    """[begin, end) of the tuples that rank ``rank`` of ``n_ranks`` keeps
+    (tb_shard_range; host arithmetic, no device needed)."""
+    b, e = C.c_int64(), C.c_int64()
+    _check(lib().tb_shard_range(int(n_tuples), int(rank), int(n_ranks), C.byref(b), C.byref(e)), "tb_shard_range")
+    return b.value, e.value
+
+
+def shard_unique_id():
+    """A new communicator id (bytes) for tb_shard_connect; one rank makes it."""
+    buf = C.create_string_buffer(SHARD_ID_BYTES)
+    _check(lib().tb_shard_unique_id(buf), "tb_shard_unique_id")
+    return buf.raw
+
+
+def _shard_opts(shard):
+    if shard is None:
+        return 0, 0
+    rank, count = shard
+    return int(rank), int(count)
+
+
 class Engine:
-    """One device handle for a Material (tb_create ... tb_destroy)."""
+    """One device handle for a Material (tb_create ... tb_destroy).
+
+    shard=(rank, count): this process keeps the rank-th part of every tuple
+    list (one GPU per rank); connect the ranks with ``shard_connect`` (or
+    tortoise_b200.shard.connect) so that collision sums are all-reduced."""
 
     def __init__(self, material, layout=LAYOUT_AUTO, allow_fp32=False, device=0, tensor_budget_bytes=0,
-                 autotune=False):
+                 autotune=False, shard=None):
         self.material = material
         self.packed = material.pack()
-        opts = Options(device, layout, int(allow_fp32), tensor_budget_bytes, 0, int(autotune))
+        opts = Options(device, layout, int(allow_fp32), tensor_budget_bytes, 0, int(autotune), *_shard_opts(shard))
         h = C.c_void_p()
         _check(lib().tb_create(C.byref(h), C.addressof(self.packed.desc), C.byref(opts)), "tb_create")
         self.h = h
@@ -151,6 +185,19 @@ class Engine:
     def write_scatt_indices(self, ch, path):
         """The channel's tuple list in the reference's .scattIndices format."""
         _check(lib().tb_write_scatt_indices(self.h, ch, os.fsencode(path)), "tb_write_scatt_indices")
+
+    def shard_info(self, ch):
+        """(index of this handle's first tuple in the full list, full list length)."""
+        b, n = C.c_int64(), C.c_int64()
+        _check(lib().tb_shard_info(self.h, ch, C.byref(b), C.byref(n)), "tb_shard_info")
+        return b.value, n.value
+
+    def shard_connect(self, unique_id, timeout_s=60.0):
+        """Joins this handle to the communicator ``unique_id`` (tb_shard_connect);
+        every rank calls it with the same id."""
+        if len(unique_id) != SHARD_ID_BYTES:
+            raise ValueError("a shard id has %d bytes" % SHARD_ID_BYTES)
+        _check(lib().tb_shard_connect(self.h, bytes(unique_id), float(timeout_s)), "tb_shard_connect")
 
     def schedule(self, ch):
         st, pr, sec = C.c_int32(), C.c_int32(), C.c_double()
@@ -305,12 +352,12 @@ class BatchEngine(Engine):
     size.  Channels and bands are numbered globally in run order."""
 
     def __init__(self, materials, layout=LAYOUT_AUTO, allow_fp32=False, device=0, tensor_budget_bytes=0,
-                 autotune=False):
+                 autotune=False, shard=None):
         self.materials = list(materials)
         self.material = self.materials[0]
         self.packs = [m.pack() for m in self.materials]
         arr = (C.c_void_p * len(self.packs))(*[C.addressof(p.desc) for p in self.packs])
-        opts = Options(device, layout, int(allow_fp32), tensor_budget_bytes, 0, int(autotune))
+        opts = Options(device, layout, int(allow_fp32), tensor_budget_bytes, 0, int(autotune), *_shard_opts(shard))
         h = C.c_void_p()
         _check(lib().tb_create_batch(C.byref(h), arr, len(self.packs), C.byref(opts)), "tb_create_batch")
         self.h = h
