@@ -212,7 +212,16 @@ def ours(args, world, rank, local, pg):
     mat, f0 = workload()
     layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32,
               "t40": E.LAYOUT_T40}[args.layout]
-    eng = E.Engine(mat, layout=layout, allow_fp32=mixed_flag(args), device=local, autotune=not args.no_tune)
+    eng = E.Engine(mat, layout=layout, allow_fp32=mixed_flag(args), device=local, autotune=not args.no_tune,
+                   shard=(rank, world) if args.shard else None)
+    if args.shard:
+        # one run, its tuples split over the ranks: every collision sum ends
+        # with an NCCL all-reduce (one rank: the same call path)
+        if pg is not None:
+            from tortoise_b200 import shard
+            shard.connect(eng, timeout_s=120.0)
+        else:
+            eng.shard_connect(E.shard_unique_id(), 120.0)
     nch = len(mat.channels)
     infos = [eng.channel_info(c) for c in range(nch)]
     ntup = sum(i["n_tuples"] for i in infos)
@@ -260,7 +269,7 @@ def ours(args, world, rank, local, pg):
     t_dev = ev0.elapsed_time(ev1) * 1e-3
     st = eng.dp45_poll()
     t_max = reduce_max(pg, t_dev, dev)
-    value = aggregate_rate(world, args.steps, t_max)
+    value = args.steps / t_max if args.shard else aggregate_rate(world, args.steps, t_max)
     drift_launch = 1 if any(b.drift_velocity != (0.0, 0.0) for b in mat.bands) else 0
     active = sum(1 for c, i in zip(mat.channels, infos) if c.amplitude != 0 and i["n_tuples"] > 0)
     launches = args.steps * (7 + 6 * (active + drift_launch) + 3)
@@ -276,7 +285,7 @@ def ours(args, world, rank, local, pg):
     r = eng.dp45(y, 0.0, t_e2e_final, DENSE)
     w1 = time.perf_counter()
     e2e_t = reduce_max(pg, w1 - w0, dev)
-    e2e_val = world * r["attempts"] / e2e_t
+    e2e_val = (1 if args.shard else world) * r["attempts"] / e2e_t
     h2d = eng.ndofs * 8 / max(1, r["attempts"])
     d2h = eng.ndofs * 8 * (1 + r["n_dense"]) / max(1, r["attempts"])
 
@@ -302,13 +311,15 @@ def ours(args, world, rank, local, pg):
             traffic = d[key]["bytes_per_tuple"] * ntup
     line = {"metric": METRIC, "value": value, "unit": "DP45 steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": {None: "f64", "t32": "f32-storage/f64-accumulate",
+            "scaling": "strong" if args.shard else "weak", "vs_baseline": None, "dtype": {None: "f64", "t32": "f32-storage/f64-accumulate",
                       "t40": "fp64-upper-40-bit-storage/f64-accumulate"}[args.mixed],
             "data": "synthetic (seeded PCG64 bump on Fermi-Dirac, Bose phonons)",
             "config": {"workload": "2-band e-ph + drift, 64x64 mesh (8192 triangles/band), NMC=50, rtol 1e-8",
                        "tuples": ntup, "channels": nch, "layouts": [i["layout"] for i in infos],
                        "schedules": [eng.schedule(c) for c in range(nch)],
-                       "dofs": eng.ndofs, "parallelism": "replicas x%d" % world,
+                       "dofs": eng.ndofs,
+                       "parallelism": ("tuple-shard x%d (NCCL all-reduce per RHS)" if args.shard else "replicas x%d")
+                       % world,
                        "l2": "moment tensors (%.1f GB) exceed L2; no flush" % (bytes_coll / 1e9)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic,
@@ -324,7 +335,7 @@ def ours(args, world, rank, local, pg):
     clk_s = clk.summary()
     if clk_s:
         line["clocks"] = clk_s
-    if rank == 0 and world == 1 and not args.no_extras and args.mixed is None:
+    if rank == 0 and world == 1 and not args.no_extras and args.mixed is None and not args.shard:
         # the north-star comparison beside the FP64 headline: mixed-precision
         # storage on this workload, and the batched ensemble against
         # sequential single-run FP64
@@ -553,6 +564,8 @@ def main():
     ap.add_argument("--rhs-only", type=int, default=0, help="profiling driver: K RHS evaluations only")
     ap.add_argument("--mesh", type=int, default=N_MESH, help="sections per side (profiling driver only)")
     ap.add_argument("--batch", type=int, default=0, help="batched ensemble of this many runs (per-run N, kT, couplings)")
+    ap.add_argument("--shard", action="store_true",
+                    help="one run with its tuples split over the ranks (NCCL all-reduce per RHS) instead of replicas")
     ap.add_argument("--adjoint", type=int, default=-1,
                     help="adjoint gradient of the 32x32 workload, checked in this many FD directions")
     args = ap.parse_args()
