@@ -394,7 +394,14 @@ def batched_measure(n_runs, steps, warmup, mixed, layout_name="auto", tune=True)
         if N not in uniq:
             uniq[N] = sum(be.channel_info(be.chan0[r] + c)["n_tuples"] for c in range(len(m.channels)))
     layouts = sorted({be.channel_info(c)["layout"] for c in range(be.channel_count())})
-    scheds = sorted({(s["stages"], s["pair"]) for s in (be.schedule(c) for c in range(be.channel_count()))})
+    # (stages, instance schedule, groups): schedule 0 one instance per thread,
+    # 1 instance pairs, 2 run-minor
+    cnt = {}
+    for c in range(be.channel_count()):
+        sc = be.schedule(c)
+        k = (sc["stages"], 2 if sc["runs"] else sc["pair"])
+        cnt[k] = cnt.get(k, 0) + 1
+    scheds = [[k[0], k[1], v] for k, v in sorted(cnt.items())]
     ndofs = be.ndofs
     be.close()
     del f, acc
@@ -531,10 +538,18 @@ def rhs_only(args):
     launch list and kernel captures summarised under profiles/)."""
     import torch
     from tortoise_b200 import engine as E
-    mat, f0 = workload(args.mesh)
+    from tortoise_b200 import workloads as W
     layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32,
               "t40": E.LAYOUT_T40}[args.layout]
-    eng = E.Engine(mat, layout=layout, allow_fp32=mixed_flag(args), autotune=not args.no_tune)
+    if args.batch:
+        # a batch of args.batch runs of one structure (mesh args.mesh): the
+        # groups shared by many runs (run-minor contraction)
+        mats, states = W.ensemble_runs(args.batch, seed=3, Ns=(args.mesh,))
+        eng = E.BatchEngine(mats, layout=layout, allow_fp32=mixed_flag(args), autotune=not args.no_tune)
+        mat, f0 = mats[0], np.concatenate(states)
+    else:
+        mat, f0 = workload(args.mesh)
+        eng = E.Engine(mat, layout=layout, allow_fp32=mixed_flag(args), autotune=not args.no_tune)
     f = torch.tensor(f0, device="cuda")
     out = torch.zeros_like(f)
     torch.cuda.synchronize()
@@ -543,9 +558,9 @@ def rhs_only(args):
         eng.rhs_device(f.data_ptr(), out.data_ptr())
     eng.synchronize()
     dt = time.perf_counter() - t0
-    print(json.dumps({"rhs_only": args.rhs_only, "mesh": args.mesh, "layouts": [eng.channel_info(c)["layout"]
-                      for c in range(len(mat.channels))], "schedules": [eng.schedule(c) for c in range(len(mat.channels))],
-                      "seconds": dt}), flush=True)
+    print(json.dumps({"rhs_only": args.rhs_only, "mesh": args.mesh, "runs": args.batch or 1,
+                      "layouts": [eng.channel_info(c)["layout"] for c in range(len(mat.channels))],
+                      "schedules": [eng.schedule(c) for c in range(len(mat.channels))], "seconds": dt}), flush=True)
     eng.close()
 
 
@@ -561,7 +576,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and batched measurements")
     ap.add_argument("--no-tune", action="store_true", help="fixed contraction schedule (no autotuner)")
-    ap.add_argument("--rhs-only", type=int, default=0, help="profiling driver: K RHS evaluations only")
+    ap.add_argument("--rhs-only", type=int, default=0,
+                    help="profiling driver: K RHS evaluations only (with --batch R: R runs of mesh --mesh)")
     ap.add_argument("--mesh", type=int, default=N_MESH, help="sections per side (profiling driver only)")
     ap.add_argument("--batch", type=int, default=0, help="batched ensemble of this many runs (per-run N, kT, couplings)")
     ap.add_argument("--shard", action="store_true",

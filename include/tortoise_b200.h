@@ -276,10 +276,12 @@ int tb_read_scatt_indices(const char* path, int nlegs, const int32_t* nsplit, in
                           int32_t* umk, int64_t capacity);
 
 /* Contraction schedule of a channel's moment-tensor group: bulk-copy
- * pipeline stages (1 or 2), whether two instances share each moment read (1)
- * and, after tb_options.autotune, the fastest measured launch time in seconds
- * (0 when not tuned).  Monte-Carlo channels report 0, 0, 0.  No counterpart
- * in the reference. */
+ * pipeline stages (1 or 2); the instance schedule in `pair` -- 0 one
+ * instance per thread, 1 two instances share each moment read, 2 run-minor
+ * (one warp per tuple, one lane per run, for groups shared by many runs of a
+ * batch); and, after tb_options.autotune, the fastest measured launch time
+ * in seconds (0 when not tuned).  Monte-Carlo channels report 0, 0, 0.  No
+ * counterpart in the reference. */
 int tb_channel_schedule(const tb_handle* h, int ch, int32_t* stages, int32_t* pair, double* seconds);
 
 /* Out-scattering rates, state-shaped, M^-1 applied (replaces

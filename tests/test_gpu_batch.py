@@ -112,4 +112,35 @@ def test_autotuned_schedule_gives_the_same_operator(gpu_lib):
         assert s["stages"] in (1, 2) and s["pair"] in (0, 1) and s["tuned_seconds"] > 0.0
         assert plain.schedule(0)["tuned_seconds"] == 0.0
     mc = E.BatchEngine(mats, layout=E.LAYOUT_MC64, autotune=True)
-    assert mc.schedule(0) == {"stages": 0, "pair": 0, "tuned_seconds": 0.0}
+    assert mc.schedule(0) == {"stages": 0, "pair": 0, "runs": 0, "tuned_seconds": 0.0}
+
+
+@pytest.mark.parametrize("layout", [E.LAYOUT_T64, E.LAYOUT_T40, E.LAYOUT_T32])
+def test_run_minor_contraction_equals_individual_runs(gpu_lib, layout):
+    """Groups shared by 16 runs or more take the run-minor contraction (one
+    warp per tuple, one lane per run, f and the results staged run-minor).
+    40 runs of two structures (4x4 and 6x6, about 20 runs each, so the second
+    chunk of 32 lanes is partly idle): every run's RHS equals its RHS alone to
+    1e-12, and a short DP45 integration reproduces every run's own
+    accept/reject sequence and dense outputs to 1e-10.  With one run switched
+    off (amplitudes 0), its lane emits nothing."""
+    mats, states = W.ensemble_runs(40, seed=7, Ns=(4, 6))
+    be = E.BatchEngine(mats, layout=layout)
+    assert all(be.schedule(c)["runs"] for c in range(be.channel_count()))
+    f = np.concatenate(states)
+    got = be.split(be.rhs(f))
+    singles = [E.Engine(m, layout=layout) for m in mats]
+    for e1, x, g in zip(singles, states, got):
+        assert rel_l2(g, e1.rhs(x)) < 1e-12
+    res = be.dp45(f, 0.0, 0.05, 0.025)
+    for r in (0, 1, 17, 39):
+        ref = singles[r].dp45(states[r], 0.0, 0.05, 0.025)
+        run = res["runs"][r]
+        assert run["status"] == 0
+        assert [run["attempts"], run["accepted"], run["rejected"]] == [ref["attempts"], ref["accepted"], ref["rejected"]]
+        assert rel_l2(run["dense"], ref["dense"]) < 1e-10
+    for c in range(len(mats[5].channels)):
+        be.set_amplitude(be.chan0[5] + c, 0.0)
+    after = be.split(be.rhs(f, drift=False))
+    assert np.linalg.norm(after[5]) == 0.0
+    assert rel_l2(after[6], singles[6].rhs(states[6], drift=False)) < 1e-12

@@ -546,8 +546,14 @@ int choose_layouts(tb_handle* h) {
             else budget -= bytes;
         }
         G.layout = want;
-        if (want != TB_LAYOUT_MC64)
+        if (want != TB_LAYOUT_MC64) {
             TB_TRY(build_tensor(G.dev, G.tup.d, G.tup.cap, G.tup.n, kind, G.tensor, h->stream));
+            std::vector<int> runs_of;
+            for (int id : G.insts) runs_of.push_back(h->insts[id].run);
+            std::sort(runs_of.begin(), runs_of.end());
+            const bool distinct = std::adjacent_find(runs_of.begin(), runs_of.end()) == runs_of.end();
+            TB_TRY(prepare_runs(G.dev, int(G.insts.size()), distinct, G.tensor, h->stream));
+        }
     }
     return TB_OK;
 }
@@ -758,7 +764,8 @@ int tb_channel_schedule(const tb_handle* h, int ch, int32_t* stages, int32_t* pa
     const GroupChan& G = h->groups[h->insts[ch].group];
     const bool tensor = G.layout != TB_LAYOUT_MC64;
     if (stages) *stages = tensor ? G.tensor.stages : 0;
-    if (pair) *pair = (tensor && G.L <= 3 && G.insts.size() > 1) ? G.tensor.pair : 0;
+    if (pair)
+        *pair = !tensor ? 0 : G.tensor.runs ? 2 : (G.L <= 3 && G.insts.size() > 1) ? G.tensor.pair : 0;
     if (seconds) *seconds = tensor ? G.tensor.tuned_seconds : 0.0;
     return TB_OK;
 }

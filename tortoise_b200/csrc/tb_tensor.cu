@@ -78,8 +78,12 @@ int64_t tensor_bytes(int L, int kind, int64_t n) {
 
 void MomentTensor::release() {
     if (d) cudaFree(d);
+    if (fT) cudaFree(fT);
+    if (accT) cudaFree(accT);
     d = nullptr;
+    fT = accT = nullptr;
     n = ntiles = 0;
+    runs = np = runs_distinct = 0;
 }
 
 // ------------------------------------------------------------ precompute
@@ -453,6 +457,295 @@ __global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, const InstDe
     }
 }
 
+// ------------------------------------------------- run-minor contraction
+// For a group shared by many runs (a batched ensemble) the per-thread
+// contraction above spends most of its instructions on per-tuple work that
+// every instance repeats (moment loads and widening, tuple ids, scatter
+// keys) and gathers each run's f from its own, distant slice of the state.
+// Here one warp contracts one staged tuple for 32 runs at once, lane = run:
+//   k_runs_gather     the legs' f of every instance into fT[leg][dof][np]
+//                     (32x32 shared-memory transpose, coalesced both ways);
+//   k_collision_runs  per tuple, the moments are read at one shared-memory
+//                     address by all lanes (broadcast), the lanes' f rows and
+//                     their reductions into accT are coalesced 256-byte rows;
+//   k_runs_scatter    accT back into the state-layout accumulator, cleared.
+// The arithmetic per instance is that of contract_tuple (NI = 1).
+struct RunsDev {
+    double* fT;
+    double* accT;
+    int64_t loff[TB_MAX_LEGS];
+    int64_t ndof[TB_MAX_LEGS];
+    int np;
+};
+
+// a[l] for a kernel-parameter array without a local-memory copy of it
+__device__ __forceinline__ int64_t leg_pick(const int64_t (&a)[TB_MAX_LEGS], int l) {
+    return l == 0 ? a[0] : l == 1 ? a[1] : l == 2 ? a[2] : a[3];
+}
+
+constexpr int RUNS_THREADS = 256;
+constexpr int RUNS_MIN = 8;           // smallest group given the buffers
+constexpr int RUNS_DEFAULT_MIN = 16;  // untuned handles use the path from here
+constexpr int RUNS_NP_MAX = 1024;     // s_amp: at most 8 KB of shared memory
+
+__global__ void __launch_bounds__(256) k_runs_gather(const InstDev* __restrict__ insts, int n_insts, RunsDev R,
+                                                     const double* __restrict__ f) {
+    __shared__ double tile[32][33];
+    const int l = blockIdx.z;
+    const int64_t ndof = leg_pick(R.ndof, l), loff = leg_pick(R.loff, l);
+    const int64_t d0 = int64_t(blockIdx.x) * 32;
+    const int i0 = blockIdx.y * 32;
+    if (d0 >= ndof) return;   // uniform in the block
+    for (int k = threadIdx.y; k < 32; k += 8) {
+        const int i = i0 + k;
+        const int64_t d = d0 + threadIdx.x;
+        tile[k][threadIdx.x] = (i < n_insts && d < ndof) ? __ldg(f + insts[i].foff[l] + d) : 0.0;
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += 8) {
+        const int64_t d = d0 + k;
+        if (d < ndof) R.fT[loff + d * R.np + i0 + threadIdx.x] = tile[threadIdx.x][k];
+    }
+}
+
+// Every leg in turn through one block of 32 x 32 threads, so that a (dof,
+// instance) pair stays with one thread for all legs; then, when the group's
+// instances belong to distinct runs (DISTINCT), no two threads add into one
+// coefficient and the adds need no atomics (two legs of one band are added by
+// the same thread).  The block's instance offsets are staged in shared
+// memory, so each add waits on one global load only.
+template <bool DISTINCT>
+__global__ void __launch_bounds__(1024) k_runs_scatter(const InstDev* __restrict__ insts, int n_insts, RunsDev R,
+                                                       int nlegs, double* __restrict__ acc) {
+    __shared__ double tile[32][33];
+    __shared__ int64_t s_foff[TB_MAX_LEGS][32];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int64_t d0 = int64_t(blockIdx.x) * 32;
+    const int i0 = blockIdx.y * 32;
+    if (ty < nlegs) s_foff[ty][tx] = (i0 + tx < n_insts) ? insts[i0 + tx].foff[ty] : 0;
+    for (int l = 0; l < nlegs; ++l) {
+        const int64_t ndof = leg_pick(R.ndof, l), loff = leg_pick(R.loff, l);
+        if (d0 >= ndof) continue;   // uniform in the block
+        {
+            const int64_t d = d0 + ty;
+            double v = 0.0;
+            if (d < ndof) {
+                double* p = R.accT + loff + d * R.np + i0 + tx;
+                v = *p;
+                *p = 0.0;
+            }
+            tile[ty][tx] = v;
+        }
+        __syncthreads();   // also publishes s_foff on the first leg
+        {
+            const int i = i0 + ty;
+            const int64_t d = d0 + tx;
+            if (i < n_insts && d < ndof) {
+                const double v = tile[tx][ty];
+                double* o = acc + s_foff[l][ty] + d;
+                if (DISTINCT) *o += v;
+                else if (v != 0.0) atomicAdd(o, v);
+            }
+        }
+        __syncthreads();   // the tile is reused by the next leg
+    }
+}
+
+// One tuple (staged at column t of the tile) for the instance of this lane.
+template <int L, int KIND, int TT>
+__device__ __forceinline__ void contract_run(const ChanDev& c, const RunsDev& R, const int (&e)[L], int t, int i,
+                                             double amp, const unsigned char* __restrict__ tile) {
+    constexpr int K = TDim<L>::K, KM = TDim<L>::KM, NMOM = TDim<L>::NMOM;
+    auto M = [&](int j) { return tile_moment<KIND, NMOM, TT>(tile, t, j); };
+    double v[K];
+    {
+        double A[L][3], B[L][3];
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            const double d = c.leg[l].dir, st = c.leg[l].stat;
+            const double* fe = R.fT + R.loff[l] + int64_t(3 * e[l]) * R.np + i;
+            const double ka = (l == 0 ? -1.0 : 1.0) * 0.5;
+            const double ca = (1. - d) * st + (1. + d);
+            const double cb = (1. + d) * st + (1. - d);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const double unit = (j == 0) ? 1.0 : 0.0;
+                const double fj = __ldg(fe + j * R.np);
+                A[l][j] = ka * ((1. - d) * unit + ca * fj);
+                B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            int r = j;
+            double pa = 1.0, pb = 1.0;
+#pragma unroll
+            for (int l = L - 1; l >= 0; --l) {
+                const int Jl = r % 3;
+                r /= 3;
+                pa *= A[l][Jl];
+                pb *= B[l][Jl];
+            }
+            v[j] = pa + pb;
+        }
+    }
+    // independent FMA chains: three partial sums for the constant mode and,
+    // per km, the r1 / r2 rows of every leg together (the warp has few
+    // siblings on its scheduler to hide FMA latency behind)
+    double r0a = 0.0, r0b = 0.0, r0c = 0.0;
+#pragma unroll
+    for (int j = 0; j < K; j += 3) {
+        r0a = fma(M(j), v[j], r0a);
+        r0b = fma(M(j + 1), v[j + 1], r0b);
+        r0c = fma(M(j + 2), v[j + 2], r0c);
+    }
+    const double r0 = (r0a + r0b) + r0c;
+    double r1[L], r2[L];
+#pragma unroll
+    for (int lam = 0; lam < L; ++lam) { r1[lam] = 0.0; r2[lam] = 0.0; }
+#pragma unroll
+    for (int km = 0; km < KM; ++km) {
+#pragma unroll
+        for (int lam = 0; lam < L; ++lam) {
+            int sstep = 1;
+#pragma unroll
+            for (int l = L - 1; l > lam; --l) sstep *= 3;
+            const int hi = km / sstep, lo = km % sstep;
+            const int j0 = hi * 3 * sstep + lo;
+            const int j1 = j0 + sstep, j2 = j0 + 2 * sstep;
+            const int qa = K + (lam * 3 + 0) * KM + km;
+            const double qxx = M(qa), qxy = M(qa + KM), qyy = M(qa + 2 * KM);
+            const double s1 = M(j1), s2 = M(j2);
+            r1[lam] = fma(s1, v[j0], r1[lam]);
+            r1[lam] = fma(qxx, v[j1], r1[lam]);
+            r1[lam] = fma(qxy, v[j2], r1[lam]);
+            r2[lam] = fma(s2, v[j0], r2[lam]);
+            r2[lam] = fma(qxy, v[j1], r2[lam]);
+            r2[lam] = fma(qyy, v[j2], r2[lam]);
+        }
+    }
+    if (amp != 0.0) {
+#pragma unroll
+        for (int lam = 0; lam < L; ++lam) {
+            const double d = c.leg[lam].dir;
+            double* o = R.accT + R.loff[lam] + int64_t(3 * e[lam]) * R.np + i;
+            atomicAdd(o, d * (r0 * amp));
+            atomicAdd(o + R.np, d * (r1[lam] * amp));
+            atomicAdd(o + 2 * R.np, d * (r2[lam] * amp));
+        }
+    }
+}
+
+// DEC (40-bit moments): the staged tile is widened once, cooperatively, into
+// an FP64 copy that the contraction reads; the stage is refilled at once, so
+// one stage already overlaps the next copy with the contraction.
+template <int L, int KIND, int TT, int STAGES>
+__global__ void __launch_bounds__(RUNS_THREADS) k_collision_runs(ChanDev c, const InstDev* __restrict__ insts,
+                                                                 int n_insts, RunsDev R,
+                                                                 const unsigned char* __restrict__ mom, int64_t ntiles,
+                                                                 const int32_t* __restrict__ tup, int64_t stride,
+                                                                 int64_t n, const DPCtl* __restrict__ ctl,
+                                                                 int* __restrict__ err_flag) {
+    constexpr uint32_t TILE_BYTES = uint32_t(TBytes<L, KIND>::B) * TT;
+    constexpr int NMOM = TDim<L>::NMOM;
+    constexpr bool DEC = KIND == TK_F40;
+    constexpr int KREAD = DEC ? TK_F64 : KIND;
+    constexpr size_t DEC_BYTES = DEC ? sizeof(double) * NMOM * TT : 0;
+    constexpr int NW = RUNS_THREADS / 32;
+    static_assert(TT % NW == 0, "tile tuples must split evenly over the warps");
+    constexpr int TPW = TT / NW;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char* stage_buf = smem_raw;
+    double* dec = reinterpret_cast<double*>(smem_raw + size_t(STAGES) * TILE_BYTES);
+    double* s_amp = reinterpret_cast<double*>(smem_raw + size_t(STAGES) * TILE_BYTES + DEC_BYTES);
+    __shared__ __align__(8) uint64_t bars[STAGES];
+    __shared__ int s_any;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_any = 0;
+    __syncthreads();
+    // amplitude of every lane's instance, 0 for padding, switched-off and
+    // finished runs (those lanes compute along but emit nothing)
+    for (int i = tid; i < R.np; i += RUNS_THREADS) {
+        double a = 0.0;
+        if (i < n_insts) {
+            const InstDev in = insts[i];
+            if (in.amplitude != 0.0 && !(ctl && ctl[in.run].done)) a = in.amplitude;
+        }
+        s_amp[i] = a;
+        if (a != 0.0) s_any = 1;
+    }
+    __syncthreads();
+    if (!s_any) return;   // uniform in the block
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            const int64_t tile = blockIdx.x + (int64_t)s * gridDim.x;
+            if (tile < ntiles) {
+                mbar_expect_tx_arrive(&bars[s], TILE_BYTES);
+                bulk_g2s(stage_buf + (size_t)s * TILE_BYTES, mom + tile * (int64_t)TILE_BYTES, TILE_BYTES, &bars[s]);
+            }
+        }
+    }
+    const int nch = R.np >> 5;
+    for (int64_t it = 0;; ++it) {
+        const int64_t tile = blockIdx.x + it * gridDim.x;
+        if (tile >= ntiles) break;
+        const int s = int(it % STAGES);
+        const uint32_t parity = uint32_t((it / STAGES) & 1);
+        if (!mbar_wait(&bars[s], parity)) {
+            if (tid == 0) atomicExch(err_flag, 1);
+            for (int k = 0; k < STAGES; ++k) {
+                const int64_t itk = it + ((k - s + STAGES) % STAGES);
+                if (blockIdx.x + itk * gridDim.x < ntiles) mbar_wait(&bars[k], uint32_t((itk / STAGES) & 1), 1 << 16);
+            }
+            return;
+        }
+        const unsigned char* sm = stage_buf + (size_t)s * TILE_BYTES;
+        auto refill = [&]() {
+            if (tid == 0) {
+                const int64_t next = tile + (int64_t)STAGES * gridDim.x;
+                if (next < ntiles) {
+                    mbar_expect_tx_arrive(&bars[s], TILE_BYTES);
+                    bulk_g2s(stage_buf + (size_t)s * TILE_BYTES, mom + next * (int64_t)TILE_BYTES, TILE_BYTES,
+                             &bars[s]);
+                }
+            }
+        };
+        const unsigned char* rd = sm;
+        if constexpr (DEC) {
+            for (int k = tid; k < NMOM * TT; k += RUNS_THREADS)
+                dec[k] = tile_moment<KIND, NMOM, TT>(sm, k % TT, k / TT);
+            __syncthreads();   // dec complete, stage s consumed
+            refill();
+            rd = reinterpret_cast<const unsigned char*>(dec);
+        }
+        // warp w: tuples [w TPW, (w+1) TPW) of the tile, each for every
+        // chunk of 32 instances
+#pragma unroll 1
+        for (int tt = 0; tt < TPW; ++tt) {
+            const int t = warp * TPW + tt;
+            const int64_t gi = tile * TT + t;
+            if (gi >= n) break;   // uniform in the warp
+            int e[L];
+#pragma unroll
+            for (int l = 0; l < L; ++l) e[l] = __ldg(tup + l * stride + gi);
+#pragma unroll 1
+            for (int ch = 0; ch < nch; ++ch) {
+                const int i = (ch << 5) + lane;
+                const double amp = s_amp[i];
+                if (__all_sync(0xffffffffu, amp == 0.0)) continue;
+                contract_run<L, KREAD, TT>(c, R, e, t, i, amp, rd);
+            }
+        }
+        __syncthreads();   // every warp is done with stage s (and dec)
+        if constexpr (!DEC) refill();
+    }
+}
+
 template <int L, int KIND>
 static int build_t(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, MomentTensor& T, cudaStream_t s) {
     constexpr int TT = TTile<L, KIND>::TT;
@@ -496,6 +789,97 @@ int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n
 
 static int* g_err_flag = nullptr;
 
+static int ensure_err_flag() {
+    if (!g_err_flag) {
+        TB_CUDA(cudaMalloc(&g_err_flag, sizeof(int)));
+        TB_CUDA(cudaMemset(g_err_flag, 0, sizeof(int)));
+    }
+    return TB_OK;
+}
+
+static RunsDev runs_dev(const ChanDev& c, const MomentTensor& T) {
+    RunsDev R{};
+    R.fT = T.fT;
+    R.accT = T.accT;
+    R.np = T.np;
+    for (int l = 0; l < TB_MAX_LEGS; ++l) {
+        R.loff[l] = T.loff[l];
+        R.ndof[l] = l < c.L ? 3 * int64_t(c.leg[l].ne) : 0;
+    }
+    return R;
+}
+
+// gather -> run-minor contraction -> scatter (three launches on s)
+template <int L, int KIND, int STAGES>
+static int launch_runs(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T, const int32_t* tup,
+                       int64_t stride, int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s) {
+    constexpr int TT = TTile<L, KIND>::TT;
+    const RunsDev R = runs_dev(c, T);
+    int64_t maxd = 0;
+    for (int l = 0; l < L; ++l) maxd = std::max(maxd, R.ndof[l]);
+    const dim3 tb(32, 8), tg(unsigned((maxd + 31) / 32), unsigned(T.np / 32), unsigned(L));
+    k_runs_gather<<<tg, tb, 0, s>>>(insts, n_insts, R, f);
+    TB_CUDA(cudaGetLastError());
+    auto kern = k_collision_runs<L, KIND, TT, STAGES>;
+    const size_t fixed = size_t(STAGES) * TT * tuple_bytes(L, KIND) +
+                         (KIND == TK_F40 ? sizeof(double) * TDim<L>::NMOM * TT : 0);
+    const size_t smem = fixed + sizeof(double) * size_t(T.np);
+    static bool attr = false;
+    if (!attr) {
+        TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(fixed + sizeof(double) * RUNS_NP_MAX)));
+        attr = true;
+    }
+    TB_TRY(ensure_err_flag());
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, RUNS_THREADS, smem);
+    if (per_sm < 1) per_sm = 1;
+    int64_t grid = int64_t(nsm) * per_sm;
+    if (grid > T.ntiles) grid = T.ntiles;
+    if (grid >= 1) {
+        kern<<<unsigned(grid), RUNS_THREADS, smem, s>>>(c, insts, n_insts, R, static_cast<const unsigned char*>(T.d),
+                                                       T.ntiles, tup, stride, n, ctl, g_err_flag);
+        TB_CUDA(cudaGetLastError());
+    }
+    const dim3 sg(tg.x, tg.y, 1), sb(32, 32);
+    if (T.runs_distinct) k_runs_scatter<true><<<sg, sb, 0, s>>>(insts, n_insts, R, L, acc);
+    else k_runs_scatter<false><<<sg, sb, 0, s>>>(insts, n_insts, R, L, acc);
+    TB_CUDA(cudaGetLastError());
+    return TB_OK;
+}
+
+int prepare_runs(const ChanDev& c, int n_insts, bool distinct_runs, MomentTensor& T, cudaStream_t s) {
+    if (c.L > 3 || n_insts < RUNS_MIN || T.fT || !T.d) return TB_OK;
+    const int np = (n_insts + 31) & ~31;
+    if (np > RUNS_NP_MAX) return TB_OK;
+    int64_t tot = 0;
+    for (int l = 0; l < c.L; ++l) {
+        T.loff[l] = tot;
+        tot += 3 * int64_t(c.leg[l].ne) * np;
+    }
+    const size_t bytes = sizeof(double) * size_t(tot);
+    if (cudaMalloc(&T.fT, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        T.fT = nullptr;
+        return TB_OK;
+    }
+    if (cudaMalloc(&T.accT, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(T.fT);
+        T.fT = nullptr;
+        T.accT = nullptr;
+        return TB_OK;
+    }
+    TB_CUDA(cudaMemsetAsync(T.accT, 0, bytes, s));
+    T.np = np;
+    T.runs_distinct = distinct_runs ? 1 : 0;
+    T.runs = n_insts >= RUNS_DEFAULT_MIN ? 1 : 0;
+    return TB_OK;
+}
+
 template <int L, int KIND, int STAGES, bool PAIR, bool RATE = false>
 static int launch_variant(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T,
                           const int32_t* tup, int64_t stride, int64_t n, const double* f, double* acc,
@@ -508,10 +892,7 @@ static int launch_variant(const ChanDev& c, const InstDev* insts, int n_insts, c
         TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
         attr = true;
     }
-    if (!g_err_flag) {
-        TB_CUDA(cudaMalloc(&g_err_flag, sizeof(int)));
-        TB_CUDA(cudaMemset(g_err_flag, 0, sizeof(int)));
-    }
+    TB_TRY(ensure_err_flag());
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -536,6 +917,11 @@ static int launch_t(const ChanDev& c, const InstDev* insts, int n_insts, const M
                     int rate_leg) {
     if (rate_leg >= 0)   // diagnostic operator: one fixed schedule
         return launch_variant<L, KIND, 2, false, true>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+    if constexpr (L <= 3) {
+        if (T.runs && T.fT)
+            return T.stages == 1 ? launch_runs<L, KIND, 1>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s)
+                                 : launch_runs<L, KIND, 2>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
+    }
     const bool pair = (L <= 3) && n_insts > 1 && T.pair;
     if (T.stages == 1) {
         return pair ? launch_variant<L, KIND, 1, (L <= 3)>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg)
@@ -571,14 +957,15 @@ int tune_tensor(const ChanDev& c, const InstDev* insts, int n_insts, MomentTenso
     const int64_t bucket = int64_t(std::llround(std::log2(double(n)) * 8.0));
     const std::tuple<int, int, int64_t, int> key(c.L, T.kind, bucket, n_insts);
     static std::mutex mu;
-    static std::map<std::tuple<int, int, int64_t, int>, std::tuple<int, int, double>> cache;
+    static std::map<std::tuple<int, int, int64_t, int>, std::tuple<int, int, int, double>> cache;
     {
         std::lock_guard<std::mutex> lk(mu);
         auto it = cache.find(key);
         if (it != cache.end()) {
             T.stages = std::get<0>(it->second);
             T.pair = std::get<1>(it->second);
-            T.tuned_seconds = std::get<2>(it->second);
+            T.runs = T.fT ? std::get<2>(it->second) : 0;
+            T.tuned_seconds = std::get<3>(it->second);
             return TB_OK;
         }
     }
@@ -586,13 +973,17 @@ int tune_tensor(const ChanDev& c, const InstDev* insts, int n_insts, MomentTenso
     TB_CUDA(cudaEventCreate(&e0));
     TB_CUDA(cudaEventCreate(&e1));
     double best = 1e300;
-    int bs = T.stages, bp = T.pair;
+    int bs = T.stages, bp = T.pair, br = T.runs;
     const int pairs_max = (c.L <= 3 && n_insts > 1) ? 1 : 0;
+    const int runs_max = T.fT ? 1 : 0;
     int rc = TB_OK;
     for (int st = 1; st <= 2 && rc == TB_OK; ++st)
-        for (int pr = 0; pr <= pairs_max && rc == TB_OK; ++pr) {
+        for (int pr = 0; pr <= pairs_max + runs_max && rc == TB_OK; ++pr) {
+            // pr: 0 one instance per thread, 1 instance pairs, 2 run-minor
+            if (pr == 1 && !pairs_max) continue;
             T.stages = st;
-            T.pair = pr;
+            T.pair = pr == 1;
+            T.runs = pr == 2;
             rc = launch_collision_tensor(c, insts, n_insts, T, tup, stride, n, f, acc, nullptr, s);   // warm-up
             if (rc != TB_OK) break;
             constexpr int REPS = 3;
@@ -604,16 +995,17 @@ int tune_tensor(const ChanDev& c, const InstDev* insts, int n_insts, MomentTenso
             float ms = 0.f;
             cudaEventElapsedTime(&ms, e0, e1);
             const double sec = 1e-3 * double(ms) / REPS;
-            if (sec < best) { best = sec; bs = st; bp = pr; }
+            if (sec < best) { best = sec; bs = st; bp = T.pair; br = T.runs; }
         }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     T.stages = bs;
     T.pair = bp;
+    T.runs = br;
     if (rc != TB_OK) return rc;
     T.tuned_seconds = best;
     std::lock_guard<std::mutex> lk(mu);
-    cache[key] = std::make_tuple(bs, bp, best);
+    cache[key] = std::make_tuple(bs, bp, br, best);
     return TB_OK;
 }
 

@@ -19,6 +19,14 @@ struct MomentTensor {
     int stages = 2;
     int pair = 1;
     double tuned_seconds = 0.0;   // best measured launch time (0: not tuned)
+    // run-minor contraction for a group shared by many runs (k_collision_runs
+    // in tb_tensor.cu): used when runs = 1; the buffers come from prepare_runs
+    int runs = 0;
+    int np = 0;                   // instances rounded up to a multiple of 32
+    int runs_distinct = 0;        // every instance belongs to another run
+    double* fT = nullptr;         // [leg][3 ne_leg][np]: the legs' f, run-minor
+    double* accT = nullptr;       // same shape; all zero between launches
+    int64_t loff[4] = {0, 0, 0, 0};
     void release();
 };
 
@@ -32,8 +40,14 @@ int launch_collision_tensor(const ChanDev& c, const InstDev* insts, int n_insts,
                             const int32_t* tup, int64_t stride, int64_t n, const double* f, double* acc,
                             const DPCtl* ctl, cudaStream_t s, int rate_leg = -1);
 
+// Buffers of the run-minor contraction for a group of n_insts instances
+// (legs <= 3, 8 <= n_insts <= 1024); sets runs = 1 from 16 instances on.
+// Does nothing for other groups, or when the device memory is short.
+int prepare_runs(const ChanDev& c, int n_insts, bool distinct_runs, MomentTensor& T, cudaStream_t s);
+
 // Autotuner: times the contraction of one group for every schedule
-// (stages 1 / 2, instance pairs off / on where several instances exist) on
+// (stages 1 / 2, instance pairs off / on where several instances exist, the
+// run-minor contraction where prepare_runs gave it buffers) on
 // the device data and keeps the fastest in T.  f is any state of the handle's
 // size; acc is scratch (left dirty).  A process-wide cache keyed by
 // (legs, storage kind, tuple count, instance count) skips repeated timing.

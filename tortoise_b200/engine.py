@@ -202,7 +202,8 @@ class Engine:
     def schedule(self, ch):
         st, pr, sec = C.c_int32(), C.c_int32(), C.c_double()
         _check(lib().tb_channel_schedule(self.h, ch, C.byref(st), C.byref(pr), C.byref(sec)), "tb_channel_schedule")
-        return {"stages": st.value, "pair": pr.value, "tuned_seconds": sec.value}
+        return {"stages": st.value, "pair": int(pr.value == 1), "runs": int(pr.value == 2),
+                "tuned_seconds": sec.value}
 
     def tuples(self, ch):
         info = self.channel_info(ch)
