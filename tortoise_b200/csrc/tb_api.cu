@@ -396,6 +396,13 @@ int build_runs(tb_handle* h, const tb_problem_desc* const* descs, int nruns) {
                     lg.dir = double(cd.dir[l]);
                     lg.stat = B.stat;
                     lg.ne = B.ne;
+                    {
+                        const double d = lg.dir, st = lg.stat, ka = (l == 0 ? -1.0 : 1.0) * 0.5;
+                        lg.fa = ka * ((1. - d) * st + (1. + d));
+                        lg.fa0 = ka * (1. - d);
+                        lg.fb = 0.5 * ((1. + d) * st + (1. - d));
+                        lg.fb0 = 0.5 * (1. + d);
+                    }
                     av *= h->meshes[B.mesh].vol * 2.0;
                 }
                 c.amp_vol = av;

@@ -69,6 +69,12 @@ struct LegDev {
     double dir;           // +1 in, -1 out
     double stat;          // -1 fermion, +1 boson
     int ne;
+    // The leg's loss / gain forms (ScatteringChannel.cpp:633-641),
+    //   A_j = ka ((1 - d) [j = 0] + ca f_j),  B_j = 1/2 ((1 + d) [j = 0] + cb f_j),
+    // as A_j = fa f_j + fa0 [j = 0], B_j = fb f_j + fb0 [j = 0]: ka = -1/2 on
+    // leg 0 and 1/2 elsewhere, ca, cb = +-2, so every folded product is exact
+    // and the forms round exactly as the unfolded ones.
+    double fa, fa0, fb, fb0;
 };
 
 struct ChanDev {

@@ -272,23 +272,20 @@ __device__ __forceinline__ void contract_tuple(const ChanDev& c, const InstDev (
         double A[L][3], B[L][3];
 #pragma unroll
         for (int l = 0; l < L; ++l) {
-            const double d = c.leg[l].dir, st = c.leg[l].stat;
+            const LegDev& lg = c.leg[l];
             const double* fe = f + in[q].foff[l] + 3 * (int64_t)e[l];
-            const double ka = (l == 0 ? -1.0 : 1.0) * 0.5;
-            const double ca = (1. - d) * st + (1. + d);
-            const double cb = (1. + d) * st + (1. - d);
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const double unit = (j == 0) ? 1.0 : 0.0;
-                const double fj = __ldg(fe + j);
-                A[l][j] = ka * ((1. - d) * unit + ca * fj);
-                B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
-            }
+            const double f0 = __ldg(fe), f1 = __ldg(fe + 1), f2 = __ldg(fe + 2);
+            A[l][0] = fma(lg.fa, f0, lg.fa0);
+            A[l][1] = lg.fa * f1;
+            A[l][2] = lg.fa * f2;
+            B[l][0] = fma(lg.fb, f0, lg.fb0);
+            B[l][1] = lg.fb * f1;
+            B[l][2] = lg.fb * f2;
             if (RATE && l == rate_leg) {
                 // scattering rate of this leg: constant in / out unit forms
-                // (ScatteringChannel.cpp:562-564)
-                A[l][0] = (l == 0 ? -1.0 : 1.0) * ca; A[l][1] = 0.0; A[l][2] = 0.0;
-                B[l][0] = cb; B[l][1] = 0.0; B[l][2] = 0.0;
+                // (ScatteringChannel.cpp:562-564): (+-1) ca and cb, i.e. 2 fa, 2 fb
+                A[l][0] = 2.0 * lg.fa; A[l][1] = 0.0; A[l][2] = 0.0;
+                B[l][0] = 2.0 * lg.fb; B[l][1] = 0.0; B[l][2] = 0.0;
             }
         }
 #pragma unroll
@@ -562,18 +559,15 @@ __device__ __forceinline__ void contract_run(const ChanDev& c, const RunsDev& R,
         double A[L][3], B[L][3];
 #pragma unroll
         for (int l = 0; l < L; ++l) {
-            const double d = c.leg[l].dir, st = c.leg[l].stat;
+            const LegDev& lg = c.leg[l];
             const double* fe = R.fT + R.loff[l] + int64_t(3 * e[l]) * R.np + i;
-            const double ka = (l == 0 ? -1.0 : 1.0) * 0.5;
-            const double ca = (1. - d) * st + (1. + d);
-            const double cb = (1. + d) * st + (1. - d);
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const double unit = (j == 0) ? 1.0 : 0.0;
-                const double fj = __ldg(fe + j * R.np);
-                A[l][j] = ka * ((1. - d) * unit + ca * fj);
-                B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
-            }
+            const double f0 = __ldg(fe), f1 = __ldg(fe + R.np), f2 = __ldg(fe + 2 * R.np);
+            A[l][0] = fma(lg.fa, f0, lg.fa0);
+            A[l][1] = lg.fa * f1;
+            A[l][2] = lg.fa * f2;
+            B[l][0] = fma(lg.fb, f0, lg.fb0);
+            B[l][1] = lg.fb * f1;
+            B[l][2] = lg.fb * f2;
         }
 #pragma unroll
         for (int j = 0; j < K; ++j) {
@@ -627,11 +621,11 @@ __device__ __forceinline__ void contract_run(const ChanDev& c, const RunsDev& R,
     if (amp != 0.0) {
 #pragma unroll
         for (int lam = 0; lam < L; ++lam) {
-            const double d = c.leg[lam].dir;
+            const double da = c.leg[lam].dir * amp;   // d = +-1: d (r amp) == r (d amp)
             double* o = R.accT + R.loff[lam] + int64_t(3 * e[lam]) * R.np + i;
-            atomicAdd(o, d * (r0 * amp));
-            atomicAdd(o + R.np, d * (r1[lam] * amp));
-            atomicAdd(o + 2 * R.np, d * (r2[lam] * amp));
+            atomicAdd(o, r0 * da);
+            atomicAdd(o + R.np, r1[lam] * da);
+            atomicAdd(o + 2 * R.np, r2[lam] * da);
         }
     }
 }
