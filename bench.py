@@ -532,6 +532,58 @@ def adjoint(args):
     eng.close()
 
 
+def small_ee(args):
+    """The reference's CPU-runnable case: one parabolic band on a 16x16 mesh
+    (512 triangles), electron-electron scattering with a constant matrix
+    element, Fermi-Dirac kT 0.1 / mu 0.3 plus the seeded bump, DP45 with
+    rtol 1e-6 / atol 1e-9 to t = 10 (dense output every 1.0).  The whole
+    integration runs through the C ABI from host buffers (tb_dp45_integrate);
+    beside it, the oracle's time for one right-hand side on all host cores,
+    measured on a bounded sample of the device's tuple list and scaled to the
+    whole list, times the number of right-hand sides the GPU run needed."""
+    from tortoise_b200 import engine as E
+    from tortoise_b200 import workloads as W
+    import oracle
+    mat = W.parabolic_ee(16)
+    f0 = W.initial_status(mat, kT=0.1, seed=0).vec
+    t_setup = time.perf_counter()
+    eng = E.Engine(mat, autotune=not args.no_tune)
+    t_setup = time.perf_counter() - t_setup
+    info = eng.channel_info(0)
+    eng.dp45(f0, 0.0, 0.01, 0.01)   # warm-up (graph capture, first launches)
+    with ClockSampler(0) as clk:
+        w0 = time.perf_counter()
+        r = eng.dp45(f0, 0.0, 10.0, 1.0, max_dense=11)
+        w1 = time.perf_counter()
+    gpu_s = w1 - w0
+    line = {"workload": "16x16 parabolic band, e-e constant matrix element (512 triangles), rtol 1e-6, t = 10",
+            "tuples": info["n_tuples"], "layout": info["layout"], "setup_s": t_setup,
+            "gpu": {"seconds": gpu_s, "status": r["status"], "attempts": r["attempts"], "accepted": r["accepted"],
+                    "rejected": r["rejected"], "rhs_evals": r["rhs_evals"], "t": r["t"],
+                    "attempts_per_s": r["attempts"] / gpu_s}}
+    if not args.no_cpu:
+        ids, umk = eng.tuples(0)
+        m = min(len(umk), 200_000)
+        o = oracle.Oracle(mat, enumerate_tuples=False, nthreads=os.cpu_count())
+        o.set_tuples(0, ids[:m], umk[:m])
+        o.channel_propagate(0, f0, 0, min(m, 1000))   # warm-up
+        samples = []
+        for _ in range(3):
+            a = time.perf_counter()
+            o.channel_propagate(0, f0, 0, m)
+            samples.append((time.perf_counter() - a) * len(umk) / m)
+        t_rhs = statistics.median(samples)
+        line["cpu_oracle"] = {"seconds_per_rhs": t_rhs, "cores": os.cpu_count(), "kind": "port",
+                              "sample": "first %d of %d tuples, scaled; median of 3" % (m, len(umk)),
+                              "projected_seconds": t_rhs * r["rhs_evals"]}
+        line["gpu_vs_cpu"] = line["cpu_oracle"]["projected_seconds"] / gpu_s
+    c = clk.summary()
+    if c:
+        line["clocks"] = c
+    print(json.dumps(line), flush=True)
+    eng.close()
+
+
 def rhs_only(args):
     """Profiling driver: K right-hand-side evaluations (collision + drift +
     M^-1) of the workload on the device, nothing else (used for the ncu
@@ -580,11 +632,16 @@ def main():
                     help="profiling driver: K RHS evaluations only (with --batch R: R runs of mesh --mesh)")
     ap.add_argument("--mesh", type=int, default=N_MESH, help="sections per side (profiling driver only)")
     ap.add_argument("--batch", type=int, default=0, help="batched ensemble of this many runs (per-run N, kT, couplings)")
+    ap.add_argument("--small-ee", action="store_true",
+                    help="16x16 one-band e-e integration to t = 10 (the reference's CPU-runnable case) vs the oracle")
     ap.add_argument("--shard", action="store_true",
                     help="one run with its tuples split over the ranks (NCCL all-reduce per RHS) instead of replicas")
     ap.add_argument("--adjoint", type=int, default=-1,
                     help="adjoint gradient of the 32x32 workload, checked in this many FD directions")
     args = ap.parse_args()
+    if args.small_ee:
+        small_ee(args)
+        return
     if args.adjoint >= 0:
         adjoint(args)
         return
