@@ -395,11 +395,11 @@ def batched_measure(n_runs, steps, warmup, mixed, layout_name="auto", tune=True)
             uniq[N] = sum(be.channel_info(be.chan0[r] + c)["n_tuples"] for c in range(len(m.channels)))
     layouts = sorted({be.channel_info(c)["layout"] for c in range(be.channel_count())})
     # (stages, instance schedule, groups): schedule 0 one instance per thread,
-    # 1 instance pairs, 2 run-minor
+    # 1 instance pairs, 2 / 3 / 4 run-minor with 32 / 8 / 4 runs per lane group
     cnt = {}
     for c in range(be.channel_count()):
         sc = be.schedule(c)
-        k = (sc["stages"], 2 if sc["runs"] else sc["pair"])
+        k = (sc["stages"], {32: 2, 8: 3, 4: 4}[sc["runs"]] if sc["runs"] else sc["pair"])
         cnt[k] = cnt.get(k, 0) + 1
     scheds = [[k[0], k[1], v] for k, v in sorted(cnt.items())]
     ndofs = be.ndofs

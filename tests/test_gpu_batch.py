@@ -118,7 +118,9 @@ def test_autotuned_schedule_gives_the_same_operator(gpu_lib):
 @pytest.mark.parametrize("layout", [E.LAYOUT_T64, E.LAYOUT_T40, E.LAYOUT_T32])
 def test_run_minor_contraction_equals_individual_runs(gpu_lib, layout):
     """Groups shared by 16 runs or more take the run-minor contraction (one
-    warp per tuple, one lane per run, f and the results staged run-minor).
+    lane per run, lane groups of 8 runs by default, f and the results staged
+    run-minor); every other schedule, pinned with tb_set_channel_schedule,
+    gives the same operator.
     40 runs of two structures (4x4 and 6x6, about 20 runs each, so the second
     chunk of 32 lanes is partly idle): every run's RHS equals its RHS alone to
     1e-12, and a short DP45 integration reproduces every run's own
@@ -126,12 +128,21 @@ def test_run_minor_contraction_equals_individual_runs(gpu_lib, layout):
     off (amplitudes 0), its lane emits nothing."""
     mats, states = W.ensemble_runs(40, seed=7, Ns=(4, 6))
     be = E.BatchEngine(mats, layout=layout)
-    assert all(be.schedule(c)["runs"] for c in range(be.channel_count()))
+    assert all(be.schedule(c)["runs"] == 8 for c in range(be.channel_count()))
     f = np.concatenate(states)
-    got = be.split(be.rhs(f))
     singles = [E.Engine(m, layout=layout) for m in mats]
-    for e1, x, g in zip(singles, states, got):
-        assert rel_l2(g, e1.rhs(x)) < 1e-12
+    refs = [e1.rhs(x) for e1, x in zip(singles, states)]
+    # every pinned schedule: lane groups of 32 / 8 / 4 runs, the per-thread
+    # paths, one or two bulk-copy stages
+    for stages in (1, 2):
+        for kw in ({"runs": 32}, {"runs": 8}, {"runs": 4}, {"pair": 0}, {"pair": 1}):
+            for c in range(be.channel_count()):
+                be.set_schedule(c, stages, **kw)
+            got = be.split(be.rhs(f))
+            for g, ref in zip(got, refs):
+                assert rel_l2(g, ref) < 1e-12, (stages, kw)
+    for c in range(be.channel_count()):
+        be.set_schedule(c, 1, runs=8)
     res = be.dp45(f, 0.0, 0.05, 0.025)
     for r in (0, 1, 17, 39):
         ref = singles[r].dp45(states[r], 0.0, 0.05, 0.025)

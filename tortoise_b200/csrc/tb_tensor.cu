@@ -633,7 +633,11 @@ __device__ __forceinline__ void contract_run(const ChanDev& c, const RunsDev& R,
 // DEC (40-bit moments): the staged tile is widened once, cooperatively, into
 // an FP64 copy that the contraction reads; the stage is refilled at once, so
 // one stage already overlaps the next copy with the contraction.
-template <int L, int KIND, int TT, int STAGES>
+// S runs per lane group: a warp takes 32 / S tuples at a time, each for S
+// runs, so a group of n runs pads to a multiple of S rather than of 32; each
+// instruction still serves 32 lanes, the moment reads hit 32 / S adjacent
+// words and every f row / reduction stays whole 32-byte sectors (S >= 4).
+template <int L, int KIND, int TT, int STAGES, int S>
 __global__ void __launch_bounds__(RUNS_THREADS) k_collision_runs(ChanDev c, const InstDev* __restrict__ insts,
                                                                  int n_insts, RunsDev R,
                                                                  const unsigned char* __restrict__ mom, int64_t ntiles,
@@ -648,6 +652,8 @@ __global__ void __launch_bounds__(RUNS_THREADS) k_collision_runs(ChanDev c, cons
     constexpr int NW = RUNS_THREADS / 32;
     static_assert(TT % NW == 0, "tile tuples must split evenly over the warps");
     constexpr int TPW = TT / NW;
+    constexpr int G = 32 / S;   // tuples per warp step
+    static_assert(TPW % G == 0, "a warp's tuples must split into steps of 32 / S");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char* stage_buf = smem_raw;
     double* dec = reinterpret_cast<double*>(smem_raw + size_t(STAGES) * TILE_BYTES);
@@ -684,7 +690,8 @@ __global__ void __launch_bounds__(RUNS_THREADS) k_collision_runs(ChanDev c, cons
             }
         }
     }
-    const int nch = R.np >> 5;
+    const int nch = (n_insts + S - 1) / S;   // nch * S <= np (np: a multiple of 32)
+    const int g = lane / S, sl = lane % S;
     for (int64_t it = 0;; ++it) {
         const int64_t tile = blockIdx.x + it * gridDim.x;
         if (tile >= ntiles) break;
@@ -717,20 +724,22 @@ __global__ void __launch_bounds__(RUNS_THREADS) k_collision_runs(ChanDev c, cons
             refill();
             rd = reinterpret_cast<const unsigned char*>(dec);
         }
-        // warp w: tuples [w TPW, (w+1) TPW) of the tile, each for every
-        // chunk of 32 instances
+        // warp w: tuples [w TPW, (w+1) TPW) of the tile, G at a time (lane
+        // group g takes tuple tt + g), each for every chunk of S instances;
+        // lanes past the list's end contract element 0 with amplitude 0
 #pragma unroll 1
-        for (int tt = 0; tt < TPW; ++tt) {
-            const int t = warp * TPW + tt;
+        for (int tt = 0; tt < TPW; tt += G) {
+            if (tile * TT + warp * TPW + tt >= n) break;   // uniform in the warp
+            const int t = warp * TPW + tt + g;
             const int64_t gi = tile * TT + t;
-            if (gi >= n) break;   // uniform in the warp
+            const bool tv = gi < n;
             int e[L];
 #pragma unroll
-            for (int l = 0; l < L; ++l) e[l] = __ldg(tup + l * stride + gi);
+            for (int l = 0; l < L; ++l) e[l] = tv ? __ldg(tup + l * stride + gi) : 0;
 #pragma unroll 1
             for (int ch = 0; ch < nch; ++ch) {
-                const int i = (ch << 5) + lane;
-                const double amp = s_amp[i];
+                const int i = ch * S + sl;
+                const double amp = tv ? s_amp[i] : 0.0;
                 if (__all_sync(0xffffffffu, amp == 0.0)) continue;
                 contract_run<L, KREAD, TT>(c, R, e, t, i, amp, rd);
             }
@@ -804,7 +813,7 @@ static RunsDev runs_dev(const ChanDev& c, const MomentTensor& T) {
 }
 
 // gather -> run-minor contraction -> scatter (three launches on s)
-template <int L, int KIND, int STAGES>
+template <int L, int KIND, int STAGES, int S>
 static int launch_runs(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T, const int32_t* tup,
                        int64_t stride, int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s) {
     constexpr int TT = TTile<L, KIND>::TT;
@@ -814,7 +823,7 @@ static int launch_runs(const ChanDev& c, const InstDev* insts, int n_insts, cons
     const dim3 tb(32, 8), tg(unsigned((maxd + 31) / 32), unsigned(T.np / 32), unsigned(L));
     k_runs_gather<<<tg, tb, 0, s>>>(insts, n_insts, R, f);
     TB_CUDA(cudaGetLastError());
-    auto kern = k_collision_runs<L, KIND, TT, STAGES>;
+    auto kern = k_collision_runs<L, KIND, TT, STAGES, S>;
     const size_t fixed = size_t(STAGES) * TT * tuple_bytes(L, KIND) +
                          (KIND == TK_F40 ? sizeof(double) * TDim<L>::NMOM * TT : 0);
     const size_t smem = fixed + sizeof(double) * size_t(T.np);
@@ -870,7 +879,7 @@ int prepare_runs(const ChanDev& c, int n_insts, bool distinct_runs, MomentTensor
     TB_CUDA(cudaMemsetAsync(T.accT, 0, bytes, s));
     T.np = np;
     T.runs_distinct = distinct_runs ? 1 : 0;
-    T.runs = n_insts >= RUNS_DEFAULT_MIN ? 1 : 0;
+    T.runs = n_insts >= RUNS_DEFAULT_MIN ? 8 : 0;
     return TB_OK;
 }
 
@@ -912,9 +921,12 @@ static int launch_t(const ChanDev& c, const InstDev* insts, int n_insts, const M
     if (rate_leg >= 0)   // diagnostic operator: one fixed schedule
         return launch_variant<L, KIND, 2, false, true>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
     if constexpr (L <= 3) {
-        if (T.runs && T.fT)
-            return T.stages == 1 ? launch_runs<L, KIND, 1>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s)
-                                 : launch_runs<L, KIND, 2>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s);
+        if (T.runs && T.fT) {
+#define TB_RUNS(ST, SS) launch_runs<L, KIND, ST, SS>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s)
+            if (T.stages == 1) return T.runs == 4 ? TB_RUNS(1, 4) : T.runs == 8 ? TB_RUNS(1, 8) : TB_RUNS(1, 32);
+            return T.runs == 4 ? TB_RUNS(2, 4) : T.runs == 8 ? TB_RUNS(2, 8) : TB_RUNS(2, 32);
+#undef TB_RUNS
+        }
     }
     const bool pair = (L <= 3) && n_insts > 1 && T.pair;
     if (T.stages == 1) {
@@ -969,15 +981,16 @@ int tune_tensor(const ChanDev& c, const InstDev* insts, int n_insts, MomentTenso
     double best = 1e300;
     int bs = T.stages, bp = T.pair, br = T.runs;
     const int pairs_max = (c.L <= 3 && n_insts > 1) ? 1 : 0;
-    const int runs_max = T.fT ? 1 : 0;
+    const int runs_max = T.fT ? 3 : 0;
     int rc = TB_OK;
     for (int st = 1; st <= 2 && rc == TB_OK; ++st)
-        for (int pr = 0; pr <= pairs_max + runs_max && rc == TB_OK; ++pr) {
-            // pr: 0 one instance per thread, 1 instance pairs, 2 run-minor
+        for (int pr = 0; pr <= 1 + runs_max && rc == TB_OK; ++pr) {
+            // pr: 0 one instance per thread, 1 instance pairs, 2 / 3 / 4
+            // run-minor with 32 / 8 / 4 runs per lane group
             if (pr == 1 && !pairs_max) continue;
             T.stages = st;
             T.pair = pr == 1;
-            T.runs = pr == 2;
+            T.runs = pr == 2 ? 32 : pr == 3 ? 8 : pr == 4 ? 4 : 0;
             rc = launch_collision_tensor(c, insts, n_insts, T, tup, stride, n, f, acc, nullptr, s);   // warm-up
             if (rc != TB_OK) break;
             constexpr int REPS = 3;

@@ -20,7 +20,8 @@ struct MomentTensor {
     int pair = 1;
     double tuned_seconds = 0.0;   // best measured launch time (0: not tuned)
     // run-minor contraction for a group shared by many runs (k_collision_runs
-    // in tb_tensor.cu): used when runs = 1; the buffers come from prepare_runs
+    // in tb_tensor.cu): runs = the lane-group width (4, 8 or 32 runs per
+    // tuple), 0 = off; the buffers come from prepare_runs
     int runs = 0;
     int np = 0;                   // instances rounded up to a multiple of 32
     int runs_distinct = 0;        // every instance belongs to another run
@@ -41,7 +42,7 @@ int launch_collision_tensor(const ChanDev& c, const InstDev* insts, int n_insts,
                             const DPCtl* ctl, cudaStream_t s, int rate_leg = -1);
 
 // Buffers of the run-minor contraction for a group of n_insts instances
-// (legs <= 3, 8 <= n_insts <= 1024); sets runs = 1 from 16 instances on.
+// (legs <= 3, 8 <= n_insts <= 1024); sets runs = 8 from 16 instances on.
 // Does nothing for other groups, or when the device memory is short.
 int prepare_runs(const ChanDev& c, int n_insts, bool distinct_runs, MomentTensor& T, cudaStream_t s);
 

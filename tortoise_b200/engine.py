@@ -91,6 +91,7 @@ def lib():
                                             C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int64]
         L.tb_channel_schedule.argtypes = [vp, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                           C.POINTER(C.c_double)]
+        L.tb_set_channel_schedule.argtypes = [vp, C.c_int, C.c_int32, C.c_int32]
         L.tb_create_batch.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int, C.POINTER(Options)]
         L.tb_num_runs.argtypes = [vp]
         L.tb_run_info.argtypes = [vp, C.c_int, C.POINTER(i64), C.POINTER(i64), C.POINTER(C.c_int32),
@@ -199,10 +200,17 @@ class Engine:
             raise ValueError("a shard id has %d bytes" % SHARD_ID_BYTES)
         _check(lib().tb_shard_connect(self.h, bytes(unique_id), float(timeout_s)), "tb_shard_connect")
 
+    def set_schedule(self, ch, stages, pair=0, runs=0):
+        """Pins the contraction schedule of channel ch's group (tb_set_channel_schedule):
+        runs = 32, 8 or 4 selects the run-minor contraction, else pair = 0 or 1."""
+        code = {32: 2, 8: 3, 4: 4}[runs] if runs else int(pair)
+        _check(lib().tb_set_channel_schedule(self.h, ch, int(stages), code), "tb_set_channel_schedule")
+
     def schedule(self, ch):
         st, pr, sec = C.c_int32(), C.c_int32(), C.c_double()
         _check(lib().tb_channel_schedule(self.h, ch, C.byref(st), C.byref(pr), C.byref(sec)), "tb_channel_schedule")
-        return {"stages": st.value, "pair": int(pr.value == 1), "runs": int(pr.value == 2),
+        # runs: run-minor lane-group width (32, 8 or 4 runs per tuple), 0 = off
+        return {"stages": st.value, "pair": int(pr.value == 1), "runs": {2: 32, 3: 8, 4: 4}.get(pr.value, 0),
                 "tuned_seconds": sec.value}
 
     def tuples(self, ch):
