@@ -218,8 +218,33 @@ int tb_channel_propagate(tb_handle* h, int ch, const double* f, double* out, int
  * value per run: result[n_runs]. */
 int tb_relative_error(tb_handle* h, const double* err, const double* pop, double* result, int flags);
 
-/* MaterialStatus::applyConstraints for time-independent constraints. */
+/* MaterialStatus::applyConstraints for time-independent constraints (refused
+ * while a constraint callback is set: use tb_apply_constraints_at). */
 int tb_apply_constraints(tb_handle* h, double* f, int flags);
+
+/* Time-dependent constrained populations: Band::constrainedPopulation
+ * (include/Physics/Material/Band.hpp:70-74), a std::function<Function(Real)>
+ * in the reference, as a C callback.  fn(user, band, t, population) writes the
+ * Ne*3 linear-form coefficients of constrained band `band` (global band index)
+ * at time t and returns 0 (non-zero: failure, the integration stops with
+ * TB_ERR_ARG).  While it is set, every enforceValue of the integrator
+ * (MaterialStatus::applyConstraints(time), MaterialStatus.cpp:198-206) takes
+ * the constrained bands from it -- at the stage times t + c_i dt, at t + dt and
+ * at the dense-output times -- and MaterialTimeStatus::timeStepVetoer
+ * (src/Physics/Status/MaterialTimeStatus.cpp:60-100) limits the step at the
+ * start and after every accepted step, as DormandPrince54.hpp:554, 638-640 do.
+ * The callback runs on a CUDA host thread between the kernels of an attempt:
+ * it must not call CUDA.  At most TB_TC_DENSE_PER_STEP dense outputs per step
+ * (TB_ERR_CAPACITY beyond).  The adjoint and tb_dp45_replay refuse a handle
+ * with a callback.  fn = NULL returns to the constant populations of the
+ * description. */
+typedef int (*tb_constraint_fn)(void* user, int32_t band, double t, double* population);
+#define TB_TC_DENSE_PER_STEP 8
+int tb_set_constraint_fn(tb_handle* h, tb_constraint_fn fn, void* user);
+
+/* MaterialStatus::applyConstraints(t): the constrained bands of f take their
+ * populations at time t (the callback's, else the constant ones). */
+int tb_apply_constraints_at(tb_handle* h, double* f, double t, int flags);
 
 /* Dormand-Prince 5(4) from t0 to t_final with dense output every dense_step,
  * entirely on the device: Algorithms::dormandPrince54 (include/Generics/

@@ -56,6 +56,11 @@ def lib():
                               C.POINTER(C.c_int), C.c_int, C.c_int, i64, C.POINTER(i64), dp]
         L.or_dp45_replay.argtypes = [vp, dp, dp, i64, C.c_double, dp, C.c_int, C.c_int]
         L.or_scattering_rates.argtypes = [vp, C.c_int, C.c_int, dp, dp, C.c_int]
+        L.or_set_constraint_fn.argtypes = [vp, C.c_void_p, vp]
+        L.or_apply_constraints_at.restype = C.c_int
+        L.or_apply_constraints_at.argtypes = [vp, dp, C.c_double]
+        L.or_veto_step.restype = C.c_double
+        L.or_veto_step.argtypes = [vp, C.c_double, C.c_double, C.c_double]
         _lib = L
     return _lib
 
@@ -66,6 +71,23 @@ def _dp(a):
 
 def _ip(a):
     return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+# int fn(void* user, int32 band, double t, double* population[Ne*3])
+CONSTRAINT_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_double, C.POINTER(C.c_double))
+
+
+def constraint_callback(material, fn):
+    """A C callback filling band b's coefficients with fn(b, t) (0 = success)."""
+    sizes = [b.mesh.ne * 3 for b in material.bands]
+
+    def cb(user, band, t, out):
+        try:
+            np.ctypeslib.as_array(out, shape=(sizes[band],))[:] = fn(int(band), float(t))
+            return 0
+        except Exception:
+            return 1
+    return CONSTRAINT_FN(cb)
 
 
 class Oracle:
@@ -79,6 +101,9 @@ class Oracle:
         if not self.h:
             raise RuntimeError("oracle: " + lib().or_last_error().decode())
         self.ndofs = lib().or_num_dofs(self.h)
+        bands = material.bands
+        if any(b.constrained and callable(b.constrainedPopulation) for b in bands):
+            self.set_constraint(lambda b, t: bands[b].population_at(t))
 
     def __del__(self):
         try:
@@ -115,6 +140,21 @@ class Oracle:
 
     def set_amplitude(self, ch, a):
         lib().or_set_amplitude(self.h, ch, float(a))
+
+    def set_constraint(self, fn):
+        """Time-dependent constrained populations: fn(band, t) -> Ne*3
+        coefficients for every constrained band (None: the constant ones)."""
+        self._cfn = None if fn is None else constraint_callback(self.material, fn)
+        lib().or_set_constraint_fn(self.h, C.cast(self._cfn, C.c_void_p) if self._cfn else None, None)
+
+    def apply_constraints_at(self, f, t):
+        f = np.ascontiguousarray(f, dtype=np.float64).copy()
+        if lib().or_apply_constraints_at(self.h, _dp(f), float(t)) != 0:
+            raise RuntimeError("oracle: " + lib().or_last_error().decode())
+        return f
+
+    def veto_step(self, t, dt, dense):
+        return lib().or_veto_step(self.h, float(t), float(dt), float(dense))
 
     def channel_propagate(self, ch, f, t0=0, t1=-1, inverse_mass=True, out=None):
         f = np.ascontiguousarray(f, dtype=np.float64)

@@ -200,6 +200,11 @@ struct Channel {
     int64_t n_prefilter = 0, n_det = 0;
 };
 
+// Time-dependent constrained populations (Band::constrainedPopulation, a
+// std::function<Function(Real)> in the reference, Band.hpp:70-74): a callback
+// filling band `band`'s Ne*3 linear-form coefficients at time t; 0 = success.
+typedef int (*or_constraint_fn)(void* user, int32_t band, double t, double* population);
+
 struct Problem {
     tb_region region;
     std::vector<Mesh> meshes;
@@ -207,6 +212,8 @@ struct Problem {
     std::vector<Channel> chans;
     std::vector<int64_t> off;  // band offsets into the status vector
     int64_t ndofs = 0;
+    or_constraint_fn cfn = nullptr;   // null: the time-independent cpop of each band
+    void* cuser = nullptr;
 };
 
 // -------------------------------------------------- delta-constrained geometry
@@ -787,6 +794,90 @@ static void apply_constraints(const Problem& P, double* f) {
             std::copy(P.bands[b].cpop.begin(), P.bands[b].cpop.end(), f + P.off[b]);
 }
 
+// MaterialStatus::applyConstraints(time): every constrained band takes
+// constrainedPopulation(t) -- the callback when one is set.
+static void apply_constraints_at(const Problem& P, double t, double* f) {
+    if (!P.cfn) { apply_constraints(P, f); return; }
+    for (size_t b = 0; b < P.bands.size(); ++b)
+        if (P.bands[b].constrained && P.cfn(P.cuser, int32_t(b), t, f + P.off[b]) != 0)
+            throw std::runtime_error("constraint callback failed");
+}
+
+// Function<2> element-wise operations as the reference evaluates them
+// (Function.cpp:75-80, 152-159, 172-175, 338-341): + - and scalar * act on
+// the linear-form coefficients, Function + scalar on c0 only, fabs and
+// Function / Function go to the nodal values and back, max() is the largest
+// nodal value.
+static void fn_fabs(const double* c, double* out, int64_t ne) {
+    for (int64_t e = 0; e < ne; ++e) {
+        double n[3];
+        to_nodal(c + 3 * e, n);
+        for (int k = 0; k < 3; ++k) n[k] = std::fabs(n[k]);
+        to_lin(n, out + 3 * e);
+    }
+}
+
+// MaterialTimeStatus::timeStepVetoer, MaterialTimeStatus.cpp:60-100: the
+// largest step from times[0] such that every constrained band stays, at the
+// dense-step probes inside each stage interval, within 1.3 |left - right| +
+// atol + rtol |average| of the interval's average (nodally).
+static double veto_step(const Problem& P, const double* times, int ntimes, double dense) {
+    double critical = times[ntimes - 1];
+    bool found = false;
+    for (size_t b = 0; b < P.bands.size() && !found; ++b) {
+        const Band& bd = P.bands[b];
+        if (!bd.constrained) continue;
+        const int64_t ne = P.meshes[bd.mesh].ne, n = 3 * ne;
+        std::vector<double> left(n), right(n), avg(n), acc(n), tmp(n), tmp2(n), mid(n);
+        auto pop = [&](double t, double* out) {
+            if (P.cfn) {
+                if (P.cfn(P.cuser, int32_t(b), t, out) != 0) throw std::runtime_error("constraint callback failed");
+            } else {
+                std::copy(bd.cpop.begin(), bd.cpop.end(), out);
+            }
+        };
+        double tt = times[0] + dense;
+        pop(times[0], left.data());
+        pop(times[1], right.data());
+        for (int i = 0; i < ntimes - 1 && !found; ++i) {
+            if (i != 0) {
+                left.swap(right);
+                pop(times[i + 1], right.data());
+            }
+            for (int64_t k = 0; k < n; ++k) avg[k] = 0.5 * (left[k] + right[k]);
+            // (1 + 0.3) fabs(left - right) + atol + rtol fabs(avg)
+            for (int64_t k = 0; k < n; ++k) tmp[k] = left[k] - right[k];
+            fn_fabs(tmp.data(), tmp2.data(), ne);
+            for (int64_t k = 0; k < n; ++k) acc[k] = (1. + 0.3) * tmp2[k];
+            for (int64_t e = 0; e < ne; ++e) acc[3 * e] += bd.abs_tol;
+            fn_fabs(avg.data(), tmp2.data(), ne);
+            for (int64_t k = 0; k < n; ++k) acc[k] = acc[k] + bd.rel_tol * tmp2[k];
+            while (tt < times[i + 1]) {
+                pop(tt, mid.data());
+                for (int64_t k = 0; k < n; ++k) tmp[k] = mid[k] - avg[k];
+                fn_fabs(tmp.data(), tmp2.data(), ne);
+                double mx = -INFINITY;
+                for (int64_t e = 0; e < ne; ++e) {
+                    double a[3], q[3], r[3], lin[3];
+                    to_nodal(tmp2.data() + 3 * e, a);
+                    to_nodal(acc.data() + 3 * e, q);
+                    for (int k = 0; k < 3; ++k) r[k] = a[k] / q[k];
+                    to_lin(r, lin);   // the quotient is stored in linear form ...
+                    to_nodal(lin, r); // ... and max() reads it back nodally
+                    for (int k = 0; k < 3; ++k) mx = std::max(mx, r[k]);
+                }
+                if (mx > 1.) {
+                    critical = tt;
+                    found = true;
+                    break;
+                }
+                tt += dense;
+            }
+        }
+    }
+    return critical - times[0];
+}
+
 // --------------------------------------------------------------------- DP54
 // Algorithms::dormandPrince54 (3rd overload), DormandPrince54.hpp:479-665,
 // driven as MaterialTimeStatus::propagate does (MaterialTimeStatus.cpp:102-137).
@@ -798,11 +889,13 @@ struct DPStats {
     int failed = 0;
 };
 
-template <class RHS, class ENF, class NORM>
+// enforce_fn(t, v) is enforceValue at time t; veto_fn(times[6]) the
+// timeStepVetoer (applied at the start and after every accepted step).
+template <class RHS, class ENF, class NORM, class VETO>
 static int dp54_core(int64_t n, double* y_io, double t0, double tf, double dense, double* dense_out,
                      double* dense_t, int max_dense, int* n_dense, int64_t max_attempts, DPStats& st, RHS rhs_fn,
-                     ENF enforce_fn, NORM norm_fn) {
-    // stage times c2..c5 only enter through timeOp's unused time argument
+                     ENF enforce_fn, NORM norm_fn, VETO veto_fn) {
+    const double c2 = 1. / 5., c3 = 3. / 10., c4 = 4. / 5., c5 = 8. / 9.;
     const double a21 = 1. / 5., a31 = 3. / 40., a32 = 9. / 40., a41 = 44. / 45., a42 = -56. / 15., a43 = 32. / 9.,
                  a51 = 19372. / 6561., a52 = -25360. / 2187., a53 = 64448. / 6561., a54 = -212. / 729.,
                  a61 = 9017. / 3168., a62 = -355. / 33., a63 = 46732. / 5247., a64 = 49. / 176.,
@@ -819,39 +912,43 @@ static int dp54_core(int64_t n, double* y_io, double t0, double tf, double dense
     double olderror = 1.0;
     *n_dense = 0;
     auto f_rhs = [&](const double* in, double* out) { rhs_fn(in, out); ++st.rhs_evals; };
-    auto enforce = [&](double* v) { enforce_fn(v); };
+    auto enforce = [&](double tt, double* v) { enforce_fn(tt, v); };
+    auto veto = [&]() {
+        const double times[6] = {t, t + c2 * dt, t + c3 * dt, t + c4 * dt, t + c5 * dt, t + dt};
+        dt = std::min(dt, veto_fn(times));
+    };
     // k1 = timeOp(t, enforceValue(t, y))
     std::copy(y.begin(), y.end(), tmp.begin());
-    enforce(tmp.data());
+    enforce(t, tmp.data());
     f_rhs(tmp.data(), k1.data());
-    dt = std::min(dt, (t + dt) - t);
+    veto();
     // Expression templates of the reference evaluate currentY + (a*dt)*k1 + ...
     // left to right; the same order is used here.
     while (t < tf && notfailed) {
         if (max_attempts > 0 && st.attempts >= max_attempts) break;
         ++st.attempts;
         for (int64_t i = 0; i < n; ++i) tmp[i] = y[i] + (a21 * dt) * k1[i];
-        enforce(tmp.data()); f_rhs(tmp.data(), k2.data());
+        enforce(t + c2 * dt, tmp.data()); f_rhs(tmp.data(), k2.data());
         for (int64_t i = 0; i < n; ++i) tmp[i] = y[i] + (a31 * dt) * k1[i] + (a32 * dt) * k2[i];
-        enforce(tmp.data()); f_rhs(tmp.data(), k3.data());
+        enforce(t + c3 * dt, tmp.data()); f_rhs(tmp.data(), k3.data());
         for (int64_t i = 0; i < n; ++i) tmp[i] = y[i] + (a41 * dt) * k1[i] + (a42 * dt) * k2[i] + (a43 * dt) * k3[i];
-        enforce(tmp.data()); f_rhs(tmp.data(), k4.data());
+        enforce(t + c4 * dt, tmp.data()); f_rhs(tmp.data(), k4.data());
         for (int64_t i = 0; i < n; ++i)
             tmp[i] = y[i] + (a51 * dt) * k1[i] + (a52 * dt) * k2[i] + (a53 * dt) * k3[i] + (a54 * dt) * k4[i];
-        enforce(tmp.data()); f_rhs(tmp.data(), k5.data());
+        enforce(t + c5 * dt, tmp.data()); f_rhs(tmp.data(), k5.data());
         for (int64_t i = 0; i < n; ++i)
             tmp[i] = y[i] + (a61 * dt) * k1[i] + (a62 * dt) * k2[i] + (a63 * dt) * k3[i] + (a64 * dt) * k4[i] +
                      (a65 * dt) * k5[i];
-        enforce(tmp.data()); f_rhs(tmp.data(), k6.data());
+        enforce(t + dt, tmp.data()); f_rhs(tmp.data(), k6.data());
         for (int64_t i = 0; i < n; ++i)
             y5[i] = y[i] + (dt * b1) * k1[i] + (dt * b3) * k3[i] + (dt * b4) * k4[i] + (dt * b5) * k5[i] +
                     (dt * b6) * k6[i];
-        enforce(y5.data());
+        enforce(t + dt, y5.data());
         f_rhs(y5.data(), k7.data());
         for (int64_t i = 0; i < n; ++i)
             tmp2[i] = y[i] + (dt * bh1) * k1[i] + (dt * bh3) * k3[i] + (dt * bh4) * k4[i] + (dt * bh5) * k5[i] +
                       (dt * bh6) * k6[i] + (dt * bh7) * k7[i];
-        enforce(tmp2.data());
+        enforce(t + dt, tmp2.data());
         for (int64_t i = 0; i < n; ++i) err[i] = y5[i] - tmp2[i];
         const double errNorm = norm_fn(err.data(), y5.data());
         st.last_err = errNorm;
@@ -869,7 +966,7 @@ static int dp54_core(int64_t n, double* y_io, double t0, double tf, double dense
                     for (int64_t i = 0; i < n; ++i)
                         o[i] = y[i] + (s * dt * bt1) * k1[i] + (s * dt * bt3) * k3[i] + (s * dt * bt4) * k4[i] +
                                (s * dt * bt5) * k5[i] + (s * dt * bt6) * k6[i] + (s * dt * bt7) * k7[i];
-                    enforce(o);
+                    enforce(denseTime, o);
                     dense_t[*n_dense] = denseTime;
                 }
                 ++*n_dense;
@@ -886,7 +983,7 @@ static int dp54_core(int64_t n, double* y_io, double t0, double tf, double dense
             }
             if (rejected) dt *= std::min(1.0, scale);
             else dt *= scale;
-            dt = std::min(dt, (t + dt) - t);
+            veto();
             rejected = false;
             olderror = errNorm;
             ++st.accepted;
@@ -965,8 +1062,9 @@ static int dp54(const Problem& P, double* y_io, double t0, double tf, double den
     return dp54_core(
         P.ndofs, y_io, t0, tf, dense, dense_out, dense_t, max_dense, n_dense, max_attempts, st,
         [&](const double* in, double* out) { rhs(P, in, out, nthreads, drift); },
-        [&](double* v) { apply_constraints(P, v); },
-        [&](const double* err, const double* y5) { return relative_error(P, err, y5); });
+        [&](double t, double* v) { apply_constraints_at(P, t, v); },
+        [&](const double* err, const double* y5) { return relative_error(P, err, y5); },
+        [&](const double* times) { return veto_step(P, times, 6, dense); });
 }
 
 // ------------------------------------------------------------ construction
@@ -1135,13 +1233,45 @@ void or_mass_matrix(void* h, int mesh, double* M, double* Minv) {
 
 void or_apply_constraints(void* h, double* f) { apply_constraints(*static_cast<Problem*>(h), f); }
 
+// Time-dependent constrained populations for every constrained band (null:
+// back to the time-independent ones).
+void or_set_constraint_fn(void* h, or_constraint_fn fn, void* user) {
+    Problem& P = *static_cast<Problem*>(h);
+    P.cfn = fn;
+    P.cuser = user;
+}
+
+int or_apply_constraints_at(void* h, double* f, double t) {
+    try {
+        apply_constraints_at(*static_cast<Problem*>(h), t, f);
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return TB_ERR_ARG;
+    }
+    return TB_OK;
+}
+
+// The time-step veto of MaterialTimeStatus::timeStepVetoer for the six stage
+// times of a step of size dt from t (a check of the restatement).
+double or_veto_step(void* h, double t, double dt, double dense) {
+    const double c2 = 1. / 5., c3 = 3. / 10., c4 = 4. / 5., c5 = 8. / 9.;
+    const double times[6] = {t, t + c2 * dt, t + c3 * dt, t + c4 * dt, t + c5 * dt, t + dt};
+    return veto_step(*static_cast<Problem*>(h), times, 6, dense);
+}
+
 // stats: [attempts, accepted, rejected, rhs_evals] and dstats: [t, dt, last_err]
 int or_dp45(void* h, double* y, double t0, double tf, double dense, double* dense_out, double* dense_t,
             int max_dense, int* n_dense, int nthreads, int drift, int64_t max_attempts, int64_t* stats,
             double* dstats) {
     DPStats st;
-    int rc = dp54(*static_cast<Problem*>(h), y, t0, tf, dense, dense_out, dense_t, max_dense, n_dense, nthreads,
+    int rc;
+    try {
+        rc = dp54(*static_cast<Problem*>(h), y, t0, tf, dense, dense_out, dense_t, max_dense, n_dense, nthreads,
                   drift != 0, max_attempts, st);
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return TB_ERR_ARG;
+    }
     stats[0] = st.attempts; stats[1] = st.accepted; stats[2] = st.rejected; stats[3] = st.rhs_evals;
     dstats[0] = st.t; dstats[1] = st.dt; dstats[2] = st.last_err;
     return rc;
@@ -1191,8 +1321,9 @@ int or_dp45_scalar_example(double t0, double y0, double tf, double dense, double
     int rc = dp54_core(
         2, ya, t0, tf, dense, dense2.data(), dense_t, max_dense, n_dense, 0, st,
         [&](const double* in, double* out) { out[0] = std::cos(in[1]); out[1] = 1.0; },
-        [&](double*) {},
-        [&](const double* err, const double*) { return 10000000000000. * err[0] * err[0]; });
+        [&](double, double*) {},
+        [&](const double* err, const double*) { return 10000000000000. * err[0] * err[0]; },
+        [&](const double* times) { return times[5] - times[0]; });
     for (int i = 0; i < std::min(*n_dense, max_dense); ++i) dense_out[i] = dense2[2 * size_t(i)];
     stats[0] = st.attempts; stats[1] = st.accepted; stats[2] = st.rejected; stats[3] = st.rhs_evals;
     (void)y;

@@ -157,3 +157,42 @@ def test_scattering_rates_are_twice_the_affine_slope():
     # the whole-status sum is the sum over channels and legs
     tot = sum(o.scattering_rates(f, ch) for ch in range(len(mat.channels)))
     assert np.allclose(o.scattering_rates(f), tot, rtol=1e-13, atol=0)
+
+
+def test_time_step_veto_of_a_pulsed_bath():
+    """MaterialTimeStatus::timeStepVetoer, restated: a constant or linear
+    constrained history never shortens the step; a Gaussian pulse inside the
+    tested step cuts it at the first dense-step probe that leaves the
+    tolerance band, a whole number of dense steps after t; and a
+    DP45 integration through the pulse takes more attempts than one with the
+    bath held fixed."""
+    import numpy as np
+    from tortoise_b200 import workloads as W
+    from tortoise_b200.model import nodal_to_linform
+    mat = W.pulsed_bath(4)
+    o = oracle.Oracle(mat)
+    ph = mat.bands[2]
+    # well before the pulse: flat history, no veto
+    assert o.veto_step(0.0, 0.01, 0.001) == (0.0 + 0.01) - 0.0
+    # a linear history: the probes sit within half the interval change
+    base = ph.population_at(0.0)
+    o.set_constraint(lambda b, t: base * (1.0 + t))
+    assert o.veto_step(0.05, 0.1, 0.001) == (0.05 + 0.1) - 0.05
+    # the pulse (t 0.12, width 0.02) inside the stage interval [0.09, 0.24]
+    # of a step of 0.3 from 0: the first probe beyond 1.3 |left - right|
+    # (+ tolerances) from the interval average cuts the step there
+    o.set_constraint(lambda b, t: ph.population_at(t))
+    v = o.veto_step(0.0, 0.3, 0.001)
+    assert 0.09 < v < 0.12, v
+    k = v / 0.001
+    assert abs(k - round(k)) < 1e-6, k
+    f0 = W.initial_status(mat, seed=2).vec
+    pulsed = o.dp45(f0, 0.0, 0.3, 0.01)
+    o.set_constraint(lambda b, t: ph.population_at(0.0))
+    flat = o.dp45(f0, 0.0, 0.3, 0.01)
+    assert pulsed["rc"] == 0 and flat["rc"] == 0
+    assert pulsed["attempts"] > flat["attempts"], (pulsed["attempts"], flat["attempts"])
+    # the bath follows the pulse in the dense outputs
+    off = o.band_offset(2)
+    for t, y in zip(pulsed["dense_t"], pulsed["dense"]):
+        assert np.array_equal(y[off:off + ph.mesh.ne * 3], ph.population_at(t))

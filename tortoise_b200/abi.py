@@ -95,7 +95,10 @@ class PackedProblem:
             barr[i].penalisation = b.penalisationUnphysicalPopulation
             barr[i].constrained = 1 if b.constrained else 0
             if b.constrained:
-                cp = np.ascontiguousarray(b.constrainedPopulation, dtype=np.float64)
+                # a time-dependent population is installed as a callback after
+                # creation (tb_set_constraint_fn); the description holds zeros
+                cp = (np.zeros(b.mesh.ne * 3) if callable(b.constrainedPopulation)
+                      else np.ascontiguousarray(b.constrainedPopulation, dtype=np.float64))
                 self._keep.append(cp)
                 barr[i].constrained_population = dptr(cp)
             barr[i].drift_velocity[:] = [float(x) for x in b.drift_velocity]

@@ -26,6 +26,7 @@ SOURCES = {
     "tb_vjp.cu": [],
     "tb_adjoint.cu": [],
     "tb_shard.cu": [],
+    "tb_constraints.cu": [],
 }
 
 

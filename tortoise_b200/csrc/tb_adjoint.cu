@@ -433,6 +433,7 @@ int tb_dp45_replay(tb_handle* h, const double* f0, const double* dts, int64_t n_
                    int flags) {
     if (!h || !f0 || !dts || !f_out || n_steps < 1) { set_error("bad argument"); return TB_ERR_ARG; }
     if (!(dense_s > 0.0) || !(dense_s <= 1.0001)) { set_error("dense_s must lie in (0, 1.0001]"); return TB_ERR_ARG; }
+    if (h->cfn) { set_error("the replay has no time-dependent constraints"); return TB_ERR_ARG; }
     TB_CUDA(cudaSetDevice(h->device));
     TB_TRY(adj_base(h));
     AdjointState* A = h->adj;
@@ -472,6 +473,7 @@ int tb_adjoint_forward(tb_handle* h, const double* f0, double t0, double t1, dou
     if (!h || !f0) { set_error("null argument"); return TB_ERR_ARG; }
     if (h->runs.size() != 1) { set_error("the adjoint integrates single-run handles"); return TB_ERR_ARG; }
     if (checkpoint_every < 1 || max_steps < 1) { set_error("checkpoint_every and max_steps must be >= 1"); return TB_ERR_ARG; }
+    if (h->cfn) { set_error("the adjoint has no time-dependent constraints"); return TB_ERR_ARG; }
     if (!(t1 > t0) || !(dense_step > 0.0) || dense_step > (t1 - t0) * (1.0 + 1e-12)) {
         set_error("need t1 > t0 and 0 < dense_step <= t1 - t0");
         return TB_ERR_ARG;

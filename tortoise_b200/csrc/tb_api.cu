@@ -323,6 +323,9 @@ int build_runs(tb_handle* h, const tb_problem_desc* const* descs, int nruns) {
         bd.penal = B.penal;
         bd.constrained = B.constrained;
         bd.cpop = d_cpop;
+        bd.coff = B.constrained ? h->cdofs : -1;
+        h->coff.push_back(bd.coff);
+        if (B.constrained) h->cdofs += 3 * int64_t(B.ne);
         bd.vel[0] = B.vel[0];
         bd.vel[1] = B.vel[1];
         if (B.vel[0] != 0.0 || B.vel[1] != 0.0) h->any_drift = true;
@@ -630,6 +633,7 @@ int dp_alloc(tb_handle* h, int64_t max_dense) {
 
 int record_attempt(tb_handle* h, int flags) {
     const DPBufs& B = h->dp;
+    if (h->cfn) TB_TRY(tc_record_pre_attempt(h));   // veto + constrained values of this attempt
     TB_TRY(launch_stage(h->ed, B, 0, h->stream));
     for (int s = 1; s <= 5; ++s) {
         TB_TRY(run_rhs_acc(h, B.tmp, B.acc, B.ctl, flags, -1));
@@ -721,6 +725,7 @@ int tb_destroy(tb_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->graph) cudaGraphExecDestroy(h->graph);
     shard_release(h);
+    tc_release(h);
     adjoint_release(h);
     for (auto& G : h->groups) { G.tup.release(); G.tensor.release(); }
     for (double* p : h->dev_allocs) cudaFree(p);
@@ -1021,6 +1026,7 @@ int tb_relative_error(tb_handle* h, const double* err, const double* pop, double
 
 int tb_apply_constraints(tb_handle* h, double* f, int flags) {
     if (!h || !f) { set_error("null argument"); return TB_ERR_ARG; }
+    if (h->cfn) { set_error("the constraints depend on time: use tb_apply_constraints_at"); return TB_ERR_ARG; }
     TB_CUDA(cudaSetDevice(h->device));
     const size_t bytes = sizeof(double) * size_t(h->ndofs);
     if (flags & TB_PTR_HOST) {
@@ -1080,15 +1086,18 @@ int dp_begin(tb_handle* h, const double* f0, const double* t0, const double* t_f
         c.min_step = dense_step[r] / 10000.;
         c.olderror = 1.0;
         c.dt = dense_step[r];
-        c.dt = std::min(c.dt, (c.t + c.dt) - c.t);   // timeStepVetoer with no time-dependent constraints
+        // timeStepVetoer: with no time-dependent constraints it returns
+        // (t + dt) - t; with them tc_begin applies it below
+        if (!h->cfn) c.dt = std::min(c.dt, (c.t + c.dt) - c.t);
         c.dense_cap = max_dense;
         c.rhs_evals = 1;
         c.done = (t0[r] < t_final[r]) ? 0 : 1;
         c.last_dense_step = -1;
     }
+    if (h->cfn) TB_TRY(tc_begin(h));   // values at t0 into slot 0, first dt vetoed
     TB_CUDA(cudaMemcpyAsync(B.ctl, h->h_ctl, sizeof(DPCtl) * nruns, cudaMemcpyHostToDevice, h->stream));
     // k1 = timeOp(t0, enforceValue(t0, y0))
-    TB_TRY(launch_enforce(h->ed, B.y, B.tmp, h->stream));
+    TB_TRY(launch_enforce(h->ed, B.y, B.tmp, h->stream, h->cfn ? h->d_ctv : nullptr));
     TB_CUDA(cudaMemsetAsync(B.acc, 0, bytes, h->stream));
     TB_TRY(run_rhs_acc(h, B.tmp, B.acc, nullptr, rflags, -1));
     TB_TRY(launch_k1(h->ed, B, h->stream));

@@ -110,6 +110,7 @@ struct BandDev {
     double stat, abs_tol, rel_tol, penal;
     int constrained;
     const double* cpop;   // device, [ne*3] or null
+    int64_t coff;         // offset of the band in a slot of time-dependent constrained values (-1: none)
     double vel[2];
 };
 

@@ -37,9 +37,11 @@ __constant__ double c_b[6] = {35. / 384., 0., 500. / 1113., 125. / 192., -2187. 
 __constant__ double c_bh[7] = {5179. / 57600., 0., 7571. / 16695., 393. / 640., -92097. / 339200., 187. / 2100.,
                                1. / 40.};
 
-__device__ __forceinline__ void enforce3(const BandDev& bd, int e, double v[3]) {
+// enforceValue on one element: constrained bands take the slot of
+// time-dependent values cv when given, else their constant population.
+__device__ __forceinline__ void enforce3(const BandDev& bd, int e, double v[3], const double* cv = nullptr) {
     if (bd.constrained) {
-        const double* cp = bd.cpop + 3 * (int64_t)e;
+        const double* cp = (cv ? cv + bd.coff : bd.cpop) + 3 * (int64_t)e;
         v[0] = cp[0]; v[1] = cp[1]; v[2] = cp[2];
     }
 }
@@ -54,6 +56,8 @@ __global__ void __launch_bounds__(256) k_stage(ElemDev ed, DPBufs B) {
     if (ctl.done) return;
     const double dt = ctl.dt;
     const BandDev& bd = ed.bands[band];
+    // slot of the enforce time: t + c_{S+2} dt for S <= 3, t + dt after
+    const double* cv = B.tc ? B.ctv + (S <= 4 ? S : 4) * B.cdofs : nullptr;
     double srel = 0.0, spen = 0.0;
     const int e = (blockIdx.x - ed.blk_first[band]) * blockDim.x + threadIdx.x;
     if (e < bd.ne) {
@@ -76,7 +80,7 @@ __global__ void __launch_bounds__(256) k_stage(ElemDev ed, DPBufs B) {
                 for (int j = 0; j <= S; ++j) t = t + (c_A[S + 1][j] * dt) * B.k[j][o + c];
                 v[c] = t;
             }
-            enforce3(bd, e, v);
+            enforce3(bd, e, v, cv);
 #pragma unroll
             for (int c = 0; c < 3; ++c) B.tmp[o + c] = v[c];
         } else if (S == 5) {
@@ -91,7 +95,7 @@ __global__ void __launch_bounds__(256) k_stage(ElemDev ed, DPBufs B) {
                 t = t + (dt * c_b[5]) * B.k[5][o + c];
                 v[c] = t;
             }
-            enforce3(bd, e, v);
+            enforce3(bd, e, v, cv);
 #pragma unroll
             for (int c = 0; c < 3; ++c) B.y5[o + c] = v[c];
         } else {
@@ -107,7 +111,7 @@ __global__ void __launch_bounds__(256) k_stage(ElemDev ed, DPBufs B) {
                 t = t + (dt * c_bh[6]) * B.k[6][o + c];
                 v[c] = t;
             }
-            enforce3(bd, e, v);
+            enforce3(bd, e, v, cv);
             double err[3], p5[3];
 #pragma unroll
             for (int c = 0; c < 3; ++c) { p5[c] = B.y5[o + c]; err[c] = p5[c] - v[c]; }
@@ -184,6 +188,7 @@ __global__ void k_controller(ElemDev ed, DPBufs B) {
             dtime += c->dense_step;
         }
         if (k > TB_MAX_DENSE_PER_STEP) { c->status = TB_ERR_CAPACITY; k = TB_MAX_DENSE_PER_STEP; }
+        if (B.tc && k > c->tc_ndense) c->status = TB_ERR_CAPACITY;   // a dense time without constrained values
         c->n_now = k;
         c->dense_time = dtime;
         if (k > 0) {
@@ -209,7 +214,10 @@ __global__ void k_controller(ElemDev ed, DPBufs B) {
         }
         if (c->rejected) dt *= fmin(1.0, scale);
         else dt *= scale;
-        dt = fmin(dt, (t + dt) - t);
+        // timeStepVetoer: without time-dependent constraints it returns
+        // (t + dt) - t; with them the host node applies it before the next attempt
+        if (B.tc) c->veto_pending = 1;
+        else dt = fmin(dt, (t + dt) - t);
         c->rejected = 0;
         c->olderror = errNorm;
         c->accepted += 1;
@@ -271,7 +279,14 @@ __global__ void __launch_bounds__(256) k_dense_commit(ElemDev ed, DPBufs B) {
             t = t + (s * dt * bt7) * B.k[6][o + cc];
             v[cc] = t;
         }
-        enforce3(bd, e, v);
+        const double* cv = nullptr;
+        if (B.tc) {
+            // the slot the host filled for this dense time (the controller
+            // flagged TB_ERR_CAPACITY if there is none)
+            for (int m = 0; m < c->tc_ndense; ++m)
+                if (c->tc_dense_t[m] == c->dense_t[k]) { cv = B.ctv + (5 + m) * B.cdofs; break; }
+        }
+        enforce3(bd, e, v, cv);
         double* out = B.dense + run.dense_off + slot * run.ndofs + (o - run.dof_off);
         out[0] = v[0]; out[1] = v[1]; out[2] = v[2];
     }
@@ -330,19 +345,19 @@ int launch_k1(const ElemDev& ed, const DPBufs& B, cudaStream_t st) {
     return TB_OK;
 }
 
-__global__ void k_enforce(ElemDev ed, const double* src, double* dst) {
+__global__ void k_enforce(ElemDev ed, const double* src, double* dst, const double* cv) {
     const int band = ed.blk_band[blockIdx.x];
     const BandDev& bd = ed.bands[band];
     const int e = (blockIdx.x - ed.blk_first[band]) * blockDim.x + threadIdx.x;
     if (e >= bd.ne) return;
     const int64_t o = bd.off + 3 * (int64_t)e;
     double v[3] = {src[o], src[o + 1], src[o + 2]};
-    enforce3(bd, e, v);
+    enforce3(bd, e, v, cv);
     dst[o] = v[0]; dst[o + 1] = v[1]; dst[o + 2] = v[2];
 }
 
-int launch_enforce(const ElemDev& ed, const double* src, double* dst, cudaStream_t st) {
-    k_enforce<<<ed.nblk, 256, 0, st>>>(ed, src, dst);
+int launch_enforce(const ElemDev& ed, const double* src, double* dst, cudaStream_t st, const double* cv) {
+    k_enforce<<<ed.nblk, 256, 0, st>>>(ed, src, dst, cv);
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }

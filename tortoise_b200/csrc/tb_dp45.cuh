@@ -6,6 +6,11 @@
 namespace tb {
 
 #define TB_MAX_DENSE_PER_STEP 64
+// dense outputs per step with time-dependent constraints (TB_ERR_CAPACITY beyond)
+#define TB_TC_DENSE TB_TC_DENSE_PER_STEP
+// slots of time-dependent constrained values per attempt: the stage times
+// t + c2 dt, t + c3 dt, t + c4 dt, t + c5 dt, t + dt, then the dense times
+#define TB_TC_SLOTS (5 + TB_TC_DENSE)
 
 // Controller state, resident in device memory; only the controller kernel
 // writes the scalars, every other kernel reads dt / done / skip / acc_now.
@@ -26,6 +31,10 @@ struct DPCtl {
     long long max_attempts;  // 0 = unbounded
     long long last_dense_step;  // index (among accepted steps) of the step that made the last dense output
     double last_dense_s;        // its dense-output fraction s in (0, 1.0001]
+    // time-dependent constraints (written by the host node before an attempt)
+    int veto_pending;           // an accepted step left timeStepVetoer to the host
+    int tc_ndense;              // dense times with constrained values in this attempt's slots
+    double tc_dense_t[TB_TC_DENSE];
 };
 
 // Per-run layout inside the concatenated state of a batch.
@@ -58,6 +67,11 @@ struct DPBufs {
     double* ckpt;
     long long ckpt_every;
     long long ckpt_cap;
+    // time-dependent constraints (tc = 1): the constrained bands' values at
+    // the attempt's times, [TB_TC_SLOTS][cdofs] (BandDev::coff within a slot)
+    const double* ctv;
+    long long cdofs;
+    int tc;
 };
 
 // Stage kernel s (0..6) of one attempt:
@@ -71,8 +85,9 @@ int launch_controller(const ElemDev& ed, const DPBufs& B, cudaStream_t st);
 int launch_dense_commit(const ElemDev& ed, const DPBufs& B, cudaStream_t st);
 // k1 = M^-1 acc, acc = 0 (first evaluation of an integration).
 int launch_k1(const ElemDev& ed, const DPBufs& B, cudaStream_t st);
-// dst = enforce(src)  (applyConstraints)
-int launch_enforce(const ElemDev& ed, const double* src, double* dst, cudaStream_t st);
+// dst = enforce(src)  (applyConstraints); cv: one slot of time-dependent
+// constrained values, or null for the bands' constant populations
+int launch_enforce(const ElemDev& ed, const double* src, double* dst, cudaStream_t st, const double* cv = nullptr);
 // Band::relativeError partial sums per element block for arbitrary err/pop:
 // part[blk] (relative term), part[nblk + blk] (penalisation term).
 int launch_error_norm(const ElemDev& ed, const double* err, const double* pop, double* part, cudaStream_t st);

@@ -88,6 +88,14 @@ struct tb_handle {
     void* comm = nullptr;
     double comm_timeout = 60.0;
     bool comm_failed = false;
+    // time-dependent constraints (tb_constraints.cu)
+    tb_constraint_fn cfn = nullptr;
+    void* cuser = nullptr;
+    int64_t cdofs = 0;                 // constrained dofs of all runs (one slot)
+    std::vector<int64_t> coff;         // per band: offset in a slot, -1 unconstrained
+    double* d_ctv = nullptr;           // device slots [TB_TC_SLOTS][cdofs]
+    double* h_ctv = nullptr;           // pinned host copy the host node fills
+    tb::DPCtl* h_ctl_tc = nullptr;     // pinned controllers the host node reads and edits
 };
 
 
@@ -107,5 +115,10 @@ int shard_tuples(tb_handle* h, GroupChan& G);          // keep this rank's part 
 int shard_allreduce(tb_handle* h, double* buf, size_t n);   // in-place sum over the ranks (no-op unconnected)
 int stream_wait(tb_handle* h);                         // stream sync, bounded when connected
 void shard_release(tb_handle* h);
+
+// tb_constraints.cu
+int tc_record_pre_attempt(tb_handle* h);   // the host node + copies at the head of the attempt graph
+int tc_begin(tb_handle* h);                // t0 values into slot 0, initial veto of every run's dt
+void tc_release(tb_handle* h);
 
 }  // namespace tb

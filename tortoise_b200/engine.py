@@ -106,6 +106,8 @@ def lib():
                                            dp, C.POINTER(AdjointStats), C.c_int]
         L.tb_adjoint_steps.argtypes = [vp, dp, i64, C.POINTER(i64), dp]
         L.tb_dp45_replay.argtypes = [vp, vp, dp, i64, C.c_double, vp, C.c_int]
+        L.tb_set_constraint_fn.argtypes = [vp, C.c_void_p, vp]
+        L.tb_apply_constraints_at.argtypes = [vp, vp, C.c_double, C.c_int]
         L.tb_shard_range.argtypes = [i64, C.c_int, C.c_int, C.POINTER(i64), C.POINTER(i64)]
         L.tb_shard_unique_id.argtypes = [C.c_char_p]
         L.tb_shard_connect.argtypes = [vp, C.c_char_p, C.c_double]
@@ -124,6 +126,9 @@ def _hp(a):
 
 
 SHARD_ID_BYTES = 128
+
+# tb_constraint_fn: int fn(void* user, int32 band, double t, double* population)
+CONSTRAINT_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_double, C.POINTER(C.c_double))
 
 
 def shard_range(n_tuples, rank, n_ranks):
@@ -164,6 +169,44 @@ class Engine:
         _check(lib().tb_create(C.byref(h), C.addressof(self.packed.desc), C.byref(opts)), "tb_create")
         self.h = h
         self.ndofs = lib().tb_num_dofs(h)
+        self._install_constraints()
+
+    def _bands(self):
+        return list(self.material.bands)
+
+    def _install_constraints(self):
+        """Bands whose constrainedPopulation is a callable of time get it as
+        the handle's constraint callback."""
+        bands = self._bands()
+        if any(b.constrained and callable(b.constrainedPopulation) for b in bands):
+            self.set_constraint(lambda b, t: bands[b].population_at(t))
+
+    def set_constraint(self, fn):
+        """Time-dependent constrained populations (tb_set_constraint_fn):
+        fn(band, t) -> Ne*3 coefficients of constrained band `band` (global
+        index) at time t; None returns to the description's constant ones."""
+        if fn is None:
+            self._cfn = None
+            _check(lib().tb_set_constraint_fn(self.h, None, None), "tb_set_constraint_fn")
+            return
+        sizes = [b.mesh.ne * 3 for b in self._bands()]
+        self.constraint_error = None
+
+        def cb(user, band, t, out):
+            try:
+                np.ctypeslib.as_array(out, shape=(sizes[band],))[:] = fn(int(band), float(t))
+                return 0
+            except Exception as exc:   # reported as TB_ERR_ARG by the library
+                self.constraint_error = exc
+                return 1
+        self._cfn = CONSTRAINT_FN(cb)
+        _check(lib().tb_set_constraint_fn(self.h, C.cast(self._cfn, C.c_void_p), None), "tb_set_constraint_fn")
+
+    def apply_constraints_at(self, f, t):
+        """MaterialStatus::applyConstraints(t) on a host state (returns a copy)."""
+        f = np.ascontiguousarray(f, dtype=np.float64).copy()
+        _check(lib().tb_apply_constraints_at(self.h, _hp(f), float(t), PTR_HOST), "tb_apply_constraints_at")
+        return f
 
     def close(self):
         if getattr(self, "h", None):
@@ -372,6 +415,7 @@ class BatchEngine(Engine):
         self.h = h
         self.ndofs = lib().tb_num_dofs(h)
         self.nruns = len(self.packs)
+        self._install_constraints()
         self.slices, self.chan0 = [], []
         for r in range(self.nruns):
             off, n = C.c_int64(), C.c_int64()
@@ -379,6 +423,9 @@ class BatchEngine(Engine):
             _check(lib().tb_run_info(h, r, C.byref(off), C.byref(n), C.byref(b0), C.byref(c0)), "tb_run_info")
             self.slices.append(slice(off.value, off.value + n.value))
             self.chan0.append(c0.value)
+
+    def _bands(self):
+        return [b for m in self.materials for b in m.bands]
 
     def tuples(self, ch):
         r = max(i for i in range(self.nruns) if self.chan0[i] <= ch)

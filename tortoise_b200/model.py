@@ -153,10 +153,22 @@ class Band:
         self.constrainedPopulation = None
         self.drift_velocity = (0.0, 0.0)
 
-    def constrain(self, population_coeffs):
-        """Band::constrained with a time-independent constrainedPopulation."""
+    def constrain(self, population):
+        """Band::constrained with its constrainedPopulation (Band.hpp:70-74):
+        an array of Ne*3 linear-form coefficients (time-independent, e.g. a
+        reservoir) or a callable t -> coefficients (e.g. a laser pulse); a
+        callable is evaluated by the integrator at every enforce time and drives
+        the time-step veto, as the reference's std::function does."""
         self.constrained = True
-        self.constrainedPopulation = np.ascontiguousarray(population_coeffs, dtype=np.float64)
+        if callable(population):
+            self.constrainedPopulation = population
+        else:
+            self.constrainedPopulation = np.ascontiguousarray(population, dtype=np.float64)
+
+    def population_at(self, t):
+        """constrainedPopulation(t) (the array itself when time-independent)."""
+        p = self.constrainedPopulation
+        return np.ascontiguousarray(p(t) if callable(p) else p, dtype=np.float64)
 
 
 class ScatteringChannel:

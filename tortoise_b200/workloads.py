@@ -69,11 +69,29 @@ def initial_status(mat, kT=0.1, mu=0.3, kT_phonon=0.05, seed=0, bump_amplitude=0
             nod = fd + bump_amplitude * (1.0 - fd) * g
         else:
             if b.constrained:
-                st[b.name] = b.constrainedPopulation
+                st[b.name] = b.population_at(0.0)
                 continue
             nod = 1.0 / (np.exp(E / kT_phonon) - 1.0)
         st[b.name] = nodal_to_linform(nod)
     return st
+
+
+def pulsed_bath(N=6, t_pulse=0.12, width=0.02, kT_base=0.05, kT_peak=0.15, **kw):
+    """Two-band e-ph + drift whose optical-phonon band (hw = 0.2, band 2) is a
+    bath constrained to a Bose population at a temperature that follows a
+    Gaussian pulse in time, kT(t) = kT_base + (kT_peak - kT_base)
+    exp(-((t - t_pulse) / width)^2): a time-dependent constrainedPopulation,
+    as a laser-heated reservoir."""
+    mat = build_material(N, ("P", "D"), (0.2,), ee=False, eph=True, field=(0.1, 0.0), rtol=1e-6, atol=1e-9,
+                         phonon_bath=True, **kw)
+    ph = mat.bands[2]
+    ne = ph.mesh.ne
+
+    def population(t):
+        kT = kT_base + (kT_peak - kT_base) * np.exp(-((t - t_pulse) / width) ** 2)
+        return nodal_to_linform(np.full((ne, 3), 1.0 / (np.exp(0.2 / kT) - 1.0)))
+    ph.constrain(population)
+    return mat
 
 
 # The benchmark workloads, named by what they hold.
