@@ -201,6 +201,22 @@ int tb_channel_info(const tb_handle* h, int ch, int64_t* n_tuples, int64_t* n_pr
                     int32_t* layout);
 /* Copies a channel's tuple list to host memory: ids[n*L] (tuple-major), umk[n]. */
 int tb_get_tuples(const tb_handle* h, int ch, int32_t* ids, int32_t* umk);
+/* A channel's k-dependent matrix element: ScatteringChannel::functAmplitude
+ * (include/Physics/Scattering/ScatteringChannel.hpp:74), evaluated as
+ * constructAmplitude does (src/Physics/Scattering/ScatteringChannel.cpp:
+ * 399-415): once per tuple, at the barycentres of the tuple's elements
+ * (Mesh<2>::elemCentre, src/Geometry/Structured/DirectSpace/Mesh.cpp:533-535),
+ * fullAmplitude = amplitude * volumes * functAmplitude.  fn(user, n, nlegs,
+ * barycentres, out) gets n tuples at a time -- barycentres[(i*nlegs + l)*2 +
+ * {0,1}] = k_x, k_y of leg l's element of tuple i -- writes out[n] and returns
+ * 0.  It is called inside this call only.  The factors belong to the
+ * channel's structure group (every run of a batch that shares the tuple list);
+ * the moment tensor, if any, is rebuilt with them folded in.  As in the
+ * reference, the tuple list itself was chosen with functAmplitude = 1.  fn =
+ * NULL returns to 1.  No state is kept of fn. */
+typedef int (*tb_amplitude_fn)(void* user, int64_t n, int32_t nlegs, const double* barycentres, double* out);
+int tb_set_channel_amplitude_fn(tb_handle* h, int ch, tb_amplitude_fn fn, void* user);
+
 /* ScatteringChannel::amplitude (coupling constant); 0 disables the channel
  * like MaterialStatus::propagate does (MaterialStatus.cpp:149). */
 int tb_set_amplitude(tb_handle* h, int ch, double amplitude);

@@ -57,6 +57,8 @@ def lib():
         L.or_dp45_replay.argtypes = [vp, dp, dp, i64, C.c_double, dp, C.c_int, C.c_int]
         L.or_scattering_rates.argtypes = [vp, C.c_int, C.c_int, dp, dp, C.c_int]
         L.or_set_constraint_fn.argtypes = [vp, C.c_void_p, vp]
+        L.or_set_channel_amplitude_fn.restype = C.c_int
+        L.or_set_channel_amplitude_fn.argtypes = [vp, C.c_int, C.c_void_p, vp]
         L.or_apply_constraints_at.restype = C.c_int
         L.or_apply_constraints_at.argtypes = [vp, dp, C.c_double]
         L.or_veto_step.restype = C.c_double
@@ -104,6 +106,9 @@ class Oracle:
         bands = material.bands
         if any(b.constrained and callable(b.constrainedPopulation) for b in bands):
             self.set_constraint(lambda b, t: bands[b].population_at(t))
+        for ch, c in enumerate(material.channels):
+            if getattr(c, "functAmplitude", None) is not None:
+                self.set_channel_amplitude(ch, c.functAmplitude)
 
     def __del__(self):
         try:
@@ -146,6 +151,16 @@ class Oracle:
         coefficients for every constrained band (None: the constant ones)."""
         self._cfn = None if fn is None else constraint_callback(self.material, fn)
         lib().or_set_constraint_fn(self.h, C.cast(self._cfn, C.c_void_p) if self._cfn else None, None)
+
+    def set_channel_amplitude(self, ch, fn):
+        """functAmplitude of channel ch for its current tuple list:
+        fn(barycentres[n, nlegs, 2]) -> factors[n] (None: 1)."""
+        from tortoise_b200.engine import amplitude_callback
+        errors = []
+        cb = amplitude_callback(fn, errors) if fn is not None else None
+        rc = lib().or_set_channel_amplitude_fn(self.h, ch, C.cast(cb, C.c_void_p) if cb else None, None)
+        if rc != 0:
+            raise errors[0] if errors else RuntimeError("oracle: " + lib().or_last_error().decode())
 
     def apply_constraints_at(self, f, t):
         f = np.ascontiguousarray(f, dtype=np.float64).copy()

@@ -197,6 +197,7 @@ struct Channel {
     std::vector<double> mc, mc_pre;   // [nmc*R]
     std::vector<int32_t> tuples;      // [n*L]
     std::vector<int32_t> tumk;        // [n]
+    std::vector<double> tamp;         // functAmplitude per tuple (empty: 1)
     int64_t n_prefilter = 0, n_det = 0;
 };
 
@@ -470,7 +471,7 @@ static void enumerate(const Problem& P, Channel& c, int nthreads) {
 // of that leg become the constant in / out unit forms and only its block is
 // kept, subtracted with the leg's direction.
 static void single_propagator(const Problem& P, const Channel& c, const double* f, const int32_t* e, int umk,
-                              double* out, int which = -1) {
+                              double* out, int which = -1, double funct_amp = 1.0) {
     const int L = c.L;
     Geom g;
     build_geom(P, c, e, umk, g);
@@ -515,7 +516,7 @@ static void single_propagator(const Problem& P, const Channel& c, const double* 
         }
     }
     const double scale = 1.0 / (factorial_norm(L) * double(c.nmc) * std::fabs(g.det));
-    const double amp = full_amplitude(P, c, c.amplitude);
+    const double amp = full_amplitude(P, c, c.amplitude) * funct_amp;
     for (int l = 0; l < L; ++l) {
         if (which >= 0 && l != which) continue;
         double* o = out + P.off[c.band[l]] + 3 * size_t(e[l]);
@@ -538,7 +539,8 @@ static void channel_propagate_range(const Problem& P, const Channel& c, const do
     auto work = [&](int t) {
         int64_t a = t0 + n * t / nthreads, b = t0 + n * (t + 1) / nthreads;
         for (int64_t i = a; i < b; ++i)
-            single_propagator(P, c, f, &c.tuples[size_t(i) * c.L], c.tumk[size_t(i)], part[t].data(), which);
+            single_propagator(P, c, f, &c.tuples[size_t(i) * c.L], c.tumk[size_t(i)], part[t].data(), which,
+                              c.tamp.empty() ? 1.0 : c.tamp[size_t(i)]);
     };
     std::vector<std::thread> th;
     for (int t = 1; t < nthreads; ++t) th.emplace_back(work, t);
@@ -1182,6 +1184,7 @@ void or_set_tuples(void* h, int ch, int64_t n, const int32_t* ids, const int32_t
     Channel& c = static_cast<Problem*>(h)->chans[ch];
     c.tuples.assign(ids, ids + size_t(n) * c.L);
     c.tumk.assign(umk, umk + size_t(n));
+    static_cast<Problem*>(h)->chans[size_t(ch)].tamp.clear();   // the factors follow the list
 }
 
 void or_set_amplitude(void* h, int ch, double a) { static_cast<Problem*>(h)->chans[ch].amplitude = a; }
@@ -1246,6 +1249,40 @@ int or_apply_constraints_at(void* h, double* f, double t) {
         apply_constraints_at(*static_cast<Problem*>(h), t, f);
     } catch (const std::exception& e) {
         g_err = e.what();
+        return TB_ERR_ARG;
+    }
+    return TB_OK;
+}
+
+// ScatteringChannel::functAmplitude at the element barycentres of every tuple
+// of channel ch (constructAmplitude, ScatteringChannel.cpp:399-415; Mesh<2>::
+// elemCentre, Mesh.cpp:533-535 through Mesh<2>::operator(), Mesh.cpp:503-509),
+// computed for the channel's current tuple list; fn = null: 1.
+typedef int (*or_amplitude_fn)(void* user, int64_t n, int32_t nlegs, const double* barycentres, double* out);
+int or_set_channel_amplitude_fn(void* h, int ch, or_amplitude_fn fn, void* user) {
+    Problem& P = *static_cast<Problem*>(h);
+    Channel& c = P.chans[size_t(ch)];
+    c.tamp.clear();
+    if (!fn) return TB_OK;
+    const int64_t n = int64_t(c.tumk.size());
+    std::vector<double> bary(size_t(n) * c.L * 2);
+    const double r = 0.333333333;
+    for (int64_t i = 0; i < n; ++i)
+        for (int l = 0; l < c.L; ++l) {
+            const Mesh& m = P.meshes[P.bands[c.band[l]].mesh];
+            const int e = c.tuples[size_t(i) * c.L + l];
+            const int sec = e / 2, par = e % 2;
+            const double sx = double(sec % m.nx), sy = double(sec / m.nx);
+            const double px = sx + (kVert[par][1][0] * r + kVert[par][2][0] * r);
+            const double py = sy + (kVert[par][1][1] * r + kVert[par][2][1] * r);
+            double* o = &bary[(size_t(i) * c.L + l) * 2];
+            o[0] = m.origin[0] + (m.dG[0][0] * px + m.dG[0][1] * py);
+            o[1] = m.origin[1] + (m.dG[1][0] * px + m.dG[1][1] * py);
+        }
+    c.tamp.resize(size_t(n));
+    if (n > 0 && fn(user, n, c.L, bary.data(), c.tamp.data()) != 0) {
+        c.tamp.clear();
+        g_err = "amplitude callback failed";
         return TB_ERR_ARG;
     }
     return TB_OK;

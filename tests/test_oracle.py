@@ -196,3 +196,31 @@ def test_time_step_veto_of_a_pulsed_bath():
     off = o.band_offset(2)
     for t, y in zip(pulsed["dense_t"], pulsed["dense"]):
         assert np.array_equal(y[off:off + ph.mesh.ne * 3], ph.population_at(t))
+
+
+def test_funct_amplitude_scales_each_tuple():
+    """ScatteringChannel::functAmplitude, restated: a factor of 1 per tuple
+    leaves the operator bit for bit, 2 doubles it exactly, and the
+    barycentres handed to the function are the element centroids of
+    Mesh<2>::elemCentre (reference point 0.333333333 each way)."""
+    import numpy as np
+    from tortoise_b200 import workloads as W
+    mat = W.build_material(4, ("P", "D"), (0.2,), ee=False, eph=True, rtol=1e-6, atol=1e-9)
+    f = W.initial_status(mat, seed=4).vec
+    o = oracle.Oracle(mat)
+    base = o.rhs(f, drift=False)
+    o.set_channel_amplitude(0, lambda b: np.ones(len(b)))
+    assert np.array_equal(o.rhs(f, drift=False), base)
+    seen = []
+
+    def two(b):
+        seen.append(b.copy())
+        return np.full(len(b), 2.0)
+    o.set_channel_amplitude(0, two)
+    only0 = o.channel_propagate(0, f)
+    o.set_channel_amplitude(0, None)
+    assert np.array_equal(only0, 2.0 * o.channel_propagate(0, f))
+    ids, _ = o.tuples(0)
+    mesh = mat.bands[mat.channels[0].legBandNumber[0]].mesh
+    cent = mesh.vertices().mean(axis=1)            # (ne, 2) element centroids
+    assert np.abs(seen[0][:, 0, :] - cent[ids[:, 0]]).max() < 1e-8

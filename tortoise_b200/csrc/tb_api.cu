@@ -727,7 +727,11 @@ int tb_destroy(tb_handle* h) {
     shard_release(h);
     tc_release(h);
     adjoint_release(h);
-    for (auto& G : h->groups) { G.tup.release(); G.tensor.release(); }
+    for (auto& G : h->groups) {
+        G.tup.release();
+        G.tensor.release();
+        if (G.d_tamp) cudaFree(G.d_tamp);
+    }
     for (double* p : h->dev_allocs) cudaFree(p);
     for (void* p : h->dev_raw) cudaFree(p);
     if (h->dp.dense) cudaFree(h->dp.dense);
@@ -896,6 +900,65 @@ int tb_read_scatt_indices(const char* path, int nlegs, const int32_t* nsplit, in
     }
     std::fclose(fp);
     return rc;
+}
+
+// Mesh<2>::elemCentre (Mesh.cpp:533-535): the point (0.333333333,
+// 0.333333333) of the reference element mapped as Mesh<2>::operator()(elem,
+// refCoord) does (Mesh.cpp:503-509): origin + dG (section + E refCoord), E the
+// element's vertices 1 and 2 in its reference section.
+static void elem_centre(const HostMesh& m, int e, double out[2]) {
+    const double r = 0.333333333;
+    const int s = e / 2, par = e % 2;
+    const double sx = double(s % m.nx), sy = double(s / m.nx);
+    const double px = sx + (kVert[par][1][0] * r + kVert[par][2][0] * r);
+    const double py = sy + (kVert[par][1][1] * r + kVert[par][2][1] * r);
+    out[0] = m.origin[0] + (m.dG[0][0] * px + m.dG[0][1] * py);
+    out[1] = m.origin[1] + (m.dG[1][0] * px + m.dG[1][1] * py);
+}
+
+int tb_set_channel_amplitude_fn(tb_handle* h, int ch, tb_amplitude_fn fn, void* user) {
+    if (!h || ch < 0 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
+    TB_CUDA(cudaSetDevice(h->device));
+    TB_TRY(stream_wait(h));
+    const ChanInst& I = h->insts[ch];
+    GroupChan& G = h->groups[I.group];
+    const int L = G.L;
+    const int64_t n = G.tup.n;
+    if (G.d_tamp) { cudaFree(G.d_tamp); G.d_tamp = nullptr; }
+    G.dev.tamp = nullptr;
+    if (fn && n > 0) {
+        if (cudaMalloc(&G.d_tamp, sizeof(double) * size_t(n)) != cudaSuccess) {
+            G.d_tamp = nullptr;
+            set_error("amplitude table allocation failed");
+            return TB_ERR_OOM;
+        }
+        const HostMesh* lm[TB_MAX_LEGS];
+        for (int l = 0; l < L; ++l) lm[l] = &h->meshes[h->bands[I.band[l]].mesh];
+        const int64_t chunk = int64_t(1) << 20;
+        std::vector<int32_t> ids(size_t(L + 1) * size_t(std::min(n, chunk)));
+        std::vector<double> bary(size_t(std::min(n, chunk)) * L * 2), fac(size_t(std::min(n, chunk)));
+        for (int64_t a = 0; a < n; a += chunk) {
+            const int64_t m = std::min(chunk, n - a);
+            for (int l = 0; l < L; ++l)
+                TB_CUDA(cudaMemcpy(ids.data() + size_t(l) * m, G.tup.d + size_t(l) * G.tup.cap + a,
+                                   sizeof(int32_t) * size_t(m), cudaMemcpyDeviceToHost));
+            for (int64_t i = 0; i < m; ++i)
+                for (int l = 0; l < L; ++l) elem_centre(*lm[l], ids[size_t(l) * m + i], &bary[(size_t(i) * L + l) * 2]);
+            if (fn(user, m, L, bary.data(), fac.data()) != 0) {
+                cudaFree(G.d_tamp);
+                G.d_tamp = nullptr;
+                set_error("amplitude callback failed");
+                return TB_ERR_ARG;
+            }
+            TB_CUDA(cudaMemcpy(G.d_tamp + a, fac.data(), sizeof(double) * size_t(m), cudaMemcpyHostToDevice));
+        }
+        G.dev.tamp = G.d_tamp;
+    }
+    if (G.layout != TB_LAYOUT_MC64 && G.tensor.d)
+        TB_TRY(refill_tensor(G.dev, G.tup.d, G.tup.cap, G.tup.n, G.tensor, h->stream));
+    TB_TRY(stream_wait(h));
+    if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }   // kernels take the channel by value
+    return TB_OK;
 }
 
 int tb_set_amplitude(tb_handle* h, int ch, double amplitude) {

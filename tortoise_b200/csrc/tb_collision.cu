@@ -73,11 +73,14 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* 
                 mg[r] = 32.0 * 1.1102230246251565e-16 * (sc + fabs(a0[r]) + sg);
             }
         }
+        // functAmplitude of this tuple (fullAmplitude = amplitude * volumes * functAmplitude)
+        const double tf = (c.tamp && valid) ? __ldg(c.tamp + i) : 1.0;
         for (int k = 0; k < n_insts; ++k) {
             const InstDev in = insts[k];
             if (in.amp_full == 0.0) continue;
             if (ctl && ctl[in.run].done) continue;
             if (!__any_sync(0xffffffffu, valid)) continue;
+            const double ampt = in.amp_full * tf;
             // commonLinForm0 (A, direct) and commonLinForm1 (B, time reversed),
             // ScatteringChannel.cpp:633-641
             double A[L][3], B[L][3];
@@ -151,13 +154,13 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* 
                 const double d = RATE ? -c.leg[l].dir : c.leg[l].dir;
                 const int64_t key = in.foff[l] + 3 * (int64_t)e[l];
                 if (l < L - 1) {
-                    warp_scatter3(valid ? key : -1, acc + key, d * ((scale * s0) * in.amp_full),
-                                  d * ((scale * sx[l]) * in.amp_full), d * ((scale * sy[l]) * in.amp_full));
+                    warp_scatter3(valid ? key : -1, acc + key, d * ((scale * s0) * ampt),
+                                  d * ((scale * sx[l]) * ampt), d * ((scale * sy[l]) * ampt));
                 } else if (valid) {
                     double* o = acc + key;
-                    atomicAdd(o + 0, d * ((scale * s0) * in.amp_full));
-                    atomicAdd(o + 1, d * ((scale * sx[l]) * in.amp_full));
-                    atomicAdd(o + 2, d * ((scale * sy[l]) * in.amp_full));
+                    atomicAdd(o + 0, d * ((scale * s0) * ampt));
+                    atomicAdd(o + 1, d * ((scale * sx[l]) * ampt));
+                    atomicAdd(o + 2, d * ((scale * sy[l]) * ampt));
                 }
             }
         }

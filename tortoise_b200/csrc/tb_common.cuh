@@ -90,6 +90,9 @@ struct ChanDev {
     double gvec[4];       // region gVec, column-major
     const double* umk;    // [n_umk*2] device
     const double* mc;     // [nmc*R] device
+    // functAmplitude at the tuple's element barycentres, one factor per tuple
+    // of the group's list (ScatteringChannel.cpp:399-415); null: 1
+    const double* tamp = nullptr;
 };
 
 // Mesh data needed by the element-wise kernels.

@@ -23,6 +23,7 @@ struct GroupChan {
     double* d_mc = nullptr;
     double* d_mc_pre = nullptr;
     DeviceTuples tup;             // this handle's part of the list (all of it unless sharded)
+    double* d_tamp = nullptr;     // functAmplitude per tuple of tup (dev.tamp), or null
     int64_t shard_begin = 0;      // index of tup's first tuple in the full list
     int64_t n_total = 0;          // length of the full list
     int64_t diag[3] = {0, 0, 0};

@@ -174,6 +174,7 @@ __global__ void __launch_bounds__(256) k_build_moments(ChanDev c, const int32_t*
                 }
             }
             norm = c.amp_vol / (c.fact * double(c.nmc) * fabs(g.det));
+            if (c.tamp) norm *= __ldg(c.tamp + i);   // functAmplitude folded into the moments
         }
         const int64_t tile = i / TT, pos = i % TT;
         if (KIND == TK_F64) {
@@ -749,6 +750,19 @@ __global__ void __launch_bounds__(RUNS_THREADS) k_collision_runs(ChanDev c, cons
     }
 }
 
+// Fills T.d (allocated, sized for n tuples of this kind) with the moments.
+template <int L, int KIND>
+static int fill_t(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, MomentTensor& T, cudaStream_t s) {
+    constexpr int TT = TTile<L, KIND>::TT;
+    TB_CUDA(cudaMemsetAsync(T.d, 0, size_t(tensor_bytes(L, KIND, n)), s));
+    const size_t smem = sizeof(double) * size_t(c.nmc) * c.R;
+    int64_t blocks = (n * 32 + 255) / 256;
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    k_build_moments<L, KIND><<<unsigned(blocks), 256, smem, s>>>(c, tup, stride, n, T.d, TT);
+    TB_CUDA(cudaGetLastError());
+    return TB_OK;
+}
+
 template <int L, int KIND>
 static int build_t(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, MomentTensor& T, cudaStream_t s) {
     constexpr int TT = TTile<L, KIND>::TT;
@@ -771,6 +785,23 @@ static int build_t(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t
     T.nmom = TDim<L>::NMOM;
     T.kind = KIND;
     return TB_OK;
+}
+
+int refill_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, MomentTensor& T, cudaStream_t s) {
+    if (!T.d || T.n != n) { set_error("refill of a tensor that was not built for this list"); return TB_ERR_ARG; }
+    switch (c.L * 3 + T.kind) {
+        case 6: return fill_t<2, TK_F64>(c, tup, stride, n, T, s);
+        case 7: return fill_t<2, TK_F32>(c, tup, stride, n, T, s);
+        case 8: return fill_t<2, TK_F40>(c, tup, stride, n, T, s);
+        case 9: return fill_t<3, TK_F64>(c, tup, stride, n, T, s);
+        case 10: return fill_t<3, TK_F32>(c, tup, stride, n, T, s);
+        case 11: return fill_t<3, TK_F40>(c, tup, stride, n, T, s);
+        case 12: return fill_t<4, TK_F64>(c, tup, stride, n, T, s);
+        case 13: return fill_t<4, TK_F32>(c, tup, stride, n, T, s);
+        case 14: return fill_t<4, TK_F40>(c, tup, stride, n, T, s);
+    }
+    set_error("nlegs must be 2..4");
+    return TB_ERR_ARG;
 }
 
 int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, int kind, MomentTensor& T,

@@ -36,6 +36,10 @@ int64_t tensor_bytes(int L, int kind, int64_t n_tuples);
 int tile_tuples(int L, int kind);
 int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, int kind, MomentTensor& T,
                  cudaStream_t s);
+// Recomputes the moments of an existing tensor in place (same list, kind,
+// schedule and run-minor buffers), e.g. after the channel's per-tuple
+// amplitudes (ChanDev::tamp) changed.
+int refill_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, MomentTensor& T, cudaStream_t s);
 // rate_leg >= 0: scattering rate of that leg instead (see launch_collision_mc)
 int launch_collision_tensor(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T,
                             const int32_t* tup, int64_t stride, int64_t n, const double* f, double* acc,

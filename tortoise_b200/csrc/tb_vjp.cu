@@ -111,6 +111,7 @@ __global__ void __launch_bounds__(128) k_vjp_mc(ChanDev c, const InstDev* __rest
         double Ci[3][3];
         dc_inverse<L>(g, Ci);
         const double scale = valid ? 1.0 / (c.fact * double(c.nmc) * fabs(g.det)) : 0.0;
+        const double tf = (c.tamp && valid) ? __ldg(c.tamp + i) : 1.0;   // functAmplitude of the tuple
         for (int k = 0; k < n_insts; ++k) {
             const InstDev in = insts[k];
             double A[L][3], B[L][3], sa[L], sb[L];
@@ -155,7 +156,7 @@ __global__ void __launch_bounds__(128) k_vjp_mc(ChanDev c, const InstDev* __rest
                 }
             }
             if (valid) {
-                const double sc = scale * in.amp_full;
+                const double sc = scale * (in.amp_full * tf);
 #pragma unroll
                 for (int l = 0; l < L; ++l) {
                     double* o = grad_f + in.foff[l] + 3 * (int64_t)e[l];
@@ -163,7 +164,7 @@ __global__ void __launch_bounds__(128) k_vjp_mc(ChanDev c, const InstDev* __rest
                     for (int j = 0; j < 3; ++j) atomicAdd(o + j, sc * (sa[l] * gA[l][j] + sb[l] * gB[l][j]));
                 }
             }
-            block_atomic_sum(valid ? scale * c.amp_vol * gamp : 0.0, grad_amp + k);
+            block_atomic_sum(valid ? scale * (c.amp_vol * tf) * gamp : 0.0, grad_amp + k);
         }
     }
 }

@@ -107,6 +107,7 @@ def lib():
         L.tb_adjoint_steps.argtypes = [vp, dp, i64, C.POINTER(i64), dp]
         L.tb_dp45_replay.argtypes = [vp, vp, dp, i64, C.c_double, vp, C.c_int]
         L.tb_set_constraint_fn.argtypes = [vp, C.c_void_p, vp]
+        L.tb_set_channel_amplitude_fn.argtypes = [vp, C.c_int, C.c_void_p, vp]
         L.tb_apply_constraints_at.argtypes = [vp, vp, C.c_double, C.c_int]
         L.tb_shard_range.argtypes = [i64, C.c_int, C.c_int, C.POINTER(i64), C.POINTER(i64)]
         L.tb_shard_unique_id.argtypes = [C.c_char_p]
@@ -129,6 +130,21 @@ SHARD_ID_BYTES = 128
 
 # tb_constraint_fn: int fn(void* user, int32 band, double t, double* population)
 CONSTRAINT_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_double, C.POINTER(C.c_double))
+# tb_amplitude_fn: int fn(void* user, int64 n, int32 nlegs, const double* barycentres, double* out)
+AMPLITUDE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double))
+
+
+def amplitude_callback(fn, errors):
+    """A tb_amplitude_fn calling fn(barycentres[n, nlegs, 2]) -> factors[n]."""
+    def cb(user, n, nlegs, bary, out):
+        try:
+            b = np.ctypeslib.as_array(bary, shape=(int(n), int(nlegs), 2))
+            np.ctypeslib.as_array(out, shape=(int(n),))[:] = fn(b)
+            return 0
+        except Exception as exc:
+            errors.append(exc)
+            return 1
+    return AMPLITUDE_FN(cb)
 
 
 def shard_range(n_tuples, rank, n_ranks):
@@ -174,12 +190,31 @@ class Engine:
     def _bands(self):
         return list(self.material.bands)
 
+    def _channels(self):
+        return list(self.material.channels)
+
     def _install_constraints(self):
         """Bands whose constrainedPopulation is a callable of time get it as
-        the handle's constraint callback."""
+        the handle's constraint callback; channels with a functAmplitude get
+        their per-tuple factors."""
         bands = self._bands()
         if any(b.constrained and callable(b.constrainedPopulation) for b in bands):
             self.set_constraint(lambda b, t: bands[b].population_at(t))
+        for ch, c in enumerate(self._channels()):
+            if getattr(c, "functAmplitude", None) is not None:
+                self.set_channel_amplitude(ch, c.functAmplitude)
+
+    def set_channel_amplitude(self, ch, fn):
+        """ScatteringChannel::functAmplitude (tb_set_channel_amplitude_fn):
+        fn(barycentres[n, nlegs, 2]) -> factors[n], evaluated once per tuple at
+        its elements' barycentres; None returns to 1.  In a batch the factors
+        belong to the channel's structure group."""
+        errors = []
+        cb = amplitude_callback(fn, errors) if fn is not None else None
+        rc = lib().tb_set_channel_amplitude_fn(self.h, ch, C.cast(cb, C.c_void_p) if cb else None, None)
+        if rc != 0 and errors:
+            raise errors[0]
+        _check(rc, "tb_set_channel_amplitude_fn")
 
     def set_constraint(self, fn):
         """Time-dependent constrained populations (tb_set_constraint_fn):
@@ -426,6 +461,9 @@ class BatchEngine(Engine):
 
     def _bands(self):
         return [b for m in self.materials for b in m.bands]
+
+    def _channels(self):
+        return [c for m in self.materials for c in m.channels]
 
     def tuples(self, ch):
         r = max(i for i in range(self.nruns) if self.chan0[i] <= ch)

@@ -182,6 +182,11 @@ class ScatteringChannel:
         self.legBandNumber = [int(b) for b in band_numbers]
         self.legDirection = [int(d) for d in directions]
         self.amplitude = 1.0
+        # ScatteringChannel::functAmplitude (ScatteringChannel.hpp:74): None
+        # is the reference's default 1; else a vectorised callable
+        # barycentres[n, nlegs, 2] -> factors[n] (one per tuple, at its
+        # elements' barycentres)
+        self.functAmplitude = None
         self.numMCPoints = material.defaultNMCPointsScatterings
         self.minimumDeterminant = material.defaultMinimumDeterminantScatterings
         self.scattElemeThreshold = material.defaultScattElemeThresholdScatterings
