@@ -395,11 +395,11 @@ def batched_measure(n_runs, steps, warmup, mixed, layout_name="auto", tune=True)
             uniq[N] = sum(be.channel_info(be.chan0[r] + c)["n_tuples"] for c in range(len(m.channels)))
     layouts = sorted({be.channel_info(c)["layout"] for c in range(be.channel_count())})
     # (stages, instance schedule, groups): schedule 0 one instance per thread,
-    # 1 instance pairs, 2 / 3 / 4 run-minor with 32 / 8 / 4 runs per lane group
+    # 1 instance pairs, 2 / 3 / 4 / 5 run-minor with 32 / 8 / 4 / 16 runs per lane group
     cnt = {}
     for c in range(be.channel_count()):
         sc = be.schedule(c)
-        k = (sc["stages"], {32: 2, 8: 3, 4: 4}[sc["runs"]] if sc["runs"] else sc["pair"])
+        k = (sc["stages"], {32: 2, 8: 3, 4: 4, 16: 5}[sc["runs"]] if sc["runs"] else sc["pair"])
         cnt[k] = cnt.get(k, 0) + 1
     scheds = [[k[0], k[1], v] for k, v in sorted(cnt.items())]
     ndofs = be.ndofs
@@ -584,6 +584,78 @@ def small_ee(args):
     eng.close()
 
 
+def large(args):
+    """The large batched mixed-precision configuration: 16 runs of the
+    three-band (parabola, Dirac cone, heavy hole), two-phonon (0.15, 0.25) e-ph
+    material on a 128x128 mesh (32,768 triangles per band), rtol 1e-8, one
+    structure shared by all runs, reduced-precision moments (FP32 or 40-bit),
+    FP64 products, gain - loss, error norm and step control.  Times args.steps
+    DP45 attempts of the whole batch after args.warmup, the collision operator
+    alone, and states the error of one right-hand side of run 0 against the
+    FP64 Monte-Carlo operator."""
+    import torch
+    from tortoise_b200 import engine as E
+    from tortoise_b200 import workloads as W
+    kind = args.large
+    mats, states = W.large_batch(16, 128)
+    f0 = np.concatenate(states)
+    t0 = time.perf_counter()
+    be = E.BatchEngine(mats, allow_fp32={"t32": 1, "t40": 2}[kind], autotune=not args.no_tune)
+    setup = time.perf_counter() - t0
+    nch = be.channel_count()
+    per_run = len(mats[0].channels)
+    infos = [be.channel_info(c) for c in range(per_run)]
+    ntup = sum(i["n_tuples"] for i in infos)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.ExternalStream(be.stream_ptr(), device=dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f = torch.tensor(f0, device=dev)
+    acc = torch.zeros_like(f)
+    be.collision_accumulate(f.data_ptr(), acc.data_ptr())
+    be.synchronize()
+    ev0.record(stream)
+    for _ in range(3):
+        be.collision_accumulate(f.data_ptr(), acc.data_ptr())
+    ev1.record(stream)
+    ev1.synchronize()
+    t_coll = ev0.elapsed_time(ev1) * 1e-3 / 3
+    del f, acc
+    be.dp45_begin(f0, 0.0, 20.0, 2.0, 0)
+    be.dp45_advance(args.warmup)
+    be.synchronize()
+    with ClockSampler(0) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        be.dp45_advance(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+    t_dev = ev0.elapsed_time(ev1) * 1e-3
+    be.dp45_poll()
+    st = [be.run_stats(r) for r in range(len(mats))]
+    scheds = sorted({(sc["stages"], sc["runs"], sc["pair"]) for sc in (be.schedule(c) for c in range(per_run))
+                     if sc["stages"]})
+    # one RHS of run 0 against the FP64 Monte-Carlo operator of that run alone
+    out = be.split(be.rhs(f0))[0]
+    be.close()
+    ref = E.Engine(mats[0], layout=E.LAYOUT_MC64).rhs(states[0])
+    err = float(np.linalg.norm(out - ref) / np.linalg.norm(ref))
+    bytes_mom = ntup * moment_bytes(3, kind)
+    line = {"large": True, "workload": "16 runs x three-band two-phonon e-ph, 128x128 mesh (32768 triangles/band), "
+                                      "rtol 1e-8, one shared structure", "dtype": kind, "runs": len(mats),
+            "tuples": ntup, "channels_per_run": per_run, "dofs": int(f0.size), "setup_s": setup,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_attempt": 1e3 * t_dev / args.steps,
+            "run_attempts_per_s": len(mats) * args.steps / t_dev,
+            "collision_ms": 1e3 * t_coll, "moment_gb": bytes_mom / 1e9,
+            "run_tuples_per_s": ntup * len(mats) / t_coll,
+            "rhs_error_vs_fp64_mc": err,
+            "schedules": scheds,
+            "attempts": [s["attempts"] for s in st], "t": [s["t"] for s in st]}
+    c = clk.summary()
+    if c:
+        line["clocks"] = c
+    print(json.dumps(line), flush=True)
+
+
 def rhs_only(args):
     """Profiling driver: K right-hand-side evaluations (collision + drift +
     M^-1) of the workload on the device, nothing else (used for the ncu
@@ -632,6 +704,8 @@ def main():
                     help="profiling driver: K RHS evaluations only (with --batch R: R runs of mesh --mesh)")
     ap.add_argument("--mesh", type=int, default=N_MESH, help="sections per side (profiling driver only)")
     ap.add_argument("--batch", type=int, default=0, help="batched ensemble of this many runs (per-run N, kT, couplings)")
+    ap.add_argument("--large", nargs="?", const="t32", default=None, choices=["t32", "t40"],
+                    help="16-run 128x128 three-band two-phonon batch with FP32 (default) or 40-bit moments")
     ap.add_argument("--small-ee", action="store_true",
                     help="16x16 one-band e-e integration to t = 10 (the reference's CPU-runnable case) vs the oracle")
     ap.add_argument("--shard", action="store_true",
@@ -639,6 +713,9 @@ def main():
     ap.add_argument("--adjoint", type=int, default=-1,
                     help="adjoint gradient of the 32x32 workload, checked in this many FD directions")
     args = ap.parse_args()
+    if args.large:
+        large(args)
+        return
     if args.small_ee:
         small_ee(args)
         return

@@ -318,9 +318,9 @@ int tb_read_scatt_indices(const char* path, int nlegs, const int32_t* nsplit, in
 
 /* Contraction schedule of a channel's moment-tensor group: bulk-copy
  * pipeline stages (1 or 2); the instance schedule in `pair` -- 0 one
- * instance per thread, 1 two instances share each moment read, 2 / 3 / 4
- * run-minor (one lane per run, 32 / 8 / 4 runs per tuple and 1 / 4 / 8
- * tuples per warp, for groups shared by many runs of a batch); and, after
+ * instance per thread, 1 two instances share each moment read, 2 / 3 / 4 / 5
+ * run-minor (one lane per run, 32 / 8 / 4 / 16 runs per tuple and 1 / 4 / 8 /
+ * 2 tuples per warp, for groups shared by many runs of a batch); and, after
  * tb_options.autotune, the fastest measured launch time in seconds (0 when
  * not tuned).  Monte-Carlo channels report 0, 0, 0.  No
  * counterpart in the reference. */
@@ -328,7 +328,7 @@ int tb_channel_schedule(const tb_handle* h, int ch, int32_t* stages, int32_t* pa
 
 /* Pins the contraction schedule of a channel's moment-tensor group (every
  * channel of that group): stages 1..2, pair as tb_channel_schedule reports it
- * (2..4 only for groups of 8..1024 runs with at most 3 legs).  The result is
+ * (2..5 only for groups of 8..1024 runs with at most 3 legs).  The result is
  * the same up to FP64 summation order; the time is not.  No counterpart in the
  * reference. */
 int tb_set_channel_schedule(tb_handle* h, int ch, int32_t stages, int32_t pair);

@@ -132,10 +132,10 @@ def test_run_minor_contraction_equals_individual_runs(gpu_lib, layout):
     f = np.concatenate(states)
     singles = [E.Engine(m, layout=layout) for m in mats]
     refs = [e1.rhs(x) for e1, x in zip(singles, states)]
-    # every pinned schedule: lane groups of 32 / 8 / 4 runs, the per-thread
+    # every pinned schedule: lane groups of 32 / 16 / 8 / 4 runs, the per-thread
     # paths, one or two bulk-copy stages
     for stages in (1, 2):
-        for kw in ({"runs": 32}, {"runs": 8}, {"runs": 4}, {"pair": 0}, {"pair": 1}):
+        for kw in ({"runs": 32}, {"runs": 16}, {"runs": 8}, {"runs": 4}, {"pair": 0}, {"pair": 1}):
             for c in range(be.channel_count()):
                 be.set_schedule(c, stages, **kw)
             got = be.split(be.rhs(f))

@@ -785,6 +785,7 @@ int tb_channel_schedule(const tb_handle* h, int ch, int32_t* stages, int32_t* pa
                 : G.tensor.runs == 32 ? 2
                 : G.tensor.runs == 8  ? 3
                 : G.tensor.runs == 4  ? 4
+                : G.tensor.runs == 16 ? 5
                 : (G.L <= 3 && G.insts.size() > 1) ? G.tensor.pair
                                                    : 0;
     if (seconds) *seconds = tensor ? G.tensor.tuned_seconds : 0.0;
@@ -795,7 +796,7 @@ int tb_set_channel_schedule(tb_handle* h, int ch, int32_t stages, int32_t pair) 
     if (!h || ch < 0 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
     GroupChan& G = h->groups[h->insts[ch].group];
     if (G.layout == TB_LAYOUT_MC64) { set_error("Monte-Carlo channels have no contraction schedule"); return TB_ERR_ARG; }
-    if (stages < 1 || stages > 2 || pair < 0 || pair > 4) { set_error("stages must be 1..2 and pair 0..4"); return TB_ERR_ARG; }
+    if (stages < 1 || stages > 2 || pair < 0 || pair > 5) { set_error("stages must be 1..2 and pair 0..5"); return TB_ERR_ARG; }
     if (pair >= 2 && !G.tensor.fT) {
         set_error("the run-minor contraction needs a group of 8..1024 runs with at most 3 legs");
         return TB_ERR_ARG;
@@ -804,7 +805,7 @@ int tb_set_channel_schedule(tb_handle* h, int ch, int32_t stages, int32_t pair) 
     TB_CUDA(cudaStreamSynchronize(h->stream));
     G.tensor.stages = stages;
     G.tensor.pair = pair == 1 ? 1 : 0;
-    G.tensor.runs = pair == 2 ? 32 : pair == 3 ? 8 : pair == 4 ? 4 : 0;
+    G.tensor.runs = pair == 2 ? 32 : pair == 3 ? 8 : pair == 4 ? 4 : pair == 5 ? 16 : 0;
     if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }   // the captured launches change
     return TB_OK;
 }

@@ -635,7 +635,8 @@ __device__ __forceinline__ void contract_run(const ChanDev& c, const RunsDev& R,
 // an FP64 copy that the contraction reads; the stage is refilled at once, so
 // one stage already overlaps the next copy with the contraction.
 // S runs per lane group: a warp takes 32 / S tuples at a time, each for S
-// runs, so a group of n runs pads to a multiple of S rather than of 32; each
+// runs (S = 4, 8, 16, 32), so a group of n runs pads to a multiple of S
+// rather than of 32; each
 // instruction still serves 32 lanes, the moment reads hit 32 / S adjacent
 // words and every f row / reduction stays whole 32-byte sectors (S >= 4).
 template <int L, int KIND, int TT, int STAGES, int S>
@@ -954,8 +955,11 @@ static int launch_t(const ChanDev& c, const InstDev* insts, int n_insts, const M
     if constexpr (L <= 3) {
         if (T.runs && T.fT) {
 #define TB_RUNS(ST, SS) launch_runs<L, KIND, ST, SS>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s)
-            if (T.stages == 1) return T.runs == 4 ? TB_RUNS(1, 4) : T.runs == 8 ? TB_RUNS(1, 8) : TB_RUNS(1, 32);
-            return T.runs == 4 ? TB_RUNS(2, 4) : T.runs == 8 ? TB_RUNS(2, 8) : TB_RUNS(2, 32);
+            if (T.stages == 1)
+                return T.runs == 4 ? TB_RUNS(1, 4) : T.runs == 8 ? TB_RUNS(1, 8) : T.runs == 16 ? TB_RUNS(1, 16)
+                                                                                 : TB_RUNS(1, 32);
+            return T.runs == 4 ? TB_RUNS(2, 4) : T.runs == 8 ? TB_RUNS(2, 8) : T.runs == 16 ? TB_RUNS(2, 16)
+                                                                             : TB_RUNS(2, 32);
 #undef TB_RUNS
         }
     }
@@ -1012,16 +1016,16 @@ int tune_tensor(const ChanDev& c, const InstDev* insts, int n_insts, MomentTenso
     double best = 1e300;
     int bs = T.stages, bp = T.pair, br = T.runs;
     const int pairs_max = (c.L <= 3 && n_insts > 1) ? 1 : 0;
-    const int runs_max = T.fT ? 3 : 0;
+    const int runs_max = T.fT ? 4 : 0;
     int rc = TB_OK;
     for (int st = 1; st <= 2 && rc == TB_OK; ++st)
         for (int pr = 0; pr <= 1 + runs_max && rc == TB_OK; ++pr) {
-            // pr: 0 one instance per thread, 1 instance pairs, 2 / 3 / 4
-            // run-minor with 32 / 8 / 4 runs per lane group
+            // pr: 0 one instance per thread, 1 instance pairs, 2 / 3 / 4 / 5
+            // run-minor with 32 / 8 / 4 / 16 runs per lane group
             if (pr == 1 && !pairs_max) continue;
             T.stages = st;
             T.pair = pr == 1;
-            T.runs = pr == 2 ? 32 : pr == 3 ? 8 : pr == 4 ? 4 : 0;
+            T.runs = pr == 2 ? 32 : pr == 3 ? 8 : pr == 4 ? 4 : pr == 5 ? 16 : 0;
             rc = launch_collision_tensor(c, insts, n_insts, T, tup, stride, n, f, acc, nullptr, s);   // warm-up
             if (rc != TB_OK) break;
             constexpr int REPS = 3;

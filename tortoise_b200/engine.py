@@ -280,15 +280,15 @@ class Engine:
 
     def set_schedule(self, ch, stages, pair=0, runs=0):
         """Pins the contraction schedule of channel ch's group (tb_set_channel_schedule):
-        runs = 32, 8 or 4 selects the run-minor contraction, else pair = 0 or 1."""
-        code = {32: 2, 8: 3, 4: 4}[runs] if runs else int(pair)
+        runs = 32, 16, 8 or 4 selects the run-minor contraction, else pair = 0 or 1."""
+        code = {32: 2, 8: 3, 4: 4, 16: 5}[runs] if runs else int(pair)
         _check(lib().tb_set_channel_schedule(self.h, ch, int(stages), code), "tb_set_channel_schedule")
 
     def schedule(self, ch):
         st, pr, sec = C.c_int32(), C.c_int32(), C.c_double()
         _check(lib().tb_channel_schedule(self.h, ch, C.byref(st), C.byref(pr), C.byref(sec)), "tb_channel_schedule")
-        # runs: run-minor lane-group width (32, 8 or 4 runs per tuple), 0 = off
-        return {"stages": st.value, "pair": int(pr.value == 1), "runs": {2: 32, 3: 8, 4: 4}.get(pr.value, 0),
+        # runs: run-minor lane-group width (32, 16, 8 or 4 runs per tuple), 0 = off
+        return {"stages": st.value, "pair": int(pr.value == 1), "runs": {2: 32, 3: 8, 4: 4, 5: 16}.get(pr.value, 0),
                 "tuned_seconds": sec.value}
 
     def tuples(self, ch):
@@ -474,6 +474,12 @@ class BatchEngine(Engine):
         _check(lib().tb_get_tuples(self.h, ch, ids.ctypes.data_as(C.POINTER(C.c_int32)),
                                    umk.ctypes.data_as(C.POINTER(C.c_int32))), "tb_get_tuples")
         return ids, umk
+
+    def run_stats(self, r):
+        """Run r's integration counters as of the last dp45_poll (tb_dp45_run_stats)."""
+        rs = DP45Stats()
+        _check(lib().tb_dp45_run_stats(self.h, int(r), C.byref(rs)), "tb_dp45_run_stats")
+        return rs.as_dict()
 
     def split(self, vec):
         return [np.asarray(vec)[s] for s in self.slices]

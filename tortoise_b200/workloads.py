@@ -113,6 +113,23 @@ def three_band_two_phonon(N=128, ee=False, **kw):
     return build_material(N, ("P", "D", "H"), (0.15, 0.25), ee=ee, eph=True, rtol=1e-8, atol=1e-9, **kw)
 
 
+def large_batch(n_runs=16, N=128, seed=4242, **kw):
+    """A batch of n_runs three-band, two-phonon runs (three_band_two_phonon,
+    e-ph channels) on one N x N mesh: per run kT uniform in [0.03, 0.2], e-ph
+    couplings uniform in [0.5, 2.0] and a seeded bump; one structure, so all
+    runs share the tuple lists and moment tensors.  Returns (materials, initial
+    state vectors)."""
+    rng = np.random.default_rng(seed)
+    mats, states = [], []
+    for r in range(n_runs):
+        kT = float(rng.uniform(0.03, 0.2))
+        amp = float(rng.uniform(0.5, 2.0))
+        m = three_band_two_phonon(N, eph_amplitude=amp, **kw)
+        mats.append(m)
+        states.append(initial_status(m, kT=kT, seed=int(rng.integers(1 << 30))).vec)
+    return mats, states
+
+
 def ensemble_runs(n_runs=256, seed=2024, Ns=(16, 24, 32, 48, 64), ee=False, **kw):
     """Batched ensemble: per run N uniform in Ns, kT uniform in [0.03, 0.2],
     coupling constants uniform in [0.5, 2.0] and a seeded bump; bands, phonon,
