@@ -550,6 +550,29 @@ def small_ee(args):
     eng = E.Engine(mat, autotune=not args.no_tune)
     t_setup = time.perf_counter() - t_setup
     info = eng.channel_info(0)
+    # the collision operator alone, CUDA events on the library's stream:
+    # the quadrature over the points inside the simplices only (the default)
+    # and over every point of every tuple
+    import torch
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.ExternalStream(eng.stream_ptr(), device=dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fd = torch.tensor(f0, device=dev)
+    acc = torch.zeros_like(fd)
+    coll = {}
+    for inside in (False, True):
+        eng.set_schedule(0, 0, inside_only=inside)
+        for _ in range(2):
+            eng.collision_accumulate(fd.data_ptr(), acc.data_ptr())
+        eng.synchronize()
+        reps = 5
+        ev0.record(stream)
+        for _ in range(reps):
+            eng.collision_accumulate(fd.data_ptr(), acc.data_ptr())
+        ev1.record(stream)
+        ev1.synchronize()
+        coll["inside_only" if inside else "every_point"] = ev0.elapsed_time(ev1) / reps
+    n_in, p_in = eng.points_inside(0)
     eng.dp45(f0, 0.0, 0.01, 0.01)   # warm-up (graph capture, first launches)
     with ClockSampler(0) as clk:
         w0 = time.perf_counter()
@@ -558,6 +581,9 @@ def small_ee(args):
     gpu_s = w1 - w0
     line = {"workload": "16x16 parabolic band, e-e constant matrix element (512 triangles), rtol 1e-6, t = 10",
             "tuples": info["n_tuples"], "layout": info["layout"], "setup_s": t_setup,
+            "tuples_with_points_inside": n_in, "points_inside": p_in,
+            "points_evaluated_every_point": info["n_tuples"] * mat.channels[0].numMCPoints,
+            "collision_ms_per_rhs": coll,
             "gpu": {"seconds": gpu_s, "status": r["status"], "attempts": r["attempts"], "accepted": r["accepted"],
                     "rejected": r["rejected"], "rhs_evals": r["rhs_evals"], "t": r["t"],
                     "attempts_per_s": r["attempts"] / gpu_s}}

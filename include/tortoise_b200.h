@@ -322,13 +322,25 @@ int tb_read_scatt_indices(const char* path, int nlegs, const int32_t* nsplit, in
  * run-minor (one lane per run, 32 / 8 / 4 / 16 runs per tuple and 1 / 4 / 8 /
  * 2 tuples per warp, for groups shared by many runs of a batch); and, after
  * tb_options.autotune, the fastest measured launch time in seconds (0 when
- * not tuned).  Monte-Carlo channels report 0, 0, 0.  No
- * counterpart in the reference. */
+ * not tuned).  Monte-Carlo channels report stages 0, 0 seconds and pair 6
+ * when the quadrature visits only the points inside the simplices (a list
+ * of the tuples with such points and a 64-bit mask per tuple, built at
+ * creation when the channel has at most 64 Monte-Carlo points; same sums as
+ * the full quadrature for finite f), else 0 (every point of every tuple).
+ * No counterpart in the reference. */
 int tb_channel_schedule(const tb_handle* h, int ch, int32_t* stages, int32_t* pair, double* seconds);
+
+/* Monte-Carlo channels: the tuples with at least one point inside the
+ * simplices and the number of such (tuple, point) pairs, i.e. the work the
+ * quadrature does per instance; -1, -1 when the channel has no such list
+ * (moment-tensor layout, or more than 64 Monte-Carlo points).  On a sharded
+ * handle, this handle's part.  No counterpart in the reference. */
+int tb_channel_points_inside(const tb_handle* h, int ch, int64_t* n_tuples, int64_t* n_points);
 
 /* Pins the contraction schedule of a channel's moment-tensor group (every
  * channel of that group): stages 1..2, pair as tb_channel_schedule reports it
- * (2..5 only for groups of 8..1024 runs with at most 3 legs).  The result is
+ * (2..5 only for groups of 8..1024 runs with at most 3 legs).  Monte-Carlo
+ * groups take stages 0 with pair 0 (every point) or 6 (points inside only).  The result is
  * the same up to FP64 summation order; the time is not.  No counterpart in the
  * reference. */
 int tb_set_channel_schedule(tb_handle* h, int ch, int32_t stages, int32_t pair);

@@ -36,6 +36,7 @@ def lib():
         L.or_num_tuples.restype = i64
         L.or_num_tuples.argtypes = [vp, C.c_int]
         L.or_enum_counts.argtypes = [vp, C.c_int, C.POINTER(i64), C.POINTER(i64)]
+        L.or_points_inside.argtypes = [vp, C.c_int, C.POINTER(i64), C.POINTER(i64), ip]
         L.or_get_tuples.argtypes = [vp, C.c_int, ip, ip]
         L.or_set_tuples.argtypes = [vp, C.c_int, i64, ip, ip]
         L.or_set_amplitude.argtypes = [vp, C.c_int, C.c_double]
@@ -128,6 +129,14 @@ class Oracle:
         a, b = C.c_int64(), C.c_int64()
         lib().or_enum_counts(self.h, ch, C.byref(a), C.byref(b))
         return a.value, b.value
+
+    def points_inside(self, ch, per_tuple=False):
+        """(tuples with a Monte-Carlo point inside the simplices, such points),
+        plus the count of every tuple of the list when per_tuple is set."""
+        a, b = C.c_int64(), C.c_int64()
+        cnt = np.zeros(self.num_tuples(ch), dtype=np.int32) if per_tuple else None
+        lib().or_points_inside(self.h, ch, C.byref(a), C.byref(b), _ip(cnt) if per_tuple else None)
+        return (a.value, b.value, cnt) if per_tuple else (a.value, b.value)
 
     def tuples(self, ch):
         n = self.num_tuples(ch)

@@ -1190,6 +1190,36 @@ void or_set_tuples(void* h, int ch, int64_t n, const int32_t* ids, const int32_t
 void or_set_amplitude(void* h, int ch, double a) { static_cast<Problem*>(h)->chans[ch].amplitude = a; }
 
 // ScatteringChannel::propagate restricted to tuples [t0,t1) (out += ...).
+// Tuples of a channel's list with at least one Monte-Carlo point whose
+// ThetapC * ThetaFC is 1 (IntegratorCore.hpp:318-320) and the number of such
+// (tuple, point) pairs: the terms of TypeB that are not the integrand times 0.
+// per_tuple (optional, one int32 per tuple of the list): that tuple's count.
+void or_points_inside(void* h, int ch, int64_t* n_tuples, int64_t* n_points, int32_t* per_tuple) {
+    const Problem& P = *static_cast<Problem*>(h);
+    const Channel& c = P.chans[ch];
+    const int L = c.L, R = 2 * (L - 2) + 1;
+    int64_t nt = 0, np = 0;
+    for (size_t i = 0; i < c.tumk.size(); ++i) {
+        if (per_tuple) per_tuple[i] = 0;
+        Geom g;
+        build_geom(P, c, &c.tuples[i * size_t(L)], c.tumk[i], g);
+        if (std::fabs(g.det) < c.min_det) continue;
+        double DCinv[3][3];
+        inv3(g.DC, DCinv);
+        MCPoint mp;
+        int64_t k = 0;
+        for (int m = 0; m < c.nmc; ++m) {
+            mc_point(L, g, DCinv, &c.mc[size_t(m) * R], mp);
+            k += mp.theta ? 1 : 0;
+        }
+        nt += k > 0 ? 1 : 0;
+        np += k;
+        if (per_tuple) per_tuple[i] = int32_t(k);
+    }
+    *n_tuples = nt;
+    *n_points = np;
+}
+
 void or_channel_propagate(void* h, int ch, const double* f, double* out, int64_t t0, int64_t t1, int nthreads,
                           int inverse_mass) {
     Problem& P = *static_cast<Problem*>(h);

@@ -112,7 +112,7 @@ def test_autotuned_schedule_gives_the_same_operator(gpu_lib):
         assert s["stages"] in (1, 2) and s["pair"] in (0, 1) and s["tuned_seconds"] > 0.0
         assert plain.schedule(0)["tuned_seconds"] == 0.0
     mc = E.BatchEngine(mats, layout=E.LAYOUT_MC64, autotune=True)
-    assert mc.schedule(0) == {"stages": 0, "pair": 0, "runs": 0, "tuned_seconds": 0.0}
+    assert mc.schedule(0) == {"stages": 0, "pair": 0, "runs": 0, "tuned_seconds": 0.0, "inside_only": True}
 
 
 @pytest.mark.parametrize("layout", [E.LAYOUT_T64, E.LAYOUT_T40, E.LAYOUT_T32])
@@ -155,3 +155,25 @@ def test_run_minor_contraction_equals_individual_runs(gpu_lib, layout):
     after = be.split(be.rhs(f, drift=False))
     assert np.linalg.norm(after[5]) == 0.0
     assert rel_l2(after[6], singles[6].rhs(states[6], drift=False)) < 1e-12
+
+
+def test_points_inside_only_beyond_the_shared_accumulator(gpu_lib):
+    """256 runs of one 4x4 two-band structure with e-e channels: the
+    Monte-Carlo kernel's shared-memory copy of the accumulator (one block per
+    run) would exceed its limit, so it adds straight into the global
+    accumulator.  Against the same handle pinned to every Monte-Carlo point,
+    and against a batch of the first 8 runs (shared-memory copies), the
+    operator must not change (1e-13)."""
+    mats, states = W.ensemble_runs(256, seed=9, Ns=(4,), ee=True)
+    f = np.concatenate(states)
+    be = E.BatchEngine(mats, layout=E.LAYOUT_MC64)
+    per_run = len(mats[0].channels)
+    live = [c for c in range(per_run) if be.channel_info(c)["n_tuples"]]
+    assert live and all(be.schedule(c).get("inside_only") for c in live)
+    a = be.rhs(f)
+    small = E.BatchEngine(mats[:8], layout=E.LAYOUT_MC64)
+    s = small.rhs(np.concatenate(states[:8]))
+    assert rel_l2(a[:s.size], s) < 1e-13
+    for c in live:
+        be.set_schedule(c, 0, inside_only=False)
+    assert rel_l2(a, be.rhs(f)) < 1e-13

@@ -101,6 +101,37 @@ def test_larger_ee_against_live_oracle(gpu_lib):
     assert rel_l2(eng.rhs(f0), o.rhs(f0)) < 1e-12
 
 
+@pytest.mark.parametrize("name", CASES + ["ee_n8"])
+def test_points_inside_only_equal_the_full_quadrature(gpu_lib, name):
+    """Monte-Carlo channels visit only the points whose ThetapC * ThetaFC is 1
+    (decided once per handle, kept as a 64-bit mask per tuple, tuples without
+    such a point dropped); the kept tuples and points are exactly the
+    oracle's.  Pinned back to every point of every tuple, the operator and
+    the scattering rates must not change: the skipped terms are the
+    integrand times 0 (1e-13: FP64 atomics order, and fused rather than
+    reference-order coordinates for points near a simplex edge)."""
+    if name == "ee_n8":
+        mat = W.parabolic_ee(8)
+        f0 = W.initial_status(mat, kT=0.1, seed=11).vec
+    else:
+        mat, f0 = _setup(name)
+    eng = E.Engine(mat, layout=E.LAYOUT_MC64)
+    chans = [c for c in range(len(mat.channels)) if eng.channel_info(c)["n_tuples"] > 0]
+    assert chans and all(eng.schedule(c).get("inside_only") for c in chans)
+    o = oracle.Oracle(mat)
+    for c in chans:
+        assert eng.points_inside(c) == o.points_inside(c)
+    a, ra = eng.rhs(f0), eng.scattering_rates(f0)
+    for c in chans:
+        eng.set_schedule(c, 0, inside_only=False)
+        assert "inside_only" not in eng.schedule(c)
+    b, rb = eng.rhs(f0), eng.scattering_rates(f0)
+    assert rel_l2(a, b) < 1e-13
+    assert rel_l2(ra, rb) < 1e-13
+    with pytest.raises(E.TortoiseError):
+        eng.set_schedule(chans[0], 1)
+
+
 @pytest.mark.parametrize("variant", ["umklapp", "nonsquare", "partial_mesh", "empty_channel", "zero_amplitude"])
 def test_edge_cases(gpu_lib, variant):
     from tortoise_b200.model import Material, Mesh, Region, IN, OUT, FERMION, BOSON

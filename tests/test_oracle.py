@@ -224,3 +224,27 @@ def test_funct_amplitude_scales_each_tuple():
     mesh = mat.bands[mat.channels[0].legBandNumber[0]].mesh
     cent = mesh.vertices().mean(axis=1)            # (ne, 2) element centroids
     assert np.abs(seen[0][:, 0, :] - cent[ids[:, 0]]).max() < 1e-8
+
+
+@pytest.mark.parametrize("name", ["ee_n4", "eph_n4"])
+def test_tuples_without_points_inside_contribute_exactly_zero(name):
+    """The device quadrature visits only the Monte-Carlo points whose
+    ThetapC * ThetaFC is 1 and drops the tuples that have none.  On the
+    oracle, one thread, reference order: the dropped tuples give exactly zero
+    and the list without them gives the same operator bit for bit."""
+    build, seed, kT = cases()[name]
+    mat = build()
+    f0 = W.initial_status(mat, kT=kT, seed=seed).vec
+    o = oracle.Oracle(mat, nthreads=1)
+    for ch, c in enumerate(mat.channels):
+        n_in, p_in, cnt = o.points_inside(ch, per_tuple=True)
+        assert n_in == np.count_nonzero(cnt) and p_in == cnt.sum()
+        assert 0 < p_in < cnt.size * c.numMCPoints
+        ids, umk = o.tuples(ch)
+        full = o.channel_propagate(ch, f0)
+        sub = oracle.Oracle(mat, enumerate_tuples=False, nthreads=1)
+        if n_in < cnt.size:
+            sub.set_tuples(ch, ids[cnt == 0], umk[cnt == 0])
+            assert not np.any(sub.channel_propagate(ch, f0))
+        sub.set_tuples(ch, ids[cnt > 0], umk[cnt > 0])
+        assert np.array_equal(sub.channel_propagate(ch, f0), full)

@@ -27,6 +27,7 @@ SOURCES = {
     "tb_adjoint.cu": [],
     "tb_shard.cu": [],
     "tb_constraints.cu": [],
+    "tb_theta.cu": [],
 }
 
 

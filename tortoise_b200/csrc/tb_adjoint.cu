@@ -372,8 +372,13 @@ static int vjp_at(tb_handle* h, const double* Y, int flags) {
         for (size_t gi = 0; gi < h->groups.size(); ++gi) {
             GroupChan& G = h->groups[gi];
             if (G.tup.n == 0 || G.insts.empty()) continue;
-            TB_TRY(launch_collision_vjp(G.dev, G.d_insts, int(G.insts.size()), G.layout, G.tensor, G.tup.d, G.tup.cap,
-                                        G.tup.n, Y, A->u, A->g, A->gamp + A->gamp_off[gi], h->stream));
+            if (G.layout == TB_LAYOUT_MC64 && G.theta.use)   // the tuples and points inside the simplices only
+                TB_TRY(launch_collision_vjp(G.dev, G.d_insts, int(G.insts.size()), G.layout, G.tensor, G.theta.ids,
+                                            G.theta.n, G.theta.n, Y, A->u, A->g, A->gamp + A->gamp_off[gi], h->stream,
+                                            G.theta.mask, G.theta.perm));
+            else
+                TB_TRY(launch_collision_vjp(G.dev, G.d_insts, int(G.insts.size()), G.layout, G.tensor, G.tup.d,
+                                            G.tup.cap, G.tup.n, Y, A->u, A->g, A->gamp + A->gamp_off[gi], h->stream));
         }
         TB_TRY(shard_allreduce(h, A->g, size_t(h->ndofs)));   // sharded: all ranks' partial VJPs
     }

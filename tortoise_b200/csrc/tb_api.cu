@@ -409,6 +409,21 @@ int build_runs(tb_handle* h, const tb_problem_desc* const* descs, int nruns) {
                     av *= h->meshes[B.mesh].vol * 2.0;
                 }
                 c.amp_vol = av;
+                // segments of the shared-memory accumulator: the distinct
+                // bands of the legs, in leg order
+                c.nseg = 0;
+                c.sinst = 0;
+                for (int l = 0; l < G.L; ++l) {
+                    int s = 0;
+                    while (s < c.nseg && cd.band[c.seg_leg[s]] != cd.band[l]) ++s;
+                    if (s == c.nseg) {
+                        c.seg_leg[s] = l;
+                        c.seg_off[s] = c.sinst;
+                        c.sinst += 3 * c.leg[l].ne;
+                        ++c.nseg;
+                    }
+                    c.sseg[l] = c.seg_off[s];
+                }
                 c.fact = 1.0;
                 for (int i = 0; i < G.L - 2; ++i) c.fact *= 2.0;
                 c.min_det = cd.min_det;
@@ -474,6 +489,8 @@ int build_runs(tb_handle* h, const tb_problem_desc* const* descs, int nruns) {
     }
     for (auto& G : h->groups) TB_TRY(shard_tuples(h, G));
     TB_TRY(choose_layouts(h));
+    for (auto& G : h->groups)
+        if (G.layout == TB_LAYOUT_MC64) TB_TRY(build_theta_list(G.dev, G.tup, G.theta, h->stream));
     if (h->opts.autotune) TB_TRY(autotune(h));
     TB_CUDA(cudaStreamSynchronize(h->stream));
     return TB_OK;
@@ -483,6 +500,17 @@ int build_runs(tb_handle* h, const tb_problem_desc* const* descs, int nruns) {
 
 // The RHS accumulation (pre-M^-1) of the input state into acc (which must be zero).
 namespace tb {
+// The Monte-Carlo collision of group G: over its ThetaList when in use, else
+// the full quadrature of every tuple.
+static int launch_group_mc(tb_handle* h, GroupChan& G, const InstDev* insts, int n_insts, const double* d_in,
+                           double* d_acc, const DPCtl* ctl, int rate_leg) {
+    if (G.theta.use)
+        return launch_collision_mc(G.dev, insts, n_insts, G.theta.ids, G.theta.n, G.theta.n, d_in, d_acc, ctl,
+                                   h->stream, 148 * 32, rate_leg, G.theta.mask, G.theta.perm);
+    return launch_collision_mc(G.dev, insts, n_insts, G.tup.d, G.tup.cap, G.tup.n, d_in, d_acc, ctl, h->stream,
+                               148 * 32, rate_leg);
+}
+
 int run_rhs_acc(tb_handle* h, const double* d_in, double* d_acc, const DPCtl* ctl, int flags, int only_inst) {
     if (!(flags & TB_NO_COLLISIONS)) {
         for (size_t gi = 0; gi < h->groups.size(); ++gi) {
@@ -500,8 +528,7 @@ int run_rhs_acc(tb_handle* h, const double* d_in, double* d_acc, const DPCtl* ct
                 if (!any) continue;
             }
             if (G.layout == TB_LAYOUT_MC64) {
-                TB_TRY(launch_collision_mc(G.dev, insts, n_insts, G.tup.d, G.tup.cap, G.tup.n, d_in, d_acc, ctl,
-                                           h->stream, 148 * 32));
+                TB_TRY(launch_group_mc(h, G, insts, n_insts, d_in, d_acc, ctl, -1));
             } else {
                 TB_TRY(launch_collision_tensor(G.dev, insts, n_insts, G.tensor, G.tup.d, G.tup.cap, G.tup.n, d_in,
                                                d_acc, ctl, h->stream));
@@ -730,6 +757,7 @@ int tb_destroy(tb_handle* h) {
     for (auto& G : h->groups) {
         G.tup.release();
         G.tensor.release();
+        G.theta.release();
         if (G.d_tamp) cudaFree(G.d_tamp);
     }
     for (double* p : h->dev_allocs) cudaFree(p);
@@ -775,13 +803,22 @@ int tb_channel_info(const tb_handle* h, int ch, int64_t* n_tuples, int64_t* n_pr
     return TB_OK;
 }
 
+int tb_channel_points_inside(const tb_handle* h, int ch, int64_t* n_tuples, int64_t* n_points) {
+    if (!h || ch < 0 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
+    const GroupChan& G = h->groups[h->insts[ch].group];
+    const bool has = G.layout == TB_LAYOUT_MC64 && G.theta.built;
+    if (n_tuples) *n_tuples = has ? G.theta.n : -1;
+    if (n_points) *n_points = has ? G.theta.points : -1;
+    return TB_OK;
+}
+
 int tb_channel_schedule(const tb_handle* h, int ch, int32_t* stages, int32_t* pair, double* seconds) {
     if (!h || ch < 0 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
     const GroupChan& G = h->groups[h->insts[ch].group];
     const bool tensor = G.layout != TB_LAYOUT_MC64;
     if (stages) *stages = tensor ? G.tensor.stages : 0;
     if (pair)
-        *pair = !tensor                ? 0
+        *pair = !tensor                ? (G.theta.use ? 6 : 0)
                 : G.tensor.runs == 32 ? 2
                 : G.tensor.runs == 8  ? 3
                 : G.tensor.runs == 4  ? 4
@@ -795,7 +832,21 @@ int tb_channel_schedule(const tb_handle* h, int ch, int32_t* stages, int32_t* pa
 int tb_set_channel_schedule(tb_handle* h, int ch, int32_t stages, int32_t pair) {
     if (!h || ch < 0 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
     GroupChan& G = h->groups[h->insts[ch].group];
-    if (G.layout == TB_LAYOUT_MC64) { set_error("Monte-Carlo channels have no contraction schedule"); return TB_ERR_ARG; }
+    if (G.layout == TB_LAYOUT_MC64) {
+        if (stages != 0 || (pair != 0 && pair != 6)) {
+            set_error("Monte-Carlo channels take stages 0 and pair 0 (every point) or 6 (points inside only)");
+            return TB_ERR_ARG;
+        }
+        if (pair == 6 && !G.theta.built) {
+            set_error("this channel has no list of points inside (more than 64 Monte-Carlo points)");
+            return TB_ERR_ARG;
+        }
+        TB_CUDA(cudaSetDevice(h->device));
+        TB_CUDA(cudaStreamSynchronize(h->stream));
+        G.theta.use = pair == 6;
+        if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+        return TB_OK;
+    }
     if (stages < 1 || stages > 2 || pair < 0 || pair > 5) { set_error("stages must be 1..2 and pair 0..5"); return TB_ERR_ARG; }
     if (pair >= 2 && !G.tensor.fT) {
         set_error("the run-minor contraction needs a group of 8..1024 runs with at most 3 legs");
@@ -1033,8 +1084,7 @@ int tb_scattering_rates(tb_handle* h, int ch, int leg, const double* f, double* 
         for (int l = 0; l < G.L; ++l) {
             if (leg >= 0 && l != leg) continue;
             if (G.layout == TB_LAYOUT_MC64)
-                TB_TRY(launch_collision_mc(G.dev, insts, n_insts, G.tup.d, G.tup.cap, G.tup.n, d_in, h->d_acc, nullptr,
-                                           h->stream, 148 * 32, l));
+                TB_TRY(launch_group_mc(h, G, insts, n_insts, d_in, h->d_acc, nullptr, l));
             else
                 TB_TRY(launch_collision_tensor(G.dev, insts, n_insts, G.tensor, G.tup.d, G.tup.cap, G.tup.n, d_in,
                                                h->d_acc, nullptr, h->stream, l));

@@ -13,23 +13,72 @@
 //   * the 3L results are scattered with FP64 atomics (RED) into the pre-M^-1
 //     accumulator, which stays L2-resident.
 // The kernel is FP64-FMA bound (about 55 FP64 operations per MC point for L=4).
+// LIST: the same quadrature over a ThetaList (tb_theta.cu): the tuples with at
+// least one point inside the simplices, each visiting only those points (set
+// bits of its mask, in increasing order), i.e. the dense sums without their
+// terms that are the integrand times Theta = 0.
 #include "tb_dp45.cuh"
 #include "tb_geom.cuh"
 #include "tb_kernels.cuh"
 #include "tb_scatter.cuh"
 
+// Largest shared-memory accumulator (all instances' blocks) a launch uses;
+// beyond it the results go straight to the global accumulator.
+#ifndef TB_MC_SACC_MAX_BYTES
+#define TB_MC_SACC_MAX_BYTES (160 * 1024)
+#endif
+
 namespace tb {
 
+// One Monte-Carlo point of TypeB (IntegratorCore.hpp:338-357): the legs'
+// points in reference coordinates (free legs from the table, the partially
+// and fully constrained legs from alpha), the gain-plus-loss product times
+// Theta, and its first moments per leg.
+template <int L>
+__device__ __forceinline__ void mc_point_accumulate(const double (&A)[L][3], const double (&B)[L][3],
+                                                    const double* qv, const double (&al)[3], double th, double& s0,
+                                                    double (&sx)[L], double (&sy)[L]) {
+    constexpr int R = 2 * (L - 2) + 1;
+    double px[L], py[L];
+#pragma unroll
+    for (int l = 0; l < L - 2; ++l) { px[l] = qv[2 * l]; py[l] = qv[2 * l + 1]; }
+    px[L - 2] = qv[R - 1]; py[L - 2] = al[0];
+    px[L - 1] = al[1]; py[L - 1] = al[2];
+    double pa = 1.0, pb = 1.0;
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+        pa *= (A[l][1] * px[l] + A[l][2] * py[l]) + A[l][0];
+        pb *= (B[l][1] * px[l] + B[l][2] * py[l]) + B[l][0];
+    }
+    const double common = (pa + pb) * th;
+    s0 += common;
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+        sx[l] = fma(px[l], common, sx[l]);
+        sy[l] = fma(py[l], common, sy[l]);
+    }
+}
+
 // RATE: scattering-rate variant (rate_leg >= 0), a separate instantiation so
-// that the propagate path keeps its register allocation.
-template <int L, bool RATE>
+// that the propagate path keeps its register allocation.  LIST: tup is a
+// ThetaList's ids (row stride n), mask / perm its masks and original indices.
+// SACC: the block adds its results into a shared-memory copy of the legs'
+// bands (one block of c.sinst doubles per instance) and adds that copy to
+// acc once at the end.  Small meshes make the accumulator a few KB, so FP64
+// atomics from every SM into it contend on a few L2 lines; in shared memory
+// they stay on the SM.
+template <int L, bool RATE, bool LIST, bool SACC>
 __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* __restrict__ insts, int n_insts,
                                                       const int32_t* __restrict__ tup, int64_t stride, int64_t n,
+                                                      const uint64_t* __restrict__ mask, const int32_t* __restrict__ perm,
                                                       const double* __restrict__ f, double* __restrict__ acc,
                                                       const DPCtl* __restrict__ ctl, int rate_leg) {
     extern __shared__ double s_mc[];
     constexpr int R = 2 * (L - 2) + 1;
+    double* s_acc = s_mc + c.nmc * R;   // SACC: [n_insts][c.sinst]
     for (int i = threadIdx.x; i < c.nmc * R; i += blockDim.x) s_mc[i] = c.mc[i];
+    if (SACC)
+        for (int i = threadIdx.x; i < n_insts * c.sinst; i += blockDim.x) s_acc[i] = 0.0;
     __syncthreads();
     const double inv_fact_nmc = c.fact * double(c.nmc);
     // warp-uniform loop: every lane of a warp shares `base`, so the warp
@@ -50,31 +99,11 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* 
         // simplex tests must agree with the unfused reference evaluation,
         // so every point whose fast alpha lies within a rigorous rounding
         // bound of a test boundary is re-evaluated in the exact order.
-        double G[3][R], a0[3], mg[3];
-        {
-            double rho[3];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                double t = fabs(g.N[k]);
-#pragma unroll
-                for (int j = 0; j < R; ++j) t += fabs(g.D[k][j]);
-                rho[k] = t;
-            }
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                a0[r] = Ci[r][0] * g.N[0] + Ci[r][1] * g.N[1] + Ci[r][2] * g.N[2];
-                double sg = 0.0;
-#pragma unroll
-                for (int j = 0; j < R; ++j) {
-                    G[r][j] = -(Ci[r][0] * g.D[0][j] + Ci[r][1] * g.D[1][j] + Ci[r][2] * g.D[2][j]);
-                    sg += fabs(G[r][j]);
-                }
-                const double sc = fabs(Ci[r][0]) * rho[0] + fabs(Ci[r][1]) * rho[1] + fabs(Ci[r][2]) * rho[2];
-                mg[r] = 32.0 * 1.1102230246251565e-16 * (sc + fabs(a0[r]) + sg);
-            }
-        }
+        AlphaMap<L> am;
+        alpha_map<L>(g, Ci, am);
+        const uint64_t mk0 = (LIST && valid) ? __ldg(reinterpret_cast<const unsigned long long*>(mask) + i) : 0ull;
         // functAmplitude of this tuple (fullAmplitude = amplitude * volumes * functAmplitude)
-        const double tf = (c.tamp && valid) ? __ldg(c.tamp + i) : 1.0;
+        const double tf = (c.tamp && valid) ? __ldg(c.tamp + (LIST ? int64_t(__ldg(perm + i)) : i)) : 1.0;
         for (int k = 0; k < n_insts; ++k) {
             const InstDev in = insts[k];
             if (in.amp_full == 0.0) continue;
@@ -108,43 +137,19 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* 
             double s0 = 0.0, sx[L], sy[L];
 #pragma unroll
             for (int l = 0; l < L; ++l) { sx[l] = 0.0; sy[l] = 0.0; }
-            for (int m = 0; m < c.nmc; ++m) {
-                const double* q = s_mc + m * R;
-                double qv[R];
-#pragma unroll
-                for (int j = 0; j < R; ++j) qv[j] = q[j];
-                double al[3];
-#pragma unroll
-                for (int r = 0; r < 3; ++r) {
-                    double t = a0[r];
-#pragma unroll
-                    for (int j = 0; j < R; ++j) t = fma(G[r][j], qv[j], t);
-                    al[r] = t;
+            if (LIST) {
+                for (uint64_t mk = mk0; mk; mk &= mk - 1) {
+                    const double* qv = s_mc + (__ffsll((long long)mk) - 1) * R;
+                    double al[3];
+                    alpha_fast<L>(am, qv, al);
+                    mc_point_accumulate<L>(A, B, qv, al, 1.0, s0, sx, sy);
                 }
-                const double kp0 = qv[R - 1];
-                const double tiny = 8.0 * 1.1102230246251565e-16;
-                const bool near = (fabs(al[0]) <= mg[0]) || (fabs(al[1]) <= mg[1]) || (fabs(al[2]) <= mg[2]) ||
-                                  (fabs(kp0 + al[0] - 1.0) <= mg[0] + tiny * (2.0 + fabs(al[0]))) ||
-                                  (fabs(al[1] + al[2] - 1.0) <= mg[1] + mg[2] + tiny * (1.0 + fabs(al[1]) + fabs(al[2])));
-                if (near) exact_alpha<L>(g, Ci, qv, al);
-                const bool th = theta_of(kp0, al);
-                double px[L], py[L];
-#pragma unroll
-                for (int l = 0; l < L - 2; ++l) { px[l] = qv[2 * l]; py[l] = qv[2 * l + 1]; }
-                px[L - 2] = kp0; py[L - 2] = al[0];
-                px[L - 1] = al[1]; py[L - 1] = al[2];
-                double pa = 1.0, pb = 1.0;
-#pragma unroll
-                for (int l = 0; l < L; ++l) {
-                    pa *= (A[l][1] * px[l] + A[l][2] * py[l]) + A[l][0];
-                    pb *= (B[l][1] * px[l] + B[l][2] * py[l]) + B[l][0];
-                }
-                const double common = (pa + pb) * (th ? 1.0 : 0.0);
-                s0 += common;
-#pragma unroll
-                for (int l = 0; l < L; ++l) {
-                    sx[l] = fma(px[l], common, sx[l]);
-                    sy[l] = fma(py[l], common, sy[l]);
+            } else {
+                for (int m = 0; m < c.nmc; ++m) {
+                    const double* qv = s_mc + m * R;
+                    double al[3];
+                    const bool th = alpha_theta<L>(g, Ci, am, qv, al);
+                    mc_point_accumulate<L>(A, B, qv, al, th ? 1.0 : 0.0, s0, sx, sy);
                 }
             }
             const double scale = valid ? 1.0 / (inv_fact_nmc * fabs(g.det)) : 0.0;
@@ -152,45 +157,93 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* 
             for (int l = 0; l < L; ++l) {
                 if (RATE && l != rate_leg) continue;   // uniform: the rate keeps one leg
                 const double d = RATE ? -c.leg[l].dir : c.leg[l].dir;
-                const int64_t key = in.foff[l] + 3 * (int64_t)e[l];
+                const int64_t key = SACC ? int64_t(k * c.sinst + c.sseg[l] + 3 * e[l]) : in.foff[l] + 3 * (int64_t)e[l];
+                double* const dst = (SACC ? s_acc : acc) + key;
                 if (l < L - 1) {
-                    warp_scatter3(valid ? key : -1, acc + key, d * ((scale * s0) * ampt),
-                                  d * ((scale * sx[l]) * ampt), d * ((scale * sy[l]) * ampt));
+                    warp_scatter3(valid ? key : -1, dst, d * ((scale * s0) * ampt), d * ((scale * sx[l]) * ampt),
+                                  d * ((scale * sy[l]) * ampt));
                 } else if (valid) {
-                    double* o = acc + key;
-                    atomicAdd(o + 0, d * ((scale * s0) * ampt));
-                    atomicAdd(o + 1, d * ((scale * sx[l]) * ampt));
-                    atomicAdd(o + 2, d * ((scale * sy[l]) * ampt));
+                    atomicAdd(dst + 0, d * ((scale * s0) * ampt));
+                    atomicAdd(dst + 1, d * ((scale * sx[l]) * ampt));
+                    atomicAdd(dst + 2, d * ((scale * sy[l]) * ampt));
                 }
             }
         }
     }
+    if (SACC) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < n_insts * c.sinst; i += blockDim.x) {
+            const double v = s_acc[i];
+            if (v == 0.0) continue;   // adding zero changes nothing
+            const int k = i / c.sinst, r = i - k * c.sinst;
+            int sg = 0;
+            while (sg + 1 < c.nseg && r >= c.seg_off[sg + 1]) ++sg;
+            atomicAdd(acc + insts[k].foff[c.seg_leg[sg]] + (r - c.seg_off[sg]), v);
+        }
+    }
+}
+
+template <int L, bool RATE, bool LIST, bool SACC>
+static int launch_mc(const ChanDev& c, const InstDev* insts, int n_insts, const int32_t* tup, int64_t stride,
+                     int64_t n, const uint64_t* mask, const int32_t* perm, const double* f, double* acc,
+                     const DPCtl* ctl, cudaStream_t s, int grid_hint, int rate_leg) {
+    auto kern = k_collision_mc<L, RATE, LIST, SACC>;
+    const int threads = 256;
+    int64_t blocks = (n + threads - 1) / threads;
+    size_t smem = sizeof(double) * size_t(c.nmc) * c.R;
+    if (SACC) {
+        smem += sizeof(double) * size_t(n_insts) * size_t(c.sinst);
+        static bool attr = false;
+        if (!attr) {
+            TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(TB_MC_SACC_MAX_BYTES + sizeof(double) * 64 * 5)));
+            attr = true;
+        }
+        // one wave of resident blocks: each block clears and flushes its copy once
+        int dev = 0, nsm = 148, per_sm = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+        if (per_sm < 1) per_sm = 1;
+        if (blocks > int64_t(nsm) * per_sm) blocks = int64_t(nsm) * per_sm;
+    } else if (grid_hint > 0 && blocks > grid_hint) {
+        blocks = grid_hint;
+    }
+    kern<<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, mask, perm, f, acc, ctl,
+                                                 RATE ? rate_leg : -1);
+    TB_CUDA(cudaGetLastError());
+    return TB_OK;
+}
+
+template <int L>
+static int launch_mc_l(const ChanDev& c, const InstDev* insts, int n_insts, const int32_t* tup, int64_t stride,
+                       int64_t n, const uint64_t* mask, const int32_t* perm, const double* f, double* acc,
+                       const DPCtl* ctl, cudaStream_t s, int grid_hint, int rate_leg) {
+    const bool list = mask != nullptr;
+    const bool sacc = list && c.sinst > 0 && c.nmc <= 64 &&
+                      sizeof(double) * size_t(n_insts) * size_t(c.sinst) <= TB_MC_SACC_MAX_BYTES;
+#define TB_MC_ARGS c, insts, n_insts, tup, stride, n, mask, perm, f, acc, ctl, s, grid_hint, rate_leg
+    if (rate_leg >= 0) {
+        if (sacc) return launch_mc<L, true, true, true>(TB_MC_ARGS);
+        if (list) return launch_mc<L, true, true, false>(TB_MC_ARGS);
+        return launch_mc<L, true, false, false>(TB_MC_ARGS);
+    }
+    if (sacc) return launch_mc<L, false, true, true>(TB_MC_ARGS);
+    if (list) return launch_mc<L, false, true, false>(TB_MC_ARGS);
+    return launch_mc<L, false, false, false>(TB_MC_ARGS);
+#undef TB_MC_ARGS
 }
 
 int launch_collision_mc(const ChanDev& c, const InstDev* insts, int n_insts, const int32_t* tup, int64_t stride,
                         int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s, int grid_hint,
-                        int rate_leg) {
+                        int rate_leg, const uint64_t* mask, const int32_t* perm) {
     if (n <= 0 || n_insts <= 0) return TB_OK;
-    const int threads = 256;
-    int64_t blocks = (n + threads - 1) / threads;
-    if (grid_hint > 0 && blocks > grid_hint) blocks = grid_hint;
-    const size_t smem = sizeof(double) * size_t(c.nmc) * c.R;
-#define TB_MC_LAUNCH(LL)                                                                                           \
-    if (rate_leg >= 0)                                                                                             \
-        k_collision_mc<LL, true><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, acc, \
-                                                                          ctl, rate_leg);                          \
-    else                                                                                                           \
-        k_collision_mc<LL, false><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f,     \
-                                                                           acc, ctl, -1);
     switch (c.L) {
-        case 2: TB_MC_LAUNCH(2) break;
-        case 3: TB_MC_LAUNCH(3) break;
-        case 4: TB_MC_LAUNCH(4) break;
+        case 2: return launch_mc_l<2>(c, insts, n_insts, tup, stride, n, mask, perm, f, acc, ctl, s, grid_hint, rate_leg);
+        case 3: return launch_mc_l<3>(c, insts, n_insts, tup, stride, n, mask, perm, f, acc, ctl, s, grid_hint, rate_leg);
+        case 4: return launch_mc_l<4>(c, insts, n_insts, tup, stride, n, mask, perm, f, acc, ctl, s, grid_hint, rate_leg);
         default: set_error("nlegs must be 2..4"); return TB_ERR_ARG;
     }
-#undef TB_MC_LAUNCH
-    TB_CUDA(cudaGetLastError());
-    return TB_OK;
 }
 
 // ------------------------------------------------------------ inverse mass

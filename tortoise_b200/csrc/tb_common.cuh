@@ -93,6 +93,13 @@ struct ChanDev {
     // functAmplitude at the tuple's element barycentres, one factor per tuple
     // of the group's list (ScatteringChannel.cpp:399-415); null: 1
     const double* tamp = nullptr;
+    // Shared-memory accumulation (Monte-Carlo kernels): one instance's block
+    // holds the distinct bands of the legs as segments of 3 ne doubles each.
+    int nseg = 0;
+    int sinst = 0;                    // doubles per instance (all segments)
+    int sseg[TB_MAX_LEGS] = {};       // per leg: offset of its band's segment
+    int seg_off[TB_MAX_LEGS] = {};    // per segment: offset in the block
+    int seg_leg[TB_MAX_LEGS] = {};    // per segment: a leg of that band (its foff)
 };
 
 // Mesh data needed by the element-wise kernels.

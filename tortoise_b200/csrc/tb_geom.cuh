@@ -118,6 +118,72 @@ __device__ __forceinline__ bool theta_of(double kp0, const double (&al)[3]) {
     return thp && thc;
 }
 
+// The affine map q -> alpha = G q + alpha0 (G = -DC^-1 DF, alpha0 = DC^-1 N)
+// of one tuple, for the fast fused evaluation, with a rigorous rounding
+// bound mg per coordinate: a point whose fast alpha lies farther than that
+// from every simplex boundary gets the same Theta as the unfused reference
+// order; the others are re-evaluated exactly (alpha_theta).
+template <int L>
+struct AlphaMap {
+    static constexpr int R = 2 * (L - 2) + 1;
+    double G[3][R], a0[3], mg[3];
+};
+
+template <int L>
+__device__ __forceinline__ void alpha_map(const TupleGeom<L>& g, const double (&Ci)[3][3], AlphaMap<L>& am) {
+    constexpr int R = AlphaMap<L>::R;
+    double rho[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double t = fabs(g.N[k]);
+#pragma unroll
+        for (int j = 0; j < R; ++j) t += fabs(g.D[k][j]);
+        rho[k] = t;
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        am.a0[r] = Ci[r][0] * g.N[0] + Ci[r][1] * g.N[1] + Ci[r][2] * g.N[2];
+        double sg = 0.0;
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            am.G[r][j] = -(Ci[r][0] * g.D[0][j] + Ci[r][1] * g.D[1][j] + Ci[r][2] * g.D[2][j]);
+            sg += fabs(am.G[r][j]);
+        }
+        const double sc = fabs(Ci[r][0]) * rho[0] + fabs(Ci[r][1]) * rho[1] + fabs(Ci[r][2]) * rho[2];
+        am.mg[r] = 32.0 * 1.1102230246251565e-16 * (sc + fabs(am.a0[r]) + sg);
+    }
+}
+
+// Fast constrained coordinates of point qv (fused multiply-adds).
+template <int L>
+__device__ __forceinline__ void alpha_fast(const AlphaMap<L>& am, const double* qv, double (&al)[3]) {
+    constexpr int R = AlphaMap<L>::R;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        double t = am.a0[r];
+#pragma unroll
+        for (int j = 0; j < R; ++j) t = fma(am.G[r][j], qv[j], t);
+        al[r] = t;
+    }
+}
+
+// Constrained coordinates and Theta of point qv with the reference's
+// decisions: the fast value, re-evaluated in the exact order when it lies
+// within the rounding bound of a simplex boundary.
+template <int L>
+__device__ __forceinline__ bool alpha_theta(const TupleGeom<L>& g, const double (&Ci)[3][3], const AlphaMap<L>& am,
+                                            const double* qv, double (&al)[3]) {
+    constexpr int R = AlphaMap<L>::R;
+    alpha_fast<L>(am, qv, al);
+    const double kp0 = qv[R - 1];
+    const double tiny = 8.0 * 1.1102230246251565e-16;
+    const bool near = (fabs(al[0]) <= am.mg[0]) || (fabs(al[1]) <= am.mg[1]) || (fabs(al[2]) <= am.mg[2]) ||
+                      (fabs(kp0 + al[0] - 1.0) <= am.mg[0] + tiny * (2.0 + fabs(al[0]))) ||
+                      (fabs(al[1] + al[2] - 1.0) <= am.mg[1] + am.mg[2] + tiny * (1.0 + fabs(al[1]) + fabs(al[2])));
+    if (near) exact_alpha<L>(g, Ci, qv, al);
+    return theta_of(kp0, al);
+}
+
 // Constrained coordinates of one MC point q (row of the MC table),
 // IntegratorCore.hpp:298-320:  alpha = -DC^-1 (DF q - N).
 // Returns the simplex tests ThetapC * ThetaFC (IntegratorCore.hpp:318-320);

@@ -11,6 +11,7 @@
 #include "tb_enumerate.cuh"
 #include "tb_kernels.cuh"
 #include "tb_tensor.cuh"
+#include "tb_theta.cuh"
 
 namespace tb {
 
@@ -29,6 +30,7 @@ struct GroupChan {
     int64_t diag[3] = {0, 0, 0};
     int layout = TB_LAYOUT_MC64;
     MomentTensor tensor;
+    ThetaList theta;              // Monte-Carlo layout: tuples with points inside the simplices, and which
     std::vector<int> insts;       // channel instances using it (run order)
     InstDev* d_insts = nullptr;   // [insts.size()]
 };

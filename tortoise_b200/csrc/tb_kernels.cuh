@@ -35,10 +35,12 @@ struct ElemDev {
 // (before M^-1), added into acc.  ctl (per run, may be null) lets finished
 // runs skip their work inside a batched integration.  rate_leg >= 0 computes
 // instead the scattering rate of that leg (its forms replaced by the in / out
-// unit forms, only its block kept, with the opposite sign).
+// unit forms, only its block kept, with the opposite sign).  mask / perm
+// non-null: tup, stride, n describe a ThetaList (tb_theta.cuh) and only the
+// points inside the simplices are evaluated.
 int launch_collision_mc(const ChanDev& c, const InstDev* insts, int n_insts, const int32_t* tup, int64_t stride,
                         int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s, int grid_hint,
-                        int rate_leg = -1);
+                        int rate_leg = -1, const uint64_t* mask = nullptr, const int32_t* perm = nullptr);
 
 // Vlasov drift (volume minus upwind surface term, before M^-1) of every band
 // with a nonzero drift velocity, added into acc.

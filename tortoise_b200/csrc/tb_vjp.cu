@@ -89,9 +89,12 @@ __device__ __forceinline__ void leg_forms(const ChanDev& c, const InstDev& in, c
 }
 
 // --------------------------------------------- collision VJP, Monte-Carlo
-template <int L>
+// LIST: tup / stride / n describe a ThetaList (tb_theta.cuh) and every tuple
+// visits only the set bits of its mask, the points whose Theta is 1.
+template <int L, bool LIST>
 __global__ void __launch_bounds__(128) k_vjp_mc(ChanDev c, const InstDev* __restrict__ insts, int n_insts,
                                                 const int32_t* __restrict__ tup, int64_t stride, int64_t n,
+                                                const uint64_t* __restrict__ mask, const int32_t* __restrict__ perm,
                                                 const double* __restrict__ f, const double* __restrict__ u,
                                                 double* __restrict__ grad_f, double* __restrict__ grad_amp) {
     extern __shared__ double s_mc[];
@@ -111,7 +114,9 @@ __global__ void __launch_bounds__(128) k_vjp_mc(ChanDev c, const InstDev* __rest
         double Ci[3][3];
         dc_inverse<L>(g, Ci);
         const double scale = valid ? 1.0 / (c.fact * double(c.nmc) * fabs(g.det)) : 0.0;
-        const double tf = (c.tamp && valid) ? __ldg(c.tamp + i) : 1.0;   // functAmplitude of the tuple
+        // functAmplitude of the tuple
+        const double tf = (c.tamp && valid) ? __ldg(c.tamp + (LIST ? int64_t(__ldg(perm + i)) : i)) : 1.0;
+        const uint64_t mk0 = (LIST && valid) ? __ldg(reinterpret_cast<const unsigned long long*>(mask) + i) : 0ull;
         for (int k = 0; k < n_insts; ++k) {
             const InstDev in = insts[k];
             double A[L][3], B[L][3], sa[L], sb[L];
@@ -127,7 +132,12 @@ __global__ void __launch_bounds__(128) k_vjp_mc(ChanDev c, const InstDev* __rest
 #pragma unroll
                 for (int j = 0; j < 3; ++j) { gA[l][j] = 0.0; gB[l][j] = 0.0; }
             if (valid) {
-                for (int m = 0; m < c.nmc; ++m) {
+                uint64_t mk = mk0;
+                for (int m = 0; LIST ? (mk != 0) : (m < c.nmc); ++m) {
+                    if (LIST) {
+                        m = __ffsll((long long)mk) - 1;
+                        mk &= mk - 1;
+                    }
                     const double* qv = s_mc + m * R;
                     double p[L][2];
                     if (!mc_point_exact<L>(g, Ci, qv, p)) continue;
@@ -314,18 +324,23 @@ __global__ void __launch_bounds__(128) k_vjp_tensor(ChanDev c, const InstDev* __
 
 int launch_collision_vjp(const ChanDev& c, const InstDev* insts, int n_insts, int layout, const MomentTensor& T,
                          const int32_t* tup, int64_t stride, int64_t n, const double* f, const double* u,
-                         double* grad_f, double* grad_amp, cudaStream_t s) {
+                         double* grad_f, double* grad_amp, cudaStream_t s, const uint64_t* mask,
+                         const int32_t* perm) {
     if (n <= 0 || n_insts <= 0) return TB_OK;
     const int threads = 128;
     int64_t blocks = (n + threads - 1) / threads;
     if (blocks > 148 * 64) blocks = 148 * 64;
     if (layout == TB_LAYOUT_MC64) {
         const size_t smem = sizeof(double) * size_t(c.nmc) * c.R;
+#define TB_VJP_MC(LL, LS) k_vjp_mc<LL, LS><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, \
+                                                                                 mask, perm, f, u, grad_f, grad_amp)
+        const bool list = mask != nullptr;
         switch (c.L) {
-            case 2: k_vjp_mc<2><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, u, grad_f, grad_amp); break;
-            case 3: k_vjp_mc<3><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, u, grad_f, grad_amp); break;
-            default: k_vjp_mc<4><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, f, u, grad_f, grad_amp); break;
+            case 2: if (list) TB_VJP_MC(2, true); else TB_VJP_MC(2, false); break;
+            case 3: if (list) TB_VJP_MC(3, true); else TB_VJP_MC(3, false); break;
+            default: if (list) TB_VJP_MC(4, true); else TB_VJP_MC(4, false); break;
         }
+#undef TB_VJP_MC
     } else {
         const int TT = tile_tuples(c.L, T.kind);
 #define TB_VJP_T(LL, KK) k_vjp_tensor<LL, KK><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, T.d, TT, tup, \

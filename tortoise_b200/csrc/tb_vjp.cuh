@@ -16,7 +16,8 @@ int launch_project(const ElemDev& ed, double* v, cudaStream_t s);
 // instance k of one channel group (u is the pre-M^-1 co-state).
 int launch_collision_vjp(const ChanDev& c, const InstDev* insts, int n_insts, int layout, const MomentTensor& T,
                          const int32_t* tup, int64_t stride, int64_t n, const double* f, const double* u,
-                         double* grad_f, double* grad_amp, cudaStream_t s);
+                         double* grad_f, double* grad_amp, cudaStream_t s, const uint64_t* mask = nullptr,
+                         const int32_t* perm = nullptr);
 
 // grad_f += V^T u (Vlasov drift).
 int launch_drift_vjp(const ElemDev& ed, const double* u, double* grad_f, cudaStream_t s);

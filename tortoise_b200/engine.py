@@ -92,6 +92,7 @@ def lib():
         L.tb_channel_schedule.argtypes = [vp, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                           C.POINTER(C.c_double)]
         L.tb_set_channel_schedule.argtypes = [vp, C.c_int, C.c_int32, C.c_int32]
+        L.tb_channel_points_inside.argtypes = [vp, C.c_int, C.POINTER(i64), C.POINTER(i64)]
         L.tb_create_batch.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int, C.POINTER(Options)]
         L.tb_num_runs.argtypes = [vp]
         L.tb_run_info.argtypes = [vp, C.c_int, C.POINTER(i64), C.POINTER(i64), C.POINTER(C.c_int32),
@@ -261,6 +262,13 @@ class Engine:
         _check(lib().tb_channel_info(self.h, ch, C.byref(n), C.byref(p), C.byref(d), C.byref(lay)), "tb_channel_info")
         return {"n_tuples": n.value, "n_prefilter": p.value, "n_det": d.value, "layout": LAYOUT_NAMES.get(lay.value)}
 
+    def points_inside(self, ch):
+        """(tuples with a Monte-Carlo point inside the simplices, such points),
+        or (-1, -1) when the channel has no such list."""
+        n, p = C.c_int64(), C.c_int64()
+        _check(lib().tb_channel_points_inside(self.h, ch, C.byref(n), C.byref(p)), "tb_channel_points_inside")
+        return n.value, p.value
+
     def write_scatt_indices(self, ch, path):
         """The channel's tuple list in the reference's .scattIndices format."""
         _check(lib().tb_write_scatt_indices(self.h, ch, os.fsencode(path)), "tb_write_scatt_indices")
@@ -278,18 +286,26 @@ class Engine:
             raise ValueError("a shard id has %d bytes" % SHARD_ID_BYTES)
         _check(lib().tb_shard_connect(self.h, bytes(unique_id), float(timeout_s)), "tb_shard_connect")
 
-    def set_schedule(self, ch, stages, pair=0, runs=0):
+    def set_schedule(self, ch, stages, pair=0, runs=0, inside_only=None):
         """Pins the contraction schedule of channel ch's group (tb_set_channel_schedule):
-        runs = 32, 16, 8 or 4 selects the run-minor contraction, else pair = 0 or 1."""
-        code = {32: 2, 8: 3, 4: 4, 16: 5}[runs] if runs else int(pair)
+        runs = 32, 16, 8 or 4 selects the run-minor contraction, else pair = 0 or 1.
+        Monte-Carlo channels: stages 0 and inside_only = True (only the points
+        inside the simplices) or False (every point of every tuple)."""
+        if inside_only is not None:
+            code = 6 if inside_only else 0
+        else:
+            code = {32: 2, 8: 3, 4: 4, 16: 5}[runs] if runs else int(pair)
         _check(lib().tb_set_channel_schedule(self.h, ch, int(stages), code), "tb_set_channel_schedule")
 
     def schedule(self, ch):
         st, pr, sec = C.c_int32(), C.c_int32(), C.c_double()
         _check(lib().tb_channel_schedule(self.h, ch, C.byref(st), C.byref(pr), C.byref(sec)), "tb_channel_schedule")
         # runs: run-minor lane-group width (32, 16, 8 or 4 runs per tuple), 0 = off
-        return {"stages": st.value, "pair": int(pr.value == 1), "runs": {2: 32, 3: 8, 4: 4, 5: 16}.get(pr.value, 0),
-                "tuned_seconds": sec.value}
+        d = {"stages": st.value, "pair": int(pr.value == 1), "runs": {2: 32, 3: 8, 4: 4, 5: 16}.get(pr.value, 0),
+             "tuned_seconds": sec.value}
+        if pr.value == 6:   # Monte-Carlo channel visiting only the points inside the simplices
+            d["inside_only"] = True
+        return d
 
     def tuples(self, ch):
         info = self.channel_info(ch)
