@@ -163,7 +163,7 @@ def test_points_inside_only_beyond_the_shared_accumulator(gpu_lib):
     run) would exceed its limit, so it adds straight into the global
     accumulator.  Against the same handle pinned to every Monte-Carlo point,
     and against a batch of the first 8 runs (shared-memory copies), the
-    operator must not change (1e-13)."""
+    operator must not change (1e-12, the FP64 parity bar)."""
     mats, states = W.ensemble_runs(256, seed=9, Ns=(4,), ee=True)
     f = np.concatenate(states)
     be = E.BatchEngine(mats, layout=E.LAYOUT_MC64)
@@ -173,7 +173,7 @@ def test_points_inside_only_beyond_the_shared_accumulator(gpu_lib):
     a = be.rhs(f)
     small = E.BatchEngine(mats[:8], layout=E.LAYOUT_MC64)
     s = small.rhs(np.concatenate(states[:8]))
-    assert rel_l2(a[:s.size], s) < 1e-13
+    assert rel_l2(a[:s.size], s) < 1e-12
     for c in live:
         be.set_schedule(c, 0, inside_only=False)
-    assert rel_l2(a, be.rhs(f)) < 1e-13
+    assert rel_l2(a, be.rhs(f)) < 1e-12
