@@ -27,6 +27,16 @@
 #ifndef TB_MC_SACC_MAX_BYTES
 #define TB_MC_SACC_MAX_BYTES (160 * 1024)
 #endif
+// Resident blocks per SM the list kernels are compiled for (register cap).
+#ifndef TB_MC_LIST_MIN_BLOCKS
+#define TB_MC_LIST_MIN_BLOCKS 1
+#endif
+// With the shared-memory accumulator, legs below this index merge equal
+// element keys across the warp before their atomics (the list is grouped by
+// the leg-0 element); the others add directly.
+#ifndef TB_MC_SACC_SCAN_LEGS
+#define TB_MC_SACC_SCAN_LEGS 4
+#endif
 
 namespace tb {
 
@@ -68,7 +78,7 @@ __device__ __forceinline__ void mc_point_accumulate(const double (&A)[L][3], con
 // atomics from every SM into it contend on a few L2 lines; in shared memory
 // they stay on the SM.
 template <int L, bool RATE, bool LIST, bool SACC>
-__global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* __restrict__ insts, int n_insts,
+__global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_collision_mc(ChanDev c, const InstDev* __restrict__ insts, int n_insts,
                                                       const int32_t* __restrict__ tup, int64_t stride, int64_t n,
                                                       const uint64_t* __restrict__ mask, const int32_t* __restrict__ perm,
                                                       const double* __restrict__ f, double* __restrict__ acc,
@@ -110,41 +120,79 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* 
             if (ctl && ctl[in.run].done) continue;
             if (!__any_sync(0xffffffffu, valid)) continue;
             const double ampt = in.amp_full * tf;
-            // commonLinForm0 (A, direct) and commonLinForm1 (B, time reversed),
-            // ScatteringChannel.cpp:633-641
-            double A[L][3], B[L][3];
-#pragma unroll
-            for (int l = 0; l < L; ++l) {
-                const double d = c.leg[l].dir, s = c.leg[l].stat;
-                const double* fe = f + in.foff[l] + 3 * (int64_t)e[l];
-                const double ka = (l == 0 ? -1.0 : 1.0) * 0.5;
-                const double ca = (1. - d) * s + (1. + d);
-                const double cb = (1. + d) * s + (1. - d);
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    const double unit = (j == 0) ? 1.0 : 0.0;
-                    const double fj = __ldg(fe + j);
-                    A[l][j] = ka * ((1. - d) * unit + ca * fj);
-                    B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
-                }
-                if (RATE && l == rate_leg) {
-                    // scattering rate of this leg: constant in / out unit forms
-                    // (ScatteringChannel.cpp:562-564)
-                    A[l][0] = (l == 0 ? -1.0 : 1.0) * ca; A[l][1] = 0.0; A[l][2] = 0.0;
-                    B[l][0] = cb; B[l][1] = 0.0; B[l][2] = 0.0;
-                }
-            }
             double s0 = 0.0, sx[L], sy[L];
 #pragma unroll
             for (int l = 0; l < L; ++l) { sx[l] = 0.0; sy[l] = 0.0; }
             if (LIST) {
+                // The leg forms as A = fa t + fa0, B = fb t + fb0 of the leg's
+                // linear form t = f0 + f1 x + f2 y (LegDev: fa, fb = +-1, fa0,
+                // fb0 in {0, +-1}), so only f stays in registers.
+                double fv[L][3];
+#pragma unroll
+                for (int l = 0; l < L; ++l) {
+                    const double* fe = f + in.foff[l] + 3 * (int64_t)e[l];
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) fv[l][j] = (RATE && l == rate_leg) ? (j == 0 ? 1.0 : 0.0) : __ldg(fe + j);
+                }
                 for (uint64_t mk = mk0; mk; mk &= mk - 1) {
                     const double* qv = s_mc + (__ffsll((long long)mk) - 1) * R;
                     double al[3];
                     alpha_fast<L>(am, qv, al);
-                    mc_point_accumulate<L>(A, B, qv, al, 1.0, s0, sx, sy);
+                    double px[L], py[L];
+#pragma unroll
+                    for (int l = 0; l < L - 2; ++l) { px[l] = qv[2 * l]; py[l] = qv[2 * l + 1]; }
+                    px[L - 2] = qv[R - 1]; py[L - 2] = al[0];
+                    px[L - 1] = al[1]; py[L - 1] = al[2];
+                    double pa = 1.0, pb = 1.0;
+#pragma unroll
+                    for (int l = 0; l < L; ++l) {
+                        const double t = fma(fv[l][2], py[l], fma(fv[l][1], px[l], fv[l][0]));
+                        double fa = c.leg[l].fa, fa0 = c.leg[l].fa0, fb = c.leg[l].fb, fb0 = c.leg[l].fb0;
+                        if (RATE && l == rate_leg) {
+                            // scattering rate of this leg: constant in / out unit
+                            // forms (ScatteringChannel.cpp:562-564)
+                            const double d = c.leg[l].dir, st = c.leg[l].stat;
+                            fa = (l == 0 ? -1.0 : 1.0) * ((1. - d) * st + (1. + d));
+                            fb = (1. + d) * st + (1. - d);
+                            fa0 = 0.0;
+                            fb0 = 0.0;
+                        }
+                        pa *= fma(fa, t, fa0);
+                        pb *= fma(fb, t, fb0);
+                    }
+                    const double common = pa + pb;
+                    s0 += common;
+#pragma unroll
+                    for (int l = 0; l < L; ++l) {
+                        sx[l] = fma(px[l], common, sx[l]);
+                        sy[l] = fma(py[l], common, sy[l]);
+                    }
                 }
             } else {
+                // commonLinForm0 (A, direct) and commonLinForm1 (B, time reversed),
+                // ScatteringChannel.cpp:633-641
+                double A[L][3], B[L][3];
+#pragma unroll
+                for (int l = 0; l < L; ++l) {
+                    const double d = c.leg[l].dir, s = c.leg[l].stat;
+                    const double* fe = f + in.foff[l] + 3 * (int64_t)e[l];
+                    const double ka = (l == 0 ? -1.0 : 1.0) * 0.5;
+                    const double ca = (1. - d) * s + (1. + d);
+                    const double cb = (1. + d) * s + (1. - d);
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        const double unit = (j == 0) ? 1.0 : 0.0;
+                        const double fj = __ldg(fe + j);
+                        A[l][j] = ka * ((1. - d) * unit + ca * fj);
+                        B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
+                    }
+                    if (RATE && l == rate_leg) {
+                        // scattering rate of this leg: constant in / out unit forms
+                        // (ScatteringChannel.cpp:562-564)
+                        A[l][0] = (l == 0 ? -1.0 : 1.0) * ca; A[l][1] = 0.0; A[l][2] = 0.0;
+                        B[l][0] = cb; B[l][1] = 0.0; B[l][2] = 0.0;
+                    }
+                }
                 for (int m = 0; m < c.nmc; ++m) {
                     const double* qv = s_mc + m * R;
                     double al[3];
@@ -159,7 +207,7 @@ __global__ void __launch_bounds__(256) k_collision_mc(ChanDev c, const InstDev* 
                 const double d = RATE ? -c.leg[l].dir : c.leg[l].dir;
                 const int64_t key = SACC ? int64_t(k * c.sinst + c.sseg[l] + 3 * e[l]) : in.foff[l] + 3 * (int64_t)e[l];
                 double* const dst = (SACC ? s_acc : acc) + key;
-                if (l < L - 1) {
+                if (l < L - 1 && (!SACC || l < TB_MC_SACC_SCAN_LEGS)) {
                     warp_scatter3(valid ? key : -1, dst, d * ((scale * s0) * ampt), d * ((scale * sx[l]) * ampt),
                                   d * ((scale * sy[l]) * ampt));
                 } else if (valid) {
