@@ -33,10 +33,6 @@
 #ifndef TB_MC_LIST_MIN_BLOCKS
 #define TB_MC_LIST_MIN_BLOCKS 2
 #endif
-// Single-run list launches sum leg 0 in registers (RACC below).
-#ifndef TB_MC_RACC
-#define TB_MC_RACC 1
-#endif
 // With the shared-memory accumulator, legs below this index merge equal
 // element keys across the warp before their atomics (the list is grouped by
 // the leg-0 element); the others add directly.  Merging every leg measured
@@ -83,11 +79,8 @@ __device__ __forceinline__ void mc_point_accumulate(const double (&A)[L][3], con
 // bands (one block of c.sinst doubles per instance) and adds that copy to
 // acc once at the end.  Small meshes make the accumulator a few KB, so FP64
 // atomics from every SM into it contend on a few L2 lines; in shared memory
-// they stay on the SM.  RACC (one instance, propagate): every warp walks one
-// contiguous chunk of the list, so a lane keeps its leg-0 element for tens of
-// steps (the list is grouped by it); the lane sums leg 0 in registers and adds
-// the sums to the shared copy only when its element changes.
-template <int L, bool RATE, bool LIST, bool SACC, bool RACC>
+// they stay on the SM.
+template <int L, bool RATE, bool LIST, bool SACC>
 __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_collision_mc(ChanDev c, const InstDev* __restrict__ insts, int n_insts,
                                                       const int32_t* __restrict__ tup, int64_t stride, int64_t n,
                                                       const uint64_t* __restrict__ mask, const int32_t* __restrict__ perm,
@@ -102,23 +95,10 @@ __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_colli
     __syncthreads();
     const double inv_fact_nmc = c.fact * double(c.nmc);
     // warp-uniform loop: every lane of a warp shares `base`, so the warp
-    // scatter below can reduce across lanes.  Grid-stride over blocks, or,
-    // with RACC, one contiguous chunk (a multiple of 32 tuples) per warp.
-    int64_t base0 = (int64_t)blockIdx.x * blockDim.x, bstep = (int64_t)gridDim.x * blockDim.x, bend = n;
-    int lane_off = threadIdx.x;
-    if (RACC) {
-        const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
-        const int64_t chunk = ((n + 32 * nw - 1) / (32 * nw)) * 32;
-        base0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * chunk;
-        bend = base0 + chunk < n ? base0 + chunk : n;
-        bstep = 32;
-        lane_off = threadIdx.x & 31;
-    }
-    int64_t rkey = -1;                    // RACC: the lane's current leg-0 key
-    double racc0 = 0.0, racc1 = 0.0, racc2 = 0.0;
-    for (int64_t base = base0; base < bend; base += bstep) {
-        const int64_t i = base + lane_off;
-        bool valid = i < bend;
+    // scatter below can reduce across lanes
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        bool valid = i < n;
         int e[L];
 #pragma unroll
         for (int l = 0; l < L; ++l) e[l] = valid ? __ldg(tup + l * stride + i) : 0;
@@ -230,23 +210,7 @@ __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_colli
                 const double d = RATE ? -c.leg[l].dir : c.leg[l].dir;
                 const int64_t key = SACC ? int64_t(k * c.sinst + c.sseg[l] + 3 * e[l]) : in.foff[l] + 3 * (int64_t)e[l];
                 double* const dst = (SACC ? s_acc : acc) + key;
-                if (RACC && l == 0) {
-                    if (valid) {
-                        const double v0 = d * ((scale * s0) * ampt), v1 = d * ((scale * sx[0]) * ampt),
-                                     v2 = d * ((scale * sy[0]) * ampt);
-                        if (key != rkey) {
-                            if (rkey >= 0) {
-                                atomicAdd(s_acc + rkey + 0, racc0);
-                                atomicAdd(s_acc + rkey + 1, racc1);
-                                atomicAdd(s_acc + rkey + 2, racc2);
-                            }
-                            rkey = key;
-                            racc0 = v0; racc1 = v1; racc2 = v2;
-                        } else {
-                            racc0 += v0; racc1 += v1; racc2 += v2;
-                        }
-                    }
-                } else if (l < L - 1 && (!SACC || l < TB_MC_SACC_SCAN_LEGS)) {
+                if (l < L - 1 && (!SACC || l < TB_MC_SACC_SCAN_LEGS)) {
                     warp_scatter3(valid ? key : -1, dst, d * ((scale * s0) * ampt), d * ((scale * sx[l]) * ampt),
                                   d * ((scale * sy[l]) * ampt));
                 } else if (valid) {
@@ -256,11 +220,6 @@ __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_colli
                 }
             }
         }
-    }
-    if (RACC && rkey >= 0) {
-        atomicAdd(s_acc + rkey + 0, racc0);
-        atomicAdd(s_acc + rkey + 1, racc1);
-        atomicAdd(s_acc + rkey + 2, racc2);
     }
     if (SACC) {
         __syncthreads();
@@ -275,11 +234,11 @@ __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_colli
     }
 }
 
-template <int L, bool RATE, bool LIST, bool SACC, bool RACC = false>
+template <int L, bool RATE, bool LIST, bool SACC>
 static int launch_mc(const ChanDev& c, const InstDev* insts, int n_insts, const int32_t* tup, int64_t stride,
                      int64_t n, const uint64_t* mask, const int32_t* perm, const double* f, double* acc,
                      const DPCtl* ctl, cudaStream_t s, int grid_hint, int rate_leg) {
-    auto kern = k_collision_mc<L, RATE, LIST, SACC, RACC>;
+    auto kern = k_collision_mc<L, RATE, LIST, SACC>;
     const int threads = 256;
     int64_t blocks = (n + threads - 1) / threads;
     size_t smem = sizeof(double) * size_t(c.nmc) * c.R;
@@ -320,7 +279,6 @@ static int launch_mc_l(const ChanDev& c, const InstDev* insts, int n_insts, cons
         if (list) return launch_mc<L, true, true, false>(TB_MC_ARGS);
         return launch_mc<L, true, false, false>(TB_MC_ARGS);
     }
-    if (TB_MC_RACC && sacc && n_insts == 1) return launch_mc<L, false, true, true, true>(TB_MC_ARGS);
     if (sacc) return launch_mc<L, false, true, true>(TB_MC_ARGS);
     if (list) return launch_mc<L, false, true, false>(TB_MC_ARGS);
     return launch_mc<L, false, false, false>(TB_MC_ARGS);
