@@ -691,7 +691,13 @@ def rhs_only(args):
     from tortoise_b200 import workloads as W
     layout = {"auto": E.LAYOUT_AUTO, "mc64": E.LAYOUT_MC64, "t64": E.LAYOUT_T64, "t32": E.LAYOUT_T32,
               "t40": E.LAYOUT_T40}[args.layout]
-    if args.batch:
+    if args.ee:
+        # one parabolic band with the four-leg e-e channel (Monte-Carlo
+        # quadrature over the points inside the simplices)
+        mat = W.parabolic_ee(args.mesh)
+        f0 = W.initial_status(mat, kT=0.1, seed=0).vec
+        eng = E.Engine(mat, layout=layout, autotune=not args.no_tune)
+    elif args.batch:
         # a batch of args.batch runs of one structure (mesh args.mesh): the
         # groups shared by many runs (run-minor contraction)
         mats, states = W.ensemble_runs(args.batch, seed=3, Ns=(args.mesh,))
@@ -729,6 +735,8 @@ def main():
     ap.add_argument("--rhs-only", type=int, default=0,
                     help="profiling driver: K RHS evaluations only (with --batch R: R runs of mesh --mesh)")
     ap.add_argument("--mesh", type=int, default=N_MESH, help="sections per side (profiling driver only)")
+    ap.add_argument("--ee", action="store_true",
+                    help="profiling driver on the one-band e-e workload (parabolic band, --mesh sections per side)")
     ap.add_argument("--batch", type=int, default=0, help="batched ensemble of this many runs (per-run N, kT, couplings)")
     ap.add_argument("--large", nargs="?", const="t32", default=None, choices=["t32", "t40"],
                     help="16-run 128x128 three-band two-phonon batch with FP32 (default) or 40-bit moments")
