@@ -22,14 +22,6 @@
 #include "tb_kernels.cuh"
 #include "tb_scatter.cuh"
 
-// Row stride (doubles) of the Monte-Carlo table in shared memory: R rounded
-// up to even, so that a row is read with 16-byte loads (three instead of
-// five loads per point for four legs) whose rows start 16-byte aligned.
-#ifndef TB_MC_PAD_ROWS
-#define TB_MC_PAD_ROWS 1
-#endif
-__host__ __device__ constexpr int mc_row_stride(int R) { return TB_MC_PAD_ROWS ? (R + 1) & ~1 : R; }
-
 // Largest shared-memory accumulator (all instances' blocks) a launch uses;
 // beyond it the results go straight to the global accumulator.
 #ifndef TB_MC_SACC_MAX_BYTES
@@ -94,14 +86,10 @@ __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_colli
                                                       const uint64_t* __restrict__ mask, const int32_t* __restrict__ perm,
                                                       const double* __restrict__ f, double* __restrict__ acc,
                                                       const DPCtl* __restrict__ ctl, int rate_leg) {
-    extern __shared__ __align__(16) double s_mc[];
+    extern __shared__ double s_mc[];
     constexpr int R = 2 * (L - 2) + 1;
-    constexpr int RP = mc_row_stride(R);
-    double* s_acc = s_mc + c.nmc * RP;   // SACC: [n_insts][c.sinst]
-    for (int i = threadIdx.x; i < c.nmc * RP; i += blockDim.x) {
-        const int m = i / RP, j = i - m * RP;
-        s_mc[i] = j < R ? c.mc[m * R + j] : 0.0;
-    }
+    double* s_acc = s_mc + c.nmc * R;   // SACC: [n_insts][c.sinst]
+    for (int i = threadIdx.x; i < c.nmc * R; i += blockDim.x) s_mc[i] = c.mc[i];
     if (SACC)
         for (int i = threadIdx.x; i < n_insts * c.sinst; i += blockDim.x) s_acc[i] = 0.0;
     __syncthreads();
@@ -150,21 +138,7 @@ __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_colli
                     for (int j = 0; j < 3; ++j) fv[l][j] = (RATE && l == rate_leg) ? (j == 0 ? 1.0 : 0.0) : __ldg(fe + j);
                 }
                 for (uint64_t mk = mk0; mk; mk &= mk - 1) {
-                    double qv[RP];
-                    {
-                        const double* row = s_mc + (__ffsll((long long)mk) - 1) * RP;
-                        if (RP % 2 == 0) {
-#pragma unroll
-                            for (int j = 0; j < RP; j += 2) {
-                                const double2 q2 = *reinterpret_cast<const double2*>(row + j);
-                                qv[j] = q2.x;
-                                qv[j + 1] = q2.y;
-                            }
-                        } else {
-#pragma unroll
-                            for (int j = 0; j < RP; ++j) qv[j] = row[j];
-                        }
-                    }
+                    const double* qv = s_mc + (__ffsll((long long)mk) - 1) * R;
                     double al[3];
                     alpha_fast<L>(am, qv, al);
                     double px[L], py[L];
@@ -223,7 +197,7 @@ __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_colli
                     }
                 }
                 for (int m = 0; m < c.nmc; ++m) {
-                    const double* qv = s_mc + m * RP;
+                    const double* qv = s_mc + m * R;
                     double al[3];
                     const bool th = alpha_theta<L>(g, Ci, am, qv, al);
                     mc_point_accumulate<L>(A, B, qv, al, th ? 1.0 : 0.0, s0, sx, sy);
@@ -267,13 +241,13 @@ static int launch_mc(const ChanDev& c, const InstDev* insts, int n_insts, const 
     auto kern = k_collision_mc<L, RATE, LIST, SACC>;
     const int threads = 256;
     int64_t blocks = (n + threads - 1) / threads;
-    size_t smem = sizeof(double) * size_t(c.nmc) * mc_row_stride(c.R);
+    size_t smem = sizeof(double) * size_t(c.nmc) * c.R;
     if (SACC) {
         smem += sizeof(double) * size_t(n_insts) * size_t(c.sinst);
         static bool attr = false;
         if (!attr) {
             TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(TB_MC_SACC_MAX_BYTES + sizeof(double) * 64 * 6)));
+                                         int(TB_MC_SACC_MAX_BYTES + sizeof(double) * 64 * 5)));
             attr = true;
         }
         // one wave of resident blocks: each block clears and flushes its copy once
