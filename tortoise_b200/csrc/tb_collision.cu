@@ -22,6 +22,11 @@
 #include "tb_kernels.cuh"
 #include "tb_scatter.cuh"
 
+// Inside-only quadrature: evaluate the points of a tuple two at a time.
+#ifndef TB_MC_PAIR_POINTS
+#define TB_MC_PAIR_POINTS 0
+#endif
+
 // Largest shared-memory accumulator (all instances' blocks) a launch uses;
 // beyond it the results go straight to the global accumulator.
 #ifndef TB_MC_SACC_MAX_BYTES
@@ -137,11 +142,12 @@ __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_colli
 #pragma unroll
                     for (int j = 0; j < 3; ++j) fv[l][j] = (RATE && l == rate_leg) ? (j == 0 ? 1.0 : 0.0) : __ldg(fe + j);
                 }
-                for (uint64_t mk = mk0; mk; mk &= mk - 1) {
-                    const double* qv = s_mc + (__ffsll((long long)mk) - 1) * R;
+                // One point inside: the legs' points and the gain-plus-loss
+                // product (the integrand without its Theta, which is 1 here).
+                auto point = [&](int m, double (&px)[L], double (&py)[L]) -> double {
+                    const double* qv = s_mc + m * R;
                     double al[3];
                     alpha_fast<L>(am, qv, al);
-                    double px[L], py[L];
 #pragma unroll
                     for (int l = 0; l < L - 2; ++l) { px[l] = qv[2 * l]; py[l] = qv[2 * l + 1]; }
                     px[L - 2] = qv[R - 1]; py[L - 2] = al[0];
@@ -163,14 +169,36 @@ __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_colli
                         pa *= fma(fa, t, fa0);
                         pb *= fma(fb, t, fb0);
                     }
-                    const double common = pa + pb;
+                    return pa + pb;
+                };
+                auto accumulate = [&](double common, const double (&px)[L], const double (&py)[L]) {
                     s0 += common;
 #pragma unroll
                     for (int l = 0; l < L; ++l) {
                         sx[l] = fma(px[l], common, sx[l]);
                         sy[l] = fma(py[l], common, sy[l]);
                     }
+                };
+#if TB_MC_PAIR_POINTS
+                // two points per step (independent chains), summed in order
+                for (uint64_t mk = mk0; mk;) {
+                    const int m1 = __ffsll((long long)mk) - 1;
+                    mk &= mk - 1;
+                    const bool two = mk != 0;
+                    const int m2 = two ? __ffsll((long long)mk) - 1 : m1;
+                    if (two) mk &= mk - 1;
+                    double px1[L], py1[L], px2[L], py2[L];
+                    const double c1 = point(m1, px1, py1);
+                    const double c2 = point(m2, px2, py2);
+                    accumulate(c1, px1, py1);
+                    if (two) accumulate(c2, px2, py2);
                 }
+#else
+                for (uint64_t mk = mk0; mk; mk &= mk - 1) {
+                    double px[L], py[L];
+                    accumulate(point(__ffsll((long long)mk) - 1, px, py), px, py);
+                }
+#endif
             } else {
                 // commonLinForm0 (A, direct) and commonLinForm1 (B, time reversed),
                 // ScatteringChannel.cpp:633-641
