@@ -22,11 +22,6 @@
 #include "tb_kernels.cuh"
 #include "tb_scatter.cuh"
 
-// Inside-only quadrature: evaluate the points of a tuple two at a time.
-#ifndef TB_MC_PAIR_POINTS
-#define TB_MC_PAIR_POINTS 0
-#endif
-
 // Largest shared-memory accumulator (all instances' blocks) a launch uses;
 // beyond it the results go straight to the global accumulator.
 #ifndef TB_MC_SACC_MAX_BYTES
@@ -179,26 +174,10 @@ __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_colli
                         sy[l] = fma(py[l], common, sy[l]);
                     }
                 };
-#if TB_MC_PAIR_POINTS
-                // two points per step (independent chains), summed in order
-                for (uint64_t mk = mk0; mk;) {
-                    const int m1 = __ffsll((long long)mk) - 1;
-                    mk &= mk - 1;
-                    const bool two = mk != 0;
-                    const int m2 = two ? __ffsll((long long)mk) - 1 : m1;
-                    if (two) mk &= mk - 1;
-                    double px1[L], py1[L], px2[L], py2[L];
-                    const double c1 = point(m1, px1, py1);
-                    const double c2 = point(m2, px2, py2);
-                    accumulate(c1, px1, py1);
-                    if (two) accumulate(c2, px2, py2);
-                }
-#else
                 for (uint64_t mk = mk0; mk; mk &= mk - 1) {
                     double px[L], py[L];
                     accumulate(point(__ffsll((long long)mk) - 1, px, py), px, py);
                 }
-#endif
             } else {
                 // commonLinForm0 (A, direct) and commonLinForm1 (B, time reversed),
                 // ScatteringChannel.cpp:633-641
