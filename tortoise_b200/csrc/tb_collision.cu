@@ -86,6 +86,15 @@ __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_colli
                                                       const uint64_t* __restrict__ mask, const int32_t* __restrict__ perm,
                                                       const double* __restrict__ f, double* __restrict__ acc,
                                                       const DPCtl* __restrict__ ctl, int rate_leg) {
+    // Nothing to add when every instance is switched off or its run has
+    // finished (the speculative DP45 attempts after the end of an
+    // integration): leave before walking the tuples.  Uniform in the block.
+    {
+        bool any = false;
+        for (int k = 0; k < n_insts && !any; ++k)
+            any = insts[k].amp_full != 0.0 && !(ctl && ctl[insts[k].run].done);
+        if (!any) return;
+    }
     extern __shared__ double s_mc[];
     constexpr int R = 2 * (L - 2) + 1;
     double* s_acc = s_mc + c.nmc * R;   // SACC: [n_insts][c.sinst]
