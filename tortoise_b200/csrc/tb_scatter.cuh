@@ -22,21 +22,18 @@ __device__ __forceinline__ void warp_scatter3(int64_t key, double* dst, double v
     const int64_t kprev = __shfl_up_sync(full, key, 1);
     const bool head = (lane == 0) || (kprev != key);
     const unsigned heads = __ballot_sync(full, head);
-    // The scan needs ceil(log2(longest run)) steps: the longest run of lanes
-    // that continue their predecessor's key (set bits of ~heads), plus one.
-    // Runs are long for the outermost leg and short for the others, whose
-    // steps past that length would add nothing.  Uniform in the warp.
-    int seglen = 1;
-    for (unsigned x = ~heads; x; x &= x << 1) ++seglen;
-#pragma unroll 1
-    for (int d = 1; d < seglen; d <<= 1) {
+    const unsigned le = (lane == 31) ? full : ((1u << (lane + 1)) - 1u);
+    const int seg = __popc(heads & le);
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
         const double t0 = __shfl_up_sync(full, v0, d);
         const double t1 = __shfl_up_sync(full, v1, d);
         const double t2 = __shfl_up_sync(full, v2, d);
-        // lane - d is in this lane's run iff no head in lanes (lane - d, lane]
-        if (lane >= d && (heads & (((1u << d) - 1u) << (lane - d + 1))) == 0) { v0 += t0; v1 += t1; v2 += t2; }
+        const int sg = __shfl_up_sync(full, seg, d);
+        if (lane >= d && sg == seg) { v0 += t0; v1 += t1; v2 += t2; }
     }
-    const bool tail = (lane == 31) || ((heads >> (lane + 1)) & 1u);
+    const int snext = __shfl_down_sync(full, seg, 1);
+    const bool tail = (lane == 31) || (snext != seg);
     if (tail && key >= 0) {
         atomicAdd(dst + 0, v0);
         atomicAdd(dst + 1, v1);
