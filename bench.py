@@ -342,6 +342,8 @@ def ours(args, world, rank, local, pg):
         line["mixed"] = mixed_measure(eng, mat, f0, args.steps, args.warmup, dev)
         eng.close()
         line["batched"] = batched_measure(256, 10, 3, "t40")
+        # the reference's own CPU case (one band, 16x16, four-leg e-e, t = 10)
+        line["reference_cpu_case"] = small_ee_measure(args.no_cpu, args.no_tune)
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()
@@ -533,6 +535,11 @@ def adjoint(args):
 
 
 def small_ee(args):
+    """Prints small_ee_measure's line."""
+    print(json.dumps(small_ee_measure(args.no_cpu, args.no_tune)), flush=True)
+
+
+def small_ee_measure(no_cpu=False, no_tune=False):
     """The reference's CPU-runnable case: one parabolic band on a 16x16 mesh
     (512 triangles), electron-electron scattering with a constant matrix
     element, Fermi-Dirac kT 0.1 / mu 0.3 plus the seeded bump, DP45 with
@@ -543,11 +550,10 @@ def small_ee(args):
     whole list, times the number of right-hand sides the GPU run needed."""
     from tortoise_b200 import engine as E
     from tortoise_b200 import workloads as W
-    import oracle
     mat = W.parabolic_ee(16)
     f0 = W.initial_status(mat, kT=0.1, seed=0).vec
     t_setup = time.perf_counter()
-    eng = E.Engine(mat, autotune=not args.no_tune)
+    eng = E.Engine(mat, autotune=not no_tune)
     t_setup = time.perf_counter() - t_setup
     info = eng.channel_info(0)
     # the collision operator alone, CUDA events on the library's stream:
@@ -587,7 +593,8 @@ def small_ee(args):
             "gpu": {"seconds": gpu_s, "status": r["status"], "attempts": r["attempts"], "accepted": r["accepted"],
                     "rejected": r["rejected"], "rhs_evals": r["rhs_evals"], "t": r["t"],
                     "attempts_per_s": r["attempts"] / gpu_s}}
-    if not args.no_cpu:
+    if not no_cpu:
+        import oracle   # the CPU baseline of this case
         ids, umk = eng.tuples(0)
         m = min(len(umk), 200_000)
         o = oracle.Oracle(mat, enumerate_tuples=False, nthreads=os.cpu_count())
@@ -606,8 +613,8 @@ def small_ee(args):
     c = clk.summary()
     if c:
         line["clocks"] = c
-    print(json.dumps(line), flush=True)
     eng.close()
+    return line
 
 
 def large(args):
