@@ -1326,6 +1326,17 @@ double or_veto_step(void* h, double t, double dt, double dense) {
     return veto_step(*static_cast<Problem*>(h), times, 6, dense);
 }
 
+// MaterialTimeStatus::timeStepVetoer(timesToTest, denseStep)
+// (MaterialTimeStatus.cpp:60-100) on the caller's times.
+double or_veto_times(void* h, const double* times, int ntimes, double dense) {
+    try {
+        return veto_step(*static_cast<Problem*>(h), times, ntimes, dense);
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return NAN;
+    }
+}
+
 // stats: [attempts, accepted, rejected, rhs_evals] and dstats: [t, dt, last_err]
 int or_dp45(void* h, double* y, double t0, double tf, double dense, double* dense_out, double* dense_t,
             int max_dense, int* n_dense, int nthreads, int drift, int64_t max_attempts, int64_t* stats,
