@@ -6,12 +6,16 @@
 // __graft_entry__.smoke() and by bench.py's CPU-baseline leg as the checker;
 // the product (tortoise_b200/) never links, imports or calls it.
 //
-// Parity status: the reference cannot be compiled here (Eigen 3.4 and oneTBB
-// are absent) and ships no tests or golden vectors, so this restatement is
-// pinned only by the physical identities the reference's algorithm obeys
-// (tests/test_oracle_*.py: particle-number conservation per tuple, detailed
-// balance at equilibrium, DP54 on the scalar ODE of DormandPrince54.hpp:80-106,
-// mass-matrix identities).  "parity unpinned" against the reference binary.
+// Parity status: the reference as a whole cannot be compiled here (Eigen 3.4
+// and oneTBB are absent) and ships no tests or golden vectors.  Its
+// Dormand-Prince integrator needs neither: oracle/ref_dp54_harness.cpp builds
+// it from the reference tree, and tests/test_oracle_ref_dp54.py requires the
+// restated integrator below (dp54_core) to take the same steps and give
+// bit-identical dense outputs on the same operators.  The collision operator,
+// error norm and drift are pinned only by the physical identities the
+// reference's algorithm obeys (tests/test_oracle.py: particle-number
+// conservation per tuple, detailed balance at equilibrium, mass-matrix
+// identities): "parity unpinned" against the reference binary for those.
 //
 // Every function cites the reference file:line it follows (paths relative to
 // the TORTOISE project root).
