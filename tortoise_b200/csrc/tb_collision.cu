@@ -22,12 +22,6 @@
 #include "tb_kernels.cuh"
 #include "tb_scatter.cuh"
 
-// Inside-only points: split the coordinate sums and multiply the leg factors
-// as a tree (shorter dependency chains; results change at rounding level).
-#ifndef TB_MC_SHORT_CHAINS
-#define TB_MC_SHORT_CHAINS 1
-#endif
-
 // Largest shared-memory accumulator (all instances' blocks) a launch uses;
 // beyond it the results go straight to the global accumulator.
 #ifndef TB_MC_SACC_MAX_BYTES
@@ -157,26 +151,12 @@ __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_colli
                 auto point = [&](int m, double (&px)[L], double (&py)[L]) -> double {
                     const double* qv = s_mc + m * R;
                     double al[3];
-#if TB_MC_SHORT_CHAINS
-                    // two partial sums per coordinate: a shorter dependency chain
-#pragma unroll
-                    for (int r = 0; r < 3; ++r) {
-                        double ta = am.a0[r], tb = 0.0;
-#pragma unroll
-                        for (int j = 0; j < R; ++j) {
-                            if (j % 2 == 0) ta = fma(am.G[r][j], qv[j], ta);
-                            else tb = fma(am.G[r][j], qv[j], tb);
-                        }
-                        al[r] = ta + tb;
-                    }
-#else
                     alpha_fast<L>(am, qv, al);
-#endif
 #pragma unroll
                     for (int l = 0; l < L - 2; ++l) { px[l] = qv[2 * l]; py[l] = qv[2 * l + 1]; }
                     px[L - 2] = qv[R - 1]; py[L - 2] = al[0];
                     px[L - 1] = al[1]; py[L - 1] = al[2];
-                    double fa_[L], fb_[L];
+                    double pa = 1.0, pb = 1.0;
 #pragma unroll
                     for (int l = 0; l < L; ++l) {
                         const double t = fma(fv[l][2], py[l], fma(fv[l][1], px[l], fv[l][0]));
@@ -190,24 +170,9 @@ __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_colli
                             fa0 = 0.0;
                             fb0 = 0.0;
                         }
-                        fa_[l] = fma(fa, t, fa0);
-                        fb_[l] = fma(fb, t, fb0);
+                        pa *= fma(fa, t, fa0);
+                        pb *= fma(fb, t, fb0);
                     }
-#if TB_MC_SHORT_CHAINS
-                    // the leg factors multiplied as a tree
-                    double pa = fa_[0], pb = fb_[0];
-                    if (L == 4) {
-                        pa = (fa_[0] * fa_[1]) * (fa_[2] * fa_[L - 1]);
-                        pb = (fb_[0] * fb_[1]) * (fb_[2] * fb_[L - 1]);
-                    } else {
-#pragma unroll
-                        for (int l = 1; l < L; ++l) { pa *= fa_[l]; pb *= fb_[l]; }
-                    }
-#else
-                    double pa = 1.0, pb = 1.0;
-#pragma unroll
-                    for (int l = 0; l < L; ++l) { pa *= fa_[l]; pb *= fb_[l]; }
-#endif
                     return pa + pb;
                 };
                 auto accumulate = [&](double common, const double (&px)[L], const double (&py)[L]) {
