@@ -64,6 +64,7 @@ def lib():
         L.or_apply_constraints_at.argtypes = [vp, dp, C.c_double]
         L.or_veto_step.restype = C.c_double
         L.or_veto_step.argtypes = [vp, C.c_double, C.c_double, C.c_double]
+        L.or_gauss_constants.argtypes = [dp, dp, dp]
         L.or_veto_times.restype = C.c_double
         L.or_veto_times.argtypes = [vp, dp, C.c_int, C.c_double]
         _lib = L

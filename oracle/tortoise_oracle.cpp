@@ -1330,6 +1330,18 @@ double or_veto_step(void* h, double t, double dt, double dense) {
     return veto_step(*static_cast<Problem*>(h), times, 6, dense);
 }
 
+// The order-2 Gauss rules the oracle integrates with (kGP2 / kGW2 on the
+// reference triangle, kGP1 on [0, 1]): points as (x, y) pairs, weights.
+void or_gauss_constants(double* tri_points, double* tri_weights, double* int_points) {
+    for (int q = 0; q < 3; ++q) {
+        tri_points[2 * q] = kGP2[q][0];
+        tri_points[2 * q + 1] = kGP2[q][1];
+        tri_weights[q] = kGW2[q];
+    }
+    int_points[0] = kGP1[0];
+    int_points[1] = kGP1[1];
+}
+
 // MaterialTimeStatus::timeStepVetoer(timesToTest, denseStep)
 // (MaterialTimeStatus.cpp:60-100) on the caller's times.
 double or_veto_times(void* h, const double* times, int ntimes, double dense) {
