@@ -475,6 +475,7 @@ int tb_dp45_replay(tb_handle* h, const double* f0, const double* dts, int64_t n_
 
 int tb_adjoint_forward(tb_handle* h, const double* f0, double t0, double t1, double dense_step, int checkpoint_every,
                        int64_t max_steps, double* f_obs, tb_adjoint_stats* st, int flags) {
+    NvtxRange range("tb_adjoint_forward");
     if (!h || !f0) { set_error("null argument"); return TB_ERR_ARG; }
     if (h->runs.size() != 1) { set_error("the adjoint integrates single-run handles"); return TB_ERR_ARG; }
     if (checkpoint_every < 1 || max_steps < 1) { set_error("checkpoint_every and max_steps must be >= 1"); return TB_ERR_ARG; }
@@ -557,6 +558,7 @@ int tb_adjoint_steps(tb_handle* h, double* dts, int64_t cap, int64_t* n_steps, d
 
 int tb_adjoint_backward(tb_handle* h, const double* lambda_T, double* grad_f0, double* grad_amp, tb_adjoint_stats* st,
                         int flags) {
+    NvtxRange range("tb_adjoint_backward");
     if (!h || !lambda_T) { set_error("null argument"); return TB_ERR_ARG; }
     if (!h->adj || !h->adj->have_forward) { set_error("tb_adjoint_forward was not called"); return TB_ERR_ARG; }
     TB_CUDA(cudaSetDevice(h->device));

@@ -455,6 +455,7 @@ int build_runs(tb_handle* h, const tb_problem_desc* const* descs, int nruns) {
                         mins[l] = d_minE[legband[l]];
                         maxs[l] = d_maxE[legband[l]];
                     }
+                    NvtxRange enum_range("tb_create: enumerate tuples");
                     TB_TRY(enumerate_channel(c, h->meshes.data(), h->bands.data(), legband, G.d_mc_pre, mins, maxs,
                                              h->stream, G.tup, G.diag));
                 }
@@ -488,10 +489,19 @@ int build_runs(tb_handle* h, const tb_problem_desc* const* descs, int nruns) {
         if (!I.d_single) { set_error("instance table allocation failed"); return TB_ERR_OOM; }
     }
     for (auto& G : h->groups) TB_TRY(shard_tuples(h, G));
-    TB_TRY(choose_layouts(h));
-    for (auto& G : h->groups)
-        if (G.layout == TB_LAYOUT_MC64) TB_TRY(build_theta_list(G.dev, G.tup, G.theta, h->stream));
-    if (h->opts.autotune) TB_TRY(autotune(h));
+    {
+        NvtxRange r("tb_create: layouts and moment tensors");
+        TB_TRY(choose_layouts(h));
+    }
+    {
+        NvtxRange r("tb_create: points inside the simplices");
+        for (auto& G : h->groups)
+            if (G.layout == TB_LAYOUT_MC64) TB_TRY(build_theta_list(G.dev, G.tup, G.theta, h->stream));
+    }
+    if (h->opts.autotune) {
+        NvtxRange r("tb_create: autotune");
+        TB_TRY(autotune(h));
+    }
     TB_CUDA(cudaStreamSynchronize(h->stream));
     return TB_OK;
 }
@@ -733,6 +743,7 @@ int tb_create_batch(tb_handle** out, const tb_problem_desc* const* runs, int n_r
         return TB_ERR_ARG;
     }
     h->device = h->opts.device;
+    NvtxRange range("tb_create");
     TB_CUDA(cudaSetDevice(h->device));
     TB_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     int rc = build_runs(h.get(), runs, n_runs);
@@ -1052,9 +1063,13 @@ static int rhs_common(tb_handle* h, const double* f, double* out, int flags, int
     return TB_OK;
 }
 
-int tb_rhs(tb_handle* h, const double* f, double* dfdt, int flags) { return rhs_common(h, f, dfdt, flags, -1); }
+int tb_rhs(tb_handle* h, const double* f, double* dfdt, int flags) {
+    NvtxRange range("tb_rhs");
+    return rhs_common(h, f, dfdt, flags, -1);
+}
 
 int tb_scattering_rates(tb_handle* h, int ch, int leg, const double* f, double* rates, int flags) {
+    NvtxRange range("tb_scattering_rates");
     if (!h || !f || !rates) { set_error("null argument"); return TB_ERR_ARG; }
     if (ch < -1 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
     if (leg < -1 || leg >= TB_MAX_LEGS || (ch >= 0 && leg >= h->groups[h->insts[ch].group].L)) {
@@ -1304,6 +1319,7 @@ int tb_dp45_end(tb_handle* h, double* f_out, double* dense_out, double* dense_ti
 
 int tb_dp45_integrate(tb_handle* h, double* f_inout, double t0, double t_final, double dense_step, double* dense_out,
                       double* dense_times, int64_t max_dense, tb_dp45_stats* st, int flags) {
+    NvtxRange range("tb_dp45_integrate");
     TB_TRY(tb_dp45_begin(h, f_inout, t0, t_final, dense_step, max_dense, flags));
     // speculative batches of attempts: attempts after the end are no-ops
     int64_t batch = 4;

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include <string>
@@ -23,6 +24,17 @@ const char* get_error();
             return TB_ERR_CUDA;                                                        \
         }                                                                              \
     } while (0)
+
+// A named range on the NVTX timeline around a host-side phase of the library
+// (handle creation and its steps, right-hand sides, integrations, adjoint
+// sweeps), for Nsight tools (e.g. ncu --nvtx --nvtx-include "tb_rhs/").
+// nvtx3 is header-only; with no tool attached a push / pop costs a few ns.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 #define TB_TRY(call)                      \
     do {                                  \
