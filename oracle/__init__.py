@@ -10,7 +10,8 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+# TB_ORACLE_LIB: another build of the oracle (e.g. `make -C oracle asan`)
+_LIB_PATH = os.environ.get("TB_ORACLE_LIB") or os.path.join(_HERE, "liboracle.so")
 _lib = None
 
 
