@@ -617,6 +617,57 @@ def small_ee_measure(no_cpu=False, no_tune=False):
     return line
 
 
+def to_end(args):
+    """The 64x64 two-band e-ph + drift workload integrated as its
+    configuration asks: DP45 at rtol 1e-8 from t = 0 to t = 20, dense output
+    every 2, through tb_dp45_integrate from host buffers; once with FP64
+    moments and once with 40-bit moments, whose dense outputs are compared
+    with the FP64 run's over the whole trajectory.  Beside it, the oracle's
+    time for one right-hand side on all host cores (a bounded sample of every
+    channel's tuples, scaled) times the right-hand sides the FP64 run took."""
+    from tortoise_b200 import engine as E
+    mat, f0 = workload()
+    line = {"workload": "2-band e-ph + drift, 64x64 mesh (8192 triangles/band), NMC=50, rtol 1e-8, t = 0..20",
+            "arms": {}}
+    dense_fp64 = None
+    for name, flag in (("f64", 0), ("t40", 2)):
+        t0 = time.perf_counter()
+        eng = E.Engine(mat, allow_fp32=flag, autotune=not args.no_tune)
+        setup = time.perf_counter() - t0
+        eng.dp45(f0, 0.0, 0.01, 0.01)   # warm-up: graph capture, first launches
+        with ClockSampler(0) as clk:
+            w0 = time.perf_counter()
+            r = eng.dp45(f0, 0.0, T_END, DENSE, max_dense=12)
+            w1 = time.perf_counter()
+        arm = {"seconds": w1 - w0, "setup_s": setup, "status": r["status"], "t": r["t"], "attempts": r["attempts"],
+               "accepted": r["accepted"], "rejected": r["rejected"], "rhs_evals": r["rhs_evals"],
+               "layouts": [eng.channel_info(c)["layout"] for c in range(len(mat.channels))]}
+        c = clk.summary()
+        if c:
+            arm["clocks"] = c
+        if dense_fp64 is None:
+            dense_fp64 = r["dense"]
+        else:
+            k = min(len(dense_fp64), len(r["dense"]))
+            arm["error_vs_fp64"] = max(float(np.linalg.norm(a - b) / np.linalg.norm(b))
+                                       for a, b in zip(r["dense"][:k], dense_fp64[:k]))
+            arm["error_metric"] = "max relative L2 over the dense outputs t = 2, 4, .., 20"
+        line["arms"][name] = arm
+        eng.close()
+    if not args.no_cpu:
+        import oracle   # the CPU baseline of this case
+        o = oracle.Oracle(mat, nthreads=os.cpu_count())
+        ntup = sum(o.num_tuples(c) for c in range(len(mat.channels)))
+        frac = min(1.0, 2.0e5 / max(1, ntup))
+        t_rhs = statistics.median([cpu_rhs_sample(o, mat, f0, frac)[0] for _ in range(3)])
+        n_rhs = line["arms"]["f64"]["rhs_evals"]
+        line["cpu_oracle"] = {"seconds_per_rhs": t_rhs, "cores": os.cpu_count(), "kind": "port",
+                              "sample": "first %.2f%% of every channel's tuples, scaled; median of 3" % (100 * frac),
+                              "projected_seconds": t_rhs * n_rhs}
+        line["gpu_vs_cpu"] = line["cpu_oracle"]["projected_seconds"] / line["arms"]["f64"]["seconds"]
+    print(json.dumps(line), flush=True)
+
+
 def large(args):
     """The large batched mixed-precision configuration: 16 runs of the
     three-band (parabola, Dirac cone, heavy hole), two-phonon (0.15, 0.25) e-ph
@@ -747,6 +798,8 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="batched ensemble of this many runs (per-run N, kT, couplings)")
     ap.add_argument("--large", nargs="?", const="t32", default=None, choices=["t32", "t40"],
                     help="16-run 128x128 three-band two-phonon batch with FP32 (default) or 40-bit moments")
+    ap.add_argument("--to-end", action="store_true",
+                    help="the 64x64 workload integrated to t = 20 (FP64 and 40-bit moments) vs the oracle")
     ap.add_argument("--small-ee", action="store_true",
                     help="16x16 one-band e-e integration to t = 10 (the reference's CPU-runnable case) vs the oracle")
     ap.add_argument("--shard", action="store_true",
@@ -756,6 +809,9 @@ def main():
     args = ap.parse_args()
     if args.large:
         large(args)
+        return
+    if args.to_end:
+        to_end(args)
         return
     if args.small_ee:
         small_ee(args)
