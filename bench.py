@@ -434,7 +434,74 @@ def batched_measure(n_runs, steps, warmup, mixed, layout_name="auto", tune=True)
             "clocks": clk.summary()}
 
 
+def batched_to_end(n_runs, tune=True):
+    """The ensemble of n_runs runs (ensemble_runs) integrated to t = 20 in one
+    handle, every run with its own adaptive steps (dense output every 2):
+    once with 40-bit moments and once with FP64 moments, whose dense
+    outputs are compared run by run.  The single-run FP64 path doing the same
+    work one run at a time is projected from its measured time per attempt
+    for each mesh size times every run's attempt count (the controllers are
+    the same, so a run takes the same attempts alone)."""
+    import torch
+    from tortoise_b200 import engine as E
+    from tortoise_b200 import workloads as W
+    mats, states = W.ensemble_runs(n_runs)
+    f0 = np.concatenate(states)
+    arms, dense = {}, {}
+    for name, flag in (("t40", 2), ("f64", 0)):
+        t0 = time.perf_counter()
+        be = E.BatchEngine(mats, allow_fp32=flag, autotune=tune)
+        setup = time.perf_counter() - t0
+        be.dp45(f0, 0.0, 0.01, 0.01)   # warm-up: graph capture, first launches
+        with ClockSampler(0) as clk:
+            w0 = time.perf_counter()
+            r = be.dp45(f0, 0.0, T_END, DENSE, max_dense=12)
+            w1 = time.perf_counter()
+        att = np.array([x["attempts"] for x in r["runs"]])
+        arms[name] = {"seconds": w1 - w0, "setup_s": setup, "rc": r["rc"],
+                      "all_reached_t_end": bool(all(x["t"] >= T_END for x in r["runs"])),
+                      "statuses": sorted({int(x["status"]) for x in r["runs"]}),
+                      "run_attempts": int(att.sum()), "attempts_per_run": [int(att.min()), int(np.median(att)),
+                                                                          int(att.max())],
+                      "run_attempts_per_s": float(att.sum() / (w1 - w0)), "clocks": clk.summary()}
+        dense[name] = [x["dense"] for x in r["runs"]]
+        if name == "f64":
+            attempts_f64 = att
+        be.close()
+    arms["t40"]["error_vs_fp64"] = max(
+        max(float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(da, db))
+        for da, db in zip(dense["t40"], dense["f64"]))
+    arms["t40"]["error_metric"] = "max over runs and dense outputs t = 2 .. 20 of the relative L2 vs the FP64 batch"
+    # single-run FP64 time per attempt, per mesh size
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    seq = {}
+    for r, m in enumerate(mats):
+        N = m.bands[0].mesh.nsplit[0]
+        if N in seq:
+            continue
+        eng = E.Engine(m, allow_fp32=False, autotune=tune)
+        s1 = torch.cuda.ExternalStream(eng.stream_ptr())
+        eng.dp45_begin(states[r], 0.0, 1.0e9, DENSE, 0)
+        eng.dp45_advance(3)
+        eng.synchronize()
+        ev0.record(s1)
+        eng.dp45_advance(10)
+        ev1.record(s1)
+        ev1.synchronize()
+        seq[N] = ev0.elapsed_time(ev1) * 1e-3 / 10
+        eng.close()
+    t_seq = sum(int(a) * seq[m.bands[0].mesh.nsplit[0]] for a, m in zip(attempts_f64, mats))
+    return {"runs": n_runs, "t_end": T_END, "arms": arms,
+            "sequential_fp64_ms_per_attempt_by_N": {N: 1e3 * v for N, v in sorted(seq.items())},
+            "sequential_fp64_projected_seconds": t_seq,
+            "speedup_t40_vs_sequential_fp64": t_seq / arms["t40"]["seconds"],
+            "speedup_f64_batch_vs_sequential_fp64": t_seq / arms["f64"]["seconds"]}
+
+
 def batched(args):
+    if args.to_end:
+        print(json.dumps(dict({"batched_to_end": True}, **batched_to_end(args.batch, not args.no_tune))), flush=True)
+        return
     d = batched_measure(args.batch, args.steps, args.warmup, args.mixed, args.layout, not args.no_tune)
     print(json.dumps(dict({"batched": True}, **d)), flush=True)
 
@@ -810,7 +877,7 @@ def main():
     if args.large:
         large(args)
         return
-    if args.to_end:
+    if args.to_end and not args.batch:
         to_end(args)
         return
     if args.small_ee:
