@@ -139,11 +139,12 @@ typedef struct tb_handle tb_handle;
 #define TB_LAYOUT_T64    2  /* precomputed moment tensor, FP64 storage            */
 #define TB_LAYOUT_T32    3  /* precomputed moment tensor, FP32 storage, FP64 accumulate */
 #define TB_LAYOUT_T40    4  /* moment tensor, upper 40 bits of FP64 (5 B, 2^-29 relative), FP64 accumulate */
+#define TB_LAYOUT_T48    5  /* moment tensor, upper 48 bits of FP64 (6 B, 2^-37 relative), FP64 accumulate */
 
 typedef struct tb_options {
     int32_t device;               /* CUDA device ordinal                            */
     int32_t layout;               /* TB_LAYOUT_*                                    */
-    int32_t allow_fp32;           /* AUTO for 2- and 3-leg channels: 0 -> T64, 1 -> T32, 2 -> T40 */
+    int32_t allow_fp32;           /* AUTO for 2- and 3-leg channels: 0 -> T64, 1 -> T32, 2 -> T40, 3 -> T48 */
     int64_t tensor_budget_bytes;  /* cap on precomputed-tensor memory (0: 60% free) */
     int32_t verbose;
     int32_t autotune;             /* 1: time the contraction schedules at creation, keep the fastest */

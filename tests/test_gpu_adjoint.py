@@ -38,7 +38,7 @@ def _dir_err(fd, ad, scale):
     return abs(fd - ad) / max(abs(ad), 1e-3 * scale)
 
 
-@pytest.mark.parametrize("layout", [E.LAYOUT_MC64, E.LAYOUT_T64, E.LAYOUT_T32, E.LAYOUT_T40])
+@pytest.mark.parametrize("layout", [E.LAYOUT_MC64, E.LAYOUT_T64, E.LAYOUT_T32, E.LAYOUT_T40, E.LAYOUT_T48])
 @pytest.mark.parametrize("bath", [False, True])
 def test_rhs_vjp_is_the_transpose(gpu_lib, layout, bath):
     mat = _mat(4, ee=True, bath=bath)

@@ -72,7 +72,8 @@ def test_mixed_precision_trajectory_within_1e8(gpu_lib):
     gain - loss, error norm, controller) against the FP64 path on the two-band
     e-ph + drift workload at 16x16, rtol 1e-8, to t = 1, every dense output:
     40-bit storage (T40: upper 40 bits of FP64, 2^-29) within 5e-9 relative L2
-    (measured ~1e-9), plain FP32 storage (T32) within 3e-8 (measured ~1e-8).
+    (measured ~1e-9), 48-bit storage (T48, 2^-37) within 1e-10, plain FP32
+    storage (T32) within 3e-8 (measured ~1e-8).
     A batch of three runs of that structure in T40 gives every run's FP64
     trajectory to 5e-9 as well."""
     mats, states = [], []
@@ -83,7 +84,10 @@ def test_mixed_precision_trajectory_within_1e8(gpu_lib):
     r64 = E.Engine(mats[0], layout=E.LAYOUT_T64).dp45(states[0], 0.0, 1.0, 0.25)
     r40 = E.Engine(mats[0], layout=E.LAYOUT_T40).dp45(states[0], 0.0, 1.0, 0.25)
     r32 = E.Engine(mats[0], layout=E.LAYOUT_T32).dp45(states[0], 0.0, 1.0, 0.25)
-    assert r64["status"] == 0 and r40["status"] == 0 and r32["status"] == 0
+    r48 = E.Engine(mats[0], layout=E.LAYOUT_T48).dp45(states[0], 0.0, 1.0, 0.25)
+    assert r64["status"] == 0 and r40["status"] == 0 and r32["status"] == 0 and r48["status"] == 0
+    e48 = [rel_l2(a, b) for a, b in zip(r48["dense"], r64["dense"])]
+    assert len(e48) == 4 and max(e48) < 1e-10, e48
     e40 = [rel_l2(a, b) for a, b in zip(r40["dense"], r64["dense"])]
     e32 = [rel_l2(a, b) for a, b in zip(r32["dense"], r64["dense"])]
     assert len(e40) == 4 and max(e40) < 5e-9, e40
@@ -115,7 +119,7 @@ def test_autotuned_schedule_gives_the_same_operator(gpu_lib):
     assert mc.schedule(0) == {"stages": 0, "pair": 0, "runs": 0, "tuned_seconds": 0.0, "inside_only": True}
 
 
-@pytest.mark.parametrize("layout", [E.LAYOUT_T64, E.LAYOUT_T40, E.LAYOUT_T32])
+@pytest.mark.parametrize("layout", [E.LAYOUT_T64, E.LAYOUT_T40, E.LAYOUT_T48, E.LAYOUT_T32])
 def test_run_minor_contraction_equals_individual_runs(gpu_lib, layout):
     """Groups shared by 16 runs or more take the run-minor contraction (one
     lane per run, lane groups of 8 runs by default, f and the results staged

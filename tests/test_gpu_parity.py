@@ -205,24 +205,26 @@ def test_tensor_layout_fp32_error_bound(gpu_lib, name):
     assert rel_l2(eng.rhs(f0, drift=False), g["rhs_nodrift"]) < 1e-6
 
 
+@pytest.mark.parametrize("layout,name_l,tol", [(E.LAYOUT_T40, "t40", 2e-8), (E.LAYOUT_T48, "t48", 2e-10)])
 @pytest.mark.parametrize("name", ["eph_n4", "ee_n3", "ee2_n3", "eph_bath_n4"])
-def test_tensor_layout_40bit_error_bound(gpu_lib, name):
+def test_tensor_layout_40_and_48bit_error_bound(gpu_lib, name, layout, name_l, tol):
     """Moments stored as the upper 40 bits of FP64 (sign, exponent, 28
-    mantissa bits, rounded: 2^-29 relative), rebuilt into FP64 registers:
-    every channel and the RHS within 2e-8 relative L2 of the FP64 oracle
-    (FP32 storage gives ~1.2e-7; 40 bits are 32x finer)."""
+    mantissa bits, rounded: 2^-29 relative) or the upper 48 bits (2^-37),
+    rebuilt into FP64 registers: every channel and the RHS within 2e-8
+    (40-bit) or 2e-10 (48-bit) relative L2 of the FP64 oracle (FP32 storage
+    gives ~1.2e-7; 40 bits are 32x finer, 48 bits 8192x)."""
     g = golden(name)
     mat, f0 = _setup(name)
-    eng = E.Engine(mat, layout=E.LAYOUT_T40)
+    eng = E.Engine(mat, layout=layout)
     for ch in range(len(mat.channels)):
         if eng.channel_info(ch)["n_tuples"] > 0:
-            assert eng.channel_info(ch)["layout"] == "t40"
-        assert rel_l2(eng.channel_propagate(ch, f0), g["ch%d_prop" % ch]) < 2e-8
-    assert rel_l2(eng.rhs(f0, drift=False), g["rhs_nodrift"]) < 2e-8
+            assert eng.channel_info(ch)["layout"] == name_l
+        assert rel_l2(eng.channel_propagate(ch, f0), g["ch%d_prop" % ch]) < tol
+    assert rel_l2(eng.rhs(f0, drift=False), g["rhs_nodrift"]) < tol
 
 
 @pytest.mark.parametrize("layout,tol", [(E.LAYOUT_MC64, 1e-12), (E.LAYOUT_T64, 1e-12), (E.LAYOUT_T40, 2e-8),
-                                        (E.LAYOUT_T32, 1e-6)])
+                                        (E.LAYOUT_T48, 2e-10), (E.LAYOUT_T32, 1e-6)])
 @pytest.mark.parametrize("name", CASES)
 def test_scattering_rates_parity(gpu_lib, name, layout, tol):
     """tb_scattering_rates (ScatteringChannel::scatteringRates /
@@ -297,7 +299,7 @@ def test_tuple_cache_round_trip(gpu_lib, tmp_path):
 
 
 @pytest.mark.parametrize("layout,etol", [(E.LAYOUT_MC64, 1e-12), (E.LAYOUT_T64, 1e-12), (E.LAYOUT_T40, 1e-8),
-                                         (E.LAYOUT_T32, 1e-6)])
+                                         (E.LAYOUT_T48, 1e-10), (E.LAYOUT_T32, 1e-6)])
 @pytest.mark.parametrize("name", CASES)
 def test_device_operator_conserves(gpu_lib, name, layout, etol):
     """Collision term of the device operator.  Electron number: every channel

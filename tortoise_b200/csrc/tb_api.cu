@@ -581,13 +581,19 @@ int choose_layouts(tb_handle* h) {
             // evaluation (HBM-bound contraction vs FP64-bound quadrature);
             // for L = 4 the 405-moment tensor costs more bytes than the
             // quadrature costs FP64 cycles on B200.
-            // allow_fp32 = 1: FP32 moments; 2: 40-bit (truncated FP64) moments
+            // allow_fp32 = 1: FP32 moments; 2: 40-bit, 3: 48-bit (upper bits of FP64) moments
             if (G.L <= 3)
-                want = h->opts.allow_fp32 == 1 ? TB_LAYOUT_T32 : h->opts.allow_fp32 == 2 ? TB_LAYOUT_T40 : TB_LAYOUT_T64;
+                want = h->opts.allow_fp32 == 1   ? TB_LAYOUT_T32
+                       : h->opts.allow_fp32 == 2 ? TB_LAYOUT_T40
+                       : h->opts.allow_fp32 == 3 ? TB_LAYOUT_T48
+                                                 : TB_LAYOUT_T64;
             else want = TB_LAYOUT_MC64;
         }
-        const int kind = (want == TB_LAYOUT_T32) ? TK_F32 : (want == TB_LAYOUT_T40) ? TK_F40 : TK_F64;
-        if (want == TB_LAYOUT_T32 || want == TB_LAYOUT_T64 || want == TB_LAYOUT_T40) {
+        const int kind = (want == TB_LAYOUT_T32)   ? TK_F32
+                         : (want == TB_LAYOUT_T40) ? TK_F40
+                         : (want == TB_LAYOUT_T48) ? TK_F48
+                                                   : TK_F64;
+        if (want == TB_LAYOUT_T32 || want == TB_LAYOUT_T64 || want == TB_LAYOUT_T40 || want == TB_LAYOUT_T48) {
             const int64_t bytes = tensor_bytes(G.L, kind, G.tup.n);
             if (G.tup.n == 0 || bytes > budget) want = TB_LAYOUT_MC64;
             else budget -= bytes;
@@ -732,9 +738,9 @@ int tb_create_batch(tb_handle** out, const tb_problem_desc* const* runs, int n_r
     std::unique_ptr<tb_handle> h(new tb_handle());
     if (opts) h->opts = *opts;
     else { h->opts.layout = TB_LAYOUT_AUTO; h->opts.allow_fp32 = 0; }
-    if (h->opts.layout < TB_LAYOUT_AUTO || h->opts.layout > TB_LAYOUT_T40 || h->opts.allow_fp32 < 0 ||
-        h->opts.allow_fp32 > 2) {
-        set_error("tb_options: layout must be 0..4 and allow_fp32 0..2");
+    if (h->opts.layout < TB_LAYOUT_AUTO || h->opts.layout > TB_LAYOUT_T48 || h->opts.allow_fp32 < 0 ||
+        h->opts.allow_fp32 > 3) {
+        set_error("tb_options: layout must be 0..5 and allow_fp32 0..3");
         return TB_ERR_ARG;
     }
     if (h->opts.shard_count < 0 || h->opts.shard_rank < 0 ||

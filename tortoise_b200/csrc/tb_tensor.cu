@@ -30,6 +30,9 @@
 //             the next byte of four consecutive moments into one word.  A
 //             moment is rebuilt as an FP64 register pair (upper word, byte
 //             << 24) with one byte permute: no conversion instruction.
+//   TK_F48    the upper 48 bits (36 mantissa bits: 2^-37 relative), 6 bytes
+//             per moment: the row of upper words, then rows that pack the
+//             next 16 bits of two consecutive moments into one word.
 // Products and accumulation are FP64 for every kind; the gain-minus-loss
 // vector v = ka + kb is formed in FP64 from f.
 #include <cmath>
@@ -53,21 +56,25 @@ template <int L> struct TDim {
 
 template <int L, int KIND> struct TTile {
     // tuples per tile: keeps one stage at <= ~56 KB of shared memory
-    static constexpr int TT = (L == 4) ? 32 : (KIND == TK_F32) ? 128 : (KIND == TK_F40 && L == 2) ? 128 : 64;
+    static constexpr int TT = (L == 4)                                          ? 32
+                              : (KIND == TK_F32)                                ? 128
+                              : ((KIND == TK_F40 || KIND == TK_F48) && L == 2) ? 128
+                                                                                : 64;
 };
 
 static int nmom_of(int L) { return (L == 2 ? 9 : L == 3 ? 27 : 81) * (1 + L); }
 
 int tile_tuples(int L, int kind) {
     if (L == 4) return 32;
-    if (kind == TK_F32 || (kind == TK_F40 && L == 2)) return 128;
+    if (kind == TK_F32 || ((kind == TK_F40 || kind == TK_F48) && L == 2)) return 128;
     return 64;
 }
 
 // bytes of one tuple's moments in a tile
 static int64_t tuple_bytes(int L, int kind) {
     const int64_t nm = nmom_of(L);
-    return kind == TK_F64 ? 8 * nm : kind == TK_F32 ? 4 * nm : 4 * (nm + (nm + 3) / 4);
+    return kind == TK_F64 ? 8 * nm : kind == TK_F32 ? 4 * nm : kind == TK_F48 ? 4 * (nm + (nm + 1) / 2)
+                                                                              : 4 * (nm + (nm + 3) / 4);
 }
 
 int64_t tensor_bytes(int L, int kind, int64_t n) {
@@ -187,6 +194,19 @@ __global__ void __launch_bounds__(256) k_build_moments(ChanDev c, const int32_t*
 #pragma unroll
             for (int q = 0; q < PER; ++q)
                 if (own[q]) base[(int64_t)(lane + 32 * q) * TT] = float(acc[q] * norm);
+        } else if (KIND == TK_F48) {
+            // upper 48 bits of the FP64 pattern, rounded to nearest on bit 15
+            constexpr int NH = (NMOM + 1) / 2;   // rows of packed 16-bit halves
+            uint32_t* hi = static_cast<uint32_t*>(out) + tile * (int64_t)(NMOM + NH) * TT;
+            uint16_t* lo = reinterpret_cast<uint16_t*>(hi + (int64_t)NMOM * TT);
+#pragma unroll
+            for (int q = 0; q < PER; ++q)
+                if (own[q]) {
+                    const int k = lane + 32 * q;
+                    const unsigned long long b = (unsigned long long)__double_as_longlong(acc[q] * norm) + 0x8000ull;
+                    hi[(int64_t)k * TT + pos] = uint32_t(b >> 32);
+                    lo[2 * ((int64_t)(k >> 1) * TT + pos) + (k & 1)] = uint16_t(b >> 16);
+                }
         } else {
             // upper 40 bits of the FP64 pattern, rounded to nearest on bit 23
             constexpr int NB = (NMOM + 3) / 4;   // rows of packed bytes
@@ -245,6 +265,13 @@ __device__ __forceinline__ double tile_moment(const unsigned char* __restrict__ 
         return reinterpret_cast<const double*>(tile)[j * TT + tid];
     } else if constexpr (KIND == TK_F32) {
         return double(reinterpret_cast<const float*>(tile)[j * TT + tid]);
+    } else if constexpr (KIND == TK_F48) {
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(tile);
+        const uint32_t hi = w[j * TT + tid];
+        const uint32_t lw = w[(NMOM + (j >> 1)) * TT + tid];
+        // half j % 2 of lw into the top half of the low word, zeros below
+        const uint32_t lo = (j & 1) ? (lw & 0xffff0000u) : (lw << 16);
+        return __hiloint2double(int(hi), int(lo));
     } else {
         const uint32_t* w = reinterpret_cast<const uint32_t*>(tile);
         const uint32_t hi = w[j * TT + tid];
@@ -360,7 +387,10 @@ __device__ __forceinline__ void contract_tuple(const ChanDev& c, const InstDev (
 // bytes of one tuple's moments (compile-time twin of tuple_bytes)
 template <int L, int KIND> struct TBytes {
     static constexpr int NM = TDim<L>::NMOM;
-    static constexpr int B = KIND == TK_F64 ? 8 * NM : KIND == TK_F32 ? 4 * NM : 4 * (NM + (NM + 3) / 4);
+    static constexpr int B = KIND == TK_F64   ? 8 * NM
+                             : KIND == TK_F32 ? 4 * NM
+                             : KIND == TK_F48 ? 4 * (NM + (NM + 1) / 2)
+                                              : 4 * (NM + (NM + 3) / 4);
 };
 
 // RATE: scattering-rate variant (rate_leg >= 0), a separate instantiation so
@@ -648,7 +678,7 @@ __global__ void __launch_bounds__(RUNS_THREADS) k_collision_runs(ChanDev c, cons
                                                                  int* __restrict__ err_flag) {
     constexpr uint32_t TILE_BYTES = uint32_t(TBytes<L, KIND>::B) * TT;
     constexpr int NMOM = TDim<L>::NMOM;
-    constexpr bool DEC = KIND == TK_F40;
+    constexpr bool DEC = KIND == TK_F40 || KIND == TK_F48;
     constexpr int KREAD = DEC ? TK_F64 : KIND;
     constexpr size_t DEC_BYTES = DEC ? sizeof(double) * NMOM * TT : 0;
     constexpr int NW = RUNS_THREADS / 32;
@@ -790,16 +820,19 @@ static int build_t(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t
 
 int refill_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, MomentTensor& T, cudaStream_t s) {
     if (!T.d || T.n != n) { set_error("refill of a tensor that was not built for this list"); return TB_ERR_ARG; }
-    switch (c.L * 3 + T.kind) {
-        case 6: return fill_t<2, TK_F64>(c, tup, stride, n, T, s);
-        case 7: return fill_t<2, TK_F32>(c, tup, stride, n, T, s);
-        case 8: return fill_t<2, TK_F40>(c, tup, stride, n, T, s);
-        case 9: return fill_t<3, TK_F64>(c, tup, stride, n, T, s);
-        case 10: return fill_t<3, TK_F32>(c, tup, stride, n, T, s);
-        case 11: return fill_t<3, TK_F40>(c, tup, stride, n, T, s);
-        case 12: return fill_t<4, TK_F64>(c, tup, stride, n, T, s);
-        case 13: return fill_t<4, TK_F32>(c, tup, stride, n, T, s);
-        case 14: return fill_t<4, TK_F40>(c, tup, stride, n, T, s);
+    switch (c.L * 4 + T.kind) {
+        case 8: return fill_t<2, TK_F64>(c, tup, stride, n, T, s);
+        case 9: return fill_t<2, TK_F32>(c, tup, stride, n, T, s);
+        case 10: return fill_t<2, TK_F40>(c, tup, stride, n, T, s);
+        case 11: return fill_t<2, TK_F48>(c, tup, stride, n, T, s);
+        case 12: return fill_t<3, TK_F64>(c, tup, stride, n, T, s);
+        case 13: return fill_t<3, TK_F32>(c, tup, stride, n, T, s);
+        case 14: return fill_t<3, TK_F40>(c, tup, stride, n, T, s);
+        case 15: return fill_t<3, TK_F48>(c, tup, stride, n, T, s);
+        case 16: return fill_t<4, TK_F64>(c, tup, stride, n, T, s);
+        case 17: return fill_t<4, TK_F32>(c, tup, stride, n, T, s);
+        case 18: return fill_t<4, TK_F40>(c, tup, stride, n, T, s);
+        case 19: return fill_t<4, TK_F48>(c, tup, stride, n, T, s);
     }
     set_error("nlegs must be 2..4");
     return TB_ERR_ARG;
@@ -807,16 +840,19 @@ int refill_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t 
 
 int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, int kind, MomentTensor& T,
                  cudaStream_t s) {
-    switch (c.L * 3 + kind) {
-        case 6: return build_t<2, TK_F64>(c, tup, stride, n, T, s);
-        case 7: return build_t<2, TK_F32>(c, tup, stride, n, T, s);
-        case 8: return build_t<2, TK_F40>(c, tup, stride, n, T, s);
-        case 9: return build_t<3, TK_F64>(c, tup, stride, n, T, s);
-        case 10: return build_t<3, TK_F32>(c, tup, stride, n, T, s);
-        case 11: return build_t<3, TK_F40>(c, tup, stride, n, T, s);
-        case 12: return build_t<4, TK_F64>(c, tup, stride, n, T, s);
-        case 13: return build_t<4, TK_F32>(c, tup, stride, n, T, s);
-        case 14: return build_t<4, TK_F40>(c, tup, stride, n, T, s);
+    switch (c.L * 4 + kind) {
+        case 8: return build_t<2, TK_F64>(c, tup, stride, n, T, s);
+        case 9: return build_t<2, TK_F32>(c, tup, stride, n, T, s);
+        case 10: return build_t<2, TK_F40>(c, tup, stride, n, T, s);
+        case 11: return build_t<2, TK_F48>(c, tup, stride, n, T, s);
+        case 12: return build_t<3, TK_F64>(c, tup, stride, n, T, s);
+        case 13: return build_t<3, TK_F32>(c, tup, stride, n, T, s);
+        case 14: return build_t<3, TK_F40>(c, tup, stride, n, T, s);
+        case 15: return build_t<3, TK_F48>(c, tup, stride, n, T, s);
+        case 16: return build_t<4, TK_F64>(c, tup, stride, n, T, s);
+        case 17: return build_t<4, TK_F32>(c, tup, stride, n, T, s);
+        case 18: return build_t<4, TK_F40>(c, tup, stride, n, T, s);
+        case 19: return build_t<4, TK_F48>(c, tup, stride, n, T, s);
     }
     set_error("nlegs must be 2..4");
     return TB_ERR_ARG;
@@ -857,7 +893,7 @@ static int launch_runs(const ChanDev& c, const InstDev* insts, int n_insts, cons
     TB_CUDA(cudaGetLastError());
     auto kern = k_collision_runs<L, KIND, TT, STAGES, S>;
     const size_t fixed = size_t(STAGES) * TT * tuple_bytes(L, KIND) +
-                         (KIND == TK_F40 ? sizeof(double) * TDim<L>::NMOM * TT : 0);
+                         ((KIND == TK_F40 || KIND == TK_F48) ? sizeof(double) * TDim<L>::NMOM * TT : 0);
     const size_t smem = fixed + sizeof(double) * size_t(T.np);
     static bool attr = false;
     if (!attr) {
@@ -976,16 +1012,19 @@ int launch_collision_tensor(const ChanDev& c, const InstDev* insts, int n_insts,
                             const int32_t* tup, int64_t stride, int64_t n, const double* f, double* acc,
                             const DPCtl* ctl, cudaStream_t s, int rate_leg) {
     if (n <= 0 || n_insts <= 0) return TB_OK;
-    switch (c.L * 3 + T.kind) {
-        case 6: return launch_t<2, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 7: return launch_t<2, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 8: return launch_t<2, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 9: return launch_t<3, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 10: return launch_t<3, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 11: return launch_t<3, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 12: return launch_t<4, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 13: return launch_t<4, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 14: return launch_t<4, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+    switch (c.L * 4 + T.kind) {
+        case 8: return launch_t<2, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 9: return launch_t<2, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 10: return launch_t<2, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 11: return launch_t<2, TK_F48>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 12: return launch_t<3, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 13: return launch_t<3, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 14: return launch_t<3, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 15: return launch_t<3, TK_F48>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 16: return launch_t<4, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 17: return launch_t<4, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 18: return launch_t<4, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 19: return launch_t<4, TK_F48>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
     }
     set_error("nlegs must be 2..4");
     return TB_ERR_ARG;

@@ -6,7 +6,7 @@
 namespace tb {
 
 // storage kinds of the moments (see tb_tensor.cu)
-enum { TK_F64 = 0, TK_F32 = 1, TK_F40 = 2 };
+enum { TK_F64 = 0, TK_F32 = 1, TK_F40 = 2, TK_F48 = 3 };
 
 struct MomentTensor {
     void* d = nullptr;        // moments, tile-major (see tb_tensor.cu)

@@ -244,8 +244,9 @@ __global__ void __launch_bounds__(128) k_vjp_tensor(ChanDev c, const InstDev* __
 #pragma unroll
         for (int l = 0; l < L; ++l) e[l] = valid ? __ldg(tup + l * stride + i) : 0;
         // moment j of tuple i: tile-major rows of TT tuples (FP64, FP32, or
-        // the upper 40 bits of FP64 as a word row plus packed byte rows)
-        constexpr int NB = (KIND == TK_F40) ? (NMOM + 3) / 4 : 0;
+        // the upper 40 / 48 bits of FP64 as a word row plus packed byte /
+        // half-word rows)
+        constexpr int NB = (KIND == TK_F40) ? (NMOM + 3) / 4 : (KIND == TK_F48) ? (NMOM + 1) / 2 : 0;
         constexpr int ROWB = (KIND == TK_F64) ? 8 : 4;
         const unsigned char* tb = static_cast<const unsigned char*>(mom) + (i / TT) * (int64_t)(NMOM + NB) * TT * ROWB;
         const int64_t pos = i % TT;
@@ -254,6 +255,10 @@ __global__ void __launch_bounds__(128) k_vjp_tensor(ChanDev c, const InstDev* __
                 return reinterpret_cast<const double*>(tb)[(int64_t)j * TT + pos];
             } else if constexpr (KIND == TK_F32) {
                 return double(reinterpret_cast<const float*>(tb)[(int64_t)j * TT + pos]);
+            } else if constexpr (KIND == TK_F48) {
+                const uint32_t* w = reinterpret_cast<const uint32_t*>(tb);
+                const uint32_t lw = w[(int64_t)(NMOM + (j >> 1)) * TT + pos];
+                return __hiloint2double(int(w[(int64_t)j * TT + pos]), int((j & 1) ? (lw & 0xffff0000u) : (lw << 16)));
             } else {
                 const uint32_t* w = reinterpret_cast<const uint32_t*>(tb);
                 const uint32_t lw = w[(int64_t)(NMOM + (j >> 2)) * TT + pos];
@@ -345,16 +350,19 @@ int launch_collision_vjp(const ChanDev& c, const InstDev* insts, int n_insts, in
         const int TT = tile_tuples(c.L, T.kind);
 #define TB_VJP_T(LL, KK) k_vjp_tensor<LL, KK><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, T.d, TT, tup, \
                                                                                  stride, n, f, u, grad_f, grad_amp)
-        switch (c.L * 3 + T.kind) {
-            case 6: TB_VJP_T(2, TK_F64); break;
-            case 7: TB_VJP_T(2, TK_F32); break;
-            case 8: TB_VJP_T(2, TK_F40); break;
-            case 9: TB_VJP_T(3, TK_F64); break;
-            case 10: TB_VJP_T(3, TK_F32); break;
-            case 11: TB_VJP_T(3, TK_F40); break;
-            case 12: TB_VJP_T(4, TK_F64); break;
-            case 13: TB_VJP_T(4, TK_F32); break;
-            default: TB_VJP_T(4, TK_F40); break;
+        switch (c.L * 4 + T.kind) {
+            case 8: TB_VJP_T(2, TK_F64); break;
+            case 9: TB_VJP_T(2, TK_F32); break;
+            case 10: TB_VJP_T(2, TK_F40); break;
+            case 11: TB_VJP_T(2, TK_F48); break;
+            case 12: TB_VJP_T(3, TK_F64); break;
+            case 13: TB_VJP_T(3, TK_F32); break;
+            case 14: TB_VJP_T(3, TK_F40); break;
+            case 15: TB_VJP_T(3, TK_F48); break;
+            case 16: TB_VJP_T(4, TK_F64); break;
+            case 17: TB_VJP_T(4, TK_F32); break;
+            case 18: TB_VJP_T(4, TK_F40); break;
+            default: TB_VJP_T(4, TK_F48); break;
         }
 #undef TB_VJP_T
     }

@@ -13,8 +13,8 @@ from .abi import STATUS_NAMES
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libtortoise_b200.so")
 
-LAYOUT_AUTO, LAYOUT_MC64, LAYOUT_T64, LAYOUT_T32, LAYOUT_T40 = 0, 1, 2, 3, 4
-LAYOUT_NAMES = {1: "mc64", 2: "t64", 3: "t32", 4: "t40"}
+LAYOUT_AUTO, LAYOUT_MC64, LAYOUT_T64, LAYOUT_T32, LAYOUT_T40, LAYOUT_T48 = 0, 1, 2, 3, 4, 5
+LAYOUT_NAMES = {1: "mc64", 2: "t64", 3: "t32", 4: "t40", 5: "t48"}
 PTR_HOST, NO_DRIFT, NO_COLLISIONS = 1, 2, 4
 
 _lib = None
