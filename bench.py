@@ -449,7 +449,7 @@ def batched_to_end(n_runs, tune=True):
     from tortoise_b200 import workloads as W
     mats, states = W.ensemble_runs(n_runs)
     f0 = np.concatenate(states)
-    arms, dense = {}, {}
+    arms, dense, attempts = {}, {}, {}
     for name, flag in (("f64", 0), ("t40", 2), ("t48", 3)):
         t0 = time.perf_counter()
         be = E.BatchEngine(mats, allow_fp32=flag, autotune=tune)
@@ -467,6 +467,7 @@ def batched_to_end(n_runs, tune=True):
                                                                           int(att.max())],
                       "run_attempts_per_s": float(att.sum() / (w1 - w0)), "clocks": clk.summary()}
         dense[name] = [x["dense"] for x in r["runs"]]
+        attempts[name] = att
         if name == "f64":
             attempts_f64 = att
         be.close()
@@ -476,6 +477,14 @@ def batched_to_end(n_runs, tune=True):
         arms[name]["error_vs_fp64"] = max(per_run)
         arms[name]["error_vs_fp64_median_run"] = float(np.median(per_run))
         arms[name]["runs_above_1e-8"] = int(sum(e > 1e-8 for e in per_run))
+        # a run whose controller took another accept / reject path differs
+        # from the FP64 run at the integrator's own tolerance (rtol 1e-8),
+        # whatever the storage; the runs on the FP64 run's path show the
+        # storage error alone
+        same = attempts[name] == attempts["f64"]
+        arms[name]["runs_on_another_step_path"] = int((~same).sum())
+        arms[name]["error_vs_fp64_same_step_path"] = max([e for e, k in zip(per_run, same) if k], default=0.0)
+        arms[name]["error_vs_fp64_other_step_path"] = max([e for e, k in zip(per_run, same) if not k], default=0.0)
         arms[name]["error_metric"] = "per run: max relative L2 over the dense outputs t = 2 .. 20 vs the FP64 batch"
     # single-run FP64 time per attempt, per mesh size
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
