@@ -450,7 +450,9 @@ def batched_to_end(n_runs, tune=True):
     mats, states = W.ensemble_runs(n_runs)
     f0 = np.concatenate(states)
     arms, dense, attempts = {}, {}, {}
-    for name, flag in (("f64", 0), ("t40", 2), ("t48", 3)):
+    # f64_repeat: the FP64 batch once more; its FP64 atomics add in another
+    # order, so it measures how far two FP64 runs of the ensemble differ
+    for name, flag in (("f64", 0), ("t40", 2), ("t48", 3), ("f64_repeat", 0)):
         t0 = time.perf_counter()
         be = E.BatchEngine(mats, allow_fp32=flag, autotune=tune)
         setup = time.perf_counter() - t0
@@ -471,7 +473,7 @@ def batched_to_end(n_runs, tune=True):
         if name == "f64":
             attempts_f64 = att
         be.close()
-    for name in ("t40", "t48"):
+    for name in ("t40", "t48", "f64_repeat"):
         per_run = [max(float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(da, db))
                    for da, db in zip(dense[name], dense["f64"])]
         arms[name]["error_vs_fp64"] = max(per_run)
