@@ -770,7 +770,7 @@ def large(args):
     mats, states = W.large_batch(16, 128)
     f0 = np.concatenate(states)
     t0 = time.perf_counter()
-    be = E.BatchEngine(mats, allow_fp32={"t32": 1, "t40": 2}[kind], autotune=not args.no_tune)
+    be = E.BatchEngine(mats, allow_fp32={"t32": 1, "t40": 2, "t48": 3}[kind], autotune=not args.no_tune)
     setup = time.perf_counter() - t0
     nch = be.channel_count()
     per_run = len(mats[0].channels)
@@ -883,7 +883,7 @@ def main():
     ap.add_argument("--ee", action="store_true",
                     help="profiling driver on the one-band e-e workload (parabolic band, --mesh sections per side)")
     ap.add_argument("--batch", type=int, default=0, help="batched ensemble of this many runs (per-run N, kT, couplings)")
-    ap.add_argument("--large", nargs="?", const="t32", default=None, choices=["t32", "t40"],
+    ap.add_argument("--large", nargs="?", const="t32", default=None, choices=["t32", "t40", "t48"],
                     help="16-run 128x128 three-band two-phonon batch with FP32 (default) or 40-bit moments")
     ap.add_argument("--to-end", action="store_true",
                     help="the 64x64 workload integrated to t = 20 (FP64 and 40-bit moments) vs the oracle")
