@@ -621,13 +621,13 @@ def adjoint(args):
 
 
 def small_ee(args):
-    """Prints small_ee_measure's line."""
-    print(json.dumps(small_ee_measure(args.no_cpu, args.no_tune)), flush=True)
+    """Prints small_ee_measure's line (--ee-mesh: another mesh size)."""
+    print(json.dumps(small_ee_measure(args.no_cpu, args.no_tune, args.ee_mesh)), flush=True)
 
 
-def small_ee_measure(no_cpu=False, no_tune=False):
+def small_ee_measure(no_cpu=False, no_tune=False, n_mesh=16):
     """The reference's CPU-runnable case: one parabolic band on a 16x16 mesh
-    (512 triangles), electron-electron scattering with a constant matrix
+    (512 triangles; n_mesh sections per side), electron-electron scattering with a constant matrix
     element, Fermi-Dirac kT 0.1 / mu 0.3 plus the seeded bump, DP45 with
     rtol 1e-6 / atol 1e-9 to t = 10 (dense output every 1.0).  The whole
     integration runs through the C ABI from host buffers (tb_dp45_integrate);
@@ -636,7 +636,7 @@ def small_ee_measure(no_cpu=False, no_tune=False):
     whole list, times the number of right-hand sides the GPU run needed."""
     from tortoise_b200 import engine as E
     from tortoise_b200 import workloads as W
-    mat = W.parabolic_ee(16)
+    mat = W.parabolic_ee(n_mesh)
     f0 = W.initial_status(mat, kT=0.1, seed=0).vec
     t_setup = time.perf_counter()
     eng = E.Engine(mat, autotune=not no_tune)
@@ -671,7 +671,8 @@ def small_ee_measure(no_cpu=False, no_tune=False):
         r = eng.dp45(f0, 0.0, 10.0, 1.0, max_dense=11)
         w1 = time.perf_counter()
     gpu_s = w1 - w0
-    line = {"workload": "16x16 parabolic band, e-e constant matrix element (512 triangles), rtol 1e-6, t = 10",
+    line = {"workload": "%dx%d parabolic band, e-e constant matrix element (%d triangles), rtol 1e-6, t = 10"
+                        % (n_mesh, n_mesh, 2 * n_mesh * n_mesh),
             "tuples": info["n_tuples"], "layout": info["layout"], "setup_s": t_setup,
             "tuples_with_points_inside": n_in, "points_inside": p_in,
             "points_evaluated_every_point": info["n_tuples"] * mat.channels[0].numMCPoints,
@@ -889,6 +890,7 @@ def main():
                     help="the 64x64 workload integrated to t = 20 (FP64 and 40-bit moments) vs the oracle")
     ap.add_argument("--small-ee", action="store_true",
                     help="16x16 one-band e-e integration to t = 10 (the reference's CPU-runnable case) vs the oracle")
+    ap.add_argument("--ee-mesh", type=int, default=16, help="sections per side of the --small-ee workload")
     ap.add_argument("--shard", action="store_true",
                     help="one run with its tuples split over the ranks (NCCL all-reduce per RHS) instead of replicas")
     ap.add_argument("--adjoint", type=int, default=-1,
