@@ -260,15 +260,16 @@ static int launch_mc(const ChanDev& c, const InstDev* insts, int n_insts, const 
     size_t smem = sizeof(double) * size_t(c.nmc) * c.R;
     if (SACC) {
         smem += sizeof(double) * size_t(n_insts) * size_t(c.sinst);
-        static bool attr = false;
-        if (!attr) {
-            TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(TB_MC_SACC_MAX_BYTES + sizeof(double) * 64 * 5)));
-            attr = true;
-        }
-        // one wave of resident blocks: each block clears and flushes its copy once
+        // the shared-memory limit, set once on each device the kernel runs on
+        static unsigned long long attr_devices = 0;
         int dev = 0, nsm = 148, per_sm = 1;
         cudaGetDevice(&dev);
+        if (dev < 0 || dev >= 64 || !((attr_devices >> dev) & 1ull)) {
+            TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(TB_MC_SACC_MAX_BYTES + sizeof(double) * 64 * 5)));
+            if (dev >= 0 && dev < 64) attr_devices |= 1ull << dev;
+        }
+        // one wave of resident blocks: each block clears and flushes its copy once
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
         if (per_sm < 1) per_sm = 1;

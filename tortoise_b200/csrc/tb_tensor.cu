@@ -858,13 +858,36 @@ int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n
     return TB_ERR_ARG;
 }
 
-static int* g_err_flag = nullptr;
+// The bulk-copy wait error flag of each device (allocated on first use on
+// that device, with it current), and the kernels' large-shared-memory
+// attribute, which is also set per device.
+constexpr int TB_MAX_DEVICES = 64;
+static int* g_err_flag[TB_MAX_DEVICES] = {};
 
-static int ensure_err_flag() {
-    if (!g_err_flag) {
-        TB_CUDA(cudaMalloc(&g_err_flag, sizeof(int)));
-        TB_CUDA(cudaMemset(g_err_flag, 0, sizeof(int)));
+static int current_device() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return dev;
+}
+
+static int ensure_err_flag(int** flag) {
+    const int dev = current_device();
+    if (dev < 0 || dev >= TB_MAX_DEVICES) { set_error("device ordinal beyond the library's table"); return TB_ERR_ARG; }
+    if (!g_err_flag[dev]) {
+        TB_CUDA(cudaMalloc(&g_err_flag[dev], sizeof(int)));
+        TB_CUDA(cudaMemset(g_err_flag[dev], 0, sizeof(int)));
     }
+    *flag = g_err_flag[dev];
+    return TB_OK;
+}
+
+// Sets kern's dynamic shared-memory limit once on each device.
+template <class K>
+static int ensure_smem_attr(K kern, int bytes, unsigned long long& done_devices) {
+    const int dev = current_device();
+    if (dev >= 0 && dev < TB_MAX_DEVICES && (done_devices >> dev) & 1ull) return TB_OK;
+    TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    if (dev >= 0 && dev < TB_MAX_DEVICES) done_devices |= 1ull << dev;
     return TB_OK;
 }
 
@@ -895,13 +918,10 @@ static int launch_runs(const ChanDev& c, const InstDev* insts, int n_insts, cons
     const size_t fixed = size_t(STAGES) * TT * tuple_bytes(L, KIND) +
                          ((KIND == TK_F40 || KIND == TK_F48) ? sizeof(double) * TDim<L>::NMOM * TT : 0);
     const size_t smem = fixed + sizeof(double) * size_t(T.np);
-    static bool attr = false;
-    if (!attr) {
-        TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int(fixed + sizeof(double) * RUNS_NP_MAX)));
-        attr = true;
-    }
-    TB_TRY(ensure_err_flag());
+    static unsigned long long attr_devices = 0;
+    TB_TRY(ensure_smem_attr(kern, int(fixed + sizeof(double) * RUNS_NP_MAX), attr_devices));
+    int* err_flag = nullptr;
+    TB_TRY(ensure_err_flag(&err_flag));
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -912,7 +932,7 @@ static int launch_runs(const ChanDev& c, const InstDev* insts, int n_insts, cons
     if (grid > T.ntiles) grid = T.ntiles;
     if (grid >= 1) {
         kern<<<unsigned(grid), RUNS_THREADS, smem, s>>>(c, insts, n_insts, R, static_cast<const unsigned char*>(T.d),
-                                                       T.ntiles, tup, stride, n, ctl, g_err_flag);
+                                                       T.ntiles, tup, stride, n, ctl, err_flag);
         TB_CUDA(cudaGetLastError());
     }
     const dim3 sg(tg.x, tg.y, 1), sb(32, 32);
@@ -958,12 +978,10 @@ static int launch_variant(const ChanDev& c, const InstDev* insts, int n_insts, c
     constexpr int TT = TTile<L, KIND>::TT;
     auto kern = k_collision_tensor<L, KIND, TT, STAGES, PAIR, RATE>;
     const size_t smem = size_t(STAGES) * TT * tuple_bytes(L, KIND);
-    static bool attr = false;
-    if (!attr) {
-        TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-        attr = true;
-    }
-    TB_TRY(ensure_err_flag());
+    static unsigned long long attr_devices = 0;
+    TB_TRY(ensure_smem_attr(kern, int(smem), attr_devices));
+    int* err_flag = nullptr;
+    TB_TRY(ensure_err_flag(&err_flag));
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -974,7 +992,7 @@ static int launch_variant(const ChanDev& c, const InstDev* insts, int n_insts, c
     if (grid > T.ntiles) grid = T.ntiles;
     if (grid < 1) return TB_OK;
     kern<<<unsigned(grid), TT, smem, s>>>(c, insts, n_insts, static_cast<const unsigned char*>(T.d), T.ntiles, tup,
-                                          stride, n, f, acc, ctl, g_err_flag, rate_leg);
+                                          stride, n, f, acc, ctl, err_flag, rate_leg);
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }
@@ -1091,8 +1109,9 @@ int tune_tensor(const ChanDev& c, const InstDev* insts, int n_insts, MomentTenso
 }
 
 int tensor_error_flag(int* value) {
-    if (!g_err_flag) { *value = 0; return TB_OK; }
-    TB_CUDA(cudaMemcpy(value, g_err_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    const int dev = current_device();
+    if (dev < 0 || dev >= TB_MAX_DEVICES || !g_err_flag[dev]) { *value = 0; return TB_OK; }
+    TB_CUDA(cudaMemcpy(value, g_err_flag[dev], sizeof(int), cudaMemcpyDeviceToHost));
     return TB_OK;
 }
 
