@@ -112,3 +112,27 @@ def test_oracle_integrator_with_a_pulsed_bath():
     o.set_constraint(lambda b, t: ph.population_at(0.0))
     flat = _same_run(o, f0, 0.0, 0.3, 0.01)
     assert pulsed["attempts"] > flat["attempts"]
+
+
+def test_documentation_example_through_the_reference_integrator():
+    """The scalar example of the reference's DP54 documentation
+    (DormandPrince54.hpp:80-106: y' = cos t from y(0) = 0 to t = 10, dense
+    step 1, normalised error 1e13 err^2) run by the reference's integrator,
+    against the oracle's restatement of the same example.  The oracle carries
+    t as a second state component (its core is autonomous), so the stage
+    times round a little differently: same attempts, dense outputs within
+    1e-12, and both within 1e-5 of sin t."""
+    L = _ref_lib()
+    cbs = (RHS(lambda u, t, y, out: out.__setitem__(0, np.cos(t))), ENF(lambda u, t, y: None),
+           NORM(lambda u, e, y: 10000000000000. * e[0] * e[0]),
+           VETO(lambda u, times, n, d: times[n - 1] - times[0]))
+    y0 = np.zeros(1)
+    dout, dt, st = np.zeros((64, 1)), np.zeros(64), (C.c_int64 * 4)()
+    nd = L.ref_dp54(1, y0.ctypes.data_as(DP), 0.0, 10.0, 1.0, *cbs, None, dout.ctypes.data_as(DP),
+                    dt.ctypes.data_as(DP), 64, st)
+    d, t, stats = oracle.scalar_example(0.0, 0.0, 10.0, 1.0)
+    assert nd == len(t) == 10
+    assert np.array_equal(dt[:nd], t)
+    assert list(stats[:3]) == [st[0], st[1], st[2]]
+    assert np.max(np.abs(dout[:nd, 0] - d)) < 1e-12
+    assert np.max(np.abs(dout[:nd, 0] - np.sin(dt[:nd]))) < 1e-5
