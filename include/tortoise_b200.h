@@ -150,6 +150,17 @@ typedef struct tb_options {
     int32_t autotune;             /* 1: time the contraction schedules at creation, keep the fastest */
     int32_t shard_rank;           /* tuple sharding (tb_shard_connect): this process's part ... */
     int32_t shard_count;          /* ... of shard_count parts; 0 or 1: no sharding  */
+    int32_t deterministic;        /* 1: bit-reproducible sums.  The collision, rate and VJP
+                                     kernels add their per-tuple results into exact 192-bit
+                                     fixed-point accumulators (units of 2^-112, integer
+                                     atomics) that are rounded to FP64 once per evaluation,
+                                     instead of FP64 atomics, so a result depends on the
+                                     per-tuple values only -- not on thread arrival order,
+                                     launch geometry or the contraction schedule.  Slower;
+                                     24 more bytes of device memory per dof (and per slot of
+                                     a run-minor group's accumulator).  The reference's TBB
+                                     reduce (ScatteringChannel.cpp:651-670) is itself not
+                                     reproducible across thread schedules. */
 } tb_options;
 
 /* Pointer flags */
@@ -291,8 +302,21 @@ int tb_dp45_poll(tb_handle* h, tb_dp45_stats* stats);
 int tb_dp45_end(tb_handle* h, double* f_out, double* dense_out, double* dense_times, int64_t max_dense,
                 tb_dp45_stats* stats, int flags);
 
-/* Synchronises the handle's stream. */
+/* Synchronises the handle's stream; TB_ERR_TIMEOUT when a contraction's
+ * bounded wait ran out since the last synchronising call. */
 int tb_synchronize(tb_handle* h);
+
+/* Poll limit of the moment-tensor contractions' wait for each staged tile of
+ * moments (default 2^22 polls, far above any real copy).  A wait that runs
+ * out makes its thread block record the failure, wait (with its own bound)
+ * for the copies it still has in flight, and leave its tiles out; the next
+ * synchronising call (tb_rhs / tb_scattering_rates with host buffers,
+ * tb_synchronize, tb_dp45_poll / tb_dp45_end / tb_dp45_integrate, the
+ * adjoint sweeps) returns TB_ERR_TIMEOUT, and the handle stays usable.
+ * polls = 0 gives up at once, which exercises that path.  The reference has
+ * no device waits (its only failure signal is the step-size underflow of
+ * DormandPrince54.hpp:532, 658-661). */
+int tb_set_copy_wait_limit(tb_handle* h, int64_t polls);
 
 /* The cudaStream_t every launch of this handle goes to (for event timing). */
 void* tb_get_stream(tb_handle* h);

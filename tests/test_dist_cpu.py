@@ -88,3 +88,87 @@ def test_two_ranks_share_one_id_and_split_every_tuple_list():
         assert (b0, e0, e1) == (0, b1, n), (n, g[0][1][n], g[1][1][n])
         assert b1 % 128 == 0 or b1 == n
         assert abs((e0 - b0) - (e1 - b1)) <= 128
+
+
+def _sharded_sum_rank(rank, world, port, out):
+    """One gloo rank of a tuple-sharded run on the oracle: its part of every
+    channel's tuple list (tb_shard_range), the partial operators all-reduced,
+    and a replicated DP45 on the all-reduced right-hand side driven by the
+    reference's own integrator (oracle/_ref)."""
+    import datetime
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle
+    from tortoise_b200 import engine as E
+    from tortoise_b200 import workloads as W
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        mat = W.build_material(4, ("P", "D"), (0.2,), ee=True, eph=True, field=(0.1, 0.0), rtol=1e-6, atol=1e-9)
+        f0 = W.initial_status(mat, seed=5).vec
+        o = oracle.Oracle(mat, nthreads=1)
+        parts = [E.shard_range(o.num_tuples(ch), rank, world) for ch in range(len(mat.channels))]
+        offs = [o.band_offset(b) for b in range(len(mat.bands))] + [o.ndofs]
+
+        def rhs(y, drift=True):
+            acc = np.zeros(o.ndofs)
+            for ch, (b, e) in enumerate(parts):          # ScatteringChannel::propagate over this rank's tuples
+                o.channel_propagate(ch, y, b, e, inverse_mass=True, out=acc)
+            if drift and rank == 0:                      # the replicated drift term, added once
+                for b in range(len(mat.bands)):
+                    acc[offs[b]:offs[b + 1]] += o.vlasov(b, y[offs[b]:offs[b + 1]])
+            t = torch.from_numpy(acc)
+            dist.all_reduce(t)
+            return t.numpy().copy()
+
+        full = o.rhs(f0, drift=False)
+        got = rhs(f0, drift=False)
+        err_sum = float(np.linalg.norm(got - full) / np.linalg.norm(full))
+        res = {"sum_rel_l2": err_sum, "n_tuples": [o.num_tuples(c) for c in range(len(mat.channels))],
+               "parts": parts}
+        ref_so = os.path.join(ROOT, "oracle", "_ref", "libref_dp54.so")
+        if os.path.exists(ref_so):
+            from test_oracle_ref_dp54 import reference_dp54
+            r = reference_dp54(o, f0, 0.0, 0.3, 0.1, rhs_fn=rhs)
+            res["dp"] = {k: r[k] for k in ("attempts", "accepted", "rejected", "rhs_evals", "n_dense")}
+            res["dense"] = r["dense"].tobytes()
+            if rank == 0:
+                u = o.dp45(f0, 0.0, 0.3, 0.1, max_dense=64)
+                res["unsharded"] = {k: u[k] for k in ("attempts", "accepted", "rejected", "rhs_evals", "n_dense")}
+                res["unsharded_dense_rel"] = float(np.linalg.norm(u["dense"] - r["dense"]) / np.linalg.norm(u["dense"]))
+        out.put((rank, res))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_partial_operators_sum_to_the_full_one_and_step_alike():
+    """The data plane of tuple sharding on two gloo ranks, with the oracle as
+    each rank's collision operator: every channel's tuple list split by
+    tb_shard_range, the per-rank partial operators summed by an all-reduce
+    (the reduce of ScatteringChannel.cpp:651-670 across processes) equal the
+    full operator; and a DP45 run replicated on both ranks over the
+    all-reduced right-hand side takes the same accept / reject decisions and
+    the same dense outputs on both ranks, and those of the unsharded run."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_sharded_sum_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=300) for _ in range(2))
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    r0, r1 = res[0], res[1]
+    assert r0["sum_rel_l2"] < 1e-13 and r1["sum_rel_l2"] == r0["sum_rel_l2"]
+    for n, (a, b) in zip(r0["n_tuples"], zip(r0["parts"], r1["parts"])):
+        assert a[0] == 0 and a[1] == b[0] and b[1] == n
+    assert sum(1 for a in r0["parts"] if a[1] > 0) >= 2   # both ranks hold work in several channels
+    assert sum(1 for b in r1["parts"] if b[1] > b[0]) >= 2
+    if "dp" in r0:
+        assert r0["dp"] == r1["dp"] and r0["dense"] == r1["dense"]   # replicated controller: identical
+        assert r0["dp"] == r0["unsharded"]
+        assert r0["unsharded_dense_rel"] < 1e-10

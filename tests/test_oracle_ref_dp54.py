@@ -43,14 +43,19 @@ def _ref_lib():
     return L
 
 
-def reference_dp54(o, y0, t0, tf, dense, drift=True, max_dense=64):
-    """The reference's integrator on the oracle's operators."""
+def reference_dp54(o, y0, t0, tf, dense, drift=True, max_dense=64, rhs_fn=None):
+    """The reference's integrator on the oracle's operators; rhs_fn(y) -> dy/dt
+    (numpy arrays) replaces the oracle's right-hand side when given."""
     L, OL = _ref_lib(), oracle.lib()
     n = o.ndofs
     errors = []
 
     def rhs(user, t, y, out):
-        OL.or_rhs(o.h, y, out, o.nthreads, 1 if drift else 0)
+        if rhs_fn is None:
+            OL.or_rhs(o.h, y, out, o.nthreads, 1 if drift else 0)
+        else:
+            out_np = np.ctypeslib.as_array(out, shape=(n,))
+            out_np[:] = rhs_fn(np.ctypeslib.as_array(y, shape=(n,)).copy())
 
     def enforce(user, t, y):
         if OL.or_apply_constraints_at(o.h, y, t) != 0:

@@ -76,6 +76,7 @@ struct AdjointState {
     double* rtmp = nullptr;
     double* ry5 = nullptr;
     double* gamp = nullptr;    // [slots] amplitude gradients, group-major
+    FxAcc gamp_fx{};           // deterministic mode: gamp's exact accumulator
     std::vector<int> gamp_off; // per group
     int n_slots = 0;
     // last forward sweep
@@ -128,12 +129,22 @@ static int adj_base(tb_handle* h) {
         A->gamp_off[gi + 1] = A->gamp_off[gi] + int(h->groups[gi].insts.size());
     A->n_slots = A->gamp_off.back();
     A->gamp = adj_alloc(A, size_t(std::max(A->n_slots, 1)));
+    if (h->opts.deterministic) {
+        // 3 words per slot and the poison word, in double-sized units
+        double* p3 = adj_alloc(A, size_t(3 * std::max(A->n_slots, 1) + 1));
+        if (p3) {
+            TB_CUDA(cudaMemset(p3, 0, sizeof(double) * size_t(3 * std::max(A->n_slots, 1) + 1)));
+            A->gamp_fx.w = reinterpret_cast<unsigned long long*>(p3);
+            A->gamp_fx.poison = reinterpret_cast<unsigned int*>(A->gamp_fx.w + 3 * std::max(A->n_slots, 1));
+        }
+    }
     void* p = nullptr;
     if (cudaMalloc(&p, sizeof(double*) * 6) == cudaSuccess) {
         A->allocs.push_back(p);
         A->dD = static_cast<double**>(p);
     }
-    bool ok = A->lam && A->lam_T && A->nud && A->u && A->g && A->ry && A->rtmp && A->ry5 && A->gamp && A->dD;
+    bool ok = A->lam && A->lam_T && A->nud && A->u && A->g && A->ry && A->rtmp && A->ry5 && A->gamp && A->dD &&
+              (!h->opts.deterministic || A->gamp_fx.w);
     for (int i = 0; i < 7; ++i) ok = ok && A->k[i];
     for (int i = 0; i < 6; ++i) ok = ok && A->D[i];
     if (!ok) {
@@ -372,23 +383,32 @@ static int vjp_at(tb_handle* h, const double* Y, int flags) {
         for (size_t gi = 0; gi < h->groups.size(); ++gi) {
             GroupChan& G = h->groups[gi];
             if (G.tup.n == 0 || G.insts.empty()) continue;
+            // deterministic mode: the group's amplitude slots in the exact accumulator
+            FxAcc fa = A->gamp_fx;
+            if (fa.w) fa.w += 3 * int64_t(A->gamp_off[gi]);
             if (G.layout == TB_LAYOUT_MC64 && G.theta.use)   // the tuples and points inside the simplices only
                 TB_TRY(launch_collision_vjp(G.dev, G.d_insts, int(G.insts.size()), G.layout, G.tensor, G.theta.ids,
                                             G.theta.n, G.theta.n, Y, A->u, A->g, A->gamp + A->gamp_off[gi], h->stream,
-                                            G.theta.mask, G.theta.perm));
+                                            G.theta.mask, G.theta.perm, h->fx, fa));
             else
                 TB_TRY(launch_collision_vjp(G.dev, G.d_insts, int(G.insts.size()), G.layout, G.tensor, G.tup.d,
-                                            G.tup.cap, G.tup.n, Y, A->u, A->g, A->gamp + A->gamp_off[gi], h->stream));
+                                            G.tup.cap, G.tup.n, Y, A->u, A->g, A->gamp + A->gamp_off[gi], h->stream,
+                                            nullptr, nullptr, h->fx, fa));
         }
+        TB_TRY(launch_fx_flush(h->fx, A->g, h->ndofs, h->stream));   // deterministic mode
         TB_TRY(shard_allreduce(h, A->g, size_t(h->ndofs)));   // sharded: all ranks' partial VJPs
     }
-    if (!(flags & TB_NO_DRIFT) && h->any_drift) TB_TRY(launch_drift_vjp(h->ed, A->u, A->g, h->stream));
+    if (!(flags & TB_NO_DRIFT) && h->any_drift) {
+        TB_TRY(launch_drift_vjp(h->ed, A->u, A->g, h->stream, h->fx));
+        TB_TRY(launch_fx_flush(h->fx, A->g, h->ndofs, h->stream));
+    }
     A->vjp_evals += 1;
     return TB_OK;
 }
 
 static int copy_gamp_out(tb_handle* h, double* grad_amp) {
     AdjointState* A = h->adj;
+    TB_TRY(launch_fx_flush(A->gamp_fx, A->gamp, A->n_slots, h->stream));   // deterministic mode
     TB_TRY(shard_allreduce(h, A->gamp, size_t(A->n_slots)));   // sharded: all ranks' partial sums
     std::vector<double> slots(size_t(std::max(A->n_slots, 1)));
     TB_CUDA(cudaMemcpyAsync(slots.data(), A->gamp, sizeof(double) * size_t(A->n_slots), cudaMemcpyDeviceToHost,
@@ -424,6 +444,8 @@ int tb_adjoint_rhs_vjp(tb_handle* h, const double* f, const double* theta, doubl
     }
     TB_CUDA(cudaMemsetAsync(A->g, 0, bytes, h->stream));
     TB_CUDA(cudaMemsetAsync(A->gamp, 0, sizeof(double) * size_t(std::max(A->n_slots, 1)), h->stream));
+    if (A->gamp_fx.w)   // a sweep that failed half-way may have left words behind
+        TB_CUDA(cudaMemsetAsync(A->gamp_fx.w, 0, sizeof(double) * size_t(3 * std::max(A->n_slots, 1) + 1), h->stream));
     TB_TRY(launch_minv_t(h->ed, dth, A->u, h->stream));
     TB_TRY(vjp_at(h, df, flags));
     if (flags & TB_PTR_HOST) TB_CUDA(cudaMemcpyAsync(grad_f, A->g, bytes, cudaMemcpyDeviceToHost, h->stream));
@@ -572,6 +594,8 @@ int tb_adjoint_backward(tb_handle* h, const double* lambda_T, double* grad_f0, d
     TB_CUDA(cudaMemsetAsync(A->g, 0, bytes, h->stream));
     TB_CUDA(cudaMemsetAsync(A->lam, 0, bytes, h->stream));
     TB_CUDA(cudaMemsetAsync(A->gamp, 0, sizeof(double) * size_t(std::max(A->n_slots, 1)), h->stream));
+    if (A->gamp_fx.w)   // a sweep that failed half-way may have left words behind
+        TB_CUDA(cudaMemsetAsync(A->gamp_fx.w, 0, sizeof(double) * size_t(3 * std::max(A->n_slots, 1) + 1), h->stream));
     TB_CUDA(cudaMemsetAsync(h->d_acc, 0, bytes, h->stream));
     double* const* dD = A->dD;
     const int64_t nd = A->n_steps - 1;   // the dense-output step
@@ -625,7 +649,7 @@ int tb_adjoint_backward(tb_handle* h, const double* lambda_T, double* grad_f0, d
     if (grad_amp) TB_TRY(copy_gamp_out(h, grad_amp));
     TB_TRY(stream_wait(h));
     int tflag = 0;
-    TB_TRY(tensor_error_flag(&tflag));
+    TB_TRY(take_wait_timeout(h->d_err, h->stream, &tflag));
     if (tflag) { set_error("moment-tensor copy wait ran out"); return TB_ERR_TIMEOUT; }
     if (st) {
         std::memset(st, 0, sizeof(*st));

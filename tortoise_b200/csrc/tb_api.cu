@@ -109,6 +109,21 @@ double* dev_alloc(tb_handle* h, size_t n) {
     return p;
 }
 
+int fx_alloc(tb_handle* h, int64_t n, FxAcc& out) {
+    void* p = nullptr;
+    const size_t bytes = sizeof(unsigned long long) * size_t(3 * n + 1);
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("exact accumulator allocation failed");
+        return TB_ERR_OOM;
+    }
+    h->dev_raw.push_back(p);
+    TB_CUDA(cudaMemset(p, 0, bytes));
+    out.w = static_cast<unsigned long long*>(p);
+    out.poison = reinterpret_cast<unsigned int*>(out.w + 3 * n);
+    return TB_OK;
+}
+
 template <typename T>
 T* dev_upload_raw(tb_handle* h, const T* src, size_t n) {
     void* p = nullptr;
@@ -369,6 +384,14 @@ int build_runs(tb_handle* h, const tb_problem_desc* const* descs, int nruns) {
     h->d_part = dev_alloc(h, size_t(2 * h->ed.nblk + 8));
     if (!h->d_f || !h->d_out || !h->d_acc || !h->d_part) { set_error("state allocation failed"); return TB_ERR_OOM; }
     TB_CUDA(cudaMemsetAsync(h->d_acc, 0, sizeof(double) * size_t(h->ndofs), h->stream));
+    if (h->opts.deterministic) TB_TRY(fx_alloc(h, h->ndofs, h->fx));
+    {
+        void* p = nullptr;
+        if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) { set_error("flag allocation failed"); return TB_ERR_OOM; }
+        h->dev_raw.push_back(p);
+        h->d_err = static_cast<int*>(p);
+        TB_CUDA(cudaMemset(h->d_err, 0, sizeof(int)));
+    }
     // channel groups and instances
     std::vector<int> group_chan0(group_first_run.size(), -1);
     for (int r = 0; r < nruns; ++r) {
@@ -428,6 +451,7 @@ int build_runs(tb_handle* h, const tb_problem_desc* const* descs, int nruns) {
                 for (int i = 0; i < G.L - 2; ++i) c.fact *= 2.0;
                 c.min_det = cd.min_det;
                 c.threshold = cd.threshold;
+                c.err_flag = h->d_err;
                 for (int i = 0; i < 4; ++i) c.gvec[i] = d->region.gvec[i];
                 G.d_umk = dev_upload(h, std::vector<double>(cd.umklapp, cd.umklapp + 2 * size_t(cd.n_umklapp)));
                 G.d_mc = dev_upload(h, std::vector<double>(cd.mc_points, cd.mc_points + size_t(cd.n_mc) * c.R));
@@ -516,9 +540,9 @@ static int launch_group_mc(tb_handle* h, GroupChan& G, const InstDev* insts, int
                            double* d_acc, const DPCtl* ctl, int rate_leg) {
     if (G.theta.use)
         return launch_collision_mc(G.dev, insts, n_insts, G.theta.ids, G.theta.n, G.theta.n, d_in, d_acc, ctl,
-                                   h->stream, 148 * 32, rate_leg, G.theta.mask, G.theta.perm);
+                                   h->stream, 148 * 32, rate_leg, G.theta.mask, G.theta.perm, h->fx);
     return launch_collision_mc(G.dev, insts, n_insts, G.tup.d, G.tup.cap, G.tup.n, d_in, d_acc, ctl, h->stream,
-                               148 * 32, rate_leg);
+                               148 * 32, rate_leg, nullptr, nullptr, h->fx);
 }
 
 int run_rhs_acc(tb_handle* h, const double* d_in, double* d_acc, const DPCtl* ctl, int flags, int only_inst) {
@@ -541,9 +565,11 @@ int run_rhs_acc(tb_handle* h, const double* d_in, double* d_acc, const DPCtl* ct
                 TB_TRY(launch_group_mc(h, G, insts, n_insts, d_in, d_acc, ctl, -1));
             } else {
                 TB_TRY(launch_collision_tensor(G.dev, insts, n_insts, G.tensor, G.tup.d, G.tup.cap, G.tup.n, d_in,
-                                               d_acc, ctl, h->stream));
+                                               d_acc, ctl, h->stream, -1, h->fx));
             }
         }
+        // deterministic mode: the exact sums, rounded once, into d_acc
+        TB_TRY(launch_fx_flush(h->fx, d_acc, h->ndofs, h->stream));
         // sharded: the partial collision sums of all ranks, before the
         // (replicated) drift term
         TB_TRY(shard_allreduce(h, d_acc, size_t(h->ndofs)));
@@ -605,7 +631,8 @@ int choose_layouts(tb_handle* h) {
             for (int id : G.insts) runs_of.push_back(h->insts[id].run);
             std::sort(runs_of.begin(), runs_of.end());
             const bool distinct = std::adjacent_find(runs_of.begin(), runs_of.end()) == runs_of.end();
-            TB_TRY(prepare_runs(G.dev, int(G.insts.size()), distinct, G.tensor, h->stream));
+            TB_TRY(prepare_runs(G.dev, int(G.insts.size()), distinct, G.tensor, h->stream,
+                                h->opts.deterministic != 0));
         }
     }
     return TB_OK;
@@ -741,6 +768,10 @@ int tb_create_batch(tb_handle** out, const tb_problem_desc* const* runs, int n_r
     if (h->opts.layout < TB_LAYOUT_AUTO || h->opts.layout > TB_LAYOUT_T48 || h->opts.allow_fp32 < 0 ||
         h->opts.allow_fp32 > 3) {
         set_error("tb_options: layout must be 0..5 and allow_fp32 0..3");
+        return TB_ERR_ARG;
+    }
+    if (h->opts.deterministic != 0 && h->opts.deterministic != 1) {
+        set_error("tb_options: deterministic must be 0 or 1");
         return TB_ERR_ARG;
     }
     if (h->opts.shard_count < 0 || h->opts.shard_rank < 0 ||
@@ -1047,6 +1078,18 @@ int tb_set_amplitude(tb_handle* h, int ch, double amplitude) {
     return TB_OK;
 }
 
+// TB_ERR_TIMEOUT when a contraction's bounded wait ran out since the last
+// check (the kernels that gave up left their part of the sum out).
+static int check_wait_timeout(tb_handle* h) {
+    int tflag = 0;
+    TB_TRY(take_wait_timeout(h->d_err, h->stream, &tflag));
+    if (tflag) {
+        set_error("a moment-tensor contraction gave up waiting for its staged tiles; the result is incomplete");
+        return TB_ERR_TIMEOUT;
+    }
+    return TB_OK;
+}
+
 static int rhs_common(tb_handle* h, const double* f, double* out, int flags, int only_inst) {
     if (!h || !f || !out) { set_error("null argument"); return TB_ERR_ARG; }
     TB_CUDA(cudaSetDevice(h->device));
@@ -1065,6 +1108,7 @@ static int rhs_common(tb_handle* h, const double* f, double* out, int flags, int
     if (flags & TB_PTR_HOST) {
         TB_CUDA(cudaMemcpyAsync(out, h->d_out, bytes, cudaMemcpyDeviceToHost, h->stream));
         TB_TRY(stream_wait(h));
+        TB_TRY(check_wait_timeout(h));
     }
     return TB_OK;
 }
@@ -1108,15 +1152,17 @@ int tb_scattering_rates(tb_handle* h, int ch, int leg, const double* f, double* 
                 TB_TRY(launch_group_mc(h, G, insts, n_insts, d_in, h->d_acc, nullptr, l));
             else
                 TB_TRY(launch_collision_tensor(G.dev, insts, n_insts, G.tensor, G.tup.d, G.tup.cap, G.tup.n, d_in,
-                                               h->d_acc, nullptr, h->stream, l));
+                                               h->d_acc, nullptr, h->stream, l, h->fx));
         }
     }
+    TB_TRY(launch_fx_flush(h->fx, h->d_acc, h->ndofs, h->stream));
     TB_TRY(shard_allreduce(h, h->d_acc, size_t(h->ndofs)));
     TB_TRY(launch_inverse_mass(h->ed, h->d_acc, d_res, h->stream));
     TB_CUDA(cudaMemsetAsync(h->d_acc, 0, bytes, h->stream));
     if (flags & TB_PTR_HOST) {
         TB_CUDA(cudaMemcpyAsync(rates, h->d_out, bytes, cudaMemcpyDeviceToHost, h->stream));
         TB_TRY(stream_wait(h));
+        TB_TRY(check_wait_timeout(h));
     }
     return TB_OK;
 }
@@ -1193,6 +1239,7 @@ int dp_begin(tb_handle* h, const double* f0, const double* t0, const double* t_f
     TB_TRY(dp_alloc(h, max_dense));
     const int rflags = flags & (TB_NO_DRIFT | TB_NO_COLLISIONS);
     h->dp_flags = flags;
+    h->wait_timed_out = false;
     const size_t bytes = sizeof(double) * size_t(h->ndofs);
     DPBufs& B = h->dp;
     {
@@ -1271,8 +1318,9 @@ static int poll_all(tb_handle* h) {
     TB_CUDA(cudaMemcpyAsync(h->h_ctl, h->dp.ctl, sizeof(DPCtl) * h->runs.size(), cudaMemcpyDeviceToHost, h->stream));
     TB_TRY(stream_wait(h));
     int tflag = 0;
-    TB_TRY(tensor_error_flag(&tflag));
-    if (tflag)
+    TB_TRY(take_wait_timeout(h->d_err, h->stream, &tflag));
+    if (tflag) h->wait_timed_out = true;   // sticky for this integration: its state is unreliable
+    if (h->wait_timed_out)
         for (size_t r = 0; r < h->runs.size(); ++r) { h->h_ctl[r].status = TB_ERR_TIMEOUT; h->h_ctl[r].done = 1; }
     return TB_OK;
 }
@@ -1342,6 +1390,17 @@ int tb_dp45_integrate(tb_handle* h, double* f_inout, double t0, double t_final, 
 int tb_synchronize(tb_handle* h) {
     if (!h) return TB_ERR_ARG;
     TB_TRY(stream_wait(h));
+    TB_TRY(check_wait_timeout(h));
+    return TB_OK;
+}
+
+int tb_set_copy_wait_limit(tb_handle* h, int64_t polls) {
+    if (!h) { set_error("null handle"); return TB_ERR_ARG; }
+    if (polls < 0 || polls > 0x7fffffff) { set_error("polls must lie in [0, 2^31 - 1]"); return TB_ERR_ARG; }
+    TB_CUDA(cudaSetDevice(h->device));
+    TB_TRY(stream_wait(h));
+    for (auto& G : h->groups) G.dev.wait_polls = int(polls);
+    if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }   // launches keep their arguments
     return TB_OK;
 }
 

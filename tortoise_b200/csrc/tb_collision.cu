@@ -11,7 +11,9 @@
 //   * gain-minus-loss products and the (1 + 2L) distinct output moments are
 //     accumulated in FP64 registers
 //   * the 3L results are scattered with FP64 atomics (RED) into the pre-M^-1
-//     accumulator, which stays L2-resident.
+//     accumulator, which stays L2-resident; in the deterministic mode they
+//     go to the exact fixed-point accumulator instead (tb_exact.cuh), one
+//     lane at a time.
 // The kernel is FP64-FMA bound (about 55 FP64 operations per MC point for L=4).
 // LIST: the same quadrature over a ThetaList (tb_theta.cu): the tuples with at
 // least one point inside the simplices, each visiting only those points (set
@@ -85,7 +87,7 @@ __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_colli
                                                       const int32_t* __restrict__ tup, int64_t stride, int64_t n,
                                                       const uint64_t* __restrict__ mask, const int32_t* __restrict__ perm,
                                                       const double* __restrict__ f, double* __restrict__ acc,
-                                                      const DPCtl* __restrict__ ctl, int rate_leg) {
+                                                      const DPCtl* __restrict__ ctl, int rate_leg, FxAcc fx) {
     // Nothing to add when every instance is switched off or its run has
     // finished (the speculative DP45 attempts after the end of an
     // integration): leave before walking the tuples.  Uniform in the block.
@@ -226,7 +228,11 @@ __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_colli
                 const double d = RATE ? -c.leg[l].dir : c.leg[l].dir;
                 const int64_t key = SACC ? int64_t(k * c.sinst + c.sseg[l] + 3 * e[l]) : in.foff[l] + 3 * (int64_t)e[l];
                 double* const dst = (SACC ? s_acc : acc) + key;
-                if (l < L - 1 && (!SACC || l < TB_MC_SACC_SCAN_LEGS)) {
+                if (!SACC && fx.w) {   // deterministic mode (never with SACC)
+                    if (valid)
+                        fx_add3(fx, key, d * ((scale * s0) * ampt), d * ((scale * sx[l]) * ampt),
+                                d * ((scale * sy[l]) * ampt));
+                } else if (l < L - 1 && (!SACC || l < TB_MC_SACC_SCAN_LEGS)) {
                     warp_scatter3(valid ? key : -1, dst, d * ((scale * s0) * ampt), d * ((scale * sx[l]) * ampt),
                                   d * ((scale * sy[l]) * ampt));
                 } else if (valid) {
@@ -253,7 +259,7 @@ __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_colli
 template <int L, bool RATE, bool LIST, bool SACC>
 static int launch_mc(const ChanDev& c, const InstDev* insts, int n_insts, const int32_t* tup, int64_t stride,
                      int64_t n, const uint64_t* mask, const int32_t* perm, const double* f, double* acc,
-                     const DPCtl* ctl, cudaStream_t s, int grid_hint, int rate_leg) {
+                     const DPCtl* ctl, cudaStream_t s, int grid_hint, int rate_leg, const FxAcc& fx) {
     auto kern = k_collision_mc<L, RATE, LIST, SACC>;
     const int threads = 256;
     int64_t blocks = (n + threads - 1) / threads;
@@ -278,7 +284,7 @@ static int launch_mc(const ChanDev& c, const InstDev* insts, int n_insts, const 
         blocks = grid_hint;
     }
     kern<<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, mask, perm, f, acc, ctl,
-                                                 RATE ? rate_leg : -1);
+                                                 RATE ? rate_leg : -1, fx);
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }
@@ -286,11 +292,12 @@ static int launch_mc(const ChanDev& c, const InstDev* insts, int n_insts, const 
 template <int L>
 static int launch_mc_l(const ChanDev& c, const InstDev* insts, int n_insts, const int32_t* tup, int64_t stride,
                        int64_t n, const uint64_t* mask, const int32_t* perm, const double* f, double* acc,
-                       const DPCtl* ctl, cudaStream_t s, int grid_hint, int rate_leg) {
+                       const DPCtl* ctl, cudaStream_t s, int grid_hint, int rate_leg, const FxAcc& fx) {
     const bool list = mask != nullptr;
-    const bool sacc = list && c.sinst > 0 && c.nmc <= 64 &&
+    // the shared-memory accumulator adds in FP64: not in the deterministic mode
+    const bool sacc = list && !fx.w && c.sinst > 0 && c.nmc <= 64 &&
                       sizeof(double) * size_t(n_insts) * size_t(c.sinst) <= TB_MC_SACC_MAX_BYTES;
-#define TB_MC_ARGS c, insts, n_insts, tup, stride, n, mask, perm, f, acc, ctl, s, grid_hint, rate_leg
+#define TB_MC_ARGS c, insts, n_insts, tup, stride, n, mask, perm, f, acc, ctl, s, grid_hint, rate_leg, fx
     if (rate_leg >= 0) {
         if (sacc) return launch_mc<L, true, true, true>(TB_MC_ARGS);
         if (list) return launch_mc<L, true, true, false>(TB_MC_ARGS);
@@ -304,12 +311,12 @@ static int launch_mc_l(const ChanDev& c, const InstDev* insts, int n_insts, cons
 
 int launch_collision_mc(const ChanDev& c, const InstDev* insts, int n_insts, const int32_t* tup, int64_t stride,
                         int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s, int grid_hint,
-                        int rate_leg, const uint64_t* mask, const int32_t* perm) {
+                        int rate_leg, const uint64_t* mask, const int32_t* perm, const FxAcc& fx) {
     if (n <= 0 || n_insts <= 0) return TB_OK;
     switch (c.L) {
-        case 2: return launch_mc_l<2>(c, insts, n_insts, tup, stride, n, mask, perm, f, acc, ctl, s, grid_hint, rate_leg);
-        case 3: return launch_mc_l<3>(c, insts, n_insts, tup, stride, n, mask, perm, f, acc, ctl, s, grid_hint, rate_leg);
-        case 4: return launch_mc_l<4>(c, insts, n_insts, tup, stride, n, mask, perm, f, acc, ctl, s, grid_hint, rate_leg);
+        case 2: return launch_mc_l<2>(c, insts, n_insts, tup, stride, n, mask, perm, f, acc, ctl, s, grid_hint, rate_leg, fx);
+        case 3: return launch_mc_l<3>(c, insts, n_insts, tup, stride, n, mask, perm, f, acc, ctl, s, grid_hint, rate_leg, fx);
+        case 4: return launch_mc_l<4>(c, insts, n_insts, tup, stride, n, mask, perm, f, acc, ctl, s, grid_hint, rate_leg, fx);
         default: set_error("nlegs must be 2..4"); return TB_ERR_ARG;
     }
 }
@@ -330,6 +337,30 @@ __global__ void k_inverse_mass(ElemDev ed, const double* __restrict__ acc, doubl
 int launch_inverse_mass(const ElemDev& ed, const double* acc, double* out, cudaStream_t s) {
     k_inverse_mass<<<ed.nblk, 256, 0, s>>>(ed, acc, out);
     TB_CUDA(cudaGetLastError());
+    return TB_OK;
+}
+
+// ------------------------------------------------- exact accumulator flush
+__global__ void __launch_bounds__(256) k_fx_flush(FxAcc fx, double* __restrict__ acc, int64_t n) {
+    const bool poisoned = *fx.poison != 0u;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        unsigned long long* p = fx.w + 3 * i;
+        const unsigned long long w0 = p[0], w1 = p[1], w2 = p[2];
+        const bool nz = (w0 | w1 | w2) != 0ull;
+        if (nz) { p[0] = 0ull; p[1] = 0ull; p[2] = 0ull; }
+        if (poisoned) acc[i] = __longlong_as_double(0x7ff8000000000000ll);   // NaN
+        else if (nz) acc[i] += fx_value(w0, w1, w2);
+    }
+}
+
+int launch_fx_flush(const FxAcc& fx, double* acc, int64_t n, cudaStream_t s) {
+    if (n <= 0 || !fx.w) return TB_OK;
+    int64_t blocks = (n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_fx_flush<<<unsigned(blocks), 256, 0, s>>>(fx, acc, n);
+    TB_CUDA(cudaGetLastError());
+    // every thread has read the poison word once the kernel is done
+    TB_CUDA(cudaMemsetAsync(fx.poison, 0, sizeof(unsigned int), s));
     return TB_OK;
 }
 

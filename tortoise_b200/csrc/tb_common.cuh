@@ -112,6 +112,11 @@ struct ChanDev {
     int sseg[TB_MAX_LEGS] = {};       // per leg: offset of its band's segment
     int seg_off[TB_MAX_LEGS] = {};    // per segment: offset in the block
     int seg_leg[TB_MAX_LEGS] = {};    // per segment: a leg of that band (its foff)
+    // Moment-tensor contractions: the handle's flag that a bounded wait for a
+    // staged tile ran out (then TB_ERR_TIMEOUT), and that wait's poll limit
+    // (tb_set_copy_wait_limit).
+    int* err_flag = nullptr;
+    int wait_polls = 1 << 22;
 };
 
 // Mesh data needed by the element-wise kernels.

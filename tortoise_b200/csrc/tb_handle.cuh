@@ -75,6 +75,13 @@ struct tb_handle {
     double* d_out = nullptr;
     double* d_acc = nullptr;
     double* d_part = nullptr;
+    // deterministic mode: the exact accumulator behind d_acc (3 words per
+    // dof and a poison word; w == nullptr otherwise)
+    tb::FxAcc fx{};
+    // set by a contraction kernel whose bounded wait for a staged tile ran
+    // out; read and cleared by the synchronising calls (TB_ERR_TIMEOUT)
+    int* d_err = nullptr;
+    bool wait_timed_out = false;   // the current integration met a timed-out wait
     // DP45
     tb::DPBufs dp{};
     bool dp_ready = false;
@@ -111,6 +118,10 @@ int ensure_graph(tb_handle* h, int flags);
 int dp_begin(tb_handle* h, const double* f0, const double* t0, const double* t_final, const double* dense_step,
              int64_t max_dense, int flags, const DPBufs* hooks);
 void adjoint_release(tb_handle* h);
+
+// A zeroed exact accumulator of n slots (3 words each) plus its poison word,
+// owned by the handle (deterministic mode).
+int fx_alloc(tb_handle* h, int64_t n, FxAcc& out);
 
 // tb_shard.cu
 int64_t shard_begin(int64_t n, int rank, int n_ranks);

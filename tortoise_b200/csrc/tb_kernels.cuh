@@ -2,6 +2,7 @@
 #pragma once
 
 #include "tb_common.cuh"
+#include "tb_exact.cuh"
 
 namespace tb {
 
@@ -38,9 +39,17 @@ struct ElemDev {
 // unit forms, only its block kept, with the opposite sign).  mask / perm
 // non-null: tup, stride, n describe a ThetaList (tb_theta.cuh) and only the
 // points inside the simplices are evaluated.
+// fx.w non-null (deterministic mode): the results go to the exact fixed-point
+// accumulator fx (tb_exact.cuh) instead of acc.
 int launch_collision_mc(const ChanDev& c, const InstDev* insts, int n_insts, const int32_t* tup, int64_t stride,
                         int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s, int grid_hint,
-                        int rate_leg = -1, const uint64_t* mask = nullptr, const int32_t* perm = nullptr);
+                        int rate_leg = -1, const uint64_t* mask = nullptr, const int32_t* perm = nullptr,
+                        const FxAcc& fx = FxAcc{});
+
+// acc[i] += fx slot i for i < n (rounded once to FP64), then the slots are
+// cleared; a poisoned buffer writes NaN into every acc[i] instead and the
+// poison word is cleared too.
+int launch_fx_flush(const FxAcc& fx, double* acc, int64_t n, cudaStream_t s);
 
 // Vlasov drift (volume minus upwind surface term, before M^-1) of every band
 // with a nonzero drift velocity, added into acc.

@@ -87,8 +87,10 @@ void MomentTensor::release() {
     if (d) cudaFree(d);
     if (fT) cudaFree(fT);
     if (accT) cudaFree(accT);
+    if (accTx) cudaFree(accTx);
     d = nullptr;
     fT = accT = nullptr;
+    accTx = nullptr;
     n = ntiles = 0;
     runs = np = runs_distinct = 0;
 }
@@ -289,7 +291,8 @@ __device__ __forceinline__ double tile_moment(const unsigned char* __restrict__ 
 template <int L, int KIND, int TT, int NI, bool RATE>
 __device__ __forceinline__ void contract_tuple(const ChanDev& c, const InstDev (&in)[NI], const int (&e)[L], bool valid,
                                                const unsigned char* __restrict__ tile, int tid,
-                                               const double* __restrict__ f, double* __restrict__ acc, int rate_leg) {
+                                               const double* __restrict__ f, double* __restrict__ acc, int rate_leg,
+                                               const FxAcc& fx) {
     constexpr int K = TDim<L>::K, KM = TDim<L>::KM, NMOM = TDim<L>::NMOM;
     auto M = [&](int j) { return tile_moment<KIND, NMOM, TT>(tile, tid, j); };
     // v = kron(A) + kron(B) per instance, leg 0 most significant; gain (B) /
@@ -330,14 +333,20 @@ __device__ __forceinline__ void contract_tuple(const ChanDev& c, const InstDev (
             v[q][j] = pa + pb;
         }
     }
+    // the constant mode as three interleaved FMA chains, summed (a + b) + c:
+    // the same arithmetic as contract_run, so that every schedule gives each
+    // tuple the same values
     double r0[NI];
 #pragma unroll
-    for (int q = 0; q < NI; ++q) r0[q] = 0.0;
+    for (int q = 0; q < NI; ++q) {
+        double ra = 0.0, rb = 0.0, rc = 0.0;
 #pragma unroll
-    for (int j = 0; j < K; ++j) {
-        const double w = M(j);
-#pragma unroll
-        for (int q = 0; q < NI; ++q) r0[q] = fma(w, v[q][j], r0[q]);
+        for (int j = 0; j < K; j += 3) {
+            ra = fma(M(j), v[q][j], ra);
+            rb = fma(M(j + 1), v[q][j + 1], rb);
+            rc = fma(M(j + 2), v[q][j + 2], rc);
+        }
+        r0[q] = (ra + rb) + rc;
     }
 #pragma unroll
     for (int lam = 0; lam < L; ++lam) {
@@ -372,7 +381,9 @@ __device__ __forceinline__ void contract_tuple(const ChanDev& c, const InstDev (
         for (int q = 0; q < NI; ++q) {
             const double amp = in[q].amplitude;
             const int64_t key = in[q].foff[lam] + 3 * (int64_t)e[lam];
-            if (lam < L - 1) {
+            if (fx.w) {   // deterministic mode: exact adds, lane by lane
+                if (valid) fx_add3(fx, key, d * (r0[q] * amp), d * (r1[q] * amp), d * (r2[q] * amp));
+            } else if (lam < L - 1) {
                 warp_scatter3(valid ? key : -1, acc + key, d * (r0[q] * amp), d * (r1[q] * amp), d * (r2[q] * amp));
             } else if (valid) {
                 double* o = acc + key;
@@ -401,7 +412,7 @@ __global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, const InstDe
                                                          const int32_t* __restrict__ tup, int64_t stride, int64_t n,
                                                          const double* __restrict__ f, double* __restrict__ acc,
                                                          const DPCtl* __restrict__ ctl, int* __restrict__ err_flag,
-                                                         int rate_leg) {
+                                                         int rate_leg, FxAcc fx) {
     constexpr uint32_t TILE_BYTES = uint32_t(TBytes<L, KIND>::B) * TT;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char* stage_buf = smem_raw;
@@ -435,7 +446,7 @@ __global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, const InstDe
         if (tile >= ntiles) break;
         const int s = int(it % STAGES);
         const uint32_t parity = uint32_t((it / STAGES) & 1);
-        if (!mbar_wait(&bars[s], parity)) {
+        if (!mbar_wait(&bars[s], parity, c.wait_polls)) {
             // record the failure, then give every copy still in flight a
             // bounded chance to land before the CTA releases its shared memory
             if (tid == 0) atomicExch(err_flag, 1);
@@ -465,11 +476,11 @@ __global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, const InstDe
                 while (k2 < n_insts && !active(insts[k2])) ++k2;
                 if (PAIR && k2 < n_insts) {
                     const InstDev pair[2] = {a, insts[k2]};
-                    contract_tuple<L, KIND, TT, 2, RATE>(c, pair, e, valid, sm, tid, f, acc, rate_leg);
+                    contract_tuple<L, KIND, TT, 2, RATE>(c, pair, e, valid, sm, tid, f, acc, rate_leg, fx);
                     k = k2 + 1;
                 } else {
                     const InstDev one[1] = {a};
-                    contract_tuple<L, KIND, TT, 1, RATE>(c, one, e, valid, sm, tid, f, acc, rate_leg);
+                    contract_tuple<L, KIND, TT, 1, RATE>(c, one, e, valid, sm, tid, f, acc, rate_leg, fx);
                     k = PAIR ? k2 : k + 1;
                 }
             }
@@ -501,6 +512,7 @@ __global__ void __launch_bounds__(TT) k_collision_tensor(ChanDev c, const InstDe
 struct RunsDev {
     double* fT;
     double* accT;
+    FxAcc accTx;   // deterministic mode: accT's exact twin (w null otherwise)
     int64_t loff[TB_MAX_LEGS];
     int64_t ndof[TB_MAX_LEGS];
     int np;
@@ -573,6 +585,50 @@ __global__ void __launch_bounds__(1024) k_runs_scatter(const InstDev* __restrict
                 double* o = acc + s_foff[l][ty] + d;
                 if (DISTINCT) *o += v;
                 else if (v != 0.0) atomicAdd(o, v);
+            }
+        }
+        __syncthreads();   // the tile is reused by the next leg
+    }
+}
+
+// The deterministic mode's scatter: accTx (exact words) into the handle's
+// exact accumulator fx, the same transpose as k_runs_scatter; the adds are
+// integer adds, so neither their order nor DISTINCT changes the result.
+template <bool DISTINCT>
+__global__ void __launch_bounds__(1024) k_runs_scatter_exact(const InstDev* __restrict__ insts, int n_insts,
+                                                             RunsDev R, int nlegs, FxAcc fx) {
+    __shared__ Fx tile[32][33];
+    __shared__ int64_t s_foff[TB_MAX_LEGS][32];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int64_t d0 = int64_t(blockIdx.x) * 32;
+    const int i0 = blockIdx.y * 32;
+    if (ty < nlegs) s_foff[ty][tx] = (i0 + tx < n_insts) ? insts[i0 + tx].foff[ty] : 0;
+    for (int l = 0; l < nlegs; ++l) {
+        const int64_t ndof = leg_pick(R.ndof, l), loff = leg_pick(R.loff, l);
+        if (d0 >= ndof) continue;   // uniform in the block
+        {
+            const int64_t d = d0 + ty;
+            Fx v{0ull, 0ull, 0ull};
+            if (d < ndof) {
+                unsigned long long* p = R.accTx.w + 3 * (loff + d * R.np + i0 + tx);
+                v.w0 = p[0];
+                v.w1 = p[1];
+                v.w2 = p[2];
+                if (v.w0 | v.w1 | v.w2) { p[0] = 0ull; p[1] = 0ull; p[2] = 0ull; }
+            }
+            tile[ty][tx] = v;
+        }
+        __syncthreads();   // also publishes s_foff on the first leg
+        {
+            const int i = i0 + ty;
+            const int64_t d = d0 + tx;
+            if (i < n_insts && d < ndof) {
+                const Fx v = tile[tx][ty];
+                if (v.w0 | v.w1 | v.w2) {
+                    unsigned long long* o = fx.w + 3 * (s_foff[l][ty] + d);
+                    if (DISTINCT) fx_add_plain(o, v);
+                    else fx_atomic_add(o, v);
+                }
             }
         }
         __syncthreads();   // the tile is reused by the next leg
@@ -653,10 +709,17 @@ __device__ __forceinline__ void contract_run(const ChanDev& c, const RunsDev& R,
 #pragma unroll
         for (int lam = 0; lam < L; ++lam) {
             const double da = c.leg[lam].dir * amp;   // d = +-1: d (r amp) == r (d amp)
-            double* o = R.accT + R.loff[lam] + int64_t(3 * e[lam]) * R.np + i;
-            atomicAdd(o, r0 * da);
-            atomicAdd(o + R.np, r1[lam] * da);
-            atomicAdd(o + 2 * R.np, r2[lam] * da);
+            const int64_t slot = R.loff[lam] + int64_t(3 * e[lam]) * R.np + i;
+            if (R.accTx.w) {   // deterministic mode: exact adds
+                fx_add(R.accTx, slot, r0 * da);
+                fx_add(R.accTx, slot + R.np, r1[lam] * da);
+                fx_add(R.accTx, slot + 2 * R.np, r2[lam] * da);
+            } else {
+                double* o = R.accT + slot;
+                atomicAdd(o, r0 * da);
+                atomicAdd(o + R.np, r1[lam] * da);
+                atomicAdd(o + 2 * R.np, r2[lam] * da);
+            }
         }
     }
 }
@@ -729,7 +792,7 @@ __global__ void __launch_bounds__(RUNS_THREADS) k_collision_runs(ChanDev c, cons
         if (tile >= ntiles) break;
         const int s = int(it % STAGES);
         const uint32_t parity = uint32_t((it / STAGES) & 1);
-        if (!mbar_wait(&bars[s], parity)) {
+        if (!mbar_wait(&bars[s], parity, c.wait_polls)) {
             if (tid == 0) atomicExch(err_flag, 1);
             for (int k = 0; k < STAGES; ++k) {
                 const int64_t itk = it + ((k - s + STAGES) % STAGES);
@@ -858,11 +921,8 @@ int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n
     return TB_ERR_ARG;
 }
 
-// The bulk-copy wait error flag of each device (allocated on first use on
-// that device, with it current), and the kernels' large-shared-memory
-// attribute, which is also set per device.
+// The kernels' large-shared-memory attribute, set once per device.
 constexpr int TB_MAX_DEVICES = 64;
-static int* g_err_flag[TB_MAX_DEVICES] = {};
 
 static int current_device() {
     int dev = 0;
@@ -870,14 +930,11 @@ static int current_device() {
     return dev;
 }
 
-static int ensure_err_flag(int** flag) {
-    const int dev = current_device();
-    if (dev < 0 || dev >= TB_MAX_DEVICES) { set_error("device ordinal beyond the library's table"); return TB_ERR_ARG; }
-    if (!g_err_flag[dev]) {
-        TB_CUDA(cudaMalloc(&g_err_flag[dev], sizeof(int)));
-        TB_CUDA(cudaMemset(g_err_flag[dev], 0, sizeof(int)));
-    }
-    *flag = g_err_flag[dev];
+// The handle's bounded-wait flag (ChanDev::err_flag), which every
+// contraction launch needs.
+static int channel_err_flag(const ChanDev& c, int** flag) {
+    if (!c.err_flag) { set_error("channel without its wait-timeout flag"); return TB_ERR_ARG; }
+    *flag = c.err_flag;
     return TB_OK;
 }
 
@@ -891,10 +948,14 @@ static int ensure_smem_attr(K kern, int bytes, unsigned long long& done_devices)
     return TB_OK;
 }
 
-static RunsDev runs_dev(const ChanDev& c, const MomentTensor& T) {
+static RunsDev runs_dev(const ChanDev& c, const MomentTensor& T, const FxAcc& fx) {
     RunsDev R{};
     R.fT = T.fT;
     R.accT = T.accT;
+    if (fx.w) {
+        R.accTx.w = T.accTx;
+        R.accTx.poison = fx.poison;
+    }
     R.np = T.np;
     for (int l = 0; l < TB_MAX_LEGS; ++l) {
         R.loff[l] = T.loff[l];
@@ -906,9 +967,11 @@ static RunsDev runs_dev(const ChanDev& c, const MomentTensor& T) {
 // gather -> run-minor contraction -> scatter (three launches on s)
 template <int L, int KIND, int STAGES, int S>
 static int launch_runs(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T, const int32_t* tup,
-                       int64_t stride, int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s) {
+                       int64_t stride, int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s,
+                       const FxAcc& fx) {
     constexpr int TT = TTile<L, KIND>::TT;
-    const RunsDev R = runs_dev(c, T);
+    if (fx.w && !T.accTx) { set_error("run-minor contraction without its exact accumulator"); return TB_ERR_ARG; }
+    const RunsDev R = runs_dev(c, T, fx);
     int64_t maxd = 0;
     for (int l = 0; l < L; ++l) maxd = std::max(maxd, R.ndof[l]);
     const dim3 tb(32, 8), tg(unsigned((maxd + 31) / 32), unsigned(T.np / 32), unsigned(L));
@@ -921,7 +984,7 @@ static int launch_runs(const ChanDev& c, const InstDev* insts, int n_insts, cons
     static unsigned long long attr_devices = 0;
     TB_TRY(ensure_smem_attr(kern, int(fixed + sizeof(double) * RUNS_NP_MAX), attr_devices));
     int* err_flag = nullptr;
-    TB_TRY(ensure_err_flag(&err_flag));
+    TB_TRY(channel_err_flag(c, &err_flag));
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -936,13 +999,19 @@ static int launch_runs(const ChanDev& c, const InstDev* insts, int n_insts, cons
         TB_CUDA(cudaGetLastError());
     }
     const dim3 sg(tg.x, tg.y, 1), sb(32, 32);
-    if (T.runs_distinct) k_runs_scatter<true><<<sg, sb, 0, s>>>(insts, n_insts, R, L, acc);
-    else k_runs_scatter<false><<<sg, sb, 0, s>>>(insts, n_insts, R, L, acc);
+    if (fx.w) {
+        if (T.runs_distinct) k_runs_scatter_exact<true><<<sg, sb, 0, s>>>(insts, n_insts, R, L, fx);
+        else k_runs_scatter_exact<false><<<sg, sb, 0, s>>>(insts, n_insts, R, L, fx);
+    } else if (T.runs_distinct) {
+        k_runs_scatter<true><<<sg, sb, 0, s>>>(insts, n_insts, R, L, acc);
+    } else {
+        k_runs_scatter<false><<<sg, sb, 0, s>>>(insts, n_insts, R, L, acc);
+    }
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }
 
-int prepare_runs(const ChanDev& c, int n_insts, bool distinct_runs, MomentTensor& T, cudaStream_t s) {
+int prepare_runs(const ChanDev& c, int n_insts, bool distinct_runs, MomentTensor& T, cudaStream_t s, bool exact) {
     if (c.L > 3 || n_insts < RUNS_MIN || T.fT || !T.d) return TB_OK;
     const int np = (n_insts + 31) & ~31;
     if (np > RUNS_NP_MAX) return TB_OK;
@@ -964,6 +1033,18 @@ int prepare_runs(const ChanDev& c, int n_insts, bool distinct_runs, MomentTensor
         T.accT = nullptr;
         return TB_OK;
     }
+    if (exact) {
+        if (cudaMalloc(&T.accTx, 3 * bytes) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(T.fT);
+            cudaFree(T.accT);
+            T.fT = nullptr;
+            T.accT = nullptr;
+            T.accTx = nullptr;
+            return TB_OK;
+        }
+        TB_CUDA(cudaMemsetAsync(T.accTx, 0, 3 * bytes, s));
+    }
     TB_CUDA(cudaMemsetAsync(T.accT, 0, bytes, s));
     T.np = np;
     T.runs_distinct = distinct_runs ? 1 : 0;
@@ -974,14 +1055,14 @@ int prepare_runs(const ChanDev& c, int n_insts, bool distinct_runs, MomentTensor
 template <int L, int KIND, int STAGES, bool PAIR, bool RATE = false>
 static int launch_variant(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T,
                           const int32_t* tup, int64_t stride, int64_t n, const double* f, double* acc,
-                          const DPCtl* ctl, cudaStream_t s, int rate_leg) {
+                          const DPCtl* ctl, cudaStream_t s, int rate_leg, const FxAcc& fx) {
     constexpr int TT = TTile<L, KIND>::TT;
     auto kern = k_collision_tensor<L, KIND, TT, STAGES, PAIR, RATE>;
     const size_t smem = size_t(STAGES) * TT * tuple_bytes(L, KIND);
     static unsigned long long attr_devices = 0;
     TB_TRY(ensure_smem_attr(kern, int(smem), attr_devices));
     int* err_flag = nullptr;
-    TB_TRY(ensure_err_flag(&err_flag));
+    TB_TRY(channel_err_flag(c, &err_flag));
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -992,7 +1073,7 @@ static int launch_variant(const ChanDev& c, const InstDev* insts, int n_insts, c
     if (grid > T.ntiles) grid = T.ntiles;
     if (grid < 1) return TB_OK;
     kern<<<unsigned(grid), TT, smem, s>>>(c, insts, n_insts, static_cast<const unsigned char*>(T.d), T.ntiles, tup,
-                                          stride, n, f, acc, ctl, err_flag, rate_leg);
+                                          stride, n, f, acc, ctl, err_flag, rate_leg, fx);
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }
@@ -1003,12 +1084,15 @@ static int launch_variant(const ChanDev& c, const InstDev* insts, int n_insts, c
 template <int L, int KIND>
 static int launch_t(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T, const int32_t* tup,
                     int64_t stride, int64_t n, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s,
-                    int rate_leg) {
+                    int rate_leg, const FxAcc& fx) {
+#define TB_VARIANT(ST, PR, RT) \
+    launch_variant<L, KIND, ST, PR, RT>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg, fx)
     if (rate_leg >= 0)   // diagnostic operator: one fixed schedule
-        return launch_variant<L, KIND, 2, false, true>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        return TB_VARIANT(2, false, true);
     if constexpr (L <= 3) {
-        if (T.runs && T.fT) {
-#define TB_RUNS(ST, SS) launch_runs<L, KIND, ST, SS>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s)
+        // the run-minor path needs its exact twin in the deterministic mode
+        if (T.runs && T.fT && (!fx.w || T.accTx)) {
+#define TB_RUNS(ST, SS) launch_runs<L, KIND, ST, SS>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, fx)
             if (T.stages == 1)
                 return T.runs == 4 ? TB_RUNS(1, 4) : T.runs == 8 ? TB_RUNS(1, 8) : T.runs == 16 ? TB_RUNS(1, 16)
                                                                                  : TB_RUNS(1, 32);
@@ -1018,32 +1102,31 @@ static int launch_t(const ChanDev& c, const InstDev* insts, int n_insts, const M
         }
     }
     const bool pair = (L <= 3) && n_insts > 1 && T.pair;
-    if (T.stages == 1) {
-        return pair ? launch_variant<L, KIND, 1, (L <= 3)>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg)
-                    : launch_variant<L, KIND, 1, false>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-    }
-    return pair ? launch_variant<L, KIND, 2, (L <= 3)>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg)
-                : launch_variant<L, KIND, 2, false>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+    if (T.stages == 1) return pair ? TB_VARIANT(1, (L <= 3), false) : TB_VARIANT(1, false, false);
+    return pair ? TB_VARIANT(2, (L <= 3), false) : TB_VARIANT(2, false, false);
+#undef TB_VARIANT
 }
 
 int launch_collision_tensor(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T,
                             const int32_t* tup, int64_t stride, int64_t n, const double* f, double* acc,
-                            const DPCtl* ctl, cudaStream_t s, int rate_leg) {
+                            const DPCtl* ctl, cudaStream_t s, int rate_leg, const FxAcc& fx) {
     if (n <= 0 || n_insts <= 0) return TB_OK;
+#define TB_LT(LL, KK) launch_t<LL, KK>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg, fx)
     switch (c.L * 4 + T.kind) {
-        case 8: return launch_t<2, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 9: return launch_t<2, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 10: return launch_t<2, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 11: return launch_t<2, TK_F48>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 12: return launch_t<3, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 13: return launch_t<3, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 14: return launch_t<3, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 15: return launch_t<3, TK_F48>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 16: return launch_t<4, TK_F64>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 17: return launch_t<4, TK_F32>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 18: return launch_t<4, TK_F40>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
-        case 19: return launch_t<4, TK_F48>(c, insts, n_insts, T, tup, stride, n, f, acc, ctl, s, rate_leg);
+        case 8: return TB_LT(2, TK_F64);
+        case 9: return TB_LT(2, TK_F32);
+        case 10: return TB_LT(2, TK_F40);
+        case 11: return TB_LT(2, TK_F48);
+        case 12: return TB_LT(3, TK_F64);
+        case 13: return TB_LT(3, TK_F32);
+        case 14: return TB_LT(3, TK_F40);
+        case 15: return TB_LT(3, TK_F48);
+        case 16: return TB_LT(4, TK_F64);
+        case 17: return TB_LT(4, TK_F32);
+        case 18: return TB_LT(4, TK_F40);
+        case 19: return TB_LT(4, TK_F48);
     }
+#undef TB_LT
     set_error("nlegs must be 2..4");
     return TB_ERR_ARG;
 }
@@ -1108,10 +1191,12 @@ int tune_tensor(const ChanDev& c, const InstDev* insts, int n_insts, MomentTenso
     return TB_OK;
 }
 
-int tensor_error_flag(int* value) {
-    const int dev = current_device();
-    if (dev < 0 || dev >= TB_MAX_DEVICES || !g_err_flag[dev]) { *value = 0; return TB_OK; }
-    TB_CUDA(cudaMemcpy(value, g_err_flag[dev], sizeof(int), cudaMemcpyDeviceToHost));
+int take_wait_timeout(int* flag, cudaStream_t s, int* value) {
+    *value = 0;
+    if (!flag) return TB_OK;
+    TB_CUDA(cudaMemcpyAsync(value, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TB_CUDA(cudaStreamSynchronize(s));
+    if (*value) TB_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));
     return TB_OK;
 }
 

@@ -27,6 +27,8 @@ struct MomentTensor {
     int runs_distinct = 0;        // every instance belongs to another run
     double* fT = nullptr;         // [leg][3 ne_leg][np]: the legs' f, run-minor
     double* accT = nullptr;       // same shape; all zero between launches
+    unsigned long long* accTx = nullptr;   // deterministic mode: accT's exact twin
+                                           // (3 words per slot, tb_exact.cuh); zero between launches
     int64_t loff[4] = {0, 0, 0, 0};
     void release();
 };
@@ -40,15 +42,18 @@ int build_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n
 // schedule and run-minor buffers), e.g. after the channel's per-tuple
 // amplitudes (ChanDev::tamp) changed.
 int refill_tensor(const ChanDev& c, const int32_t* tup, int64_t stride, int64_t n, MomentTensor& T, cudaStream_t s);
-// rate_leg >= 0: scattering rate of that leg instead (see launch_collision_mc)
+// rate_leg >= 0: scattering rate of that leg instead (see launch_collision_mc);
+// fx.w non-null: deterministic mode, the results go to fx instead of acc
 int launch_collision_tensor(const ChanDev& c, const InstDev* insts, int n_insts, const MomentTensor& T,
                             const int32_t* tup, int64_t stride, int64_t n, const double* f, double* acc,
-                            const DPCtl* ctl, cudaStream_t s, int rate_leg = -1);
+                            const DPCtl* ctl, cudaStream_t s, int rate_leg = -1, const FxAcc& fx = FxAcc{});
 
 // Buffers of the run-minor contraction for a group of n_insts instances
 // (legs <= 3, 8 <= n_insts <= 1024); sets runs = 8 from 16 instances on.
+// exact: also the fixed-point twin of the accumulator (deterministic mode).
 // Does nothing for other groups, or when the device memory is short.
-int prepare_runs(const ChanDev& c, int n_insts, bool distinct_runs, MomentTensor& T, cudaStream_t s);
+int prepare_runs(const ChanDev& c, int n_insts, bool distinct_runs, MomentTensor& T, cudaStream_t s,
+                 bool exact = false);
 
 // Autotuner: times the contraction of one group for every schedule
 // (stages 1 / 2, instance pairs off / on where several instances exist, the
@@ -59,7 +64,9 @@ int prepare_runs(const ChanDev& c, int n_insts, bool distinct_runs, MomentTensor
 int tune_tensor(const ChanDev& c, const InstDev* insts, int n_insts, MomentTensor& T, const int32_t* tup,
                 int64_t stride, int64_t n, const double* f, double* acc, cudaStream_t s);
 
-// 1 once a bulk-copy wait of the contraction kernel ran out (then TB_ERR_TIMEOUT)
-int tensor_error_flag(int* value);
+// *value = 1 when a bounded wait of a contraction kernel ran out since the
+// last call (the handle's flag, ChanDev::err_flag; then TB_ERR_TIMEOUT), and
+// the flag is cleared.  Waits for s (the stream the kernels ran on).
+int take_wait_timeout(int* flag, cudaStream_t s, int* value);
 
 }  // namespace tb

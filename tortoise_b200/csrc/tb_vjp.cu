@@ -24,10 +24,16 @@ template <int L> struct VDim {
     static constexpr int NMOM = K * (1 + L);
 };
 
-__device__ __forceinline__ void block_atomic_sum(double v, double* dst) {
+// Sum over the warp, then one add per warp into dst (exact into slot k of
+// fx in the deterministic mode; the warp's own sum runs in a fixed order over
+// a launch geometry that depends on the tuple count alone).
+__device__ __forceinline__ void block_atomic_sum(double v, double* dst, const FxAcc& fx, int k) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(dst, v);
+    if ((threadIdx.x & 31) == 0 && v != 0.0) {
+        if (fx.w) fx_add(fx, k, v);
+        else atomicAdd(dst, v);
+    }
 }
 
 // ---------------------------------------------------------------- M^-T
@@ -96,7 +102,8 @@ __global__ void __launch_bounds__(128) k_vjp_mc(ChanDev c, const InstDev* __rest
                                                 const int32_t* __restrict__ tup, int64_t stride, int64_t n,
                                                 const uint64_t* __restrict__ mask, const int32_t* __restrict__ perm,
                                                 const double* __restrict__ f, const double* __restrict__ u,
-                                                double* __restrict__ grad_f, double* __restrict__ grad_amp) {
+                                                double* __restrict__ grad_f, double* __restrict__ grad_amp, FxAcc fx,
+                                                FxAcc fx_amp) {
     extern __shared__ double s_mc[];
     constexpr int R = 2 * (L - 2) + 1;
     for (int i = threadIdx.x; i < c.nmc * R; i += blockDim.x) s_mc[i] = c.mc[i];
@@ -169,12 +176,17 @@ __global__ void __launch_bounds__(128) k_vjp_mc(ChanDev c, const InstDev* __rest
                 const double sc = scale * (in.amp_full * tf);
 #pragma unroll
                 for (int l = 0; l < L; ++l) {
-                    double* o = grad_f + in.foff[l] + 3 * (int64_t)e[l];
+                    const int64_t key = in.foff[l] + 3 * (int64_t)e[l];
+                    double* o = grad_f + key;
 #pragma unroll
-                    for (int j = 0; j < 3; ++j) atomicAdd(o + j, sc * (sa[l] * gA[l][j] + sb[l] * gB[l][j]));
+                    for (int j = 0; j < 3; ++j) {
+                        const double g = sc * (sa[l] * gA[l][j] + sb[l] * gB[l][j]);
+                        if (fx.w) fx_add(fx, key + j, g);
+                        else atomicAdd(o + j, g);
+                    }
                 }
             }
-            block_atomic_sum(valid ? scale * (c.amp_vol * tf) * gamp : 0.0, grad_amp + k);
+            block_atomic_sum(valid ? scale * (c.amp_vol * tf) * gamp : 0.0, grad_amp + k, fx_amp, k);
         }
     }
 }
@@ -235,7 +247,7 @@ __global__ void __launch_bounds__(128) k_vjp_tensor(ChanDev c, const InstDev* __
                                                     const void* __restrict__ mom, int TT, const int32_t* __restrict__ tup,
                                                     int64_t stride, int64_t n, const double* __restrict__ f,
                                                     const double* __restrict__ u, double* __restrict__ grad_f,
-                                                    double* __restrict__ grad_amp) {
+                                                    double* __restrict__ grad_amp, FxAcc fx, FxAcc fx_amp) {
     constexpr int K = VDim<L>::K, KM = VDim<L>::KM, NMOM = VDim<L>::NMOM;
     for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = base + threadIdx.x;
@@ -314,7 +326,9 @@ __global__ void __launch_bounds__(128) k_vjp_tensor(ChanDev c, const InstDev* __
                 const double g0 = in.amplitude * (sa[l] * gA[l][0] + sb[l] * gB[l][0]);
                 const double g1 = in.amplitude * (sa[l] * gA[l][1] + sb[l] * gB[l][1]);
                 const double g2 = in.amplitude * (sa[l] * gA[l][2] + sb[l] * gB[l][2]);
-                if (l < L - 1) {
+                if (fx.w) {   // deterministic mode: exact adds, lane by lane
+                    if (valid) fx_add3(fx, key, g0, g1, g2);
+                } else if (l < L - 1) {
                     warp_scatter3(valid ? key : -1, grad_f + (valid ? key : 0), g0, g1, g2);
                 } else if (valid) {
                     atomicAdd(grad_f + key, g0);
@@ -322,7 +336,7 @@ __global__ void __launch_bounds__(128) k_vjp_tensor(ChanDev c, const InstDev* __
                     atomicAdd(grad_f + key + 2, g2);
                 }
             }
-            block_atomic_sum(valid ? gamp : 0.0, grad_amp + k);
+            block_atomic_sum(valid ? gamp : 0.0, grad_amp + k, fx_amp, k);
         }
     }
 }
@@ -330,7 +344,7 @@ __global__ void __launch_bounds__(128) k_vjp_tensor(ChanDev c, const InstDev* __
 int launch_collision_vjp(const ChanDev& c, const InstDev* insts, int n_insts, int layout, const MomentTensor& T,
                          const int32_t* tup, int64_t stride, int64_t n, const double* f, const double* u,
                          double* grad_f, double* grad_amp, cudaStream_t s, const uint64_t* mask,
-                         const int32_t* perm) {
+                         const int32_t* perm, const FxAcc& fx, const FxAcc& fx_amp) {
     if (n <= 0 || n_insts <= 0) return TB_OK;
     const int threads = 128;
     int64_t blocks = (n + threads - 1) / threads;
@@ -338,7 +352,8 @@ int launch_collision_vjp(const ChanDev& c, const InstDev* insts, int n_insts, in
     if (layout == TB_LAYOUT_MC64) {
         const size_t smem = sizeof(double) * size_t(c.nmc) * c.R;
 #define TB_VJP_MC(LL, LS) k_vjp_mc<LL, LS><<<unsigned(blocks), threads, smem, s>>>(c, insts, n_insts, tup, stride, n, \
-                                                                                 mask, perm, f, u, grad_f, grad_amp)
+                                                                                 mask, perm, f, u, grad_f, grad_amp, \
+                                                                                 fx, fx_amp)
         const bool list = mask != nullptr;
         switch (c.L) {
             case 2: if (list) TB_VJP_MC(2, true); else TB_VJP_MC(2, false); break;
@@ -349,7 +364,8 @@ int launch_collision_vjp(const ChanDev& c, const InstDev* insts, int n_insts, in
     } else {
         const int TT = tile_tuples(c.L, T.kind);
 #define TB_VJP_T(LL, KK) k_vjp_tensor<LL, KK><<<unsigned(blocks), threads, 0, s>>>(c, insts, n_insts, T.d, TT, tup, \
-                                                                                 stride, n, f, u, grad_f, grad_amp)
+                                                                                 stride, n, f, u, grad_f, grad_amp, \
+                                                                                 fx, fx_amp)
         switch (c.L * 4 + T.kind) {
             case 8: TB_VJP_T(2, TK_F64); break;
             case 9: TB_VJP_T(2, TK_F32); break;
@@ -417,7 +433,8 @@ __device__ __forceinline__ void side_pt(int side, int q, double& x, double& y) {
     else { x = g; y = 0.; }
 }
 
-__global__ void __launch_bounds__(256) k_drift_vjp(ElemDev ed, const double* __restrict__ u, double* __restrict__ grad_f) {
+__global__ void __launch_bounds__(256) k_drift_vjp(ElemDev ed, const double* __restrict__ u, double* __restrict__ grad_f,
+                                                   FxAcc fx) {
     const int band = ed.blk_band[blockIdx.x];
     const BandDev& bd = ed.bands[band];
     const double vel0 = bd.vel[0], vel1 = bd.vel[1];
@@ -451,9 +468,13 @@ __global__ void __launch_bounds__(256) k_drift_vjp(ElemDev ed, const double* __r
     for (int b = 0; b < 3; ++b) coef += ue[b] * (m.vol * vel0 * dx[b] + m.vol * vel1 * dy[b]);
     // d/dc_j of sum_q w f(q) with f(q) = c0 + c1 x_q + c2 y_q
     const double w = TB_GW2, ga = TB_GP2_A, gbb = TB_GP2_B;
-    atomicAdd(gb + 3 * e + 0, coef * (3.0 * w));
-    atomicAdd(gb + 3 * e + 1, coef * (w * (ga + gbb + ga)));
-    atomicAdd(gb + 3 * e + 2, coef * (w * (ga + ga + gbb)));
+    auto add = [&](int64_t el, int j, double v) {
+        if (fx.w) fx_add(fx, bd.off + 3 * el + j, v);
+        else atomicAdd(gb + 3 * el + j, v);
+    };
+    add(e, 0, coef * (3.0 * w));
+    add(e, 1, coef * (w * (ga + gbb + ga)));
+    add(e, 2, coef * (w * (ga + ga + gbb)));
     // surface: out[e,b] -= s * area * sum_q 0.5 phi_b(pt(side,q)) f_ei(pt(si,q))
 #pragma unroll
     for (int side = 0; side < 3; ++side) {
@@ -475,12 +496,12 @@ __global__ void __launch_bounds__(256) k_drift_vjp(ElemDev ed, const double* __r
             g3[0] += wq; g3[1] += wq * xi; g3[2] += wq * yi;
         }
 #pragma unroll
-        for (int j = 0; j < 3; ++j) atomicAdd(gb + 3 * ei + j, g3[j]);
+        for (int j = 0; j < 3; ++j) add(ei, j, g3[j]);
     }
 }
 
-int launch_drift_vjp(const ElemDev& ed, const double* u, double* grad_f, cudaStream_t s) {
-    k_drift_vjp<<<ed.nblk, 256, 0, s>>>(ed, u, grad_f);
+int launch_drift_vjp(const ElemDev& ed, const double* u, double* grad_f, cudaStream_t s, const FxAcc& fx) {
+    k_drift_vjp<<<ed.nblk, 256, 0, s>>>(ed, u, grad_f, fx);
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }

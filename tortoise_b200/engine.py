@@ -30,7 +30,7 @@ class TortoiseError(RuntimeError):
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("layout", C.c_int32), ("allow_fp32", C.c_int32),
                 ("tensor_budget_bytes", C.c_int64), ("verbose", C.c_int32), ("autotune", C.c_int32),
-                ("shard_rank", C.c_int32), ("shard_count", C.c_int32)]
+                ("shard_rank", C.c_int32), ("shard_count", C.c_int32), ("deterministic", C.c_int32)]
 
 
 class DP45Stats(C.Structure):
@@ -82,6 +82,7 @@ def lib():
         L.tb_dp45_poll.argtypes = [vp, C.POINTER(DP45Stats)]
         L.tb_dp45_end.argtypes = [vp, vp, vp, vp, i64, C.POINTER(DP45Stats), C.c_int]
         L.tb_synchronize.argtypes = [vp]
+        L.tb_set_copy_wait_limit.argtypes = [vp, i64]
         L.tb_get_stream.restype = vp
         L.tb_get_stream.argtypes = [vp]
         L.tb_collision_accumulate.argtypes = [vp, C.c_int, vp, vp]
@@ -175,13 +176,17 @@ class Engine:
 
     shard=(rank, count): this process keeps the rank-th part of every tuple
     list (one GPU per rank); connect the ranks with ``shard_connect`` (or
-    tortoise_b200.shard.connect) so that collision sums are all-reduced."""
+    tortoise_b200.shard.connect) so that collision sums are all-reduced.
+
+    deterministic=True: bit-reproducible sums (tb_options.deterministic):
+    exact fixed-point accumulation instead of FP64 atomics."""
 
     def __init__(self, material, layout=LAYOUT_AUTO, allow_fp32=False, device=0, tensor_budget_bytes=0,
-                 autotune=False, shard=None):
+                 autotune=False, shard=None, deterministic=False):
         self.material = material
         self.packed = material.pack()
-        opts = Options(device, layout, int(allow_fp32), tensor_budget_bytes, 0, int(autotune), *_shard_opts(shard))
+        opts = Options(device, layout, int(allow_fp32), tensor_budget_bytes, 0, int(autotune), *_shard_opts(shard),
+                       int(bool(deterministic)))
         h = C.c_void_p()
         _check(lib().tb_create(C.byref(h), C.addressof(self.packed.desc), C.byref(opts)), "tb_create")
         self.h = h
@@ -319,6 +324,11 @@ class Engine:
     def set_amplitude(self, ch, a):
         _check(lib().tb_set_amplitude(self.h, ch, float(a)), "tb_set_amplitude")
 
+    def set_copy_wait_limit(self, polls):
+        """Poll limit of the contraction kernels' wait for staged moment tiles
+        (tb_set_copy_wait_limit; 0 gives up at once)."""
+        _check(lib().tb_set_copy_wait_limit(self.h, int(polls)), "tb_set_copy_wait_limit")
+
     # -- host-pointer calls ----------------------------------------------
     def rhs(self, f, drift=True, collisions=True):
         f = np.ascontiguousarray(f, dtype=np.float64)
@@ -455,12 +465,13 @@ class BatchEngine(Engine):
     size.  Channels and bands are numbered globally in run order."""
 
     def __init__(self, materials, layout=LAYOUT_AUTO, allow_fp32=False, device=0, tensor_budget_bytes=0,
-                 autotune=False, shard=None):
+                 autotune=False, shard=None, deterministic=False):
         self.materials = list(materials)
         self.material = self.materials[0]
         self.packs = [m.pack() for m in self.materials]
         arr = (C.c_void_p * len(self.packs))(*[C.addressof(p.desc) for p in self.packs])
-        opts = Options(device, layout, int(allow_fp32), tensor_budget_bytes, 0, int(autotune), *_shard_opts(shard))
+        opts = Options(device, layout, int(allow_fp32), tensor_budget_bytes, 0, int(autotune), *_shard_opts(shard),
+                       int(bool(deterministic)))
         h = C.c_void_p()
         _check(lib().tb_create_batch(C.byref(h), arr, len(self.packs), C.byref(opts)), "tb_create_batch")
         self.h = h
