@@ -140,6 +140,8 @@ typedef struct tb_handle tb_handle;
 #define TB_LAYOUT_T32    3  /* precomputed moment tensor, FP32 storage, FP64 accumulate */
 #define TB_LAYOUT_T40    4  /* moment tensor, upper 40 bits of FP64 (5 B, 2^-29 relative), FP64 accumulate */
 #define TB_LAYOUT_T48    5  /* moment tensor, upper 48 bits of FP64 (6 B, 2^-37 relative), FP64 accumulate */
+#define TB_LAYOUT_STREAM 6  /* Monte-Carlo quadrature over the points inside the simplices with the tuples
+                               enumerated again in every evaluation: no stored list (tb_options.stream_legs) */
 
 typedef struct tb_options {
     int32_t device;               /* CUDA device ordinal                            */
@@ -161,6 +163,16 @@ typedef struct tb_options {
                                      a run-minor group's accumulator).  The reference's TBB
                                      reduce (ScatteringChannel.cpp:651-670) is itself not
                                      reproducible across thread schedules. */
+    int32_t stream_legs;          /* 2..4: every channel with at least this many legs whose tuples the
+                                     library enumerates (n_tuples == 0) keeps no tuple list: each
+                                     evaluation walks the candidates of precalculateIndices
+                                     (ScatteringChannel.hpp:205-255, ScatteringChannel.cpp:476-504) on
+                                     the device again and integrates the survivors on the spot
+                                     (TB_LAYOUT_STREAM), for lists too large for device memory (four-leg
+                                     e-e on fine meshes).  Same per-tuple sums as the stored list.  Such
+                                     channels have no tuple list to read or save, take no functAmplitude
+                                     and no adjoint; tb_channel_info reports the counts of their last
+                                     evaluation.  0: every list is stored. */
 } tb_options;
 
 /* Pointer flags */
@@ -454,6 +466,14 @@ int tb_dp45_replay(tb_handle* h, const double* f0, const double* dts, int64_t n_
 int tb_band_relative_error_noalloc(const double* err, const double* pop, int64_t n_elements, double elem_volume,
                                    double statistics, double rel_tol, double abs_tol, double penalisation,
                                    double* result, void* stream);
+
+/* The device's FP64 fused multiply-add throughput in FMAs per second,
+ * measured by a register-resident kernel (8 independent FMA chains per
+ * thread, 8 blocks of 256 threads per SM) timed with CUDA events: the
+ * roofline denominator of the FP64-bound kernels (the run-minor batched
+ * contraction, the Monte-Carlo quadrature).  Takes a fraction of a second.
+ * No counterpart in the reference. */
+int tb_fp64_fma_rate(int device, double* fma_per_second);
 
 /* ---------------------------------------------- tuple sharding across GPUs
  * One run split over shard_count processes, one GPU each: the process with

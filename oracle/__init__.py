@@ -40,6 +40,7 @@ def lib():
         L.or_points_inside.argtypes = [vp, C.c_int, C.POINTER(i64), C.POINTER(i64), ip]
         L.or_get_tuples.argtypes = [vp, C.c_int, ip, ip]
         L.or_set_tuples.argtypes = [vp, C.c_int, i64, ip, ip]
+        L.or_enumerate_items.argtypes = [vp, C.c_int, i64, i64, C.c_int]
         L.or_set_amplitude.argtypes = [vp, C.c_int, C.c_double]
         L.or_channel_propagate.argtypes = [vp, C.c_int, dp, dp, i64, i64, C.c_int, C.c_int]
         L.or_rhs.argtypes = [vp, dp, dp, C.c_int, C.c_int]
@@ -155,6 +156,12 @@ class Oracle:
         ids = np.ascontiguousarray(ids, dtype=np.int32)
         umk = np.ascontiguousarray(umk, dtype=np.int32)
         lib().or_set_tuples(self.h, ch, umk.size, _ip(ids), _ip(umk))
+
+    def enumerate_items(self, ch, item0, item1):
+        """Channel ch's list becomes the tuples of work items [item0, item1):
+        (umklapp, sections of legs 0..L-2, element choice of those legs) in
+        the reference's loop order, the item index of the device's walk."""
+        lib().or_enumerate_items(self.h, int(ch), int(item0), int(item1), self.nthreads)
 
     def set_amplitude(self, ch, a):
         lib().or_set_amplitude(self.h, ch, float(a))

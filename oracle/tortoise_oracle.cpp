@@ -434,6 +434,70 @@ static void enumerate_range(const Problem& P, const Channel& c, int u, int s0_be
     }
 }
 
+// The same loops indexed by work item: item = (((u nsec0 + s0) nsec1 + s1)
+// nsec2 + s2) 2^(L-1) + comb, i.e. the position of (umklapp, sections of
+// legs 0..L-2, element choice of those legs) in the reference's loop order
+// (comb innermost, because the element loops of legs 0..L-2 run inside the
+// section loops; ScatteringChannel.hpp:216-255).  Enumerates items
+// [item0, item1) in order: a contiguous piece of the full list.
+static void enumerate_items(const Problem& P, const Channel& c, int64_t item0, int64_t item1, EnumPart& out) {
+    const int L = c.L;
+    const Mesh* ms[4];
+    const Band* bs[4];
+    for (int l = 0; l < L; ++l) { bs[l] = &P.bands[c.band[l]]; ms[l] = &P.meshes[bs[l]->mesh]; }
+    const double* G = P.region.gvec;
+    int64_t nsec[3] = {1, 1, 1};
+    for (int l = 0; l < L - 1; ++l) nsec[l] = int64_t(ms[l]->nx) * ms[l]->ny;
+    const int ncomb = 1 << (L - 1);
+    int32_t e[4];
+    for (int64_t item = item0; item < item1; ++item) {
+        const int comb = int(item % ncomb);
+        int64_t r = item / ncomb;
+        int sec[3] = {0, 0, 0};
+        for (int l = L - 2; l >= 0; --l) { sec[l] = int(r % nsec[l]); r /= nsec[l]; }
+        const int u = int(r);
+        const double ux = c.umk[2 * u], uy = c.umk[2 * u + 1];
+        const double gu[2] = {G[0] * ux + G[2] * uy, G[1] * ux + G[3] * uy};
+        Box acc{};
+        for (int l = 0; l < L - 1; ++l) {
+            Box b = box_scale(section_box(*ms[l], sec[l] % ms[l]->nx, sec[l] / ms[l]->nx), double(c.dir[l]));
+            if (l == 0) acc = b;
+            else for (int i = 0; i < 2; ++i) { acc.l[i] += b.l[i]; acc.h[i] += b.h[i]; }
+        }
+        for (int i = 0; i < 2; ++i) { acc.l[i] += gu[i]; acc.h[i] += gu[i]; }
+        acc = box_scale(acc, -double(c.dir[L - 1]));
+        int lo[2], hi[2];
+        box_to_sections(*ms[L - 1], acc, lo, hi);
+        if (!(lo[0] != hi[0] && lo[1] != hi[1])) continue;
+        double mn[4], mx[4];
+        for (int l = 0; l < L - 1; ++l) {
+            const int i = (comb >> (L - 2 - l)) & 1;
+            e[l] = 2 * sec[l] + i;
+            mn[l] = (c.dir[l] > 0) ? bs[l]->minE[e[l]] : -bs[l]->maxE[e[l]];
+            mx[l] = (c.dir[l] > 0) ? bs[l]->maxE[e[l]] : -bs[l]->minE[e[l]];
+        }
+        const Mesh& ml = *ms[L - 1];
+        for (int sy = lo[1]; sy < hi[1]; ++sy)
+            for (int sx = lo[0]; sx < hi[0]; ++sx)
+                for (int i = 0; i < 2; ++i) {
+                    e[L - 1] = 2 * (sx + sy * ml.nx) + i;
+                    const int l = L - 1;
+                    mn[l] = (c.dir[l] > 0) ? bs[l]->minE[e[l]] : -bs[l]->maxE[e[l]];
+                    mx[l] = (c.dir[l] > 0) ? bs[l]->maxE[e[l]] : -bs[l]->minE[e[l]];
+                    double minE = 0.0, maxE = 0.0;
+                    for (int k = 0; k < L; ++k) { minE += mn[k]; maxE += mx[k]; }
+                    if (!((minE <= 0.0) && (maxE >= 0.0))) continue;
+                    ++out.n_pre;
+                    bool det_ok;
+                    if (tuple_survives(P, c, e, u, det_ok)) {
+                        for (int k = 0; k < L; ++k) out.tuples.push_back(e[k]);
+                        out.tumk.push_back(u);
+                    }
+                    if (det_ok) ++out.n_det;
+                }
+    }
+}
+
 // deterministicIteration / nestedForSections / nestedForElements,
 // ScatteringChannel.hpp:205-255, driven by precalculateIndices
 // (ScatteringChannel.cpp:461-507).  Tuples are produced in the reference's
@@ -1189,6 +1253,35 @@ void or_set_tuples(void* h, int ch, int64_t n, const int32_t* ids, const int32_t
     c.tuples.assign(ids, ids + size_t(n) * c.L);
     c.tumk.assign(umk, umk + size_t(n));
     static_cast<Problem*>(h)->chans[size_t(ch)].tamp.clear();   // the factors follow the list
+}
+
+// Channel ch's tuple list becomes the tuples of work items [item0, item1)
+// (enumerate_items), over nthreads contiguous item ranges concatenated in
+// order; the prefilter and determinant counts are those of the range.
+void or_enumerate_items(void* h, int ch, int64_t item0, int64_t item1, int nthreads) {
+    Problem& P = *static_cast<Problem*>(h);
+    Channel& c = P.chans[size_t(ch)];
+    nthreads = int(std::max<int64_t>(1, std::min<int64_t>(nthreads, item1 - item0)));
+    std::vector<EnumPart> parts(static_cast<size_t>(nthreads));
+    std::vector<std::thread> th;
+    auto work = [&](int t) {
+        const int64_t a = item0 + (item1 - item0) * t / nthreads, b = item0 + (item1 - item0) * (t + 1) / nthreads;
+        enumerate_items(P, c, a, b, parts[size_t(t)]);
+    };
+    for (int t = 1; t < nthreads; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto& x : th) x.join();
+    c.tuples.clear();
+    c.tumk.clear();
+    c.tamp.clear();
+    c.n_prefilter = 0;
+    c.n_det = 0;
+    for (auto& q : parts) {
+        c.tuples.insert(c.tuples.end(), q.tuples.begin(), q.tuples.end());
+        c.tumk.insert(c.tumk.end(), q.tumk.begin(), q.tumk.end());
+        c.n_prefilter += q.n_pre;
+        c.n_det += q.n_det;
+    }
 }
 
 void or_set_amplitude(void* h, int ch, double a) { static_cast<Problem*>(h)->chans[ch].amplitude = a; }

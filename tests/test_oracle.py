@@ -248,3 +248,31 @@ def test_tuples_without_points_inside_contribute_exactly_zero(name):
             assert not np.any(sub.channel_propagate(ch, f0))
         sub.set_tuples(ch, ids[cnt > 0], umk[cnt > 0])
         assert np.array_equal(sub.channel_propagate(ch, f0), full)
+
+
+@pytest.mark.parametrize("name", ["ee_n4", "ee2_n3", "eph_n4"])
+def test_item_ranges_concatenate_to_the_full_enumeration(name):
+    """The work-item index of the streamed walk (umklapp, sections of legs
+    0..L-2, element choice; the reference's loop order): enumerating item
+    ranges and concatenating them gives the full list, in order."""
+    build, _, _ = cases()[name]
+    mat = build()
+    full = oracle.Oracle(mat)
+    part = oracle.Oracle(mat, enumerate_tuples=False)
+    pk = mat.pack()
+    for ch in range(len(mat.channels)):
+        cd = pk.desc.channels[ch]
+        n_items = cd.n_umklapp * 2 ** (cd.nlegs - 1)
+        for l in range(cd.nlegs - 1):
+            m = pk.desc.meshes[pk.desc.bands[cd.band[l]].mesh]
+            n_items *= m.nsplit[0] * m.nsplit[1]
+        ids, umk = full.tuples(ch)
+        cuts = [0, n_items // 7, n_items // 2, n_items - 1, n_items]
+        got_ids, got_umk = [], []
+        for a, b in zip(cuts[:-1], cuts[1:]):
+            part.enumerate_items(ch, a, b)
+            i, u = part.tuples(ch)
+            got_ids.append(i)
+            got_umk.append(u)
+        assert np.array_equal(np.concatenate(got_ids), ids)
+        assert np.array_equal(np.concatenate(got_umk), umk)

@@ -28,6 +28,8 @@ SOURCES = {
     "tb_shard.cu": [],
     "tb_constraints.cu": [],
     "tb_theta.cu": [],
+    "tb_probe.cu": [],
+    "tb_stream.cu": [],
 }
 
 

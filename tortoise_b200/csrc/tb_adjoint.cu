@@ -382,6 +382,7 @@ static int vjp_at(tb_handle* h, const double* Y, int flags) {
     if (!(flags & TB_NO_COLLISIONS)) {
         for (size_t gi = 0; gi < h->groups.size(); ++gi) {
             GroupChan& G = h->groups[gi];
+            if (G.stream) { set_error("the adjoint has no streamed channels (tb_options.stream_legs)"); return TB_ERR_ARG; }
             if (G.tup.n == 0 || G.insts.empty()) continue;
             // deterministic mode: the group's amplitude slots in the exact accumulator
             FxAcc fa = A->gamp_fx;

@@ -470,6 +470,44 @@ int build_runs(tb_handle* h, const tb_problem_desc* const* descs, int nruns) {
                     TB_CUDA(cudaMemcpy(G.tup.d, soa.data(), sizeof(int32_t) * soa.size(), cudaMemcpyHostToDevice));
                     G.tup.n = cd.n_tuples;
                     G.diag[0] = G.diag[1] = G.diag[2] = -1;
+                } else if (h->opts.stream_legs >= 2 && G.L >= h->opts.stream_legs) {
+                    // no stored list: the walk of precalculateIndices runs in every evaluation
+                    if (cd.n_mc > 64) { set_error("streamed channels take at most 64 Monte-Carlo points"); return TB_ERR_BAD_DESC; }
+                    StreamDev& sd = G.sdev;
+                    for (int l = 0; l < TB_MAX_LEGS; ++l) sd.nsec[l] = 1;
+                    sd.n_items = c.n_umk;
+                    for (int l = 0; l < G.L; ++l) {
+                        const int b = ri.band0 + cd.band[l];
+                        const HostMesh& m = h->meshes[h->bands[b].mesh];
+                        WalkLeg& w = sd.leg[l];
+                        w.minE = d_minE[b];
+                        w.maxE = d_maxE[b];
+                        w.nx = m.nx;
+                        w.ny = m.ny;
+                        for (int i = 0; i < 2; ++i) {
+                            w.origin[i] = m.origin[i];
+                            for (int j = 0; j < 2; ++j) { w.dG[i][j] = m.dG[i][j]; w.invdG[i][j] = m.invdG[i][j]; }
+                        }
+                        if (l < G.L - 1) {
+                            sd.nsec[l] = int64_t(m.nx) * m.ny;
+                            sd.n_items *= sd.nsec[l];
+                        }
+                    }
+                    sd.n_items *= int64_t(1) << (G.L - 1);
+                    sd.mc_pre = G.d_mc_pre;
+                    void* p = nullptr;
+                    if (cudaMalloc(&p, sizeof(unsigned long long) * 5) != cudaSuccess) {
+                        set_error("count buffer allocation failed");
+                        return TB_ERR_OOM;
+                    }
+                    h->dev_raw.push_back(p);
+                    sd.counts = static_cast<unsigned long long*>(p);
+                    TB_CUDA(cudaMemset(sd.counts, 0, sizeof(unsigned long long) * 5));
+                    G.stream = true;
+                    G.layout = TB_LAYOUT_STREAM;
+                    G.item_begin = 0;
+                    G.item_end = sd.n_items;
+                    G.diag[0] = G.diag[1] = G.diag[2] = -1;
                 } else {
                     int legband[TB_MAX_LEGS];
                     const double* mins[TB_MAX_LEGS];
@@ -545,11 +583,23 @@ static int launch_group_mc(tb_handle* h, GroupChan& G, const InstDev* insts, int
                                148 * 32, rate_leg, nullptr, nullptr, h->fx);
 }
 
+// A streamed group over this handle's work items.  Outside an integration
+// (ctl == nullptr) the launch records its counts for tb_channel_info; the
+// attempts of an integration leave them alone.
+static int launch_group_stream(tb_handle* h, GroupChan& G, const InstDev* insts, int n_insts, const double* d_in,
+                               double* d_acc, const DPCtl* ctl, int rate_leg) {
+    StreamDev sd = G.sdev;
+    if (ctl) sd.counts = nullptr;
+    else TB_CUDA(cudaMemsetAsync(sd.counts, 0, sizeof(unsigned long long) * 5, h->stream));
+    return launch_collision_stream(G.dev, sd, G.item_begin, G.item_end, insts, n_insts, d_in, d_acc, ctl, h->stream,
+                                   rate_leg, h->fx);
+}
+
 int run_rhs_acc(tb_handle* h, const double* d_in, double* d_acc, const DPCtl* ctl, int flags, int only_inst) {
     if (!(flags & TB_NO_COLLISIONS)) {
         for (size_t gi = 0; gi < h->groups.size(); ++gi) {
             GroupChan& G = h->groups[gi];
-            if (G.tup.n == 0) continue;
+            if (G.tup.n == 0 && !G.stream) continue;
             const InstDev* insts = G.d_insts;
             int n_insts = int(G.insts.size());
             if (only_inst >= 0) {
@@ -561,7 +611,9 @@ int run_rhs_acc(tb_handle* h, const double* d_in, double* d_acc, const DPCtl* ct
                 for (int id : G.insts) any |= h->insts[id].amplitude != 0.0;
                 if (!any) continue;
             }
-            if (G.layout == TB_LAYOUT_MC64) {
+            if (G.stream) {
+                TB_TRY(launch_group_stream(h, G, insts, n_insts, d_in, d_acc, ctl, -1));
+            } else if (G.layout == TB_LAYOUT_MC64) {
                 TB_TRY(launch_group_mc(h, G, insts, n_insts, d_in, d_acc, ctl, -1));
             } else {
                 TB_TRY(launch_collision_tensor(G.dev, insts, n_insts, G.tensor, G.tup.d, G.tup.cap, G.tup.n, d_in,
@@ -601,6 +653,7 @@ int choose_layouts(tb_handle* h) {
     cudaMemGetInfo(&freeb, &totalb);
     int64_t budget = h->opts.tensor_budget_bytes > 0 ? h->opts.tensor_budget_bytes : int64_t(double(freeb) * 0.6);
     for (auto& G : h->groups) {
+        if (G.stream) continue;   // TB_LAYOUT_STREAM, fixed at creation
         int want = h->opts.layout;
         if (want == TB_LAYOUT_AUTO) {
             // L = 3 and L = 2 tensors are cheaper per tuple than the Monte-Carlo
@@ -770,6 +823,10 @@ int tb_create_batch(tb_handle** out, const tb_problem_desc* const* runs, int n_r
         set_error("tb_options: layout must be 0..5 and allow_fp32 0..3");
         return TB_ERR_ARG;
     }
+    if (h->opts.stream_legs != 0 && (h->opts.stream_legs < 2 || h->opts.stream_legs > TB_MAX_LEGS)) {
+        set_error("tb_options: stream_legs must be 0 or 2..4");
+        return TB_ERR_ARG;
+    }
     if (h->opts.deterministic != 0 && h->opts.deterministic != 1) {
         set_error("tb_options: deterministic must be 0 or 1");
         return TB_ERR_ARG;
@@ -844,6 +901,18 @@ int tb_channel_info(const tb_handle* h, int ch, int64_t* n_tuples, int64_t* n_pr
                     int32_t* layout) {
     if (!h || ch < 0 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
     const GroupChan& G = h->groups[h->insts[ch].group];
+    if (G.stream) {
+        // the counts of the last evaluation outside an integration (zeros before one)
+        unsigned long long cnt[5] = {0, 0, 0, 0, 0};
+        TB_CUDA(cudaSetDevice(h->device));
+        TB_CUDA(cudaStreamSynchronize(h->stream));
+        TB_CUDA(cudaMemcpy(cnt, G.sdev.counts, sizeof(cnt), cudaMemcpyDeviceToHost));
+        if (n_tuples) *n_tuples = int64_t(cnt[2]);
+        if (n_prefilter) *n_prefilter = int64_t(cnt[0]);
+        if (n_det) *n_det = int64_t(cnt[1]);
+        if (layout) *layout = G.layout;
+        return TB_OK;
+    }
     if (n_tuples) *n_tuples = G.tup.n;
     if (n_prefilter) *n_prefilter = G.diag[0];
     if (n_det) *n_det = G.diag[1];
@@ -854,6 +923,15 @@ int tb_channel_info(const tb_handle* h, int ch, int64_t* n_tuples, int64_t* n_pr
 int tb_channel_points_inside(const tb_handle* h, int ch, int64_t* n_tuples, int64_t* n_points) {
     if (!h || ch < 0 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
     const GroupChan& G = h->groups[h->insts[ch].group];
+    if (G.stream) {
+        unsigned long long cnt[5] = {0, 0, 0, 0, 0};
+        TB_CUDA(cudaSetDevice(h->device));
+        TB_CUDA(cudaStreamSynchronize(h->stream));
+        TB_CUDA(cudaMemcpy(cnt, G.sdev.counts, sizeof(cnt), cudaMemcpyDeviceToHost));
+        if (n_tuples) *n_tuples = int64_t(cnt[4]);
+        if (n_points) *n_points = int64_t(cnt[3]);
+        return TB_OK;
+    }
     const bool has = G.layout == TB_LAYOUT_MC64 && G.theta.built;
     if (n_tuples) *n_tuples = has ? G.theta.n : -1;
     if (n_points) *n_points = has ? G.theta.points : -1;
@@ -863,6 +941,12 @@ int tb_channel_points_inside(const tb_handle* h, int ch, int64_t* n_tuples, int6
 int tb_channel_schedule(const tb_handle* h, int ch, int32_t* stages, int32_t* pair, double* seconds) {
     if (!h || ch < 0 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
     const GroupChan& G = h->groups[h->insts[ch].group];
+    if (G.stream) {
+        if (stages) *stages = 0;
+        if (pair) *pair = 7;
+        if (seconds) *seconds = 0.0;
+        return TB_OK;
+    }
     const bool tensor = G.layout != TB_LAYOUT_MC64;
     if (stages) *stages = tensor ? G.tensor.stages : 0;
     if (pair)
@@ -880,6 +964,10 @@ int tb_channel_schedule(const tb_handle* h, int ch, int32_t* stages, int32_t* pa
 int tb_set_channel_schedule(tb_handle* h, int ch, int32_t stages, int32_t pair) {
     if (!h || ch < 0 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
     GroupChan& G = h->groups[h->insts[ch].group];
+    if (G.stream) {
+        if (stages != 0 || pair != 7) { set_error("streamed channels have the one schedule stages 0, pair 7"); return TB_ERR_ARG; }
+        return TB_OK;
+    }
     if (G.layout == TB_LAYOUT_MC64) {
         if (stages != 0 || (pair != 0 && pair != 6)) {
             set_error("Monte-Carlo channels take stages 0 and pair 0 (every point) or 6 (points inside only)");
@@ -912,6 +1000,7 @@ int tb_set_channel_schedule(tb_handle* h, int ch, int32_t stages, int32_t pair) 
 int tb_get_tuples(const tb_handle* h, int ch, int32_t* ids, int32_t* umk) {
     if (!h || ch < 0 || ch >= int(h->insts.size())) { set_error("channel index out of range"); return TB_ERR_ARG; }
     const GroupChan& G = h->groups[h->insts[ch].group];
+    if (G.stream) { set_error("a streamed channel keeps no tuple list"); return TB_ERR_ARG; }
     const int64_t n = G.tup.n;
     if (n == 0) return TB_OK;
     std::vector<int32_t> soa(size_t(G.L + 1) * size_t(n));
@@ -940,6 +1029,7 @@ int tb_write_scatt_indices(const tb_handle* h, int ch, const char* path) {
     }
     const ChanInst& I = h->insts[ch];
     const GroupChan& G = h->groups[I.group];
+    if (G.stream) { set_error("a streamed channel keeps no tuple list"); return TB_ERR_ARG; }
     const int L = G.L;
     const int64_t n = G.tup.n;
     std::vector<int32_t> ids(size_t(std::max<int64_t>(n, 1)) * L), umk(size_t(std::max<int64_t>(n, 1)));
@@ -1022,6 +1112,7 @@ int tb_set_channel_amplitude_fn(tb_handle* h, int ch, tb_amplitude_fn fn, void* 
     TB_TRY(stream_wait(h));
     const ChanInst& I = h->insts[ch];
     GroupChan& G = h->groups[I.group];
+    if (G.stream && fn) { set_error("a streamed channel takes no functAmplitude (no per-tuple table)"); return TB_ERR_ARG; }
     const int L = G.L;
     const int64_t n = G.tup.n;
     if (G.d_tamp) { cudaFree(G.d_tamp); G.d_tamp = nullptr; }
@@ -1138,7 +1229,7 @@ int tb_scattering_rates(tb_handle* h, int ch, int leg, const double* f, double* 
     TB_CUDA(cudaMemsetAsync(h->d_acc, 0, bytes, h->stream));
     for (size_t gi = 0; gi < h->groups.size(); ++gi) {
         GroupChan& G = h->groups[gi];
-        if (G.tup.n == 0) continue;
+        if (G.tup.n == 0 && !G.stream) continue;
         const InstDev* insts = G.d_insts;
         int n_insts = int(G.insts.size());
         if (ch >= 0) {
@@ -1148,7 +1239,9 @@ int tb_scattering_rates(tb_handle* h, int ch, int leg, const double* f, double* 
         }
         for (int l = 0; l < G.L; ++l) {
             if (leg >= 0 && l != leg) continue;
-            if (G.layout == TB_LAYOUT_MC64)
+            if (G.stream)
+                TB_TRY(launch_group_stream(h, G, insts, n_insts, d_in, h->d_acc, nullptr, l));
+            else if (G.layout == TB_LAYOUT_MC64)
                 TB_TRY(launch_group_mc(h, G, insts, n_insts, d_in, h->d_acc, nullptr, l));
             else
                 TB_TRY(launch_collision_tensor(G.dev, insts, n_insts, G.tensor, G.tup.d, G.tup.cap, G.tup.n, d_in,

@@ -22,6 +22,7 @@
 #include "tb_dp45.cuh"
 #include "tb_geom.cuh"
 #include "tb_kernels.cuh"
+#include "tb_mcpoint.cuh"
 #include "tb_scatter.cuh"
 
 // Largest shared-memory accumulator (all instances' blocks) a launch uses;
@@ -138,57 +139,9 @@ __global__ void __launch_bounds__(256, LIST ? TB_MC_LIST_MIN_BLOCKS : 1) k_colli
 #pragma unroll
             for (int l = 0; l < L; ++l) { sx[l] = 0.0; sy[l] = 0.0; }
             if (LIST) {
-                // The leg forms as A = fa t + fa0, B = fb t + fb0 of the leg's
-                // linear form t = f0 + f1 x + f2 y (LegDev: fa, fb = +-1, fa0,
-                // fb0 in {0, +-1}), so only f stays in registers.
                 double fv[L][3];
-#pragma unroll
-                for (int l = 0; l < L; ++l) {
-                    const double* fe = f + in.foff[l] + 3 * (int64_t)e[l];
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) fv[l][j] = (RATE && l == rate_leg) ? (j == 0 ? 1.0 : 0.0) : __ldg(fe + j);
-                }
-                // One point inside: the legs' points and the gain-plus-loss
-                // product (the integrand without its Theta, which is 1 here).
-                auto point = [&](int m, double (&px)[L], double (&py)[L]) -> double {
-                    const double* qv = s_mc + m * R;
-                    double al[3];
-                    alpha_fast<L>(am, qv, al);
-#pragma unroll
-                    for (int l = 0; l < L - 2; ++l) { px[l] = qv[2 * l]; py[l] = qv[2 * l + 1]; }
-                    px[L - 2] = qv[R - 1]; py[L - 2] = al[0];
-                    px[L - 1] = al[1]; py[L - 1] = al[2];
-                    double pa = 1.0, pb = 1.0;
-#pragma unroll
-                    for (int l = 0; l < L; ++l) {
-                        const double t = fma(fv[l][2], py[l], fma(fv[l][1], px[l], fv[l][0]));
-                        double fa = c.leg[l].fa, fa0 = c.leg[l].fa0, fb = c.leg[l].fb, fb0 = c.leg[l].fb0;
-                        if (RATE && l == rate_leg) {
-                            // scattering rate of this leg: constant in / out unit
-                            // forms (ScatteringChannel.cpp:562-564)
-                            const double d = c.leg[l].dir, st = c.leg[l].stat;
-                            fa = (l == 0 ? -1.0 : 1.0) * ((1. - d) * st + (1. + d));
-                            fb = (1. + d) * st + (1. - d);
-                            fa0 = 0.0;
-                            fb0 = 0.0;
-                        }
-                        pa *= fma(fa, t, fa0);
-                        pb *= fma(fb, t, fb0);
-                    }
-                    return pa + pb;
-                };
-                auto accumulate = [&](double common, const double (&px)[L], const double (&py)[L]) {
-                    s0 += common;
-#pragma unroll
-                    for (int l = 0; l < L; ++l) {
-                        sx[l] = fma(px[l], common, sx[l]);
-                        sy[l] = fma(py[l], common, sy[l]);
-                    }
-                };
-                for (uint64_t mk = mk0; mk; mk &= mk - 1) {
-                    double px[L], py[L];
-                    accumulate(point(__ffsll((long long)mk) - 1, px, py), px, py);
-                }
+                leg_values<L, RATE>(c, in, f, e, rate_leg, fv);
+                inside_point_sums<L, RATE>(c, am, s_mc, mk0, fv, rate_leg, s0, sx, sy);
             } else {
                 // commonLinForm0 (A, direct) and commonLinForm1 (B, time reversed),
                 // ScatteringChannel.cpp:633-641

@@ -10,6 +10,7 @@
 #include "tb_dp45.cuh"
 #include "tb_enumerate.cuh"
 #include "tb_kernels.cuh"
+#include "tb_stream.cuh"
 #include "tb_tensor.cuh"
 #include "tb_theta.cuh"
 
@@ -31,6 +32,13 @@ struct GroupChan {
     int layout = TB_LAYOUT_MC64;
     MomentTensor tensor;
     ThetaList theta;              // Monte-Carlo layout: tuples with points inside the simplices, and which
+    // streamed channel (TB_LAYOUT_STREAM): the candidate walk and this
+    // handle's part [item_begin, item_end) of its work items; counts of the
+    // last evaluation (prefilter, determinant, survivors, points inside,
+    // tuples with points inside) in sdev.counts
+    bool stream = false;
+    StreamDev sdev{};
+    int64_t item_begin = 0, item_end = 0;
     std::vector<int> insts;       // channel instances using it (run order)
     InstDev* d_insts = nullptr;   // [insts.size()]
 };

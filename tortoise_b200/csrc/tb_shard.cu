@@ -131,11 +131,19 @@ int64_t shard_begin(int64_t n, int rank, int n_ranks) {
 }
 
 int shard_tuples(tb_handle* h, GroupChan& G) {
+    const int R = h->opts.shard_count;
+    const int r = h->opts.shard_rank;
+    if (G.stream) {
+        // a streamed channel splits its work items the same way
+        G.n_total = G.sdev.n_items;
+        G.item_begin = R <= 1 ? 0 : shard_begin(G.sdev.n_items, r, R);
+        G.item_end = R <= 1 ? G.sdev.n_items : shard_begin(G.sdev.n_items, r + 1, R);
+        G.shard_begin = G.item_begin;
+        return TB_OK;
+    }
     G.n_total = G.tup.n;
     G.shard_begin = 0;
-    const int R = h->opts.shard_count;
     if (R <= 1) return TB_OK;
-    const int r = h->opts.shard_rank;
     const int64_t b = shard_begin(G.tup.n, r, R), e = shard_begin(G.tup.n, r + 1, R);
     const int64_t cnt = e - b;
     DeviceTuples part;

@@ -1,0 +1,347 @@
+// tb_stream.cu -- the Monte-Carlo collision operator with its tuples
+// enumerated on the fly, for channels whose tuple list does not fit in
+// device memory (four-leg electron-electron channels on fine meshes: about
+// 2e9 surviving tuples at 32x32, 8e10 at 64x64).
+//
+// Every evaluation walks the reference's candidate space again and keeps
+// nothing between evaluations:
+//   * work items (umklapp, sections of legs 0..L-2, element choice in those
+//     sections) and, per item, the element box of the last leg: the nested
+//     loops of nestedForSections / nestedForElements (include/Physics/
+//     Scattering/ScatteringChannel.hpp:205-255) with the TrapezoidalSubset
+//     box arithmetic (src/Geometry/Structured/DirectSpace/MeshSubset.cpp);
+//   * the energy window, the determinant filter and the survival test of
+//     precalculateIndices (src/Physics/Scattering/ScatteringChannel.cpp:
+//     476-504) on the survival table;
+//   * for the survivors, which points of the quadrature table lie inside the
+//     simplices, and TypeB's sums over those points only
+//     (include/Physics/Scattering/IntegratorCore.hpp:260-357).
+// Every decision uses the same explicitly rounded operations as the stored
+// enumeration (k_enumerate, compiled unfused) and the mask builder
+// (k_theta_mask), and the sums use the stored-list kernel's code
+// (tb_mcpoint.cuh), so a streamed evaluation adds the same per-tuple values
+// as the stored-list path.
+//
+// Work distribution: a warp takes 32 work items (one per lane); the lanes
+// step through their boxes in lock step and push the candidates that pass
+// the energy window into a per-warp queue in shared memory; every 32 queued
+// candidates the warp evaluates them one per lane (determinant, survival,
+// mask, sums, scatter), so the heavy part runs on full warps whatever the box
+// sizes and the window's pass rate.
+#include "tb_dp45.cuh"
+#include "tb_mcpoint.cuh"
+#include "tb_scatter.cuh"
+#include "tb_stream.cuh"
+
+namespace tb {
+
+constexpr int ST_WARPS = 8;    // warps per block
+constexpr int ST_QUEUE = 64;   // candidate slots per warp (31 left over + 32 pushed at most)
+
+struct WBox {
+    double l[2], h[2];
+};
+
+// One section's box, shrunk by 1e-8 section units (MeshSubset.cpp:62-66),
+// in absolute coordinates.
+__device__ __forceinline__ WBox walk_section_box(const WalkLeg& m, int sx, int sy) {
+    WBox b;
+    const double lo0 = xa(double(sx), 0.00000001), lo1 = xa(double(sy), 0.00000001);
+    const double hi0 = xs(double(sx + 1), 0.00000001), hi1 = xs(double(sy + 1), 0.00000001);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        b.l[i] = xa(m.origin[i], xa(xm(m.dG[i][0], lo0), xm(m.dG[i][1], lo1)));
+        b.h[i] = xa(m.origin[i], xa(xm(m.dG[i][0], hi0), xm(m.dG[i][1], hi1)));
+    }
+    return b;
+}
+
+__device__ __forceinline__ WBox walk_box_scale(WBox b, double s) {
+    if (s >= 0.0) {
+#pragma unroll
+        for (int i = 0; i < 2; ++i) { b.l[i] = xm(b.l[i], s); b.h[i] = xm(b.h[i], s); }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const double t = b.l[i];
+            b.l[i] = xm(b.h[i], s);
+            b.h[i] = xm(t, s);
+        }
+    }
+    return b;
+}
+
+// Work item -> sections and elements of legs 0..L-2, umklapp column and the
+// section range [lo, hi) of the last leg's box (empty when lo == hi in a
+// dimension).  Decoding and box arithmetic of k_enumerate, term for term.
+template <int L>
+__device__ __forceinline__ void walk_item(const ChanDev& c, const StreamDev& sd, int64_t item, int (&e)[L], int& u,
+                                          int (&lo)[2], int (&hi)[2]) {
+    constexpr int C = 1 << (L - 1);
+    const int comb = int(item % C);
+    int64_t r = item / C;
+    int sec[TB_MAX_LEGS] = {0, 0, 0, 0};
+#pragma unroll
+    for (int l = L - 2; l >= 0; --l) {
+        sec[l] = int(r % sd.nsec[l]);
+        r /= sd.nsec[l];
+    }
+    u = int(r);
+    const double ux = c.umk[2 * u], uy = c.umk[2 * u + 1];
+    const double gu0 = xa(xm(c.gvec[0], ux), xm(c.gvec[2], uy));
+    const double gu1 = xa(xm(c.gvec[1], ux), xm(c.gvec[3], uy));
+    WBox acc;
+#pragma unroll
+    for (int l = 0; l < L - 1; ++l) {
+        const WalkLeg& m = sd.leg[l];
+        const WBox b = walk_box_scale(walk_section_box(m, sec[l] % m.nx, sec[l] / m.nx), c.leg[l].dir);
+        if (l == 0) acc = b;
+        else {
+#pragma unroll
+            for (int i = 0; i < 2; ++i) { acc.l[i] = xa(acc.l[i], b.l[i]); acc.h[i] = xa(acc.h[i], b.h[i]); }
+        }
+        e[l] = 2 * sec[l] + ((comb >> (L - 2 - l)) & 1);
+    }
+    acc.l[0] = xa(acc.l[0], gu0); acc.h[0] = xa(acc.h[0], gu0);
+    acc.l[1] = xa(acc.l[1], gu1); acc.h[1] = xa(acc.h[1], gu1);
+    acc = walk_box_scale(acc, -c.leg[L - 1].dir);
+    const WalkLeg& ml = sd.leg[L - 1];
+    const int ns[2] = {ml.nx, ml.ny};
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const double tl = xa(xm(ml.invdG[i][0], xs(acc.l[0], ml.origin[0])), xm(ml.invdG[i][1], xs(acc.l[1], ml.origin[1])));
+        const double th = xa(xm(ml.invdG[i][0], xs(acc.h[0], ml.origin[0])), xm(ml.invdG[i][1], xs(acc.h[1], ml.origin[1])));
+        const int aa = int(floor(tl));
+        const int bb = int(xa(floor(th), 1.0));
+        lo[i] = min(max(aa, 0), ns[i]);
+        hi[i] = min(max(bb, 0), ns[i]);
+    }
+}
+
+template <int L, bool RATE>
+#ifndef TB_STREAM_MIN_BLOCKS
+#define TB_STREAM_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
+    k_collision_stream(ChanDev c, StreamDev sd, int64_t it0, int64_t it1, const InstDev* __restrict__ insts,
+                       int n_insts, const double* __restrict__ f, double* __restrict__ acc,
+                       const DPCtl* __restrict__ ctl, int rate_leg, FxAcc fx) {
+    {
+        // every instance off or its run finished: nothing to add
+        bool any = false;
+        for (int k = 0; k < n_insts && !any; ++k)
+            any = insts[k].amp_full != 0.0 && !(ctl && ctl[insts[k].run].done);
+        if (!any) return;
+    }
+    constexpr int R = 2 * (L - 2) + 1;
+    extern __shared__ double s_tab[];   // [nmc R] quadrature table, then [nmc R] survival table
+    __shared__ int32_t s_q[ST_WARPS][L + 1][ST_QUEUE];
+    double* s_mc = s_tab;
+    double* s_pre = s_tab + c.nmc * R;
+    for (int i = threadIdx.x; i < c.nmc * R; i += blockDim.x) {
+        s_mc[i] = c.mc[i];
+        s_pre[i] = sd.mc_pre[i];
+    }
+    __syncthreads();
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double sqrt2 = 1.4142135623730951;   // sqrt(2.0), correctly rounded
+    double prodc = 1.0;
+#pragma unroll
+    for (int l = 0; l < L; ++l) prodc *= sqrt2;
+    const double inv_fact_nmc = c.fact * double(c.nmc);
+    unsigned long long n_pre = 0, n_det = 0, n_surv = 0, n_pts = 0, n_tin = 0;
+
+    // Evaluates `take` queued candidates from slot `first` on, one per lane.
+    auto evaluate = [&](int first, int take) {
+        const bool valid = lane < take;
+        int e[L];
+        int u = 0;
+#pragma unroll
+        for (int l = 0; l < L; ++l) e[l] = valid ? s_q[warp][l][first + lane] : 0;
+        if (valid) u = s_q[warp][L][first + lane];
+        TupleGeom<L> g;
+        tuple_geometry<L>(c, e, u, g);
+        bool ok = valid && (fabs(g.det) >= c.min_det);
+        double Ci[3][3];
+        dc_inverse<L>(g, Ci);
+        // survival test of precalculateIndices on the survival table (k_enumerate's)
+        double sum = 0.0;
+        {
+            double p[L][2];
+            for (int m = 0; m < c.nmc; ++m) {
+                const bool th = mc_point_exact<L>(g, Ci, s_pre + m * R, p);
+                sum += th ? prodc : 0.0;
+            }
+        }
+        double res = (1.0 / (c.fact * double(c.nmc) * fabs(g.det))) * sum;
+        res *= c.amp_vol;
+        n_pre += valid ? 1 : 0;
+        n_det += ok ? 1 : 0;
+        ok = ok && (fabs(res) > c.threshold);
+        n_surv += ok ? 1 : 0;
+        // the points inside the simplices on the quadrature table (k_theta_mask's)
+        AlphaMap<L> am;
+        alpha_map<L>(g, Ci, am);
+        uint64_t mk = 0;
+        if (ok)
+            for (int m = 0; m < c.nmc; ++m) {
+                double al[3];
+                if (alpha_theta<L>(g, Ci, am, s_mc + m * R, al)) mk |= 1ull << m;
+            }
+        n_pts += __popcll(mk);
+        n_tin += mk ? 1 : 0;
+        if (!__any_sync(full, mk != 0ull)) return;
+        const bool live = mk != 0ull;
+        const double scale = live ? 1.0 / (inv_fact_nmc * fabs(g.det)) : 0.0;
+        for (int k = 0; k < n_insts; ++k) {
+            const InstDev in = insts[k];
+            if (in.amp_full == 0.0) continue;
+            if (ctl && ctl[in.run].done) continue;
+            const double ampt = in.amp_full;
+            double s0 = 0.0, sx[L], sy[L];
+#pragma unroll
+            for (int l = 0; l < L; ++l) { sx[l] = 0.0; sy[l] = 0.0; }
+            if (live) {
+                double fv[L][3];
+                leg_values<L, RATE>(c, in, f, e, rate_leg, fv);
+                inside_point_sums<L, RATE>(c, am, s_mc, mk, fv, rate_leg, s0, sx, sy);
+            }
+#pragma unroll
+            for (int l = 0; l < L; ++l) {
+                if (RATE && l != rate_leg) continue;   // uniform: the rate keeps one leg
+                const double d = RATE ? -c.leg[l].dir : c.leg[l].dir;
+                const int64_t key = in.foff[l] + 3 * (int64_t)e[l];
+                const double v0 = d * ((scale * s0) * ampt), v1 = d * ((scale * sx[l]) * ampt),
+                             v2 = d * ((scale * sy[l]) * ampt);
+                if (fx.w) {
+                    if (live) fx_add3(fx, key, v0, v1, v2);
+                } else if (l < L - 1) {
+                    warp_scatter3(live ? key : -1, acc + key, v0, v1, v2);
+                } else if (live) {
+                    atomicAdd(acc + key + 0, v0);
+                    atomicAdd(acc + key + 1, v1);
+                    atomicAdd(acc + key + 2, v2);
+                }
+            }
+        }
+    };
+
+    int qn = 0;   // queued candidates (warp-uniform)
+    const int64_t stride = int64_t(gridDim.x) * ST_WARPS * 32;
+    for (int64_t base = it0 + (int64_t(blockIdx.x) * ST_WARPS + warp) * 32; base < it1; base += stride) {
+        const int64_t item = base + lane;
+        int e[L];
+        int u = 0, lo[2] = {0, 0}, hi[2] = {0, 0};
+        double mn[L], mx[L];   // energy window per leg, summed in leg order below
+        int ncand = 0;
+        if (item < it1) {
+            walk_item<L>(c, sd, item, e, u, lo, hi);
+            if (lo[0] != hi[0] && lo[1] != hi[1]) {
+                ncand = 2 * (hi[0] - lo[0]) * (hi[1] - lo[1]);
+#pragma unroll
+                for (int l = 0; l < L - 1; ++l) {
+                    const double emin = __ldg(sd.leg[l].minE + e[l]), emax = __ldg(sd.leg[l].maxE + e[l]);
+                    mn[l] = (c.leg[l].dir > 0) ? emin : -emax;
+                    mx[l] = (c.leg[l].dir > 0) ? emax : -emin;
+                }
+            }
+        }
+        const int maxc = __reduce_max_sync(full, unsigned(ncand));
+        const int nbx = hi[0] - lo[0];
+        const WalkLeg& ml = sd.leg[L - 1];
+        for (int k = 0; k < maxc; ++k) {
+            bool pass = false;
+            int el = 0;
+            if (k < ncand) {
+                const int ie = k & 1, t = k >> 1;
+                const int sx = lo[0] + t % nbx, sy = lo[1] + t / nbx;
+                el = 2 * (sx + sy * ml.nx) + ie;
+                const double emin = __ldg(ml.minE + el), emax = __ldg(ml.maxE + el);
+                mn[L - 1] = (c.leg[L - 1].dir > 0) ? emin : -emax;
+                mx[L - 1] = (c.leg[L - 1].dir > 0) ? emax : -emin;
+                double minE = 0.0, maxE = 0.0;
+#pragma unroll
+                for (int l = 0; l < L; ++l) { minE += mn[l]; maxE += mx[l]; }
+                pass = (minE <= 0.0) && (maxE >= 0.0);
+            }
+            const unsigned bal = __ballot_sync(full, pass);
+            if (pass) {
+                const int pos = qn + __popc(bal & ((1u << lane) - 1u));
+#pragma unroll
+                for (int l = 0; l < L - 1; ++l) s_q[warp][l][pos] = e[l];
+                s_q[warp][L - 1][pos] = el;
+                s_q[warp][L][pos] = u;
+            }
+            qn += __popc(bal);
+            __syncwarp();
+            if (qn >= 32) {
+                evaluate(qn - 32, 32);
+                qn -= 32;
+                __syncwarp();   // the slots are reused
+            }
+        }
+    }
+    if (qn > 0) evaluate(0, qn);
+    if (sd.counts) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            n_pre += __shfl_down_sync(full, n_pre, o);
+            n_det += __shfl_down_sync(full, n_det, o);
+            n_surv += __shfl_down_sync(full, n_surv, o);
+            n_pts += __shfl_down_sync(full, n_pts, o);
+            n_tin += __shfl_down_sync(full, n_tin, o);
+        }
+        if (lane == 0 && (n_pre | n_det | n_surv | n_pts | n_tin)) {
+            atomicAdd(sd.counts + 0, n_pre);
+            atomicAdd(sd.counts + 1, n_det);
+            atomicAdd(sd.counts + 2, n_surv);
+            atomicAdd(sd.counts + 3, n_pts);
+            atomicAdd(sd.counts + 4, n_tin);
+        }
+    }
+}
+
+template <int L, bool RATE>
+static int launch_stream(const ChanDev& c, const StreamDev& sd, int64_t it0, int64_t it1, const InstDev* insts,
+                         int n_insts, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s, int rate_leg,
+                         const FxAcc& fx) {
+    auto kern = k_collision_stream<L, RATE>;
+    const int threads = ST_WARPS * 32;
+    const size_t smem = 2 * sizeof(double) * size_t(c.nmc) * c.R;
+    int dev = 0, nsm = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    if (per_sm < 1) per_sm = 1;
+    const int64_t batches = (it1 - it0 + 31) / 32;
+    int64_t blocks = (batches + ST_WARPS - 1) / ST_WARPS;
+    // several waves of resident blocks: the work per item varies a lot
+    const int64_t cap = int64_t(nsm) * per_sm * 8;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) return TB_OK;
+    kern<<<unsigned(blocks), threads, smem, s>>>(c, sd, it0, it1, insts, n_insts, f, acc, ctl, RATE ? rate_leg : -1,
+                                                 fx);
+    TB_CUDA(cudaGetLastError());
+    return TB_OK;
+}
+
+int launch_collision_stream(const ChanDev& c, const StreamDev& sd, int64_t item_begin, int64_t item_end,
+                            const InstDev* insts, int n_insts, const double* f, double* acc, const DPCtl* ctl,
+                            cudaStream_t s, int rate_leg, const FxAcc& fx) {
+    if (item_end <= item_begin || n_insts <= 0) return TB_OK;
+    if (c.nmc > 64) { set_error("streamed channels take at most 64 Monte-Carlo points"); return TB_ERR_ARG; }
+#define TB_ST(LL) \
+    (rate_leg >= 0 ? launch_stream<LL, true>(c, sd, item_begin, item_end, insts, n_insts, f, acc, ctl, s, rate_leg, fx) \
+                   : launch_stream<LL, false>(c, sd, item_begin, item_end, insts, n_insts, f, acc, ctl, s, -1, fx))
+    switch (c.L) {
+        case 2: return TB_ST(2);
+        case 3: return TB_ST(3);
+        case 4: return TB_ST(4);
+    }
+#undef TB_ST
+    set_error("nlegs must be 2..4");
+    return TB_ERR_ARG;
+}
+
+}  // namespace tb

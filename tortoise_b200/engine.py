@@ -13,8 +13,8 @@ from .abi import STATUS_NAMES
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libtortoise_b200.so")
 
-LAYOUT_AUTO, LAYOUT_MC64, LAYOUT_T64, LAYOUT_T32, LAYOUT_T40, LAYOUT_T48 = 0, 1, 2, 3, 4, 5
-LAYOUT_NAMES = {1: "mc64", 2: "t64", 3: "t32", 4: "t40", 5: "t48"}
+LAYOUT_AUTO, LAYOUT_MC64, LAYOUT_T64, LAYOUT_T32, LAYOUT_T40, LAYOUT_T48, LAYOUT_STREAM = 0, 1, 2, 3, 4, 5, 6
+LAYOUT_NAMES = {1: "mc64", 2: "t64", 3: "t32", 4: "t40", 5: "t48", 6: "stream"}
 PTR_HOST, NO_DRIFT, NO_COLLISIONS = 1, 2, 4
 
 _lib = None
@@ -30,7 +30,8 @@ class TortoiseError(RuntimeError):
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("layout", C.c_int32), ("allow_fp32", C.c_int32),
                 ("tensor_budget_bytes", C.c_int64), ("verbose", C.c_int32), ("autotune", C.c_int32),
-                ("shard_rank", C.c_int32), ("shard_count", C.c_int32), ("deterministic", C.c_int32)]
+                ("shard_rank", C.c_int32), ("shard_count", C.c_int32), ("deterministic", C.c_int32),
+                ("stream_legs", C.c_int32)]
 
 
 class DP45Stats(C.Structure):
@@ -83,6 +84,7 @@ def lib():
         L.tb_dp45_end.argtypes = [vp, vp, vp, vp, i64, C.POINTER(DP45Stats), C.c_int]
         L.tb_synchronize.argtypes = [vp]
         L.tb_set_copy_wait_limit.argtypes = [vp, i64]
+        L.tb_fp64_fma_rate.argtypes = [C.c_int, C.POINTER(C.c_double)]
         L.tb_get_stream.restype = vp
         L.tb_get_stream.argtypes = [vp]
         L.tb_collision_accumulate.argtypes = [vp, C.c_int, vp, vp]
@@ -157,6 +159,13 @@ def shard_range(n_tuples, rank, n_ranks):
     return b.value, e.value
 
 
+def fp64_fma_rate(device=0):
+    """The device's measured FP64 FMA throughput, FMAs per second (tb_fp64_fma_rate)."""
+    v = C.c_double()
+    _check(lib().tb_fp64_fma_rate(int(device), C.byref(v)), "tb_fp64_fma_rate")
+    return v.value
+
+
 def shard_unique_id():
     """A new communicator id (bytes) for tb_shard_connect; one rank makes it."""
     buf = C.create_string_buffer(SHARD_ID_BYTES)
@@ -179,14 +188,17 @@ class Engine:
     tortoise_b200.shard.connect) so that collision sums are all-reduced.
 
     deterministic=True: bit-reproducible sums (tb_options.deterministic):
-    exact fixed-point accumulation instead of FP64 atomics."""
+    exact fixed-point accumulation instead of FP64 atomics.
+
+    stream_legs=L (2..4): channels with at least L legs keep no tuple list
+    and enumerate their tuples in every evaluation (tb_options.stream_legs)."""
 
     def __init__(self, material, layout=LAYOUT_AUTO, allow_fp32=False, device=0, tensor_budget_bytes=0,
-                 autotune=False, shard=None, deterministic=False):
+                 autotune=False, shard=None, deterministic=False, stream_legs=0):
         self.material = material
         self.packed = material.pack()
         opts = Options(device, layout, int(allow_fp32), tensor_budget_bytes, 0, int(autotune), *_shard_opts(shard),
-                       int(bool(deterministic)))
+                       int(bool(deterministic)), int(stream_legs))
         h = C.c_void_p()
         _check(lib().tb_create(C.byref(h), C.addressof(self.packed.desc), C.byref(opts)), "tb_create")
         self.h = h
@@ -310,6 +322,9 @@ class Engine:
              "tuned_seconds": sec.value}
         if pr.value == 6:   # Monte-Carlo channel visiting only the points inside the simplices
             d["inside_only"] = True
+        if pr.value == 7:   # streamed channel: tuples enumerated in every evaluation
+            d["inside_only"] = True
+            d["streamed"] = True
         return d
 
     def tuples(self, ch):
@@ -465,13 +480,13 @@ class BatchEngine(Engine):
     size.  Channels and bands are numbered globally in run order."""
 
     def __init__(self, materials, layout=LAYOUT_AUTO, allow_fp32=False, device=0, tensor_budget_bytes=0,
-                 autotune=False, shard=None, deterministic=False):
+                 autotune=False, shard=None, deterministic=False, stream_legs=0):
         self.materials = list(materials)
         self.material = self.materials[0]
         self.packs = [m.pack() for m in self.materials]
         arr = (C.c_void_p * len(self.packs))(*[C.addressof(p.desc) for p in self.packs])
         opts = Options(device, layout, int(allow_fp32), tensor_budget_bytes, 0, int(autotune), *_shard_opts(shard),
-                       int(bool(deterministic)))
+                       int(bool(deterministic)), int(stream_legs))
         h = C.c_void_p()
         _check(lib().tb_create_batch(C.byref(h), arr, len(self.packs), C.byref(opts)), "tb_create_batch")
         self.h = h
