@@ -932,6 +932,84 @@ def large(args):
     print(json.dumps(line), flush=True)
 
 
+def ee_full(args):
+    """The two-band configuration as written, e-e included: parabola + Dirac
+    cone, the four-leg e-e channels (constant matrix element 1.0) and the
+    e-ph channels of the optical branch (hw = 0.2, Bose kT = 0.05), drift
+    field (0.1, 0), rtol 1e-8, on an N x N mesh (--ee-full N).  The e-e
+    channels are streamed (their tuple lists do not fit in device memory at
+    N >= 32: about 2e9 tuples per channel at 32x32, 8e10 at 64x64); the e-ph
+    channels keep their moment tensors.  Times one collision evaluation of
+    every channel (CUDA events on the library's stream), reports the walk's
+    counts per e-e channel, then times args.steps DP45 attempts from t = 0
+    after args.warmup untimed ones."""
+    import torch
+    from tortoise_b200 import engine as E
+    from tortoise_b200 import workloads as W
+    N = args.ee_full
+    mat = W.two_band_eph_drift(N, ee=True)
+    f0 = W.initial_status(mat, kT=0.1, seed=1).vec
+    t0 = time.perf_counter()
+    eng = E.Engine(mat, stream_legs=4, autotune=not args.no_tune)
+    setup = time.perf_counter() - t0
+    nch = len(mat.channels)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.ExternalStream(eng.stream_ptr(), device=dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f = torch.tensor(f0, device=dev)
+    acc = torch.zeros_like(f)
+    per_channel, infos, inside = [], [], []
+    for c in range(nch):
+        # one channel alone (its streamed walk records its counts)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        eng.collision_accumulate(f.data_ptr(), acc.data_ptr(), ch=c)
+        ev1.record(stream)
+        ev1.synchronize()
+        per_channel.append(ev0.elapsed_time(ev1))
+        infos.append(eng.channel_info(c))
+        inside.append(eng.points_inside(c))
+    w0 = time.perf_counter()
+    eng.rhs(f0)   # one whole right-hand side from host buffers
+    t_rhs_host = time.perf_counter() - w0
+    ee_idx = [c for c in range(nch) if mat.channels[c].nlegs == 4]
+    line = {"ee_full": True, "workload": "2-band e-e + e-ph + drift, %dx%d mesh (%d triangles/band), NMC=50, "
+                                         "rtol 1e-8" % (N, N, 2 * N * N),
+            "setup_s": setup, "channels": nch, "dofs": eng.ndofs,
+            "layouts": [i["layout"] for i in infos],
+            "ee_channels": {"count": len(ee_idx),
+                            "candidates_in_energy_window": sum(infos[c]["n_prefilter"] for c in ee_idx),
+                            "with_valid_determinant": sum(infos[c]["n_det"] for c in ee_idx),
+                            "surviving_tuples": sum(infos[c]["n_tuples"] for c in ee_idx),
+                            "tuples_with_points_inside": sum(inside[c][0] for c in ee_idx),
+                            "points_inside": sum(inside[c][1] for c in ee_idx)},
+            "collision_ms_per_channel": per_channel,
+            "collision_ms_per_rhs": sum(per_channel), "collision_ms_ee": sum(per_channel[c] for c in ee_idx),
+            "collision_ms_eph": sum(per_channel[c] for c in range(nch) if c not in ee_idx),
+            "rhs_host_seconds": t_rhs_host}
+    if line["collision_ms_ee"] > 0:
+        line["ee_surviving_tuples_per_s"] = line["ee_channels"]["surviving_tuples"] / (1e-3 * line["collision_ms_ee"])
+    if args.steps > 0:
+        eng.dp45_begin(f0, 0.0, T_END, DENSE, 0)
+        eng.dp45_advance(args.warmup)
+        eng.synchronize()
+        with ClockSampler(0) as clk:
+            ev0.record(stream)
+            eng.dp45_advance(args.steps)
+            ev1.record(stream)
+            ev1.synchronize()
+        st = eng.dp45_poll()
+        line["dp45"] = {"attempts_timed": args.steps, "warmup": args.warmup,
+                        "seconds_per_attempt": ev0.elapsed_time(ev1) * 1e-3 / args.steps,
+                        "attempts_per_s": args.steps / (ev0.elapsed_time(ev1) * 1e-3),
+                        "t": st["t"], "attempts": st["attempts"], "rejected": st["rejected"], "status": st["status"]}
+        c = clk.summary()
+        if c:
+            line["clocks"] = c
+    print(json.dumps(line), flush=True)
+    eng.close()
+
+
 def rhs_only(args):
     """Profiling driver: K right-hand-side evaluations (collision + drift +
     M^-1) of the workload on the device, nothing else (used for the ncu
@@ -998,11 +1076,17 @@ def main():
     ap.add_argument("--ee-mesh", type=int, default=16, help="sections per side of the --small-ee workload")
     ap.add_argument("--shard", action="store_true",
                     help="one run with its tuples split over the ranks (NCCL all-reduce per RHS) instead of replicas")
+    ap.add_argument("--ee-full", type=int, default=0,
+                    help="the two-band workload with its e-e channels (streamed) on an N x N mesh: collision time "
+                         "per RHS and --steps DP45 attempts")
     ap.add_argument("--adjoint", type=int, default=-1,
                     help="adjoint gradient of the 32x32 workload, checked in this many FD directions")
     args = ap.parse_args()
     if args.large:
         large(args)
+        return
+    if args.ee_full:
+        ee_full(args)
         return
     if args.to_end and not args.batch:
         to_end(args)

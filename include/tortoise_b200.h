@@ -169,10 +169,11 @@ typedef struct tb_options {
                                      (ScatteringChannel.hpp:205-255, ScatteringChannel.cpp:476-504) on
                                      the device again and integrates the survivors on the spot
                                      (TB_LAYOUT_STREAM), for lists too large for device memory (four-leg
-                                     e-e on fine meshes).  Same per-tuple sums as the stored list.  Such
-                                     channels have no tuple list to read or save, take no functAmplitude
-                                     and no adjoint; tb_channel_info reports the counts of their last
-                                     evaluation.  0: every list is stored. */
+                                     e-e on fine meshes).  Same per-tuple sums as the stored list, for the
+                                     operator, the rates and the adjoint's VJP.  Such channels have no
+                                     tuple list to read or save and take no functAmplitude;
+                                     tb_channel_info reports the counts of their last evaluation
+                                     outside an integration.  0: every list is stored. */
 } tb_options;
 
 /* Pointer flags */
@@ -460,7 +461,10 @@ int tb_dp45_replay(tb_handle* h, const double* f0, const double* dts, int64_t n_
  * (held on every device that loads the library until the process exits).
  * Limit: n_elements <= 1,048,576 (TB_ERR_CAPACITY beyond).  The first call on
  * a device looks up that array's device address, so make it before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race.
+ * capture.  The address is kept for the life of the process: a process that
+ * resets the device (cudaDeviceReset) or otherwise tears down its primary
+ * context must not call this entry point on that device again.  All calls
+ * share the array: calls that overlap on the GPU race.
  * Launches on `stream` (a cudaStream_t, NULL = default stream) and does not
  * synchronise.  No counterpart in the reference. */
 int tb_band_relative_error_noalloc(const double* err, const double* pop, int64_t n_elements, double elem_volume,

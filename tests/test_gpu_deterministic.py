@@ -62,7 +62,8 @@ def test_monte_carlo_visiting_modes_are_each_reproducible(gpu_lib, name):
     try:
         for inside in (True, False):
             for ch in range(len(mat.channels)):
-                e.set_schedule(ch, 0, inside_only=inside)
+                if e.points_inside(ch)[0] >= 0:   # channels without tuples have no list of inside points
+                    e.set_schedule(ch, 0, inside_only=inside)
             r = [e.rhs(f0) for _ in range(3)]
             assert np.array_equal(r[0], r[1]) and np.array_equal(r[0], r[2])
     finally:

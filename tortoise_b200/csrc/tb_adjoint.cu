@@ -382,11 +382,15 @@ static int vjp_at(tb_handle* h, const double* Y, int flags) {
     if (!(flags & TB_NO_COLLISIONS)) {
         for (size_t gi = 0; gi < h->groups.size(); ++gi) {
             GroupChan& G = h->groups[gi];
-            if (G.stream) { set_error("the adjoint has no streamed channels (tb_options.stream_legs)"); return TB_ERR_ARG; }
-            if (G.tup.n == 0 || G.insts.empty()) continue;
+            if ((G.tup.n == 0 && !G.stream) || G.insts.empty()) continue;
             // deterministic mode: the group's amplitude slots in the exact accumulator
             FxAcc fa = A->gamp_fx;
             if (fa.w) fa.w += 3 * int64_t(A->gamp_off[gi]);
+            if (G.stream) {   // tuples enumerated again, as in the forward evaluations
+                TB_TRY(launch_vjp_stream(G.dev, G.sdev, G.item_begin, G.item_end, G.d_insts, int(G.insts.size()), Y,
+                                         A->u, A->g, A->gamp + A->gamp_off[gi], h->stream, h->fx, fa));
+                continue;
+            }
             if (G.layout == TB_LAYOUT_MC64 && G.theta.use)   // the tuples and points inside the simplices only
                 TB_TRY(launch_collision_vjp(G.dev, G.d_insts, int(G.insts.size()), G.layout, G.tensor, G.theta.ids,
                                             G.theta.n, G.theta.n, Y, A->u, A->g, A->gamp + A->gamp_off[gi], h->stream,

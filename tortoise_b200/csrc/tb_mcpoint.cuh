@@ -6,6 +6,7 @@
 #pragma once
 
 #include "tb_geom.cuh"
+#include "tb_kernels.cuh"
 
 namespace tb {
 
@@ -72,6 +73,102 @@ __device__ __forceinline__ void inside_point_sums(const ChanDev& c, const AlphaM
     for (uint64_t mk = mk0; mk; mk &= mk - 1) {
         double px[L], py[L];
         accumulate(point(__ffsll((long long)mk) - 1, px, py), px, py);
+    }
+}
+
+// Sum over the warp, then one add per warp into dst (exact into slot k of
+// fx in the deterministic mode; the warp's own sum runs in a fixed order, so
+// it depends only on which tuples share the warp).  All lanes call it.
+__device__ __forceinline__ void block_atomic_sum(double v, double* dst, const FxAcc& fx, int k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v != 0.0) {
+        if (fx.w) fx_add(fx, k, v);
+        else atomicAdd(dst, v);
+    }
+}
+
+// The loss / gain forms A, B of every leg (ScatteringChannel.cpp:633-641)
+// and their slopes sa, sb with respect to the leg's coefficients of f.
+template <int L>
+__device__ __forceinline__ void leg_forms(const ChanDev& c, const InstDev& in, const double* f, const int (&e)[L],
+                                          double (&A)[L][3], double (&B)[L][3], double (&sa)[L], double (&sb)[L]) {
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+        const double d = c.leg[l].dir, s = c.leg[l].stat;
+        const double* fe = f + in.foff[l] + 3 * (int64_t)e[l];
+        const double ka = (l == 0 ? -1.0 : 1.0) * 0.5;
+        const double ca = (1. - d) * s + (1. + d);
+        const double cb = (1. + d) * s + (1. - d);
+        sa[l] = ka * ca;    // dA[l][j] / df_j
+        sb[l] = 0.5 * cb;   // dB[l][j] / df_j
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const double unit = (j == 0) ? 1.0 : 0.0;
+            const double fj = __ldg(fe + j);
+            A[l][j] = ka * ((1. - d) * unit + ca * fj);
+            B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
+        }
+    }
+}
+
+// The transposed quadrature of one tuple for one instance (the VJP of
+// TypeB's sums): gA[l][j], gB[l][j] = d/dA[l][j], d/dB[l][j] of
+// sum_points (u-weighted test functions) x (prod A + prod B), and gamp = the
+// sum itself, over the points with Theta = 1: every point (LIST false, the
+// exact decision per point) or the set bits of mk0 in increasing order (LIST
+// true).  Zeros when valid is false.
+template <int L, bool LIST>
+__device__ __forceinline__ void vjp_point_sums(const ChanDev& c, const InstDev& in, const double* __restrict__ f,
+                                               const double* __restrict__ u, const int (&e)[L],
+                                               const TupleGeom<L>& g, const double (&Ci)[3][3], const double* s_mc,
+                                               uint64_t mk0, bool valid, double (&gA)[L][3], double (&gB)[L][3],
+                                               double& gamp, double (&sa)[L], double (&sb)[L]) {
+    constexpr int R = 2 * (L - 2) + 1;
+    double A[L][3], B[L][3];
+    leg_forms<L>(c, in, f, e, A, B, sa, sb);
+    double ul[L][3];
+#pragma unroll
+    for (int l = 0; l < L; ++l)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) ul[l][j] = c.leg[l].dir * __ldg(u + in.foff[l] + 3 * (int64_t)e[l] + j);
+    gamp = 0.0;
+#pragma unroll
+    for (int l = 0; l < L; ++l)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) { gA[l][j] = 0.0; gB[l][j] = 0.0; }
+    if (!valid) return;
+    uint64_t mk = mk0;
+    for (int m = 0; LIST ? (mk != 0) : (m < c.nmc); ++m) {
+        if (LIST) {
+            m = __ffsll((long long)mk) - 1;
+            mk &= mk - 1;
+        }
+        const double* qv = s_mc + m * R;
+        double p[L][2];
+        if (!mc_point_exact<L>(g, Ci, qv, p)) continue;
+        double av[L], bv[L];
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            av[l] = (A[l][1] * p[l][0] + A[l][2] * p[l][1]) + A[l][0];
+            bv[l] = (B[l][1] * p[l][0] + B[l][2] * p[l][1]) + B[l][0];
+        }
+        double om = 0.0;   // sum over legs of dir * (u . test functions)
+#pragma unroll
+        for (int l = 0; l < L; ++l) om += ul[l][0] + ul[l][1] * p[l][0] + ul[l][2] * p[l][1];
+        double pa = 1.0, pb = 1.0;
+#pragma unroll
+        for (int l = 0; l < L; ++l) { pa *= av[l]; pb *= bv[l]; }
+        gamp += om * (pa + pb);
+#pragma unroll
+        for (int mm = 0; mm < L; ++mm) {
+            double ra = om, rb = om;
+#pragma unroll
+            for (int l = 0; l < L; ++l)
+                if (l != mm) { ra *= av[l]; rb *= bv[l]; }
+            gA[mm][0] += ra; gA[mm][1] += ra * p[mm][0]; gA[mm][2] += ra * p[mm][1];
+            gB[mm][0] += rb; gB[mm][1] += rb * p[mm][0]; gB[mm][2] += rb * p[mm][1];
+        }
     }
 }
 

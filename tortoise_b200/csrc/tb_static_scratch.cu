@@ -15,7 +15,9 @@
 // exits.  Host code must not pass the array's name to a kernel (on the host it
 // is only a stand-in, not a device address); the device address is obtained
 // once per device with cudaGetSymbolAddress while that device is current, on
-// the first call made on that device, and reused afterwards.
+// the first call made on that device, and reused afterwards.  It belongs to
+// the device's primary context: after a cudaDeviceReset the kept address is
+// stale, so a process that resets a device must not call in again there.
 //
 // All calls share the one array, which keeps the last call's contents.  Every
 // entry a call reads is written earlier in the same call, so nothing has to

@@ -118,14 +118,22 @@ __device__ __forceinline__ void walk_item(const ChanDev& c, const StreamDev& sd,
     }
 }
 
-template <int L, bool RATE>
 #ifndef TB_STREAM_MIN_BLOCKS
 #define TB_STREAM_MIN_BLOCKS 1
 #endif
+
+// MODE: ST_PROPAGATE (the collision terms), ST_RATE (rate_leg's scattering
+// rate) or ST_VJP (acc = grad_f += the transposed terms for the co-state co,
+// grad_amp[k] += <co, dC/d amplitude_k>; the stored-list VJP's arithmetic).
+enum { ST_PROPAGATE = 0, ST_RATE = 1, ST_VJP = 2 };
+
+template <int L, int MODE>
 __global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
     k_collision_stream(ChanDev c, StreamDev sd, int64_t it0, int64_t it1, const InstDev* __restrict__ insts,
                        int n_insts, const double* __restrict__ f, double* __restrict__ acc,
-                       const DPCtl* __restrict__ ctl, int rate_leg, FxAcc fx) {
+                       const DPCtl* __restrict__ ctl, int rate_leg, FxAcc fx, const double* __restrict__ co,
+                       double* __restrict__ grad_amp, FxAcc fx_amp) {
+    constexpr bool RATE = MODE == ST_RATE;
     {
         // every instance off or its run finished: nothing to add
         bool any = false;
@@ -193,6 +201,30 @@ __global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
         n_tin += mk ? 1 : 0;
         if (!__any_sync(full, mk != 0ull)) return;
         const bool live = mk != 0ull;
+        if (MODE == ST_VJP) {
+            // k_vjp_mc's terms for the tuples of the list (tf = 1: no functAmplitude)
+            const double scale = live ? 1.0 / (c.fact * double(c.nmc) * fabs(g.det)) : 0.0;
+            for (int k = 0; k < n_insts; ++k) {
+                const InstDev in = insts[k];
+                double gA[L][3], gB[L][3], gamp, sa[L], sb[L];
+                vjp_point_sums<L, true>(c, in, f, co, e, g, Ci, s_mc, mk, live, gA, gB, gamp, sa, sb);
+                if (live) {
+                    const double sc = scale * (in.amp_full * 1.0);
+#pragma unroll
+                    for (int l = 0; l < L; ++l) {
+                        const int64_t key = in.foff[l] + 3 * (int64_t)e[l];
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) {
+                            const double gv = sc * (sa[l] * gA[l][j] + sb[l] * gB[l][j]);
+                            if (fx.w) fx_add(fx, key + j, gv);
+                            else atomicAdd(acc + key + j, gv);
+                        }
+                    }
+                }
+                block_atomic_sum(live ? scale * (c.amp_vol * 1.0) * gamp : 0.0, grad_amp + k, fx_amp, k);
+            }
+            return;
+        }
         const double scale = live ? 1.0 / (inv_fact_nmc * fabs(g.det)) : 0.0;
         for (int k = 0; k < n_insts; ++k) {
             const InstDev in = insts[k];
@@ -302,11 +334,12 @@ __global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
     }
 }
 
-template <int L, bool RATE>
+template <int L, int MODE>
 static int launch_stream(const ChanDev& c, const StreamDev& sd, int64_t it0, int64_t it1, const InstDev* insts,
                          int n_insts, const double* f, double* acc, const DPCtl* ctl, cudaStream_t s, int rate_leg,
-                         const FxAcc& fx) {
-    auto kern = k_collision_stream<L, RATE>;
+                         const FxAcc& fx, const double* co = nullptr, double* grad_amp = nullptr,
+                         const FxAcc& fx_amp = FxAcc{}) {
+    auto kern = k_collision_stream<L, MODE>;
     const int threads = ST_WARPS * 32;
     const size_t smem = 2 * sizeof(double) * size_t(c.nmc) * c.R;
     int dev = 0, nsm = 148, per_sm = 1;
@@ -320,8 +353,8 @@ static int launch_stream(const ChanDev& c, const StreamDev& sd, int64_t it0, int
     const int64_t cap = int64_t(nsm) * per_sm * 8;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) return TB_OK;
-    kern<<<unsigned(blocks), threads, smem, s>>>(c, sd, it0, it1, insts, n_insts, f, acc, ctl, RATE ? rate_leg : -1,
-                                                 fx);
+    kern<<<unsigned(blocks), threads, smem, s>>>(c, sd, it0, it1, insts, n_insts, f, acc, ctl,
+                                                 MODE == ST_RATE ? rate_leg : -1, fx, co, grad_amp, fx_amp);
     TB_CUDA(cudaGetLastError());
     return TB_OK;
 }
@@ -331,15 +364,35 @@ int launch_collision_stream(const ChanDev& c, const StreamDev& sd, int64_t item_
                             cudaStream_t s, int rate_leg, const FxAcc& fx) {
     if (item_end <= item_begin || n_insts <= 0) return TB_OK;
     if (c.nmc > 64) { set_error("streamed channels take at most 64 Monte-Carlo points"); return TB_ERR_ARG; }
-#define TB_ST(LL) \
-    (rate_leg >= 0 ? launch_stream<LL, true>(c, sd, item_begin, item_end, insts, n_insts, f, acc, ctl, s, rate_leg, fx) \
-                   : launch_stream<LL, false>(c, sd, item_begin, item_end, insts, n_insts, f, acc, ctl, s, -1, fx))
+#define TB_ST(LL)                                                                                             \
+    (rate_leg >= 0                                                                                            \
+         ? launch_stream<LL, ST_RATE>(c, sd, item_begin, item_end, insts, n_insts, f, acc, ctl, s, rate_leg, fx) \
+         : launch_stream<LL, ST_PROPAGATE>(c, sd, item_begin, item_end, insts, n_insts, f, acc, ctl, s, -1, fx))
     switch (c.L) {
         case 2: return TB_ST(2);
         case 3: return TB_ST(3);
         case 4: return TB_ST(4);
     }
 #undef TB_ST
+    set_error("nlegs must be 2..4");
+    return TB_ERR_ARG;
+}
+
+int launch_vjp_stream(const ChanDev& c, const StreamDev& sd, int64_t item_begin, int64_t item_end,
+                      const InstDev* insts, int n_insts, const double* f, const double* u, double* grad_f,
+                      double* grad_amp, cudaStream_t s, const FxAcc& fx, const FxAcc& fx_amp) {
+    if (item_end <= item_begin || n_insts <= 0) return TB_OK;
+    if (c.nmc > 64) { set_error("streamed channels take at most 64 Monte-Carlo points"); return TB_ERR_ARG; }
+    StreamDev q = sd;
+    q.counts = nullptr;
+#define TB_SV(LL) launch_stream<LL, ST_VJP>(c, q, item_begin, item_end, insts, n_insts, f, grad_f, nullptr, s, -1, \
+                                            fx, u, grad_amp, fx_amp)
+    switch (c.L) {
+        case 2: return TB_SV(2);
+        case 3: return TB_SV(3);
+        case 4: return TB_SV(4);
+    }
+#undef TB_SV
     set_error("nlegs must be 2..4");
     return TB_ERR_ARG;
 }

@@ -38,4 +38,11 @@ int launch_collision_stream(const ChanDev& c, const StreamDev& sd, int64_t item_
                             const InstDev* insts, int n_insts, const double* f, double* acc, const DPCtl* ctl,
                             cudaStream_t s, int rate_leg, const FxAcc& fx);
 
+// The transposed operator over the same work items: grad_f += C'(f)^T u
+// (or into fx) and grad_amp[k] += <u, dC/d amplitude_k> (or fx_amp slot k)
+// for every instance k -- the stored-list VJP's per-tuple terms.
+int launch_vjp_stream(const ChanDev& c, const StreamDev& sd, int64_t item_begin, int64_t item_end,
+                      const InstDev* insts, int n_insts, const double* f, const double* u, double* grad_f,
+                      double* grad_amp, cudaStream_t s, const FxAcc& fx, const FxAcc& fx_amp);
+
 }  // namespace tb

@@ -12,6 +12,7 @@
 // factors is the sum over legs of (other legs' factors) x (that leg's slope).
 #include "tb_dp45.cuh"
 #include "tb_geom.cuh"
+#include "tb_mcpoint.cuh"
 #include "tb_scatter.cuh"
 #include "tb_tensor.cuh"
 #include "tb_vjp.cuh"
@@ -24,17 +25,6 @@ template <int L> struct VDim {
     static constexpr int NMOM = K * (1 + L);
 };
 
-// Sum over the warp, then one add per warp into dst (exact into slot k of
-// fx in the deterministic mode; the warp's own sum runs in a fixed order over
-// a launch geometry that depends on the tuple count alone).
-__device__ __forceinline__ void block_atomic_sum(double v, double* dst, const FxAcc& fx, int k) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0 && v != 0.0) {
-        if (fx.w) fx_add(fx, k, v);
-        else atomicAdd(dst, v);
-    }
-}
 
 // ---------------------------------------------------------------- M^-T
 __global__ void k_minv_t(ElemDev ed, const double* __restrict__ theta, double* __restrict__ u) {
@@ -71,29 +61,6 @@ int launch_project(const ElemDev& ed, double* v, cudaStream_t s) {
     return TB_OK;
 }
 
-// ----------------------------------------------------------- forms of f
-template <int L>
-__device__ __forceinline__ void leg_forms(const ChanDev& c, const InstDev& in, const double* f, const int (&e)[L],
-                                          double (&A)[L][3], double (&B)[L][3], double (&sa)[L], double (&sb)[L]) {
-#pragma unroll
-    for (int l = 0; l < L; ++l) {
-        const double d = c.leg[l].dir, s = c.leg[l].stat;
-        const double* fe = f + in.foff[l] + 3 * (int64_t)e[l];
-        const double ka = (l == 0 ? -1.0 : 1.0) * 0.5;
-        const double ca = (1. - d) * s + (1. + d);
-        const double cb = (1. + d) * s + (1. - d);
-        sa[l] = ka * ca;    // dA[l][j] / df_j
-        sb[l] = 0.5 * cb;   // dB[l][j] / df_j
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const double unit = (j == 0) ? 1.0 : 0.0;
-            const double fj = __ldg(fe + j);
-            A[l][j] = ka * ((1. - d) * unit + ca * fj);
-            B[l][j] = 0.5 * ((1. + d) * unit + cb * fj);
-        }
-    }
-}
-
 // --------------------------------------------- collision VJP, Monte-Carlo
 // LIST: tup / stride / n describe a ThetaList (tb_theta.cuh) and every tuple
 // visits only the set bits of its mask, the points whose Theta is 1.
@@ -126,52 +93,8 @@ __global__ void __launch_bounds__(128) k_vjp_mc(ChanDev c, const InstDev* __rest
         const uint64_t mk0 = (LIST && valid) ? __ldg(reinterpret_cast<const unsigned long long*>(mask) + i) : 0ull;
         for (int k = 0; k < n_insts; ++k) {
             const InstDev in = insts[k];
-            double A[L][3], B[L][3], sa[L], sb[L];
-            leg_forms<L>(c, in, f, e, A, B, sa, sb);
-            double ul[L][3];
-#pragma unroll
-            for (int l = 0; l < L; ++l)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) ul[l][j] = c.leg[l].dir * __ldg(u + in.foff[l] + 3 * (int64_t)e[l] + j);
-            double gA[L][3], gB[L][3], gamp = 0.0;
-#pragma unroll
-            for (int l = 0; l < L; ++l)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) { gA[l][j] = 0.0; gB[l][j] = 0.0; }
-            if (valid) {
-                uint64_t mk = mk0;
-                for (int m = 0; LIST ? (mk != 0) : (m < c.nmc); ++m) {
-                    if (LIST) {
-                        m = __ffsll((long long)mk) - 1;
-                        mk &= mk - 1;
-                    }
-                    const double* qv = s_mc + m * R;
-                    double p[L][2];
-                    if (!mc_point_exact<L>(g, Ci, qv, p)) continue;
-                    double av[L], bv[L];
-#pragma unroll
-                    for (int l = 0; l < L; ++l) {
-                        av[l] = (A[l][1] * p[l][0] + A[l][2] * p[l][1]) + A[l][0];
-                        bv[l] = (B[l][1] * p[l][0] + B[l][2] * p[l][1]) + B[l][0];
-                    }
-                    double om = 0.0;   // sum over legs of dir * (u . test functions)
-#pragma unroll
-                    for (int l = 0; l < L; ++l) om += ul[l][0] + ul[l][1] * p[l][0] + ul[l][2] * p[l][1];
-                    double pa = 1.0, pb = 1.0;
-#pragma unroll
-                    for (int l = 0; l < L; ++l) { pa *= av[l]; pb *= bv[l]; }
-                    gamp += om * (pa + pb);
-#pragma unroll
-                    for (int mm = 0; mm < L; ++mm) {
-                        double ra = om, rb = om;
-#pragma unroll
-                        for (int l = 0; l < L; ++l)
-                            if (l != mm) { ra *= av[l]; rb *= bv[l]; }
-                        gA[mm][0] += ra; gA[mm][1] += ra * p[mm][0]; gA[mm][2] += ra * p[mm][1];
-                        gB[mm][0] += rb; gB[mm][1] += rb * p[mm][0]; gB[mm][2] += rb * p[mm][1];
-                    }
-                }
-            }
+            double gA[L][3], gB[L][3], gamp, sa[L], sb[L];
+            vjp_point_sums<L, LIST>(c, in, f, u, e, g, Ci, s_mc, mk0, valid, gA, gB, gamp, sa, sb);
             if (valid) {
                 const double sc = scale * (in.amp_full * tf);
 #pragma unroll
