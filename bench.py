@@ -783,9 +783,9 @@ def small_ee_measure(no_cpu=False, no_tune=False, n_mesh=16):
     if not no_cpu:
         import oracle   # the CPU baseline of this case
         ids, umk = eng.tuples(0)
-        # every tuple up to 5e7 (the 16x16 case has 2.6e7: one whole
+        # every tuple up to 1e8 (the 16x16 case has 5.8e7: one whole
         # right-hand side, also the parity reference); beyond, a sample
-        m = len(umk) if len(umk) <= 50_000_000 else 200_000
+        m = len(umk) if len(umk) <= 100_000_000 else 200_000
         o = oracle.Oracle(mat, enumerate_tuples=False, nthreads=os.cpu_count())
         o.set_tuples(0, ids[:m], umk[:m])
         o.channel_propagate(0, f0, 0, min(m, 1000))   # warm-up
@@ -1024,7 +1024,7 @@ def rhs_only(args):
         # quadrature over the points inside the simplices)
         mat = W.parabolic_ee(args.mesh)
         f0 = W.initial_status(mat, kT=0.1, seed=0).vec
-        eng = E.Engine(mat, layout=layout, autotune=not args.no_tune)
+        eng = E.Engine(mat, layout=layout, autotune=not args.no_tune, stream_legs=args.stream_legs)
     elif args.batch:
         # a batch of args.batch runs of one structure (mesh args.mesh): the
         # groups shared by many runs (run-minor contraction)
@@ -1064,6 +1064,8 @@ def main():
     ap.add_argument("--rhs-only", type=int, default=0,
                     help="profiling driver: K RHS evaluations only (with --batch R: R runs of mesh --mesh)")
     ap.add_argument("--mesh", type=int, default=N_MESH, help="sections per side (profiling driver only)")
+    ap.add_argument("--stream-legs", type=int, default=0,
+                    help="profiling driver (--ee): stream the channels with at least this many legs")
     ap.add_argument("--ee", action="store_true",
                     help="profiling driver on the one-band e-e workload (parabolic band, --mesh sections per side)")
     ap.add_argument("--batch", type=int, default=0, help="batched ensemble of this many runs (per-run N, kT, couplings)")

@@ -118,6 +118,42 @@ __device__ __forceinline__ void walk_item(const ChanDev& c, const StreamDev& sd,
     }
 }
 
+// True when no point of the Monte-Carlo domain -- every free leg's point in
+// its reference triangle, the partially constrained leg's coordinate in
+// [0, 1] -- can pass the simplex tests ThetapC * ThetaFC
+// (IntegratorCore.hpp:318-320), whatever the order the constrained
+// coordinates are evaluated in: over the whole domain one of al0, al1, al2
+// stays below 0, or kp0 + al0 or al1 + al2 stays above 1, by more than four
+// times the rounding bound am.mg (which already covers the distance between
+// the fused map and the reference-order evaluation).  Then neither table has
+// a point inside: the survival sum is 0 and the tuple does not survive.
+template <int L>
+__device__ __forceinline__ bool domain_excludes(const AlphaMap<L>& am) {
+    constexpr int R = AlphaMap<L>::R;
+    const double eps = 2.220446049250313e-16;
+    double hi[3];
+    double plo = am.a0[0];                 // min of kp0 + al0
+    double slo = am.a0[1] + am.a0[2];      // min of al1 + al2
+#pragma unroll
+    for (int r = 0; r < 3; ++r) hi[r] = am.a0[r];
+#pragma unroll
+    for (int b = 0; b < L - 2; ++b) {      // free legs: vertices (0,0), (1,0), (0,1)
+#pragma unroll
+        for (int r = 0; r < 3; ++r) hi[r] += fmax(0.0, fmax(am.G[r][2 * b], am.G[r][2 * b + 1]));
+        plo += fmin(0.0, fmin(am.G[0][2 * b], am.G[0][2 * b + 1]));
+        slo += fmin(0.0, fmin(am.G[1][2 * b] + am.G[2][2 * b], am.G[1][2 * b + 1] + am.G[2][2 * b + 1]));
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) hi[r] += fmax(0.0, am.G[r][R - 1]);   // kp0 in [0, 1]
+    plo += fmin(0.0, am.G[0][R - 1] + 1.0);
+    slo += fmin(0.0, am.G[1][R - 1] + am.G[2][R - 1]);
+    const double m0 = 4.0 * am.mg[0], m1 = 4.0 * am.mg[1], m2 = 4.0 * am.mg[2];
+    if (hi[0] < -m0 || hi[1] < -m1 || hi[2] < -m2) return true;
+    if (plo - m0 > 1.0 + 8.0 * eps * (1.0 + fabs(plo))) return true;
+    if (slo - (m1 + m2) > 1.0 + 8.0 * eps * (1.0 + fabs(slo))) return true;
+    return false;
+}
+
 #ifndef TB_STREAM_MIN_BLOCKS
 #define TB_STREAM_MIN_BLOCKS 1
 #endif
@@ -143,7 +179,9 @@ __global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
     }
     constexpr int R = 2 * (L - 2) + 1;
     extern __shared__ double s_tab[];   // [nmc R] quadrature table, then [nmc R] survival table
-    __shared__ int32_t s_q[ST_WARPS][L + 1][ST_QUEUE];
+    // per-warp candidate queues: [0] inside the energy window, [1] past the
+    // determinant filter and the domain test
+    __shared__ int32_t s_q[2][ST_WARPS][L + 1][ST_QUEUE];
     double* s_mc = s_tab;
     double* s_pre = s_tab + c.nmc * R;
     for (int i = threadIdx.x; i < c.nmc * R; i += blockDim.x) {
@@ -160,14 +198,51 @@ __global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
     const double inv_fact_nmc = c.fact * double(c.nmc);
     unsigned long long n_pre = 0, n_det = 0, n_surv = 0, n_pts = 0, n_tin = 0;
 
-    // Evaluates `take` queued candidates from slot `first` on, one per lane.
+    int q2n = 0;   // candidates in queue 1 (warp-uniform)
+
+    // Stage 1 for `take` candidates of queue 0 from slot `first` on, one per
+    // lane: the determinant filter, then the domain test; the candidates that
+    // may have a point inside go to queue 1.  Cheap next to stage 2 (about
+    // 150 operations against 2 x NMC simplex tests), and most candidates of
+    // the energy window end here.
+    auto stage1 = [&](int first, int take) {
+        const bool valid = lane < take;
+        int e[L];
+        int u = 0;
+#pragma unroll
+        for (int l = 0; l < L; ++l) e[l] = valid ? s_q[0][warp][l][first + lane] : 0;
+        if (valid) u = s_q[0][warp][L][first + lane];
+        TupleGeom<L> g;
+        tuple_geometry<L>(c, e, u, g);
+        bool ok = valid && (fabs(g.det) >= c.min_det);
+        n_pre += valid ? 1 : 0;
+        n_det += ok ? 1 : 0;
+        if (ok && c.threshold >= 0.0) {
+            double Ci[3][3];
+            dc_inverse<L>(g, Ci);
+            AlphaMap<L> am;
+            alpha_map<L>(g, Ci, am);
+            ok = !domain_excludes<L>(am);
+        }
+        const unsigned bal = __ballot_sync(full, ok);
+        if (ok) {
+            const int pos = q2n + __popc(bal & ((1u << lane) - 1u));
+#pragma unroll
+            for (int l = 0; l <= L; ++l) s_q[1][warp][l][pos] = l < L ? e[l] : u;
+        }
+        q2n += __popc(bal);
+        __syncwarp();
+    };
+
+    // Stage 2 for `take` candidates of queue 1 from slot `first` on, one per
+    // lane: survival test, mask, sums, scatter.
     auto evaluate = [&](int first, int take) {
         const bool valid = lane < take;
         int e[L];
         int u = 0;
 #pragma unroll
-        for (int l = 0; l < L; ++l) e[l] = valid ? s_q[warp][l][first + lane] : 0;
-        if (valid) u = s_q[warp][L][first + lane];
+        for (int l = 0; l < L; ++l) e[l] = valid ? s_q[1][warp][l][first + lane] : 0;
+        if (valid) u = s_q[1][warp][L][first + lane];
         TupleGeom<L> g;
         tuple_geometry<L>(c, e, u, g);
         bool ok = valid && (fabs(g.det) >= c.min_det);
@@ -184,8 +259,6 @@ __global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
         }
         double res = (1.0 / (c.fact * double(c.nmc) * fabs(g.det))) * sum;
         res *= c.amp_vol;
-        n_pre += valid ? 1 : 0;
-        n_det += ok ? 1 : 0;
         ok = ok && (fabs(res) > c.threshold);
         n_surv += ok ? 1 : 0;
         // the points inside the simplices on the quadrature table (k_theta_mask's)
@@ -301,20 +374,30 @@ __global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
             if (pass) {
                 const int pos = qn + __popc(bal & ((1u << lane) - 1u));
 #pragma unroll
-                for (int l = 0; l < L - 1; ++l) s_q[warp][l][pos] = e[l];
-                s_q[warp][L - 1][pos] = el;
-                s_q[warp][L][pos] = u;
+                for (int l = 0; l < L - 1; ++l) s_q[0][warp][l][pos] = e[l];
+                s_q[0][warp][L - 1][pos] = el;
+                s_q[0][warp][L][pos] = u;
             }
             qn += __popc(bal);
             __syncwarp();
             if (qn >= 32) {
-                evaluate(qn - 32, 32);
+                stage1(qn - 32, 32);
                 qn -= 32;
+                if (q2n >= 32) {
+                    evaluate(q2n - 32, 32);
+                    q2n -= 32;
+                }
                 __syncwarp();   // the slots are reused
             }
         }
     }
-    if (qn > 0) evaluate(0, qn);
+    if (qn > 0) stage1(0, qn);
+    if (q2n >= 32) {
+        evaluate(q2n - 32, 32);
+        q2n -= 32;
+        __syncwarp();
+    }
+    if (q2n > 0) evaluate(0, q2n);
     if (sd.counts) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
