@@ -248,22 +248,24 @@ __global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
         bool ok = valid && (fabs(g.det) >= c.min_det);
         double Ci[3][3];
         dc_inverse<L>(g, Ci);
-        // survival test of precalculateIndices on the survival table (k_enumerate's)
+        AlphaMap<L> am;
+        alpha_map<L>(g, Ci, am);
+        // survival test of precalculateIndices on the survival table: the
+        // count of k_enumerate's, with each point's simplex decision taken
+        // the way k_theta_mask takes it (the fused map, re-evaluated in the
+        // reference's order near a face: the same decisions, at a third of
+        // the cost of evaluating every point in that order)
         double sum = 0.0;
-        {
-            double p[L][2];
-            for (int m = 0; m < c.nmc; ++m) {
-                const bool th = mc_point_exact<L>(g, Ci, s_pre + m * R, p);
-                sum += th ? prodc : 0.0;
-            }
+        for (int m = 0; m < c.nmc; ++m) {
+            double al[3];
+            const bool th = alpha_theta<L>(g, Ci, am, s_pre + m * R, al);
+            sum += th ? prodc : 0.0;
         }
         double res = (1.0 / (c.fact * double(c.nmc) * fabs(g.det))) * sum;
         res *= c.amp_vol;
         ok = ok && (fabs(res) > c.threshold);
         n_surv += ok ? 1 : 0;
         // the points inside the simplices on the quadrature table (k_theta_mask's)
-        AlphaMap<L> am;
-        alpha_map<L>(g, Ci, am);
         uint64_t mk = 0;
         if (ok)
             for (int m = 0; m < c.nmc; ++m) {
