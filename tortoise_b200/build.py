@@ -40,17 +40,25 @@ def nvcc():
     return "nvcc"
 
 
-def build(verbose=False, extra=()):
-    os.makedirs(BUILD, exist_ok=True)
-    objs = []
+def build(verbose=False, extra=(), out=OUT, build_dir=BUILD):
+    """Compiles every source (in parallel, one nvcc per source) and links
+    the shared library `out`."""
+    from concurrent.futures import ThreadPoolExecutor
+    os.makedirs(build_dir, exist_ok=True)
+    cmds, objs = [], []
     for src, flags in SOURCES.items():
-        obj = os.path.join(BUILD, src.replace(".cu", ".o"))
-        cmd = [nvcc(), *ARCH, *COMMON, *flags, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.check_call(cmd)
+        obj = os.path.join(build_dir, src.replace(".cu", ".o"))
+        cmds.append([nvcc(), *ARCH, *COMMON, *flags, *extra, "-c", os.path.join(CSRC, src), "-o", obj])
         objs.append(obj)
-    cmd = [nvcc(), *ARCH, "-shared", "-o", OUT, *objs, "-lcudart", "-ldl"]
+    if verbose:
+        for cmd in cmds:
+            print(" ".join(cmd))
+    # the largest sources first, so the slowest compiles start at once
+    order = sorted(range(len(cmds)), key=lambda k: -os.path.getsize(cmds[k][-3]))
+    with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as pool:
+        for f in [pool.submit(subprocess.check_call, cmds[k]) for k in order]:
+            f.result()
+    cmd = [nvcc(), *ARCH, "-shared", "-o", out, *objs, "-lcudart", "-ldl"]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)

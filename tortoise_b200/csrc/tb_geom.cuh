@@ -129,6 +129,10 @@ struct AlphaMap {
     double G[3][R], a0[3], mg[3];
 };
 
+// Every product-sum is written as explicit fused multiply-adds in a fixed
+// order, so the map (and everything the quadrature computes from it) has the
+// same bits in every kernel that builds it, whatever the compiler would
+// contract on its own.
 template <int L>
 __device__ __forceinline__ void alpha_map(const TupleGeom<L>& g, const double (&Ci)[3][3], AlphaMap<L>& am) {
     constexpr int R = AlphaMap<L>::R;
@@ -142,14 +146,14 @@ __device__ __forceinline__ void alpha_map(const TupleGeom<L>& g, const double (&
     }
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-        am.a0[r] = Ci[r][0] * g.N[0] + Ci[r][1] * g.N[1] + Ci[r][2] * g.N[2];
+        am.a0[r] = fma(Ci[r][2], g.N[2], fma(Ci[r][1], g.N[1], __dmul_rn(Ci[r][0], g.N[0])));
         double sg = 0.0;
 #pragma unroll
         for (int j = 0; j < R; ++j) {
-            am.G[r][j] = -(Ci[r][0] * g.D[0][j] + Ci[r][1] * g.D[1][j] + Ci[r][2] * g.D[2][j]);
+            am.G[r][j] = -fma(Ci[r][2], g.D[2][j], fma(Ci[r][1], g.D[1][j], __dmul_rn(Ci[r][0], g.D[0][j])));
             sg += fabs(am.G[r][j]);
         }
-        const double sc = fabs(Ci[r][0]) * rho[0] + fabs(Ci[r][1]) * rho[1] + fabs(Ci[r][2]) * rho[2];
+        const double sc = fma(fabs(Ci[r][2]), rho[2], fma(fabs(Ci[r][1]), rho[1], __dmul_rn(fabs(Ci[r][0]), rho[0])));
         am.mg[r] = 32.0 * 1.1102230246251565e-16 * (sc + fabs(am.a0[r]) + sg);
     }
 }
@@ -182,6 +186,27 @@ __device__ __forceinline__ bool alpha_theta(const TupleGeom<L>& g, const double 
                       (fabs(al[1] + al[2] - 1.0) <= am.mg[1] + am.mg[2] + tiny * (1.0 + fabs(al[1]) + fabs(al[2])));
     if (near) exact_alpha<L>(g, Ci, qv, al);
     return theta_of(kp0, al);
+}
+
+// The decision of alpha_theta for point qv without its coordinates: a point
+// whose fused coordinates already violate a simplex test by more than the
+// rounding bound is outside whatever the evaluation order (the exact value
+// lies within the bound of the fused one), so it is decided after the fused
+// map alone; every other point goes through alpha_theta.  Most points of a
+// tuple that does not survive are decided that way.
+template <int L>
+__device__ __forceinline__ bool theta_decide(const TupleGeom<L>& g, const double (&Ci)[3][3], const AlphaMap<L>& am,
+                                             const double* qv) {
+    constexpr int R = AlphaMap<L>::R;
+    double al[3];
+    alpha_fast<L>(am, qv, al);
+    const double kp0 = qv[R - 1];
+    const double tiny = 8.0 * 1.1102230246251565e-16;
+    const bool out = (al[0] < -am.mg[0]) || (al[1] < -am.mg[1]) || (al[2] < -am.mg[2]) ||
+                     (kp0 + al[0] - 1.0 > am.mg[0] + tiny * (2.0 + fabs(al[0]))) ||
+                     (al[1] + al[2] - 1.0 > am.mg[1] + am.mg[2] + tiny * (1.0 + fabs(al[1]) + fabs(al[2])));
+    if (out) return false;
+    return alpha_theta<L>(g, Ci, am, qv, al);
 }
 
 // Constrained coordinates of one MC point q (row of the MC table),

@@ -43,6 +43,8 @@ __device__ __forceinline__ void inside_point_sums(const ChanDev& c, const AlphaM
         for (int l = 0; l < L - 2; ++l) { px[l] = qv[2 * l]; py[l] = qv[2 * l + 1]; }
         px[L - 2] = qv[R - 1]; py[L - 2] = al[0];
         px[L - 1] = al[1]; py[L - 1] = al[2];
+        // explicit products and sum: no contraction the compiler could choose
+        // differently in another kernel
         double pa = 1.0, pb = 1.0;
 #pragma unroll
         for (int l = 0; l < L; ++l) {
@@ -52,15 +54,15 @@ __device__ __forceinline__ void inside_point_sums(const ChanDev& c, const AlphaM
                 // scattering rate of this leg: constant in / out unit forms
                 // (ScatteringChannel.cpp:562-564)
                 const double d = c.leg[l].dir, st = c.leg[l].stat;
-                fa = (l == 0 ? -1.0 : 1.0) * ((1. - d) * st + (1. + d));
-                fb = (1. + d) * st + (1. - d);
+                fa = (l == 0 ? -1.0 : 1.0) * __dadd_rn(__dmul_rn(1. - d, st), 1. + d);
+                fb = __dadd_rn(__dmul_rn(1. + d, st), 1. - d);
                 fa0 = 0.0;
                 fb0 = 0.0;
             }
-            pa *= fma(fa, t, fa0);
-            pb *= fma(fb, t, fb0);
+            pa = __dmul_rn(pa, fma(fa, t, fa0));
+            pb = __dmul_rn(pb, fma(fb, t, fb0));
         }
-        return pa + pb;
+        return __dadd_rn(pa, pb);
     };
     auto accumulate = [&](double common, const double (&px)[L], const double (&py)[L]) {
         s0 += common;
@@ -147,27 +149,33 @@ __device__ __forceinline__ void vjp_point_sums(const ChanDev& c, const InstDev& 
         const double* qv = s_mc + m * R;
         double p[L][2];
         if (!mc_point_exact<L>(g, Ci, qv, p)) continue;
+        // every product-sum as explicit fused multiply-adds or rounded
+        // operations: the same bits in every kernel that runs this
         double av[L], bv[L];
 #pragma unroll
         for (int l = 0; l < L; ++l) {
-            av[l] = (A[l][1] * p[l][0] + A[l][2] * p[l][1]) + A[l][0];
-            bv[l] = (B[l][1] * p[l][0] + B[l][2] * p[l][1]) + B[l][0];
+            av[l] = __dadd_rn(fma(A[l][2], p[l][1], __dmul_rn(A[l][1], p[l][0])), A[l][0]);
+            bv[l] = __dadd_rn(fma(B[l][2], p[l][1], __dmul_rn(B[l][1], p[l][0])), B[l][0]);
         }
         double om = 0.0;   // sum over legs of dir * (u . test functions)
 #pragma unroll
-        for (int l = 0; l < L; ++l) om += ul[l][0] + ul[l][1] * p[l][0] + ul[l][2] * p[l][1];
+        for (int l = 0; l < L; ++l) om = __dadd_rn(om, fma(ul[l][2], p[l][1], fma(ul[l][1], p[l][0], ul[l][0])));
         double pa = 1.0, pb = 1.0;
 #pragma unroll
-        for (int l = 0; l < L; ++l) { pa *= av[l]; pb *= bv[l]; }
-        gamp += om * (pa + pb);
+        for (int l = 0; l < L; ++l) { pa = __dmul_rn(pa, av[l]); pb = __dmul_rn(pb, bv[l]); }
+        gamp = fma(om, __dadd_rn(pa, pb), gamp);
 #pragma unroll
         for (int mm = 0; mm < L; ++mm) {
             double ra = om, rb = om;
 #pragma unroll
             for (int l = 0; l < L; ++l)
-                if (l != mm) { ra *= av[l]; rb *= bv[l]; }
-            gA[mm][0] += ra; gA[mm][1] += ra * p[mm][0]; gA[mm][2] += ra * p[mm][1];
-            gB[mm][0] += rb; gB[mm][1] += rb * p[mm][0]; gB[mm][2] += rb * p[mm][1];
+                if (l != mm) { ra = __dmul_rn(ra, av[l]); rb = __dmul_rn(rb, bv[l]); }
+            gA[mm][0] = __dadd_rn(gA[mm][0], ra);
+            gA[mm][1] = fma(ra, p[mm][0], gA[mm][1]);
+            gA[mm][2] = fma(ra, p[mm][1], gA[mm][2]);
+            gB[mm][0] = __dadd_rn(gB[mm][0], rb);
+            gB[mm][1] = fma(rb, p[mm][0], gB[mm][1]);
+            gB[mm][2] = fma(rb, p[mm][1], gB[mm][2]);
         }
     }
 }

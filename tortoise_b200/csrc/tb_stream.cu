@@ -245,7 +245,8 @@ __global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
         if (valid) u = s_q[1][warp][L][first + lane];
         TupleGeom<L> g;
         tuple_geometry<L>(c, e, u, g);
-        bool ok = valid && (fabs(g.det) >= c.min_det);
+        const double adet = fabs(g.det);
+        bool ok = valid && (adet >= c.min_det);
         double Ci[3][3];
         dc_inverse<L>(g, Ci);
         AlphaMap<L> am;
@@ -253,25 +254,19 @@ __global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
         // survival test of precalculateIndices on the survival table: the
         // count of k_enumerate's, with each point's simplex decision taken
         // the way k_theta_mask takes it (the fused map, re-evaluated in the
-        // reference's order near a face: the same decisions, at a third of
+        // reference's order near a face: the same decisions, at a fraction of
         // the cost of evaluating every point in that order)
         double sum = 0.0;
-        for (int m = 0; m < c.nmc; ++m) {
-            double al[3];
-            const bool th = alpha_theta<L>(g, Ci, am, s_pre + m * R, al);
-            sum += th ? prodc : 0.0;
-        }
-        double res = (1.0 / (c.fact * double(c.nmc) * fabs(g.det))) * sum;
+        for (int m = 0; m < c.nmc; ++m) sum += theta_decide<L>(g, Ci, am, s_pre + m * R) ? prodc : 0.0;
+        double res = (1.0 / (c.fact * double(c.nmc) * adet)) * sum;
         res *= c.amp_vol;
         ok = ok && (fabs(res) > c.threshold);
         n_surv += ok ? 1 : 0;
         // the points inside the simplices on the quadrature table (k_theta_mask's)
         uint64_t mk = 0;
         if (ok)
-            for (int m = 0; m < c.nmc; ++m) {
-                double al[3];
-                if (alpha_theta<L>(g, Ci, am, s_mc + m * R, al)) mk |= 1ull << m;
-            }
+            for (int m = 0; m < c.nmc; ++m)
+                if (theta_decide<L>(g, Ci, am, s_mc + m * R)) mk |= 1ull << m;
         n_pts += __popcll(mk);
         n_tin += mk ? 1 : 0;
         if (!__any_sync(full, mk != 0ull)) return;
@@ -290,7 +285,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
                         const int64_t key = in.foff[l] + 3 * (int64_t)e[l];
 #pragma unroll
                         for (int j = 0; j < 3; ++j) {
-                            const double gv = sc * (sa[l] * gA[l][j] + sb[l] * gB[l][j]);
+                            const double gv = __dmul_rn(sc, fma(sb[l], gB[l][j], __dmul_rn(sa[l], gA[l][j])));
                             if (fx.w) fx_add(fx, key + j, gv);
                             else atomicAdd(acc + key + j, gv);
                         }
@@ -300,7 +295,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
             }
             return;
         }
-        const double scale = live ? 1.0 / (inv_fact_nmc * fabs(g.det)) : 0.0;
+        const double scale = live ? 1.0 / (inv_fact_nmc * adet) : 0.0;
         for (int k = 0; k < n_insts; ++k) {
             const InstDev in = insts[k];
             if (in.amp_full == 0.0) continue;

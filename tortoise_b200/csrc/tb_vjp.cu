@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(128) k_vjp_mc(ChanDev c, const InstDev* __rest
                     double* o = grad_f + key;
 #pragma unroll
                     for (int j = 0; j < 3; ++j) {
-                        const double g = sc * (sa[l] * gA[l][j] + sb[l] * gB[l][j]);
+                        const double g = __dmul_rn(sc, fma(sb[l], gB[l][j], __dmul_rn(sa[l], gA[l][j])));
                         if (fx.w) fx_add(fx, key + j, g);
                         else atomicAdd(o + j, g);
                     }
