@@ -1024,9 +1024,11 @@ def ee_full(args):
         per_channel.append(ev0.elapsed_time(ev1))
         infos.append(eng.channel_info(c))
         inside.append(eng.points_inside(c))
-    w0 = time.perf_counter()
-    eng.rhs(f0)   # one whole right-hand side from host buffers
-    t_rhs_host = time.perf_counter() - w0
+    t_rhs_host = None
+    if not args.ee_once:
+        w0 = time.perf_counter()
+        eng.rhs(f0)   # one whole right-hand side from host buffers
+        t_rhs_host = time.perf_counter() - w0
     ee_idx = [c for c in range(nch) if mat.channels[c].nlegs == 4]
     line = {"ee_full": True, "workload": "2-band e-e + e-ph + drift, %dx%d mesh (%d triangles/band), NMC=50, "
                                          "rtol 1e-8" % (N, N, 2 * N * N),
@@ -1136,6 +1138,8 @@ def main():
     ap.add_argument("--ee-full", type=int, default=0,
                     help="the two-band workload with its e-e channels (streamed) on an N x N mesh: collision time "
                          "per RHS and --steps DP45 attempts")
+    ap.add_argument("--ee-once", action="store_true",
+                    help="--ee-full: one collision evaluation per channel only, no whole RHS from host buffers")
     ap.add_argument("--adjoint-ee", type=int, default=0,
                     help="adjoint of the two-band workload with its e-e channels (streamed) on an N x N mesh")
     ap.add_argument("--adjoint-t1", type=float, default=0.02, help="end time of --adjoint-ee")
