@@ -565,16 +565,23 @@ def batched_to_end(n_runs, tune=True):
                       "run_attempts": int(att.sum()), "attempts_per_run": [int(att.min()), int(np.median(att)),
                                                                           int(att.max())],
                       "run_attempts_per_s": float(att.sum() / (w1 - w0)), "clocks": clk.summary()}
+        arms[name]["dense_outputs_per_run"] = [int(min(len(x["dense"]) for x in r["runs"])),
+                                               int(max(len(x["dense"]) for x in r["runs"]))]
+        print(json.dumps({"arm": name, **{k: arms[name][k] for k in ("seconds", "rc", "statuses",
+                                                                     "dense_outputs_per_run")}}),
+              file=sys.stderr, flush=True)
         dense[name] = [x["dense"] for x in r["runs"]]
         attempts[name] = att
         if name == "f64":
             attempts_f64 = att
         be.close()
-    det_equal = all(np.array_equal(a, b) for da, db in zip(dense["f64_det"], dense["f64_det_repeat"])
-                    for a, b in zip(da, db)) and np.array_equal(attempts["f64_det"], attempts["f64_det_repeat"])
+    det_equal = (arms["f64_det"]["rc"] == 0 and arms["f64_det_repeat"]["rc"] == 0
+                 and all(len(da) == len(db) > 0 and all(np.array_equal(a, b) for a, b in zip(da, db))
+                         for da, db in zip(dense["f64_det"], dense["f64_det_repeat"]))
+                 and np.array_equal(attempts["f64_det"], attempts["f64_det_repeat"]))
     for name in ("t40", "t48", "f64_repeat", "f64_det", "t48_det"):
         base = "f64_det" if name == "t48_det" else "f64"
-        per_run = [max(float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(da, db))
+        per_run = [max((float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(da, db)), default=np.inf)
                    for da, db in zip(dense[name], dense[base])]
         if name == "t48_det":
             arms[name]["error_vs"] = "f64_det"

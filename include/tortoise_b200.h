@@ -160,9 +160,14 @@ typedef struct tb_options {
                                      per-tuple values only -- not on thread arrival order,
                                      launch geometry or the contraction schedule.  Slower;
                                      24 more bytes of device memory per dof (and per slot of
-                                     a run-minor group's accumulator).  The reference's TBB
-                                     reduce (ScatteringChannel.cpp:651-670) is itself not
-                                     reproducible across thread schedules. */
+                                     a run-minor group's accumulator).  A non-finite
+                                     contribution makes the whole evaluation NaN; a finite one
+                                     of magnitude 2^64 or more is clamped to that range (the
+                                     huge trial stage of a step that its error norm rejects),
+                                     and tb_rhs, tb_scattering_rates, tb_synchronize, the VJP
+                                     and the adjoint sweep then return TB_ERR_NONFINITE.  The
+                                     reference's TBB reduce (ScatteringChannel.cpp:651-670) is
+                                     itself not reproducible across thread schedules. */
     int32_t stream_legs;          /* 2..4: every channel with at least this many legs whose tuples the
                                      library enumerates (n_tuples == 0) keeps no tuple list: each
                                      evaluation walks the candidates of precalculateIndices

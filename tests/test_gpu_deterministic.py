@@ -181,3 +181,50 @@ def test_non_finite_input_poisons_the_whole_sum(gpu_lib):
         assert np.array_equal(e.rhs(f0), e.rhs(f0)) and np.all(np.isfinite(e.rhs(f0)))
     finally:
         e.close()
+
+
+def test_out_of_range_contribution_is_clamped_and_reported(gpu_lib):
+    """A finite contribution of magnitude 2^64 or more (here: a state scaled
+    by 1e20, whose quadratic terms reach 1e40) is clamped to the exact
+    accumulator's range: the operator reports TB_ERR_NONFINITE, the handle
+    stays usable and its next evaluation has the bits of a fresh one.  The
+    FP64-atomic mode returns the finite huge values."""
+    mat, f0 = _setup("eph_n4")
+    e = E.Engine(mat, layout=E.LAYOUT_T64, deterministic=True)
+    plain = E.Engine(mat, layout=E.LAYOUT_T64)
+    try:
+        ref = e.rhs(f0)
+        with pytest.raises(E.TortoiseError, match="2\\^64"):
+            e.rhs(f0 * 1e20)
+        assert np.array_equal(e.rhs(f0), ref)
+        big = plain.rhs(f0 * 1e20)
+        assert np.all(np.isfinite(big)) and np.max(np.abs(big)) > 1e30
+    finally:
+        e.close()
+        plain.close()
+
+
+def test_ensemble_with_an_oversized_first_step(gpu_lib):
+    """Dense step 2 on the ensemble: the first attempts take steps far too
+    large, whose trial stages blow up past 2^64 before the error norm
+    rejects them.  In the deterministic mode the clamped stages are rejected
+    like the FP64 ones: every run reaches t = 4, two batches agree bit for
+    bit, and the FP64-atomic batch's dense outputs (t = 2, 4) agree to its
+    own tolerance (the final states lie at each run's last step, past t = 4
+    by different amounts)."""
+    mats, states = W.ensemble_runs(16, seed=5, Ns=(16,))
+    f = np.concatenate(states)
+    out = []
+    for det in (True, True, False):
+        be = E.BatchEngine(mats, layout=E.LAYOUT_T64, deterministic=det)
+        try:
+            out.append(be.dp45(f, 0.0, 4.0, 2.0, max_dense=4))
+        finally:
+            be.close()
+    a, b, p = out
+    for r in (a, b, p):
+        assert r["rc"] == 0 and all(x["status"] == 0 and x["t"] >= 4.0 for x in r["runs"])
+    assert np.array_equal(a["y"], b["y"])
+    for x, y in zip(a["runs"], p["runs"]):
+        assert len(x["dense"]) == len(y["dense"]) >= 2
+        assert rel_l2(x["dense"], y["dense"]) < 1e-6

@@ -136,6 +136,7 @@ static int adj_base(tb_handle* h) {
             TB_CUDA(cudaMemset(p3, 0, sizeof(double) * size_t(3 * std::max(A->n_slots, 1) + 1)));
             A->gamp_fx.w = reinterpret_cast<unsigned long long*>(p3);
             A->gamp_fx.poison = reinterpret_cast<unsigned int*>(A->gamp_fx.w + 3 * std::max(A->n_slots, 1));
+            A->gamp_fx.sat = h->fx.sat;   // one sticky flag per handle
         }
     }
     void* p = nullptr;
@@ -458,6 +459,9 @@ int tb_adjoint_rhs_vjp(tb_handle* h, const double* f, const double* theta, doubl
     TB_CUDA(cudaMemsetAsync(A->g, 0, bytes, h->stream));
     if (grad_amp) TB_TRY(copy_gamp_out(h, grad_amp));
     else TB_TRY(stream_wait(h));
+    bool clamped = false;
+    TB_TRY(fx_take_saturation(h, clamped));
+    if (clamped) return fx_saturation_error();
     return TB_OK;
 }
 
@@ -602,6 +606,9 @@ int tb_adjoint_backward(tb_handle* h, const double* lambda_T, double* grad_f0, d
     if (A->gamp_fx.w)   // a sweep that failed half-way may have left words behind
         TB_CUDA(cudaMemsetAsync(A->gamp_fx.w, 0, sizeof(double) * size_t(3 * std::max(A->n_slots, 1) + 1), h->stream));
     TB_CUDA(cudaMemsetAsync(h->d_acc, 0, bytes, h->stream));
+    // the forward sweep's rejected trial stages may have clamped; the
+    // backward sweep only replays accepted steps, where a clamp is an error
+    if (h->fx.sat) TB_CUDA(cudaMemsetAsync(h->fx.sat, 0, sizeof(unsigned int), h->stream));
     double* const* dD = A->dD;
     const int64_t nd = A->n_steps - 1;   // the dense-output step
     int64_t rhs = 0;
@@ -656,6 +663,9 @@ int tb_adjoint_backward(tb_handle* h, const double* lambda_T, double* grad_f0, d
     int tflag = 0;
     TB_TRY(take_wait_timeout(h->d_err, h->stream, &tflag));
     if (tflag) { set_error("moment-tensor copy wait ran out"); return TB_ERR_TIMEOUT; }
+    bool clamped = false;
+    TB_TRY(fx_take_saturation(h, clamped));
+    if (clamped) return fx_saturation_error();
     if (st) {
         std::memset(st, 0, sizeof(*st));
         st->t_obs = A->t_obs;

@@ -120,7 +120,10 @@ int fx_alloc(tb_handle* h, int64_t n, FxAcc& out) {
     h->dev_raw.push_back(p);
     TB_CUDA(cudaMemset(p, 0, bytes));
     out.w = static_cast<unsigned long long*>(p);
+    // the last word: the poison flag (cleared by every flush), then the
+    // sticky saturation flag (cleared by the host when it reports it)
     out.poison = reinterpret_cast<unsigned int*>(out.w + 3 * n);
+    out.sat = out.poison + 1;
     return TB_OK;
 }
 
@@ -799,6 +802,26 @@ void fill_stats(const DPCtl& c, tb_dp45_stats* st) {
     st->done = c.done;
 }
 
+// Deterministic mode: was a contribution clamped to the exact accumulator's
+// range since the flag was last cleared?  Reading clears it.
+int fx_take_saturation(tb_handle* h, bool& clamped) {
+    clamped = false;
+    if (!h->fx.sat) return TB_OK;
+    unsigned int v = 0;
+    TB_CUDA(cudaMemcpyAsync(&v, h->fx.sat, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+    TB_CUDA(cudaStreamSynchronize(h->stream));
+    if (v) {
+        clamped = true;
+        TB_CUDA(cudaMemsetAsync(h->fx.sat, 0, sizeof(v), h->stream));
+    }
+    return TB_OK;
+}
+
+int fx_saturation_error() {
+    set_error("deterministic mode: a contribution of magnitude 2^64 or more was clamped to the exact accumulator's "
+              "range; the result is unreliable");
+    return TB_ERR_NONFINITE;
+}
 }  // namespace tb
 
 // ====================================================================== C API
@@ -1178,6 +1201,9 @@ static int check_wait_timeout(tb_handle* h) {
         set_error("a moment-tensor contraction gave up waiting for its staged tiles; the result is incomplete");
         return TB_ERR_TIMEOUT;
     }
+    bool clamped = false;
+    TB_TRY(tb::fx_take_saturation(h, clamped));
+    if (clamped) return tb::fx_saturation_error();
     return TB_OK;
 }
 
@@ -1333,6 +1359,9 @@ int dp_begin(tb_handle* h, const double* f0, const double* t0, const double* t_f
     const int rflags = flags & (TB_NO_DRIFT | TB_NO_COLLISIONS);
     h->dp_flags = flags;
     h->wait_timed_out = false;
+    // clamped contributions of trial stages are rejected by the step's own
+    // error norm; the integration does not report them
+    if (h->fx.sat) TB_CUDA(cudaMemsetAsync(h->fx.sat, 0, sizeof(unsigned int), h->stream));
     const size_t bytes = sizeof(double) * size_t(h->ndofs);
     DPBufs& B = h->dp;
     {
@@ -1457,6 +1486,7 @@ int tb_dp45_end(tb_handle* h, double* f_out, double* dense_out, double* dense_ti
         utoff += max_dense;
     }
     TB_TRY(stream_wait(h));
+    if (h->fx.sat) TB_CUDA(cudaMemsetAsync(h->fx.sat, 0, sizeof(unsigned int), h->stream));
     if (st) *st = s;
     int worst = TB_OK;
     for (size_t r = 0; r < h->runs.size(); ++r)

@@ -24,10 +24,15 @@
 // that of an FP64 sum: each contribution is off by at most 2^-113, the sum is
 // exact, and only the final conversion rounds.
 //
-// A non-finite contribution, or one of magnitude 2^64 or more, cannot be
-// represented: it sets the buffer's poison word, and the flush then writes
-// NaN into every coefficient, which the integrator reports as
-// TB_ERR_NONFINITE.
+// A non-finite contribution cannot be represented: it sets the buffer's
+// poison word, and the flush then writes NaN into every coefficient, which
+// the integrator reports as TB_ERR_NONFINITE.  A finite contribution of
+// magnitude 2^64 or more (a trial stage of a step far too large, on its way
+// to rejection) is clamped to the largest double below 2^64 with its sign
+// and sets the saturation word: the sum stays exact and deterministic, the
+// coefficient stays huge (so the step's error norm rejects it, as it rejects
+// the unclamped FP64 value), and the host paths that return an operator
+// report the clamping as an error.
 //
 // The functions compile for the host too (the CPU tests exercise the
 // conversions and the order independence through a host build).
@@ -175,7 +180,11 @@ TB_HD void fx_add_plain(unsigned long long* p, const Fx& x) {
 struct FxAcc {
     unsigned long long* w = nullptr;
     unsigned int* poison = nullptr;
+    unsigned int* sat = nullptr;   // sticky: a contribution was clamped (null: poison instead)
 };
+
+// The largest double below 2^64: the clamp of out-of-range contributions.
+constexpr double FX_CLAMP = 18446744073709549568.0;   // 2^64 - 2^11
 
 #ifdef __CUDACC__
 // p[0..2] += x with atomics, exact for any interleaving with other adds.
@@ -198,8 +207,12 @@ __device__ __forceinline__ void fx_atomic_add(unsigned long long* p, const Fx& x
 __device__ __forceinline__ void fx_add(const FxAcc& a, int64_t slot, double v) {
     Fx x;
     if (!fx_of(v, x)) {
-        atomicOr(a.poison, 1u);
-        return;
+        if (!isfinite(v) || !a.sat) {
+            atomicOr(a.poison, 1u);
+            return;
+        }
+        atomicOr(a.sat, 1u);
+        fx_of(v < 0.0 ? -FX_CLAMP : FX_CLAMP, x);
     }
     if (x.w0 | x.w1 | x.w2) fx_atomic_add(a.w + 3 * slot, x);
 }

@@ -130,6 +130,9 @@ void adjoint_release(tb_handle* h);
 // A zeroed exact accumulator of n slots (3 words each) plus its poison word,
 // owned by the handle (deterministic mode).
 int fx_alloc(tb_handle* h, int64_t n, FxAcc& out);
+// deterministic mode's clamp flag: read (and clear) it; the error it reports
+int fx_take_saturation(tb_handle* h, bool& clamped);
+int fx_saturation_error();
 
 // tb_shard.cu
 int64_t shard_begin(int64_t n, int rank, int n_ranks);

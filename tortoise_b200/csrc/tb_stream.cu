@@ -22,12 +22,14 @@
 // (tb_mcpoint.cuh), so a streamed evaluation adds the same per-tuple values
 // as the stored-list path.
 //
-// Work distribution: a warp takes 32 work items (one per lane); the lanes
-// step through their boxes in lock step and push the candidates that pass
-// the energy window into a per-warp queue in shared memory; every 32 queued
-// candidates the warp evaluates them one per lane (determinant, survival,
-// mask, sums, scatter), so the heavy part runs on full warps whatever the box
-// sizes and the window's pass rate.
+// Work distribution: a warp walks runs of consecutive work items, 32 at a
+// time (one per lane); the lanes step through their boxes in lock step and
+// push the candidates that pass the energy window into a per-warp queue in
+// shared memory.  Three stages drain the queues, each on 32 entries at a
+// time, one per lane: determinant filter and domain test (queue 0 -> 1), the
+// survival test (queue 1 -> 2), then the points inside, the sums and the
+// scatter for the surviving tuples.  So every stage runs on full warps
+// whatever the box sizes and the pass rate of the stage before.
 #include "tb_dp45.cuh"
 #include "tb_mcpoint.cuh"
 #include "tb_scatter.cuh"
@@ -37,6 +39,7 @@ namespace tb {
 
 constexpr int ST_WARPS = 8;    // warps per block
 constexpr int ST_QUEUE = 64;   // candidate slots per warp (31 left over + 32 pushed at most)
+constexpr int ST_SPAN = 16;    // steps of 32 consecutive items per run of a warp
 
 struct WBox {
     double l[2], h[2];
@@ -71,39 +74,104 @@ __device__ __forceinline__ WBox walk_box_scale(WBox b, double s) {
     return b;
 }
 
-// Work item -> sections and elements of legs 0..L-2, umklapp column and the
-// section range [lo, hi) of the last leg's box (empty when lo == hi in a
-// dimension).  Decoding and box arithmetic of k_enumerate, term for term.
+// A lane's place in the work-item numbering, as digits (least significant
+// first): the element choice, then for legs L-2 .. 0 the section's x and y,
+// then the umklapp column.  A warp walks runs of consecutive items, so most
+// steps change the last digits only: the box sums of the legs in front
+// (legs 0..L-3) and their energies are kept from the previous item.
 template <int L>
-__device__ __forceinline__ void walk_item(const ChanDev& c, const StreamDev& sd, int64_t item, int (&e)[L], int& u,
-                                          int (&lo)[2], int (&hi)[2]) {
+struct WalkPos {
+    int comb, u;
+    int sx[TB_MAX_LEGS], sy[TB_MAX_LEGS];
+};
+
+template <int L>
+__device__ __forceinline__ void walk_decode(const StreamDev& sd, int64_t item, WalkPos<L>& p) {
     constexpr int C = 1 << (L - 1);
-    const int comb = int(item % C);
+    p.comb = int(item % C);
     int64_t r = item / C;
-    int sec[TB_MAX_LEGS] = {0, 0, 0, 0};
 #pragma unroll
     for (int l = L - 2; l >= 0; --l) {
-        sec[l] = int(r % sd.nsec[l]);
+        const int sec = int(r % sd.nsec[l]);
         r /= sd.nsec[l];
+        p.sx[l] = sec % sd.leg[l].nx;
+        p.sy[l] = sec / sd.leg[l].nx;
     }
-    u = int(r);
-    const double ux = c.umk[2 * u], uy = c.umk[2 * u + 1];
-    const double gu0 = xa(xm(c.gvec[0], ux), xm(c.gvec[2], uy));
-    const double gu1 = xa(xm(c.gvec[1], ux), xm(c.gvec[3], uy));
-    WBox acc;
+    p.u = int(r);
+}
+
+// p += 32 items.  Returns true when a digit of legs 0..L-3 or the umklapp
+// column changed (the kept box sums are stale).
+template <int L>
+__device__ __forceinline__ bool walk_advance(const StreamDev& sd, WalkPos<L>& p) {
+    constexpr int C = 1 << (L - 1);
+    int carry = 32 / C;
+    bool front = false;
 #pragma unroll
-    for (int l = 0; l < L - 1; ++l) {
-        const WalkLeg& m = sd.leg[l];
-        const WBox b = walk_box_scale(walk_section_box(m, sec[l] % m.nx, sec[l] / m.nx), c.leg[l].dir);
-        if (l == 0) acc = b;
-        else {
-#pragma unroll
-            for (int i = 0; i < 2; ++i) { acc.l[i] = xa(acc.l[i], b.l[i]); acc.h[i] = xa(acc.h[i], b.h[i]); }
+    for (int l = L - 2; l >= 0; --l) {
+        if (carry) {
+            if (l < L - 2) front = true;
+            int x = p.sx[l] + carry;
+            carry = 0;
+            if (x >= sd.leg[l].nx) { carry = x / sd.leg[l].nx; x -= carry * sd.leg[l].nx; }
+            int y = p.sy[l] + carry;
+            carry = 0;
+            if (y >= sd.leg[l].ny) { carry = y / sd.leg[l].ny; y -= carry * sd.leg[l].ny; }
+            p.sx[l] = x;
+            p.sy[l] = y;
         }
-        e[l] = 2 * sec[l] + ((comb >> (L - 2 - l)) & 1);
     }
-    acc.l[0] = xa(acc.l[0], gu0); acc.h[0] = xa(acc.h[0], gu0);
-    acc.l[1] = xa(acc.l[1], gu1); acc.h[1] = xa(acc.h[1], gu1);
+    if (carry) { p.u += carry; front = true; }
+    return front;
+}
+
+// What the legs in front contribute to an item: their box sum (legs 0..L-3),
+// the umklapp shift and the energy-window partial sums of legs 0..L-3.
+struct WalkFront {
+    WBox box;
+    double gu[2];
+    double mn, mx;
+};
+
+// The item at p: elements of legs 0..L-2, the last leg's section range
+// [lo, hi) and the energy-window sums of legs 0..L-2 (pmn, pmx; the last
+// leg's term is added per candidate).  The decoding and box arithmetic of
+// k_enumerate, term for term and in the same order (the kept front sums are
+// its partial sums); fr is refreshed when ok is false.
+template <int L>
+__device__ __forceinline__ void walk_at(const ChanDev& c, const StreamDev& sd, const WalkPos<L>& p, WalkFront& fr,
+                                        bool& ok, int (&e)[L], int (&lo)[2], int (&hi)[2], double& pmn,
+                                        double& pmx) {
+#pragma unroll
+    for (int l = 0; l < L - 1; ++l) e[l] = 2 * (p.sy[l] * sd.leg[l].nx + p.sx[l]) + ((p.comb >> (L - 2 - l)) & 1);
+    if (!ok) {
+        const double ux = c.umk[2 * p.u], uy = c.umk[2 * p.u + 1];
+        fr.gu[0] = xa(xm(c.gvec[0], ux), xm(c.gvec[2], uy));
+        fr.gu[1] = xa(xm(c.gvec[1], ux), xm(c.gvec[3], uy));
+        fr.mn = 0.0;
+        fr.mx = 0.0;
+#pragma unroll
+        for (int l = 0; l < L - 2; ++l) {
+            const WBox b = walk_box_scale(walk_section_box(sd.leg[l], p.sx[l], p.sy[l]), c.leg[l].dir);
+            if (l == 0) fr.box = b;
+            else {
+#pragma unroll
+                for (int i = 0; i < 2; ++i) { fr.box.l[i] = xa(fr.box.l[i], b.l[i]); fr.box.h[i] = xa(fr.box.h[i], b.h[i]); }
+            }
+            const double emin = __ldg(sd.leg[l].minE + e[l]), emax = __ldg(sd.leg[l].maxE + e[l]);
+            fr.mn += (c.leg[l].dir > 0) ? emin : -emax;
+            fr.mx += (c.leg[l].dir > 0) ? emax : -emin;
+        }
+        ok = true;
+    }
+    constexpr int K = L - 2;   // the leg whose section changes from item to item
+    WBox acc = walk_box_scale(walk_section_box(sd.leg[K], p.sx[K], p.sy[K]), c.leg[K].dir);
+    if (K > 0) {
+#pragma unroll
+        for (int i = 0; i < 2; ++i) { acc.l[i] = xa(fr.box.l[i], acc.l[i]); acc.h[i] = xa(fr.box.h[i], acc.h[i]); }
+    }
+    acc.l[0] = xa(acc.l[0], fr.gu[0]); acc.h[0] = xa(acc.h[0], fr.gu[0]);
+    acc.l[1] = xa(acc.l[1], fr.gu[1]); acc.h[1] = xa(acc.h[1], fr.gu[1]);
     acc = walk_box_scale(acc, -c.leg[L - 1].dir);
     const WalkLeg& ml = sd.leg[L - 1];
     const int ns[2] = {ml.nx, ml.ny};
@@ -115,6 +183,13 @@ __device__ __forceinline__ void walk_item(const ChanDev& c, const StreamDev& sd,
         const int bb = int(xa(floor(th), 1.0));
         lo[i] = min(max(aa, 0), ns[i]);
         hi[i] = min(max(bb, 0), ns[i]);
+    }
+    pmn = fr.mn;
+    pmx = fr.mx;
+    if (lo[0] != hi[0] && lo[1] != hi[1]) {
+        const double emin = __ldg(sd.leg[K].minE + e[K]), emax = __ldg(sd.leg[K].maxE + e[K]);
+        pmn += (c.leg[K].dir > 0) ? emin : -emax;
+        pmx += (c.leg[K].dir > 0) ? emax : -emin;
     }
 }
 
@@ -154,6 +229,51 @@ __device__ __forceinline__ bool domain_excludes(const AlphaMap<L>& am) {
     return false;
 }
 
+// Per-tuple thresholds of a cheaper "clearly outside" test than
+// theta_decide's: T[0] for kp0 + al0, T[1] for al1 + al2.  Over the whole
+// Monte-Carlo domain (every coordinate of q in [0, 1]) the fused
+// coordinates obey |al_r| <= B_r = |a0_r| + sum_j |G_rj| (up to a factor
+// 1 + 1e-15, covered by the 1.000001 below), so theta_decide's per-point
+// bounds mg0 + tiny (2 + |al0|) and mg1 + mg2 + tiny (1 + |al1| + |al2|) are
+// at most X = mg0 + tiny (2 + B0) and Y = mg1 + mg2 + tiny (1 + B1 + B2).
+// A point with fl(kp0 + al0) > fl(1 + 4 X) has fl(fl(kp0 + al0) - 1) > 3.8 X
+// (X >= 2 tiny, so the roundings of 1 + 4 X and of the difference cost less
+// than 0.2 X), above theta_decide's computed bound: theta_decide also calls
+// it outside.  Likewise for al1 + al2 against fl(1 + 4 Y).  The faster test
+// therefore only sends a few more points to the exact evaluation, and every
+// decision stays the reference-order one.
+template <int L>
+__device__ __forceinline__ void outside_thresholds(const AlphaMap<L>& am, double (&T)[2]) {
+    constexpr int R = AlphaMap<L>::R;
+    const double tiny = 8.0 * 1.1102230246251565e-16;
+    double B[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        double t = fabs(am.a0[r]);
+#pragma unroll
+        for (int j = 0; j < R; ++j) t += fabs(am.G[r][j]);
+        B[r] = 1.000001 * t;
+    }
+    const double X = am.mg[0] + tiny * (2.0 + B[0]);
+    const double Y = (am.mg[1] + am.mg[2]) + tiny * ((1.0 + B[1]) + B[2]);
+    T[0] = 1.0 + 4.0 * X;
+    T[1] = 1.0 + 4.0 * Y;
+}
+
+// theta_decide with the per-tuple thresholds above: the same decision.
+template <int L>
+__device__ __forceinline__ bool theta_decide_t(const TupleGeom<L>& g, const double (&Ci)[3][3], const AlphaMap<L>& am,
+                                               const double (&T)[2], const double* qv) {
+    constexpr int R = AlphaMap<L>::R;
+    double al[3];
+    alpha_fast<L>(am, qv, al);
+    const double kp0 = qv[R - 1];
+    const bool out = (al[0] < -am.mg[0]) || (al[1] < -am.mg[1]) || (al[2] < -am.mg[2]) ||
+                     (__dadd_rn(kp0, al[0]) > T[0]) || (__dadd_rn(al[1], al[2]) > T[1]);
+    if (out) return false;
+    return alpha_theta<L>(g, Ci, am, qv, al);
+}
+
 #ifndef TB_STREAM_MIN_BLOCKS
 #define TB_STREAM_MIN_BLOCKS 1
 #endif
@@ -180,8 +300,8 @@ __global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
     constexpr int R = 2 * (L - 2) + 1;
     extern __shared__ double s_tab[];   // [nmc R] quadrature table, then [nmc R] survival table
     // per-warp candidate queues: [0] inside the energy window, [1] past the
-    // determinant filter and the domain test
-    __shared__ int32_t s_q[2][ST_WARPS][L + 1][ST_QUEUE];
+    // determinant filter and the domain test, [2] surviving tuples
+    __shared__ int32_t s_q[3][ST_WARPS][L + 1][ST_QUEUE];
     double* s_mc = s_tab;
     double* s_pre = s_tab + c.nmc * R;
     for (int i = threadIdx.x; i < c.nmc * R; i += blockDim.x) {
@@ -195,10 +315,19 @@ __global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
     double prodc = 1.0;
 #pragma unroll
     for (int l = 0; l < L; ++l) prodc *= sqrt2;
+    // s_cnt[k]: prodc added k times to 0.0, in sequence
+    __shared__ double s_cnt[65];
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        s_cnt[0] = t;
+        for (int k = 1; k <= 64; ++k) s_cnt[k] = (t += prodc);
+    }
+    __syncthreads();
     const double inv_fact_nmc = c.fact * double(c.nmc);
     unsigned long long n_pre = 0, n_det = 0, n_surv = 0, n_pts = 0, n_tin = 0;
 
     int q2n = 0;   // candidates in queue 1 (warp-uniform)
+    int q3n = 0;   // surviving tuples in queue 2 (warp-uniform)
 
     // Stage 1 for `take` candidates of queue 0 from slot `first` on, one per
     // lane: the determinant filter, then the domain test; the candidates that
@@ -235,8 +364,8 @@ __global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
     };
 
     // Stage 2 for `take` candidates of queue 1 from slot `first` on, one per
-    // lane: survival test, mask, sums, scatter.
-    auto evaluate = [&](int first, int take) {
+    // lane: the survival test; the surviving tuples go to queue 2.
+    auto survive = [&](int first, int take) {
         const bool valid = lane < take;
         int e[L];
         int u = 0;
@@ -256,17 +385,52 @@ __global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
         // the way k_theta_mask takes it (the fused map, re-evaluated in the
         // reference's order near a face: the same decisions, at a fraction of
         // the cost of evaluating every point in that order)
-        double sum = 0.0;
-        for (int m = 0; m < c.nmc; ++m) sum += theta_decide<L>(g, Ci, am, s_pre + m * R) ? prodc : 0.0;
-        double res = (1.0 / (c.fact * double(c.nmc) * adet)) * sum;
+        // (the reference adds prodc for every point inside: the sum of cnt
+        // such terms is s_cnt[cnt], the same additions in the same order)
+        double T[2];
+        outside_thresholds<L>(am, T);
+        int cnt = 0;
+        for (int m = 0; m < c.nmc; ++m) cnt += theta_decide_t<L>(g, Ci, am, T, s_pre + m * R) ? 1 : 0;
+        double res = (1.0 / (c.fact * double(c.nmc) * adet)) * s_cnt[cnt];
         res *= c.amp_vol;
         ok = ok && (fabs(res) > c.threshold);
         n_surv += ok ? 1 : 0;
+        const unsigned bal = __ballot_sync(full, ok);
+        if (ok) {
+            const int pos = q3n + __popc(bal & ((1u << lane) - 1u));
+#pragma unroll
+            for (int l = 0; l <= L; ++l) s_q[2][warp][l][pos] = l < L ? e[l] : u;
+        }
+        q3n += __popc(bal);
+        __syncwarp();
+    };
+
+    // Stage 3 for `take` surviving tuples of queue 2 from slot `first` on,
+    // one per lane: the points inside, the sums, the scatter.  (The survivors
+    // are a fifth of the candidates that reach stage 2; gathered into full
+    // warps, the quadrature runs on every lane.)
+    auto evaluate = [&](int first, int take) {
+        const bool valid = lane < take;
+        int e[L];
+        int u = 0;
+#pragma unroll
+        for (int l = 0; l < L; ++l) e[l] = valid ? s_q[2][warp][l][first + lane] : 0;
+        if (valid) u = s_q[2][warp][L][first + lane];
+        TupleGeom<L> g;
+        tuple_geometry<L>(c, e, u, g);
+        const double adet = fabs(g.det);
+        double Ci[3][3];
+        dc_inverse<L>(g, Ci);
+        AlphaMap<L> am;
+        alpha_map<L>(g, Ci, am);
         // the points inside the simplices on the quadrature table (k_theta_mask's)
         uint64_t mk = 0;
-        if (ok)
+        if (valid) {
+            double T[2];
+            outside_thresholds<L>(am, T);
             for (int m = 0; m < c.nmc; ++m)
-                if (theta_decide<L>(g, Ci, am, s_mc + m * R)) mk |= 1ull << m;
+                if (theta_decide_t<L>(g, Ci, am, T, s_mc + m * R)) mk |= 1ull << m;
+        }
         n_pts += __popcll(mk);
         n_tin += mk ? 1 : 0;
         if (!__any_sync(full, mk != 0ull)) return;
@@ -330,71 +494,92 @@ __global__ void __launch_bounds__(ST_WARPS * 32, TB_STREAM_MIN_BLOCKS)
     };
 
     int qn = 0;   // queued candidates (warp-uniform)
-    const int64_t stride = int64_t(gridDim.x) * ST_WARPS * 32;
-    for (int64_t base = it0 + (int64_t(blockIdx.x) * ST_WARPS + warp) * 32; base < it1; base += stride) {
-        const int64_t item = base + lane;
-        int e[L];
-        int u = 0, lo[2] = {0, 0}, hi[2] = {0, 0};
-        double mn[L], mx[L];   // energy window per leg, summed in leg order below
-        int ncand = 0;
-        if (item < it1) {
-            walk_item<L>(c, sd, item, e, u, lo, hi);
-            if (lo[0] != hi[0] && lo[1] != hi[1]) {
-                ncand = 2 * (hi[0] - lo[0]) * (hi[1] - lo[1]);
+    // Each warp takes runs of ST_SPAN x 32 consecutive items, interleaved
+    // over the grid; the lanes hold consecutive items and step by 32.
+    const int64_t n_warps = int64_t(gridDim.x) * ST_WARPS;
+    const int64_t run = int64_t(ST_SPAN) * 32;
+    const WalkLeg& ml = sd.leg[L - 1];
+    for (int64_t rb = it0 + (int64_t(blockIdx.x) * ST_WARPS + warp) * run; rb < it1; rb += n_warps * run) {
+        WalkPos<L> p;
+        walk_decode<L>(sd, rb + lane, p);
+        WalkFront fr;
+        bool front_ok = false;
+        for (int st = 0; st < ST_SPAN; ++st) {
+            const int64_t base = rb + int64_t(st) * 32;
+            if (base >= it1) break;
+            const int64_t item = base + lane;
+            int e[L];
+            int lo[2] = {0, 0}, hi[2] = {0, 0};
+            double pmn = 0.0, pmx = 0.0;   // energy window of legs 0..L-2, summed in leg order
+            int ncand = 0;
+            if (item < it1) {
+                walk_at<L>(c, sd, p, fr, front_ok, e, lo, hi, pmn, pmx);
+                if (lo[0] != hi[0] && lo[1] != hi[1]) ncand = 2 * (hi[0] - lo[0]) * (hi[1] - lo[1]);
+            }
+            const int u = p.u;
+            const int maxc = __reduce_max_sync(full, unsigned(ncand));
+            // candidate k of the box: element 2 (cx + cy nx) + ie with
+            // cx = lo0 + (k / 2) % nbx, cy = lo1 + (k / 2) / nbx, ie = k % 2
+            int cx = lo[0], cy = lo[1], ie = 0;
+            for (int k = 0; k < maxc; ++k) {
+                bool pass = false;
+                int el = 0;
+                if (k < ncand) {
+                    el = 2 * (cx + cy * ml.nx) + ie;
+                    const double emin = __ldg(ml.minE + el), emax = __ldg(ml.maxE + el);
+                    const double minE = pmn + ((c.leg[L - 1].dir > 0) ? emin : -emax);
+                    const double maxE = pmx + ((c.leg[L - 1].dir > 0) ? emax : -emin);
+                    pass = (minE <= 0.0) && (maxE >= 0.0);
+                }
+                if (ie) {
+                    ie = 0;
+                    if (++cx == hi[0]) { cx = lo[0]; ++cy; }
+                } else {
+                    ie = 1;
+                }
+                const unsigned bal = __ballot_sync(full, pass);
+                if (pass) {
+                    const int pos = qn + __popc(bal & ((1u << lane) - 1u));
 #pragma unroll
-                for (int l = 0; l < L - 1; ++l) {
-                    const double emin = __ldg(sd.leg[l].minE + e[l]), emax = __ldg(sd.leg[l].maxE + e[l]);
-                    mn[l] = (c.leg[l].dir > 0) ? emin : -emax;
-                    mx[l] = (c.leg[l].dir > 0) ? emax : -emin;
+                    for (int l = 0; l < L - 1; ++l) s_q[0][warp][l][pos] = e[l];
+                    s_q[0][warp][L - 1][pos] = el;
+                    s_q[0][warp][L][pos] = u;
+                }
+                qn += __popc(bal);
+                __syncwarp();
+                if (qn >= 32) {
+                    stage1(qn - 32, 32);
+                    qn -= 32;
+                    if (q2n >= 32) {
+                        survive(q2n - 32, 32);
+                        q2n -= 32;
+                        if (q3n >= 32) {
+                            evaluate(q3n - 32, 32);
+                            q3n -= 32;
+                        }
+                    }
+                    __syncwarp();   // the slots are reused
                 }
             }
-        }
-        const int maxc = __reduce_max_sync(full, unsigned(ncand));
-        const int nbx = hi[0] - lo[0];
-        const WalkLeg& ml = sd.leg[L - 1];
-        for (int k = 0; k < maxc; ++k) {
-            bool pass = false;
-            int el = 0;
-            if (k < ncand) {
-                const int ie = k & 1, t = k >> 1;
-                const int sx = lo[0] + t % nbx, sy = lo[1] + t / nbx;
-                el = 2 * (sx + sy * ml.nx) + ie;
-                const double emin = __ldg(ml.minE + el), emax = __ldg(ml.maxE + el);
-                mn[L - 1] = (c.leg[L - 1].dir > 0) ? emin : -emax;
-                mx[L - 1] = (c.leg[L - 1].dir > 0) ? emax : -emin;
-                double minE = 0.0, maxE = 0.0;
-#pragma unroll
-                for (int l = 0; l < L; ++l) { minE += mn[l]; maxE += mx[l]; }
-                pass = (minE <= 0.0) && (maxE >= 0.0);
-            }
-            const unsigned bal = __ballot_sync(full, pass);
-            if (pass) {
-                const int pos = qn + __popc(bal & ((1u << lane) - 1u));
-#pragma unroll
-                for (int l = 0; l < L - 1; ++l) s_q[0][warp][l][pos] = e[l];
-                s_q[0][warp][L - 1][pos] = el;
-                s_q[0][warp][L][pos] = u;
-            }
-            qn += __popc(bal);
-            __syncwarp();
-            if (qn >= 32) {
-                stage1(qn - 32, 32);
-                qn -= 32;
-                if (q2n >= 32) {
-                    evaluate(q2n - 32, 32);
-                    q2n -= 32;
-                }
-                __syncwarp();   // the slots are reused
-            }
+            if (walk_advance<L>(sd, p)) front_ok = false;
         }
     }
+    // the queues' remainders, survivors first once queue 1 is empty
     if (qn > 0) stage1(0, qn);
-    if (q2n >= 32) {
-        evaluate(q2n - 32, 32);
-        q2n -= 32;
+    for (;;) {
+        if (q3n >= 32 || (q2n == 0 && q3n > 0)) {
+            const int t = min(q3n, 32);
+            evaluate(q3n - t, t);
+            q3n -= t;
+        } else if (q2n > 0) {
+            const int t = min(q2n, 32);
+            survive(q2n - t, t);
+            q2n -= t;
+        } else {
+            break;
+        }
         __syncwarp();
     }
-    if (q2n > 0) evaluate(0, q2n);
     if (sd.counts) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -427,7 +612,7 @@ static int launch_stream(const ChanDev& c, const StreamDev& sd, int64_t it0, int
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
     if (per_sm < 1) per_sm = 1;
-    const int64_t batches = (it1 - it0 + 31) / 32;
+    const int64_t batches = (it1 - it0 + ST_SPAN * 32 - 1) / (ST_SPAN * 32);
     int64_t blocks = (batches + ST_WARPS - 1) / ST_WARPS;
     // several waves of resident blocks: the work per item varies a lot
     const int64_t cap = int64_t(nsm) * per_sm * 8;

@@ -955,6 +955,7 @@ static RunsDev runs_dev(const ChanDev& c, const MomentTensor& T, const FxAcc& fx
     if (fx.w) {
         R.accTx.w = T.accTx;
         R.accTx.poison = fx.poison;
+        R.accTx.sat = fx.sat;
     }
     R.np = T.np;
     for (int l = 0; l < TB_MAX_LEGS; ++l) {
