@@ -636,7 +636,9 @@ __global__ void __launch_bounds__(1024) k_runs_scatter_exact(const InstDev* __re
 }
 
 // One tuple (staged at column t of the tile) for the instance of this lane.
-template <int L, int KIND, int TT>
+// EXACT: the deterministic mode's adds into R.accTx (a separate
+// instantiation, so that the FP64-atomic kernels keep their registers).
+template <int L, int KIND, int TT, bool EXACT>
 __device__ __forceinline__ void contract_run(const ChanDev& c, const RunsDev& R, const int (&e)[L], int t, int i,
                                              double amp, const unsigned char* __restrict__ tile) {
     constexpr int K = TDim<L>::K, KM = TDim<L>::KM, NMOM = TDim<L>::NMOM;
@@ -710,7 +712,7 @@ __device__ __forceinline__ void contract_run(const ChanDev& c, const RunsDev& R,
         for (int lam = 0; lam < L; ++lam) {
             const double da = c.leg[lam].dir * amp;   // d = +-1: d (r amp) == r (d amp)
             const int64_t slot = R.loff[lam] + int64_t(3 * e[lam]) * R.np + i;
-            if (R.accTx.w) {   // deterministic mode: exact adds
+            if (EXACT) {   // deterministic mode: exact adds
                 fx_add(R.accTx, slot, r0 * da);
                 fx_add(R.accTx, slot + R.np, r1[lam] * da);
                 fx_add(R.accTx, slot + 2 * R.np, r2[lam] * da);
@@ -732,7 +734,7 @@ __device__ __forceinline__ void contract_run(const ChanDev& c, const RunsDev& R,
 // rather than of 32; each
 // instruction still serves 32 lanes, the moment reads hit 32 / S adjacent
 // words and every f row / reduction stays whole 32-byte sectors (S >= 4).
-template <int L, int KIND, int TT, int STAGES, int S>
+template <int L, int KIND, int TT, int STAGES, int S, bool EXACT>
 __global__ void __launch_bounds__(RUNS_THREADS) k_collision_runs(ChanDev c, const InstDev* __restrict__ insts,
                                                                  int n_insts, RunsDev R,
                                                                  const unsigned char* __restrict__ mom, int64_t ntiles,
@@ -836,7 +838,7 @@ __global__ void __launch_bounds__(RUNS_THREADS) k_collision_runs(ChanDev c, cons
                 const int i = ch * S + sl;
                 const double amp = tv ? s_amp[i] : 0.0;
                 if (__all_sync(0xffffffffu, amp == 0.0)) continue;
-                contract_run<L, KREAD, TT>(c, R, e, t, i, amp, rd);
+                contract_run<L, KREAD, TT, EXACT>(c, R, e, t, i, amp, rd);
             }
         }
         __syncthreads();   // every warp is done with stage s (and dec)
@@ -978,12 +980,12 @@ static int launch_runs(const ChanDev& c, const InstDev* insts, int n_insts, cons
     const dim3 tb(32, 8), tg(unsigned((maxd + 31) / 32), unsigned(T.np / 32), unsigned(L));
     k_runs_gather<<<tg, tb, 0, s>>>(insts, n_insts, R, f);
     TB_CUDA(cudaGetLastError());
-    auto kern = k_collision_runs<L, KIND, TT, STAGES, S>;
+    auto kern = fx.w ? k_collision_runs<L, KIND, TT, STAGES, S, true> : k_collision_runs<L, KIND, TT, STAGES, S, false>;
     const size_t fixed = size_t(STAGES) * TT * tuple_bytes(L, KIND) +
                          ((KIND == TK_F40 || KIND == TK_F48) ? sizeof(double) * TDim<L>::NMOM * TT : 0);
     const size_t smem = fixed + sizeof(double) * size_t(T.np);
-    static unsigned long long attr_devices = 0;
-    TB_TRY(ensure_smem_attr(kern, int(fixed + sizeof(double) * RUNS_NP_MAX), attr_devices));
+    static unsigned long long attr_devices[2] = {0, 0};
+    TB_TRY(ensure_smem_attr(kern, int(fixed + sizeof(double) * RUNS_NP_MAX), attr_devices[fx.w ? 1 : 0]));
     int* err_flag = nullptr;
     TB_TRY(channel_err_flag(c, &err_flag));
     int dev = 0, nsm = 148;
