@@ -17,6 +17,9 @@ int fx_host_of(double v, unsigned long long* words) {
 
 double fx_host_value(const unsigned long long* words) { return tb::fx_value(words[0], words[1], words[2]); }
 
+// the clamp of out-of-range finite contributions
+double fx_host_clamp() { return tb::FX_CLAMP; }
+
 // acc[3] += the words of every v[i] in the given order; returns how many
 // values could not be held
 int fx_host_sum(const double* v, const long long* order, long long n, unsigned long long* acc) {

@@ -26,6 +26,7 @@ def fx(tmp_path_factory):
     L.fx_host_value.restype = C.c_double
     L.fx_host_value.argtypes = [u64p]
     L.fx_host_sum.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_longlong, u64p]
+    L.fx_host_clamp.restype = C.c_double
     return L
 
 
@@ -62,6 +63,25 @@ def test_values_beyond_the_range_are_refused(fx):
     for v in (2.0 ** 64, -(2.0 ** 64), 1e300, float("inf"), float("-inf"), float("nan")):
         ok, w = words_of(fx, v)
         assert not ok and w == [0, 0, 0], v
+
+
+def test_clamp_is_the_largest_value_on_the_grid(fx):
+    """Finite contributions of 2^64 or more are clamped to the largest double
+    below 2^64: held exactly, and many of them still sum exactly (the words
+    reach 2^79)."""
+    c = fx.fx_host_clamp()
+    assert c == 2.0 ** 64 * (1 - 2.0 ** -53) and np.nextafter(c, np.inf) == 2.0 ** 64
+    ok, w = words_of(fx, c)
+    assert ok and signed(w) == int(c) * 2 ** 112
+    ok, w = words_of(fx, -c)
+    assert ok and signed(w) == -int(c) * 2 ** 112
+    n = 1000
+    v = (C.c_double * n)(*([c] * (n - 1) + [-c]))
+    order = (C.c_longlong * n)(*range(n))
+    acc = (C.c_ulonglong * 3)()
+    assert fx.fx_host_sum(v, order, n, acc) == 0
+    assert signed(list(acc)) == (n - 2) * int(c) * 2 ** 112
+    assert fx.fx_host_value(acc) == (n - 2) * c
 
 
 def test_round_trip_is_exact_on_the_grid(fx):
