@@ -1054,6 +1054,9 @@ def ee_full(args):
     if line["collision_ms_ee"] > 0:
         line["ee_surviving_tuples_per_s"] = line["ee_channels"]["surviving_tuples"] / (1e-3 * line["collision_ms_ee"])
     if args.steps > 0:
+        # the collision figures first: a long attempt that does not finish
+        # leaves them behind
+        print(json.dumps(dict(line, partial=True)), flush=True)
         eng.dp45_begin(f0, 0.0, T_END, DENSE, 0)
         eng.dp45_advance(args.warmup)
         eng.synchronize()
