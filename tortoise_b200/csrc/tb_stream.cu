@@ -37,7 +37,11 @@
 
 namespace tb {
 
-constexpr int ST_WARPS = 8;    // warps per block
+// 4 warps per block, 3 blocks per SM: the register cap of 168 per thread
+// spills a little, but 12 resident warps per SM instead of 8 hide more of the
+// FP64 latency (a 16x16 e-e evaluation: 306 ms against 387 ms with blocks of
+// 8 warps at 221 registers, one block per SM)
+constexpr int ST_WARPS = 4;    // warps per block
 constexpr int ST_QUEUE = 64;   // candidate slots per warp (31 left over + 32 pushed at most)
 constexpr int ST_SPAN = 16;    // steps of 32 consecutive items per run of a warp
 
@@ -275,7 +279,7 @@ __device__ __forceinline__ bool theta_decide_t(const TupleGeom<L>& g, const doub
 }
 
 #ifndef TB_STREAM_MIN_BLOCKS
-#define TB_STREAM_MIN_BLOCKS 1
+#define TB_STREAM_MIN_BLOCKS 3
 #endif
 
 // MODE: ST_PROPAGATE (the collision terms), ST_RATE (rate_leg's scattering
