@@ -172,3 +172,76 @@ def test_two_ranks_partial_operators_sum_to_the_full_one_and_step_alike():
         assert r0["dp"] == r1["dp"] and r0["dense"] == r1["dense"]   # replicated controller: identical
         assert r0["dp"] == r0["unsharded"]
         assert r0["unsharded_dense_rel"] < 1e-10
+
+
+def _item_sharded_rank(rank, world, port, out):
+    """One gloo rank of a run whose four-leg channels are streamed and
+    sharded by work item (the split of tb_shard_range over the items of
+    the walk, not over stored tuples): the oracle enumerates and integrates
+    exactly this rank's items, the partial operators are all-reduced."""
+    import datetime
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    import oracle
+    from tortoise_b200 import engine as E
+    from tortoise_b200 import workloads as W
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        mat = W.build_material(4, ("P", "D"), (0.2,), ee=True, eph=True, field=(0.1, 0.0), rtol=1e-6, atol=1e-9)
+        f0 = W.initial_status(mat, seed=5).vec
+        pk = mat.pack()
+        part = oracle.Oracle(mat, enumerate_tuples=False, nthreads=1)
+        acc = np.zeros(part.ndofs)
+        res = {"items": [], "tuples": []}
+        for ch, c in enumerate(mat.channels):
+            if c.nlegs != 4:
+                continue
+            cd = pk.desc.channels[ch]
+            n = cd.n_umklapp * 2 ** (cd.nlegs - 1)
+            for l in range(cd.nlegs - 1):
+                m = pk.desc.meshes[pk.desc.bands[cd.band[l]].mesh]
+                n *= m.nsplit[0] * m.nsplit[1]
+            b, e = E.shard_range(n, rank, world)
+            part.enumerate_items(ch, b, e)
+            part.channel_propagate(ch, f0, out=acc)
+            res["items"].append((n, b, e))
+            res["tuples"].append(part.num_tuples(ch))
+        t = torch.from_numpy(acc)
+        dist.all_reduce(t)
+        full = oracle.Oracle(mat, nthreads=1)
+        ref = np.zeros(full.ndofs)
+        for ch, c in enumerate(mat.channels):
+            if c.nlegs == 4:
+                full.channel_propagate(ch, f0, out=ref)
+        res["full_tuples"] = [full.num_tuples(ch) for ch, c in enumerate(mat.channels) if c.nlegs == 4]
+        res["rel"] = float(np.linalg.norm(t.numpy() - ref) / np.linalg.norm(ref))
+        out.put((rank, res))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_split_the_streamed_work_items():
+    """Streamed four-leg channels sharded over two gloo ranks: the work items
+    of the walk split by tb_shard_range hold every tuple of the full
+    enumeration exactly once (the per-rank tuple counts add up), and the
+    all-reduced partial operators equal the full one."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_item_sharded_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=300) for _ in range(2))
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    r0, r1 = res[0], res[1]
+    assert r0["items"] and len(r0["items"]) == len(r1["items"])
+    for (n, b0, e0), (m, b1, e1) in zip(r0["items"], r1["items"]):
+        assert n == m and b0 == 0 and e0 == b1 and e1 == n
+    assert [a + b for a, b in zip(r0["tuples"], r1["tuples"])] == r0["full_tuples"]
+    assert all(a > 0 for a in r0["tuples"]) and all(b > 0 for b in r1["tuples"])
+    assert r0["rel"] < 1e-13 and r1["rel"] == r0["rel"]
