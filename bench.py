@@ -1000,7 +1000,7 @@ def ee_full(args):
     e-ph channels of the optical branch (hw = 0.2, Bose kT = 0.05), drift
     field (0.1, 0), rtol 1e-8, on an N x N mesh (--ee-full N).  The e-e
     channels are streamed (their tuple lists do not fit in device memory at
-    N >= 32: about 2e9 tuples per channel at 32x32, 8e10 at 64x64); the e-ph
+    N >= 32: about 2e9 tuples per channel at 32x32, 3e10 at 64x64); the e-ph
     channels keep their moment tensors.  Times one collision evaluation of
     every channel (CUDA events on the library's stream), reports the walk's
     counts per e-e channel, then times args.steps DP45 attempts from t = 0

@@ -1,7 +1,7 @@
 // tb_stream.cu -- the Monte-Carlo collision operator with its tuples
 // enumerated on the fly, for channels whose tuple list does not fit in
 // device memory (four-leg electron-electron channels on fine meshes: about
-// 2e9 surviving tuples at 32x32, 8e10 at 64x64).
+// 2e9 surviving tuples at 32x32, 3e10 at 64x64).
 //
 // Every evaluation walks the reference's candidate space again and keeps
 // nothing between evaluations:
